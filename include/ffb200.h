@@ -1,0 +1,195 @@
+/*
+ * ffb200 — C ABI of the B200 flow-filter library (libffb200.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns an
+ * ff_status.  The C++ drop-in classes (include/flowfilter/gpu/*.h) and the Python
+ * package sit on top of this ABI.  Each declaration names the reference interface
+ * it replaces (file:line inside the reference project jadarve/optical-flow-filter).
+ *
+ * Conventions
+ *   - images are row-major with an explicit row pitch in bytes; two-channel fields
+ *     (flow, gradient) are interleaved float pairs (x, y) as in the reference;
+ *   - uint8 images are read as v/255 (the reference's normalised texture reads);
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream);
+ *   - device pointers must stay valid until the work queued on `stream` finishes;
+ *   - functions ending in _async only enqueue work; the others block like the
+ *     reference's stages, which synchronise the host at the end of compute()
+ *     (src/gpu/pipeline.cu:72-82).
+ *   - errors never exit the process (the reference calls exit(), src/gpu/error.cu:22);
+ *     ff_last_error() returns a thread-local message for the last failure.
+ */
+#ifndef FFB200_H_
+#define FFB200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ff_status {
+    FF_OK = 0,
+    FF_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument / bare std::exception on a bad value */
+    FF_ERR_LOGIC = 2,            /* reference: std::logic_error (e.g. compute() on an unconfigured stage) */
+    FF_ERR_OUT_OF_RANGE = 3,     /* level index out of bounds (flowfilter.cu:756-759) */
+    FF_ERR_SHAPE = 4,            /* shapes do not match (src/gpu/image.cu:113-119) */
+    FF_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+    FF_ERR_OUT_OF_MEMORY = 6,    /* device or host allocation failed */
+    FF_ERR_UNSUPPORTED = 7       /* a valid request this build does not support */
+} ff_status;
+
+/* Host image view, ABI-identical to flowfilter::image_t (include/flowfilter/image.h:30-49). */
+typedef struct ff_image {
+    int height;
+    int width;
+    int depth;
+    size_t pitch;     /* row pitch in bytes */
+    size_t itemSize;  /* bytes per channel item: 1 (uint8) or 4 (float32) */
+    void* data;
+} ff_image;
+
+typedef struct ff_filter ff_filter; /* opaque: a single-level, delta-level or pyramidal filter */
+
+/* ------------------------------------------------------------ library */
+const char* ff_last_error(void);
+const char* ff_status_string(ff_status s);
+/* Library version as an integer (major*10000 + minor*100 + patch). */
+int ff_version(void);
+/* Select the CUDA device used by filters created afterwards on this thread (the
+ * reference pins device 0 in every Stage constructor, src/gpu/pipeline.cu:26). */
+ff_status ff_set_device(int device);
+
+/* ------------------------------------------------------------ device buffers
+ * Replaces GPUImage allocate/upload/download/copyFrom/clear (src/gpu/image.cu:81-197). */
+ff_status ff_malloc_pitch(void** dptr, size_t* pitch, size_t width_bytes, size_t height);
+ff_status ff_free(void* dptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device (synchronous, 2D) */
+ff_status ff_memcpy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width_bytes,
+                      size_t height, int kind);
+ff_status ff_memset2d(void* dptr, size_t pitch, int value, size_t width_bytes, size_t height);
+
+/* ------------------------------------------------------------ filters
+ * FlowFilter(height, width, smoothIterations, maxflow, gamma) with an owned uint8
+ * input image (src/gpu/flowfilter.cu:45-76); FlowFilter(h, w) is (h, w, 1, 1, 1). */
+ff_status ff_filter_create(int height, int width, int smooth_iterations, float maxflow, float gamma,
+                           ff_filter** out);
+/* FlowFilter(GPUImage inputImage) over an external device image of item size 1 or 4
+ * (src/gpu/flowfilter.cu:32-38, configure() :84-122): gamma 1 (unscaled), maxflow 1,
+ * one smoothing iteration, border 3.  The image is read on every compute(). */
+ff_status ff_filter_create_on_device_image(const void* image, size_t pitch, int item_size, int height,
+                                           int width, ff_filter** out);
+/* DeltaFlowFilter(GPUImage inputImage, GPUImage inputFlow) (src/gpu/flowfilter.cu:349-426):
+ * a finer level that refines the external coarse flow field (height_c x width_c x 2 floats). */
+ff_status ff_delta_filter_create(const void* image, size_t pitch, int item_size, int height, int width,
+                                 const void* coarse_flow, size_t coarse_pitch, int height_c, int width_c,
+                                 ff_filter** out);
+/* PyramidalFlowFilter(height, width, levels) with an owned uint8 input (flowfilter.cu:631-682). */
+ff_status ff_pyramidal_create(int height, int width, int levels, ff_filter** out);
+ff_status ff_filter_destroy(ff_filter* f);
+
+ff_status ff_filter_shape(const ff_filter* f, int* height, int* width, int* levels);
+/* Kind of filter: 0 FlowFilter, 1 DeltaFlowFilter, 2 PyramidalFlowFilter. */
+ff_status ff_filter_kind(const ff_filter* f, int* kind);
+ff_status ff_filter_level_shape(const ff_filter* f, int level, int* height, int* width);
+
+/* Parameters.  Level 0 is the finest level; single-level filters use level 0.
+ * setGamma scales by 1/255^2 for uint8 inputs (flowfilter.cu:276-285, 559-568);
+ * ff_filter_get_gamma returns the scaled value, as the reference's getGamma does. */
+ff_status ff_filter_set_gamma(ff_filter* f, int level, float gamma);
+ff_status ff_filter_get_gamma(const ff_filter* f, int level, float* gamma);
+/* setMaxFlow: iterations = ceil(maxflow) (flowfilter.cu:293-296); pyramids halve the
+ * value per level and give the top level maxflow/2^(L-1) (flowfilter.cu:849-866). */
+ff_status ff_filter_set_max_flow(ff_filter* f, float maxflow);
+ff_status ff_filter_get_max_flow(const ff_filter* f, float* maxflow);
+ff_status ff_filter_set_smooth_iterations(ff_filter* f, int level, int iterations);
+ff_status ff_filter_get_smooth_iterations(const ff_filter* f, int level, int* iterations);
+/* Applies to every level (the reference's pyramid loop overruns, flowfilter.cu:873-875). */
+ff_status ff_filter_set_propagation_border(ff_filter* f, int border);
+ff_status ff_filter_get_propagation_border(const ff_filter* f, int* border);
+ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, int* iterations);
+
+/* Stream used by the blocking calls (default: a non-blocking stream owned by the filter). */
+ff_status ff_filter_set_stream(ff_filter* f, void* stream);
+
+/* loadImage(image_t&) (flowfilter.cu:218-220, 728-731): synchronous host upload with
+ * the caller's pitch; shape and item size must match (src/gpu/image.cu:96-120). */
+ff_status ff_filter_load_image_host(ff_filter* f, const ff_image* image);
+/* Enqueue a device-to-device copy of a frame into the filter's input buffer. */
+ff_status ff_filter_load_image_device_async(ff_filter* f, const void* image, size_t pitch, void* stream);
+/* Read the next frames directly from a caller-owned device image (no copy).  The
+ * pointer must stay valid and unchanged until the compute that reads it completes. */
+ff_status ff_filter_bind_image_device(ff_filter* f, const void* image, size_t pitch);
+
+/* compute() (flowfilter.cu:125-153, 685-716): one frame; blocks until done and
+ * records elapsedTime() in milliseconds. */
+ff_status ff_filter_compute(ff_filter* f);
+/* Enqueue one frame on `stream` without blocking (elapsed time not updated). */
+ff_status ff_filter_compute_async(ff_filter* f, void* stream);
+/* Phase API of FlowFilter / DeltaFlowFilter (flowfilter.cu:155-197, 460-503). */
+ff_status ff_filter_compute_image_model(ff_filter* f);
+ff_status ff_filter_compute_propagation(ff_filter* f);
+ff_status ff_filter_compute_update(ff_filter* f);
+ff_status ff_filter_elapsed_ms(const ff_filter* f, float* ms);
+
+/* downloadFlow (flowfilter.cu:238-240, 734-741): level-0 smoothed flow, H x W x 2 floats. */
+ff_status ff_filter_download_flow_host(ff_filter* f, ff_image* flow);
+/* downloadImage (flowfilter.cu:242-244, 744-751): level-0 updated image (current a0). */
+ff_status ff_filter_download_image_host(ff_filter* f, ff_image* image);
+/* Device views of the current results, valid until the next compute on the filter.
+ * which: 0 smoothed flow (downloadFlow), 1 getFlow() (unsmoothed for single-level
+ * filters, flowfilter.cu:266-268; smoothed for delta and pyramidal filters,
+ * :545-547, 718-725), 2 updated image. */
+ff_status ff_filter_device_result(ff_filter* f, int which, void** dptr, size_t* pitch);
+/* Copy any level's state to the host for inspection: which as above plus 3 = delta flow. */
+ff_status ff_filter_level_state_host(ff_filter* f, int level, int which, void* dst, size_t dst_pitch);
+
+/* ------------------------------------------------------------ stages
+ * Stateless kernels over caller-owned device buffers (the stage classes of
+ * src/gpu/{imagemodel,pyramid,propagation,update,flowsmoothing}.cu).  `ws` is a
+ * caller-provided device workspace of at least the size the matching
+ * *_workspace_size call returns (may be NULL when that size is 0). */
+
+/* ImagePyramid level step (pyramid.cu:110-167, pyramid_k.cu:14-145): X pass then Y pass
+ * of [1/4, 1/2, 1/4] at stride 2; uint8 results truncate (unsigned char)(255*s). */
+ff_status ff_stage_pyramid_down(const void* in, size_t in_pitch, int item_size, int height, int width,
+                                void* out, size_t out_pitch, void* stream);
+/* ImageModel::compute (imagemodel.cu:93-113, imagemodel_k.cu:31-133): a0 (float) and
+ * gradient (float pairs) from a uint8 or float image. */
+ff_status ff_stage_image_model(const void* img, size_t img_pitch, int item_size, int height, int width,
+                               float* a0, size_t a0_pitch, float* grad, size_t grad_pitch, void* stream);
+/* FlowPropagator::compute (propagation.cu:80-134): `iterations` upwind sub-steps
+ * (X then Y), dt = 1/iterations, pixels within `border` of the edge unchanged. */
+size_t ff_stage_propagate_workspace_size(int height, int width);
+ff_status ff_stage_propagate(const float* flow, size_t flow_pitch, int height, int width, int iterations,
+                             int border, float* out, size_t out_pitch, void* ws, void* stream);
+/* FlowPropagatorPayload::compute (propagation.cu:324-373): flow plus a scalar and a
+ * vector payload advected with the flow's dominant velocity. */
+size_t ff_stage_propagate_payload_workspace_size(int height, int width);
+ff_status ff_stage_propagate_payload(const float* flow, size_t flow_pitch, const float* scalar,
+                                     size_t scalar_pitch, const float* vector, size_t vector_pitch,
+                                     int height, int width, int iterations, int border, float* out_flow,
+                                     size_t out_flow_pitch, float* out_scalar, size_t out_scalar_pitch,
+                                     float* out_vector, size_t out_vector_pitch, void* ws, void* stream);
+/* FlowUpdate::compute (update.cu:97-116, update_k.cu:15-79). gamma is used as given. */
+ff_status ff_stage_update(const float* a0, size_t a0_pitch, const float* grad, size_t grad_pitch,
+                          const float* a0_old, size_t a0_old_pitch, const float* flow, size_t flow_pitch,
+                          int height, int width, float gamma, float maxflow, float* out_flow,
+                          size_t out_flow_pitch, float* out_image, size_t out_image_pitch, void* stream);
+/* DeltaFlowUpdate::compute (update.cu:328-349, update_k.cu:82-173). */
+ff_status ff_stage_delta_update(const float* a0, size_t a0_pitch, const float* grad, size_t grad_pitch,
+                                const float* a0_old, size_t a0_old_pitch, const float* delta,
+                                size_t delta_pitch, const float* coarse, size_t coarse_pitch, int height_c,
+                                int width_c, int height, int width, float gamma, float maxflow,
+                                float* out_flow, size_t out_flow_pitch, float* out_delta,
+                                size_t out_delta_pitch, float* out_image, size_t out_image_pitch,
+                                void* stream);
+/* FlowSmoother::compute (flowsmoothing.cu:74-108): `iterations` x (5-tap box X, then Y). */
+size_t ff_stage_smooth_workspace_size(int height, int width);
+ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int width, int iterations,
+                          float* out, size_t out_pitch, void* ws, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFB200_H_ */

@@ -1,0 +1,505 @@
+// Filter objects: buffers, parameter rules and the per-frame schedule.
+//
+// Reference schedule (src/gpu/flowfilter.cu:685-716): pyramid; image model and
+// propagation of every level; top update; delta updates finest first.  Because the
+// finest levels update before coarser ones, a delta level h < L-2 reads level h+1's
+// smoothed flow of the PREVIOUS frame, and level L-2 reads the top level's
+// UNSMOOTHED flow of this frame (flowfilter.cu:663-672).  With ping-pong state this
+// is: coarse(h) = fs[cur] of level h+1, or fu of the top level for h = L-2.
+#include "filter.h"
+
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+
+namespace ffb {
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    ff_status s = (e == cudaErrorMemoryAllocation) ? FF_ERR_OUT_OF_MEMORY : FF_ERR_CUDA;
+    throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void Buf::alloc(int h_, int w_, int bpp_) {
+    release();
+    h = h_;
+    w = w_;
+    bpp = bpp_;
+    if (h <= 0 || w <= 0) return;
+    check_cuda(cudaMallocPitch(&p, &pitch, (size_t)w * bpp, (size_t)h), "cudaMallocPitch");
+    check_cuda(cudaMemset2D(p, pitch, 0, (size_t)w * bpp, (size_t)h), "cudaMemset2D");
+}
+
+void Buf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    pitch = 0;
+}
+
+void Buf::clear(cudaStream_t s) {
+    if (p) check_cuda(cudaMemset2DAsync(p, pitch, 0, row_bytes(), (size_t)h, s), "cudaMemset2DAsync");
+}
+
+void Level::alloc_state() {
+    for (int k = 0; k < 2; ++k) {
+        fs[k].alloc(H, W, 8);
+        io[k].alloc(H, W, 4);
+        if (delta) d[k].alloc(H, W, 8);
+    }
+    if (!delta) fu.alloc(H, W, 8);
+}
+
+void Level::alloc_scratch() {
+    if (a0.p) return;
+    a0.alloc(H, W, 4);
+    grad.alloc(H, W, 8);
+    fp.alloc(H, W, 8);
+    t1.alloc(H, W, 8);
+    if (delta) {
+        ip.alloc(H, W, 4);
+        dp.alloc(H, W, 8);
+        t2.alloc(H, W, 4);
+        t3.alloc(H, W, 8);
+        fut.alloc(H, W, 8);
+    }
+}
+
+void Level::release() {
+    for (int k = 0; k < 2; ++k) {
+        fs[k].release();
+        io[k].release();
+        d[k].release();
+    }
+    for (Buf* b : {&fu, &a0, &grad, &fp, &ip, &dp, &t1, &t2, &t3, &fut}) b->release();
+}
+
+Filter::Filter(Kind kind, int H, int W, int levels, int item) : kind_(kind), H_(H), W_(W), L_(levels), item_(item) {
+    if (H <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "height should be greater than zero, got: " + std::to_string(H));
+    if (W <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "width should be greater than zero, got: " + std::to_string(W));
+    if (levels <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "levels should be greater than zero, got: " + std::to_string(levels));
+    if (item != 1 && item != 4) throw Error(FF_ERR_INVALID_ARGUMENT, "item size should be 1 or 4: " + std::to_string(item));
+    if (kind != Kind::Pyramidal && levels != 1) throw Error(FF_ERR_INVALID_ARGUMENT, "single-level filter with levels != 1");
+    try {
+        check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        own_stream_ = true;
+        check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
+        lv_.resize(L_);
+        if (kind == Kind::Pyramidal) {
+            // ImagePyramid::configure: integer halving, X then Y (pyramid.cu:74-83)
+            input_.alloc(H, W, item);
+            int h = H, w = W;
+            pyr_.resize(L_ - 1);
+            for (int l = 0; l < L_; ++l) {
+                if (l > 0) {
+                    w /= 2;
+                    h /= 2;
+                    if (h <= 0 || w <= 0)
+                        throw Error(FF_ERR_INVALID_ARGUMENT, "pyramid level " + std::to_string(l) + " has zero size");
+                    pyr_[l - 1].alloc(h, w, item);
+                }
+                Level& v = lv_[l];
+                v.delta = l < L_ - 1;
+                v.H = h;
+                v.W = w;
+                v.item = item;
+                v.img = l == 0 ? input_.p : pyr_[l - 1].p;
+                v.img_pitch = l == 0 ? input_.pitch : pyr_[l - 1].pitch;
+            }
+            for (int l = 0; l < L_ - 1; ++l) {
+                lv_[l].Hc = lv_[l + 1].H;
+                lv_[l].Wc = lv_[l + 1].W;
+            }
+        } else {
+            Level& v = lv_[0];
+            v.delta = kind == Kind::Delta;
+            v.H = H;
+            v.W = W;
+            v.item = item;
+        }
+        // configure() defaults: FlowUpdate/DeltaFlowUpdate(gamma 1, maxflow 1),
+        // FlowSmoother(1), FlowPropagator(1), border 3 (flowfilter.cu:100-107, 393-402)
+        for (Level& v : lv_) v.alloc_state();
+        check_cuda(cudaDeviceSynchronize(), "configure");
+    } catch (...) {
+        for (Level& v : lv_) v.release();
+        for (Buf& b : pyr_) b.release();
+        input_.release();
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (own_stream_) cudaStreamDestroy(stream_);
+        throw;
+    }
+}
+
+Filter::~Filter() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (Level& v : lv_) v.release();
+    for (Buf& b : pyr_) b.release();
+    input_.release();
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+Level& Filter::level(int l) {
+    if (l < 0 || l >= L_) throw Error(FF_ERR_OUT_OF_RANGE, "level index out of bounds: " + std::to_string(l));
+    return lv_[l];
+}
+const Level& Filter::level(int l) const {
+    if (l < 0 || l >= L_) throw Error(FF_ERR_OUT_OF_RANGE, "level index out of bounds: " + std::to_string(l));
+    return lv_[l];
+}
+
+// FlowFilter::setGamma / DeltaFlowFilter::setGamma: gamma/255^2 for uint8 input
+// (flowfilter.cu:276-285, 559-568); FlowUpdate::setGamma rejects gamma <= 0 (update.cu:124-132)
+void Filter::set_gamma(int l, float g) {
+    Level& v = level(l);
+    const float eff = v.item == 1 ? g / (255.0f * 255.0f) : g;
+    if (!(eff > 0.0f)) throw Error(FF_ERR_INVALID_ARGUMENT, "gamma should be greater than zero: " + std::to_string(g));
+    v.gamma = eff;
+}
+float Filter::gamma(int l) const { return level(l).gamma; }
+
+// setMaxFlow: iterations = int(ceilf(maxflow)) must be > 0 (propagation.cu:137-148);
+// pyramids halve per level, top = maxflow / 2^(L-1) (flowfilter.cu:849-866)
+void Filter::set_max_flow(float m) {
+    float ml = m;
+    std::vector<float> per(L_);
+    if (L_ == 1) {
+        per[0] = m;
+    } else {
+        for (int l = 0; l < L_ - 1; ++l) {
+            per[l] = ml;
+            ml /= 2.0f;
+        }
+        per[L_ - 1] = ml;
+    }
+    for (float x : per)
+        if (!((int)ceilf(x) > 0))
+            throw Error(FF_ERR_INVALID_ARGUMENT, "propagation iterations should be greater than zero, maxflow: " + std::to_string(m));
+    for (int l = 0; l < L_; ++l) {
+        lv_[l].maxflow = per[l];
+        lv_[l].iters = (int)ceilf(per[l]);
+    }
+}
+float Filter::max_flow() const { return lv_[0].maxflow; }
+
+void Filter::set_smooth(int l, int n) {
+    Level& v = level(l);
+    if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "smooth iterations should be greater than zero: " + std::to_string(n));
+    v.smooth = n;
+}
+int Filter::smooth(int l) const { return level(l).smooth; }
+
+void Filter::set_border(int b) {
+    if (b < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "border should be greater or equal zero: " + std::to_string(b));
+    for (Level& v : lv_) v.border = b;
+}
+int Filter::border() const { return lv_[L_ - 1].border; }
+int Filter::iterations(int l) const { return level(l).iters; }
+
+void Filter::set_stream(cudaStream_t s) {
+    if (own_stream_ && stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+    own_stream_ = false;
+    stream_ = s;
+}
+
+void Filter::check_image_shape(int h, int w, int depth, int item) const {
+    if (h != H_ || w != W_ || depth != 1 || item != item_)
+        throw Error(FF_ERR_SHAPE, "GPUImage::upload(): shapes do not match. Required: [" + std::to_string(H_) + ", " +
+                                      std::to_string(W_) + ", 1][" + std::to_string(item_) + "], passed: [" +
+                                      std::to_string(h) + ", " + std::to_string(w) + ", " + std::to_string(depth) +
+                                      "][" + std::to_string(item) + "]");
+}
+
+void Filter::load_host(const ff_image& img) {
+    check_image_shape(img.height, img.width, img.depth, (int)img.itemSize);
+    if (!img.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image data");
+    Level& v = lv_[0];
+    if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    check_cuda(cudaMemcpy2DAsync(const_cast<void*>(v.img), v.img_pitch, img.data, img.pitch, (size_t)W_ * item_,
+                                 (size_t)H_, cudaMemcpyHostToDevice, stream_),
+               "upload");
+    check_cuda(cudaStreamSynchronize(stream_), "upload");
+}
+
+void Filter::load_device_async(const void* img, size_t pitch, cudaStream_t s) {
+    Level& v = lv_[0];
+    if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
+    check_cuda(cudaMemcpy2DAsync(const_cast<void*>(v.img), v.img_pitch, img, pitch, (size_t)W_ * item_, (size_t)H_,
+                                 cudaMemcpyDeviceToDevice, s ? s : stream_),
+               "load_device");
+}
+
+void Filter::bind_device(const void* img, size_t pitch) {
+    if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
+    if (pitch < (size_t)W_ * item_) throw Error(FF_ERR_INVALID_ARGUMENT, "pitch smaller than a row");
+    if (((uintptr_t)img % 16) || (pitch % 16))
+        throw Error(FF_ERR_INVALID_ARGUMENT, "bound images need 16-byte aligned rows");
+    lv_[0].img = img;
+    lv_[0].img_pitch = pitch;
+}
+
+void Filter::set_external_image(const void* img, size_t pitch) { bind_device(img, pitch); }
+
+void Filter::set_external_coarse(const void* flow, size_t pitch, int Hc, int Wc) {
+    if (!flow) throw Error(FF_ERR_INVALID_ARGUMENT, "null coarse flow");
+    if (Hc <= 0 || Wc <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "coarse flow shape");
+    if (pitch < (size_t)Wc * 8) throw Error(FF_ERR_INVALID_ARGUMENT, "coarse pitch smaller than a row");
+    Level& v = lv_[0];
+    v.coarse = flow;
+    v.coarse_pitch = pitch;
+    v.Hc = Hc;
+    v.Wc = Wc;
+}
+
+void Filter::coarse_of(int l, const void** p, size_t* pitch, int* Hc, int* Wc) const {
+    const Level& v = lv_[l];
+    if (kind_ != Kind::Pyramidal) {
+        *p = v.coarse;
+        *pitch = v.coarse_pitch;
+    } else if (l == L_ - 2) {
+        *p = lv_[L_ - 1].fu.p;
+        *pitch = lv_[L_ - 1].fu.pitch;
+    } else {
+        *p = lv_[l + 1].fs[cur_].p;
+        *pitch = lv_[l + 1].fs[cur_].pitch;
+    }
+    *Hc = v.Hc;
+    *Wc = v.Wc;
+}
+
+// ------------------------------------------------------------------ unfused path
+void Filter::model_unfused(int l, cudaStream_t s) {
+    Level& v = lv_[l];
+    v.alloc_scratch();
+    check_cuda(launch_image_model(v.img, v.img_pitch, v.item, v.H, v.W, (float*)v.a0.p, v.a0.pitch,
+                                  (float*)v.grad.p, v.grad.pitch, s),
+               "image model");
+}
+
+void Filter::propagate_unfused(int l, cudaStream_t s) {
+    Level& v = lv_[l];
+    v.alloc_scratch();
+    const Buf& fs = v.fs[cur_];
+    if (!v.delta) {
+        check_cuda(launch_propagate((const float*)fs.p, fs.pitch, v.H, v.W, v.iters, v.border, (float*)v.fp.p,
+                                    v.fp.pitch, (float*)v.t1.p, v.t1.pitch, s),
+                   "propagate");
+    } else {
+        const Buf& io = v.io[cur_];
+        const Buf& d = v.d[cur_];
+        check_cuda(launch_propagate_payload((const float*)fs.p, fs.pitch, (const float*)io.p, io.pitch,
+                                            (const float*)d.p, d.pitch, v.H, v.W, v.iters, v.border, (float*)v.fp.p,
+                                            v.fp.pitch, (float*)v.ip.p, v.ip.pitch, (float*)v.dp.p, v.dp.pitch,
+                                            (float*)v.t1.p, v.t1.pitch, (float*)v.t2.p, v.t2.pitch, (float*)v.t3.p,
+                                            v.t3.pitch, s),
+                   "propagate payload");
+    }
+}
+
+void Filter::update_unfused(int l, cudaStream_t s) {
+    Level& v = lv_[l];
+    v.alloc_scratch();
+    const int nxt = cur_ ^ 1;
+    if (!v.delta) {
+        const Buf& io = v.io[cur_];
+        check_cuda(launch_update((const float*)v.a0.p, v.a0.pitch, (const float*)v.grad.p, v.grad.pitch,
+                                 (const float*)io.p, io.pitch, (const float*)v.fp.p, v.fp.pitch, v.H, v.W, v.gamma,
+                                 v.maxflow, (float*)v.fu.p, v.fu.pitch, (float*)v.io[nxt].p, v.io[nxt].pitch,
+                                 v.first ? 1 : 0, s),
+                   "update");
+        check_cuda(launch_smooth((const float*)v.fu.p, v.fu.pitch, v.H, v.W, v.smooth, (float*)v.fs[nxt].p,
+                                 v.fs[nxt].pitch, (float*)v.t1.p, v.t1.pitch, s),
+                   "smooth");
+    } else {
+        const void* cp;
+        size_t cpitch;
+        int Hc, Wc;
+        coarse_of(l, &cp, &cpitch, &Hc, &Wc);
+        if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
+        check_cuda(launch_delta_update((const float*)v.a0.p, v.a0.pitch, (const float*)v.grad.p, v.grad.pitch,
+                                       (const float*)v.ip.p, v.ip.pitch, (const float*)v.dp.p, v.dp.pitch,
+                                       (const float*)cp, cpitch, Hc, Wc, v.H, v.W, v.gamma, v.maxflow,
+                                       (float*)v.fut.p, v.fut.pitch, (float*)v.d[nxt].p, v.d[nxt].pitch,
+                                       (float*)v.io[nxt].p, v.io[nxt].pitch, v.first ? 1 : 0, s),
+                   "delta update");
+        check_cuda(launch_smooth((const float*)v.fut.p, v.fut.pitch, v.H, v.W, v.smooth, (float*)v.fs[nxt].p,
+                                 v.fs[nxt].pitch, (float*)v.t1.p, v.t1.pitch, s),
+                   "smooth");
+    }
+}
+
+void Filter::step_level_unfused(int l, cudaStream_t s) {
+    model_unfused(l, s);
+    propagate_unfused(l, s);
+    update_unfused(l, s);
+}
+
+void Filter::step_level(int l, cudaStream_t s) {
+    Level& v = lv_[l];
+    if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    if (fused_ && fused_available(v.delta, v.item, v.iters, v.smooth)) {
+        const int nxt = cur_ ^ 1;
+        LevelArgs a{};
+        a.H = v.H;
+        a.W = v.W;
+        a.item = v.item;
+        a.img = v.img;
+        a.img_pitch = v.img_pitch;
+        a.fs_in = (const float*)v.fs[cur_].p;
+        a.fs_in_pitch = v.fs[cur_].pitch;
+        a.io_in = (const float*)v.io[cur_].p;
+        a.io_in_pitch = v.io[cur_].pitch;
+        a.fs_out = (float*)v.fs[nxt].p;
+        a.fs_out_pitch = v.fs[nxt].pitch;
+        a.io_out = (float*)v.io[nxt].p;
+        a.io_out_pitch = v.io[nxt].pitch;
+        if (v.delta) {
+            a.d_in = (const float*)v.d[cur_].p;
+            a.d_in_pitch = v.d[cur_].pitch;
+            a.d_out = (float*)v.d[nxt].p;
+            a.d_out_pitch = v.d[nxt].pitch;
+            const void* cp;
+            coarse_of(l, &cp, &a.coarse_pitch, &a.Hc, &a.Wc);
+            if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
+            a.coarse = (const float*)cp;
+        } else {
+            a.fu_out = (float*)v.fu.p;
+            a.fu_out_pitch = v.fu.pitch;
+        }
+        a.gamma = v.gamma;
+        a.maxflow = v.maxflow;
+        a.border = v.border;
+        a.first = v.first ? 1 : 0;
+        check_cuda(launch_fused_level(v.delta, v.iters, v.smooth, a, s), "fused level");
+    } else {
+        step_level_unfused(l, s);
+    }
+}
+
+void Filter::compute_async(cudaStream_t s) {
+    if (!s) s = stream_;
+    if (kind_ == Kind::Pyramidal) {
+        for (int l = 1; l < L_; ++l) {
+            const Level& fine = lv_[l - 1];
+            check_cuda(launch_pyramid_down(fine.img, fine.img_pitch, item_, fine.H, fine.W, pyr_[l - 1].p,
+                                           pyr_[l - 1].pitch, s),
+                       "pyramid");
+        }
+    }
+    // top first (level L-2 reads its fresh unsmoothed flow), then the delta levels
+    for (int l = L_ - 1; l >= 0; --l) step_level(l, s);
+    cur_ ^= 1;
+    for (Level& v : lv_) v.first = false;
+    phase_ = 0;
+}
+
+void Filter::compute() {
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    compute_async(stream_);
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(ev1_), "compute");
+    check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
+}
+
+// phase API (FlowFilter / DeltaFlowFilter computeImageModel / Propagation / Update)
+void Filter::phase_model() {
+    if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
+    if (!lv_[0].img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    model_unfused(0, stream_);
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(ev1_), "computeImageModel");
+    check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
+    phase_ = 1;
+}
+
+void Filter::phase_propagation() {
+    if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    propagate_unfused(0, stream_);
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(ev1_), "computePropagation");
+    check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
+    phase_ = 2;
+}
+
+void Filter::phase_update() {
+    if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    update_unfused(0, stream_);
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(ev1_), "computeUpdate");
+    check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
+    cur_ ^= 1;
+    lv_[0].first = false;
+    phase_ = 0;
+}
+
+// ------------------------------------------------------------------ results
+void Filter::result(int which, void** p, size_t* pitch) {
+    const Level& v = lv_[0];
+    const Buf* b = nullptr;
+    switch (which) {
+        case 0: b = &v.fs[cur_]; break;
+        case 1:
+            if (kind_ == Kind::Single || (kind_ == Kind::Pyramidal && L_ == 1)) b = &v.fu;
+            else b = &v.fs[cur_];
+            break;
+        case 2: b = &v.io[cur_]; break;
+        default: throw Error(FF_ERR_INVALID_ARGUMENT, "unknown result selector " + std::to_string(which));
+    }
+    *p = b->p;
+    *pitch = b->pitch;
+}
+
+void Filter::download_flow(ff_image& out) {
+    if (out.height != H_ || out.width != W_ || out.depth != 2 || out.itemSize != 4)
+        throw Error(FF_ERR_SHAPE, "GPUImage::download(): shapes do not match. Required: [" + std::to_string(H_) + ", " +
+                                      std::to_string(W_) + ", 2][4]");
+    if (!out.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null flow buffer");
+    const Buf& b = lv_[0].fs[cur_];
+    check_cuda(cudaMemcpy2DAsync(out.data, out.pitch, b.p, b.pitch, b.row_bytes(), (size_t)b.h, cudaMemcpyDeviceToHost,
+                                 stream_),
+               "downloadFlow");
+    check_cuda(cudaStreamSynchronize(stream_), "downloadFlow");
+}
+
+void Filter::download_image(ff_image& out) {
+    if (out.height != H_ || out.width != W_ || out.depth != 1 || out.itemSize != 4)
+        throw Error(FF_ERR_SHAPE, "GPUImage::download(): shapes do not match. Required: [" + std::to_string(H_) + ", " +
+                                      std::to_string(W_) + ", 1][4]");
+    if (!out.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image buffer");
+    const Buf& b = lv_[0].io[cur_];
+    check_cuda(cudaMemcpy2DAsync(out.data, out.pitch, b.p, b.pitch, b.row_bytes(), (size_t)b.h, cudaMemcpyDeviceToHost,
+                                 stream_),
+               "downloadImage");
+    check_cuda(cudaStreamSynchronize(stream_), "downloadImage");
+}
+
+void Filter::level_state(int l, int which, void* dst, size_t dst_pitch) {
+    const Level& v = level(l);
+    const Buf* b = nullptr;
+    switch (which) {
+        case 0: b = &v.fs[cur_]; break;
+        case 1: b = v.delta ? nullptr : &v.fu; break;
+        case 2: b = &v.io[cur_]; break;
+        case 3: b = v.delta ? &v.d[cur_] : nullptr; break;
+        default: break;
+    }
+    if (!b || !b->p) throw Error(FF_ERR_UNSUPPORTED, "level state " + std::to_string(which) + " not kept for level " + std::to_string(l));
+    if (!dst) throw Error(FF_ERR_INVALID_ARGUMENT, "null destination");
+    check_cuda(cudaMemcpy2DAsync(dst, dst_pitch, b->p, b->pitch, b->row_bytes(), (size_t)b->h, cudaMemcpyDeviceToHost,
+                                 stream_),
+               "level state");
+    check_cuda(cudaStreamSynchronize(stream_), "level state");
+}
+
+}  // namespace ffb

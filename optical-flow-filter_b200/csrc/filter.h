@@ -1,0 +1,146 @@
+// Host-side filter objects behind the C ABI (capi.cu).
+//
+// One Filter covers the reference's three composites (src/gpu/flowfilter.cu):
+//   FlowFilter          one "top" level on an owned uint8 image or an external image
+//   DeltaFlowFilter     one "delta" level refining an external coarse flow
+//   PyramidalFlowFilter an owned uint8 input, an image pyramid, L-1 delta levels and a top
+//
+// Filter state lives in HBM in ping-pong pairs (read the previous frame's copy, write
+// this frame's), so every level of a frame can be computed by one fused kernel that
+// reads its neighbours' halo pixels without racing other tiles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ffb200.h"
+
+namespace ffb {
+
+// error carrying an ff_status across the C++ layer
+struct Error : std::runtime_error {
+    ff_status status;
+    Error(ff_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void check_cuda(cudaError_t e, const char* what);
+
+// pitched device buffer (owning)
+struct Buf {
+    void* p = nullptr;
+    size_t pitch = 0;
+    int h = 0, w = 0;   // pixels
+    int bpp = 0;        // bytes per pixel
+    void alloc(int h_, int w_, int bpp_);
+    void release();
+    void clear(cudaStream_t s);
+    size_t row_bytes() const { return (size_t)w * bpp; }
+};
+
+enum class Kind { Single = 0, Delta = 1, Pyramidal = 2 };
+
+struct Level {
+    bool delta = false;
+    int H = 0, W = 0;
+    int item = 1;                // input image item size
+    const void* img = nullptr;   // level image (device)
+    size_t img_pitch = 0;
+    Buf fs[2], io[2], d[2];      // ping-pong state: smoothed flow, old image, delta flow
+    Buf fu;                      // unsmoothed updated flow (top levels)
+    // coarse flow source for delta levels
+    const void* coarse = nullptr;  // external coarse flow (standalone DeltaFlowFilter)
+    size_t coarse_pitch = 0;
+    int Hc = 0, Wc = 0;
+    float gamma = 1.0f;          // value used by the update (already scaled for uint8 input)
+    float maxflow = 1.0f;
+    int iters = 1;               // propagation iterations = ceil(maxflow)
+    int smooth = 1;
+    int border = 3;
+    bool first = true;
+    // scratch of the unfused path (allocated on first use)
+    Buf a0, grad, fp, ip, dp, t1, t2, t3, fut;
+    void alloc_state();
+    void alloc_scratch();
+    void release();
+};
+
+class Filter {
+public:
+    Filter(Kind kind, int H, int W, int levels, int item);
+    ~Filter();
+    Filter(const Filter&) = delete;
+    Filter& operator=(const Filter&) = delete;
+
+    Kind kind() const { return kind_; }
+    int height() const { return H_; }
+    int width() const { return W_; }
+    int levels() const { return L_; }
+    int item() const { return item_; }
+    Level& level(int l);
+    const Level& level(int l) const;
+
+    // parameters (reference setter rules)
+    void set_gamma(int level, float g);
+    float gamma(int level) const;
+    void set_max_flow(float m);
+    float max_flow() const;
+    void set_smooth(int level, int n);
+    int smooth(int level) const;
+    void set_border(int b);
+    int border() const;
+    int iterations(int level) const;
+
+    void set_stream(cudaStream_t s);
+    cudaStream_t stream() const { return stream_; }
+
+    // inputs
+    void load_host(const ff_image& img);
+    void load_device_async(const void* img, size_t pitch, cudaStream_t s);
+    void bind_device(const void* img, size_t pitch);
+    void set_external_image(const void* img, size_t pitch);
+    void set_external_coarse(const void* flow, size_t pitch, int Hc, int Wc);
+
+    // compute
+    void compute();                       // blocking, records elapsed time
+    void compute_async(cudaStream_t s);   // enqueue only
+    void phase_model();
+    void phase_propagation();
+    void phase_update();
+    float elapsed_ms() const { return elapsed_; }
+
+    // results (current frame)
+    void result(int which, void** p, size_t* pitch);
+    void download_flow(ff_image& out);
+    void download_image(ff_image& out);
+    void level_state(int level, int which, void* dst, size_t dst_pitch);
+
+    // force the unfused per-stage path (for testing both paths)
+    void set_fused(bool on) { fused_ = on; }
+
+private:
+    void step_level(int l, cudaStream_t s);
+    void step_level_unfused(int l, cudaStream_t s);
+    void model_unfused(int l, cudaStream_t s);
+    void propagate_unfused(int l, cudaStream_t s);
+    void update_unfused(int l, cudaStream_t s);
+    void coarse_of(int l, const void** p, size_t* pitch, int* Hc, int* Wc) const;
+    void check_image_shape(int h, int w, int depth, int item) const;
+
+    Kind kind_;
+    int H_, W_, L_, item_;
+    Buf input_;                    // owned level-0 input (Single owned, Pyramidal)
+    std::vector<Buf> pyr_;         // pyr_[l-1] = level l image
+    std::vector<Level> lv_;
+    int cur_ = 0;                  // index of the latest state copy
+    cudaStream_t stream_ = nullptr;
+    bool own_stream_ = false;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    float elapsed_ = 0.0f;
+    bool fused_ = true;
+    int phase_ = 0;                // phase API progress: 0 none, 1 model, 2 propagated
+};
+
+}  // namespace ffb

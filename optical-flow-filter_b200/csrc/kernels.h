@@ -1,0 +1,55 @@
+// Host-side launchers of the device kernels (stage_kernels.cu, level_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace ffb {
+
+// ---- per-stage kernels (stage_kernels.cu)
+cudaError_t launch_pyramid_down(const void* in, size_t in_pitch, int item, int H, int W, void* out,
+                                size_t out_pitch, cudaStream_t s);
+cudaError_t launch_image_model(const void* img, size_t pitch, int item, int H, int W, float* a0, size_t a0p,
+                               float* grad, size_t gp, cudaStream_t s);
+cudaError_t launch_propagate(const float* flow, size_t fp, int H, int W, int N, int border, float* out, size_t op,
+                             float* tmp, size_t tp, cudaStream_t s);
+cudaError_t launch_propagate_payload(const float* flow, size_t fp, const float* sc, size_t sp, const float* ve,
+                                     size_t vp, int H, int W, int N, int border, float* of, size_t ofp, float* os,
+                                     size_t osp, float* ov, size_t ovp, float* tf, size_t tfp, float* ts, size_t tsp,
+                                     float* tv, size_t tvp, cudaStream_t s);
+cudaError_t launch_update(const float* a0, size_t a0p, const float* grad, size_t gp, const float* old, size_t olp,
+                          const float* flow, size_t fp, int H, int W, float gamma, float maxflow, float* of,
+                          size_t ofp, float* oi, size_t oip, int first, cudaStream_t s);
+cudaError_t launch_delta_update(const float* a0, size_t a0p, const float* grad, size_t gp, const float* old,
+                                size_t olp, const float* delta, size_t dp, const float* coarse, size_t cp, int Hc,
+                                int Wc, int H, int W, float gamma, float maxflow, float* of, size_t ofp, float* od,
+                                size_t odp, float* oi, size_t oip, int first, cudaStream_t s);
+cudaError_t launch_smooth(const float* flow, size_t fp, int H, int W, int S, float* out, size_t op, float* tmp,
+                          size_t tp, cudaStream_t s);
+
+// ---- fused per-level kernels (level_kernels.cu)
+struct LevelArgs {
+    int H, W;
+    int item;            // input image item size (1 or 4)
+    const void* img;     // level image
+    size_t img_pitch;
+    // state read (previous frame) and written (this frame)
+    const float* fs_in;  size_t fs_in_pitch;   // smoothed flow (float2)
+    const float* io_in;  size_t io_in_pitch;   // old image (float)
+    const float* d_in;   size_t d_in_pitch;    // delta flow (float2), delta levels
+    float* fs_out;       size_t fs_out_pitch;
+    float* io_out;       size_t io_out_pitch;
+    float* d_out;        size_t d_out_pitch;   // delta levels
+    float* fu_out;       size_t fu_out_pitch;  // unsmoothed flow (float2), top levels; may be null
+    // coarse flow (delta levels)
+    const float* coarse; size_t coarse_pitch; int Hc, Wc;
+    float gamma, maxflow;
+    int border;
+    int first;
+};
+
+// true if a fused kernel exists for this (delta, item, iterations, smoothing)
+bool fused_available(bool delta, int item, int N, int S);
+cudaError_t launch_fused_level(bool delta, int N, int S, const LevelArgs& a, cudaStream_t s);
+
+}  // namespace ffb

@@ -1,0 +1,177 @@
+"""Generate golden fixtures by running the REFERENCE library (test infrastructure).
+
+Two steps:
+
+  python oracle/make_reference_fixtures.py run  --out DIR   (on a machine with a GPU)
+      builds nothing; needs oracle/_ref/ref_driver (``make -C oracle ref``).  Writes the
+      stage inputs, runs the reference driver on them and on the parity sequences,
+      and leaves raw outputs in DIR.
+
+  python oracle/make_reference_fixtures.py pack --raw DIR
+      packs DIR into the small committed fixtures under tests/golden/.
+
+The parity sequences are regenerated from seeds by flowfilter_b200.synthetic; the
+fixtures carry a sha256 of the frames so a drifting generator is detected.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "optical-flow-filter_b200"))
+
+from flowfilter_b200 import synthetic  # noqa: E402
+
+DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+# stage inputs: odd sizes so the pyramid's integer halving and the edges are exercised
+STAGE_H, STAGE_W = 53, 70
+
+# parity sequences (name -> parameters).  levels 0 = single-level FlowFilter.
+CASES = {
+    "constant_320x240_L1": dict(seq="constant", frames=100, levels=0, maxflow=4.0,
+                                gamma=[10.0], smooth=[1], dump=[1, 2, 10, 50, 99]),
+    "rotzoom_640x480_L2": dict(seq="rotzoom", frames=300, levels=2, maxflow=4.0,
+                               gamma=[10.0, 50.0], smooth=[2, 4], dump=[1, 10, 100, 299]),
+    "bumps_2048x1088_L3": dict(seq="bumps", frames=60, levels=3, maxflow=4.0,
+                               gamma=[5.0, 20.0, 50.0], smooth=[1, 2, 4], dump=[1, 20, 59]),
+    "odd_77x61_L1": dict(seq="constant", frames=40, levels=0, maxflow=2.5, gamma=[3.0],
+                         smooth=[2], dump=list(range(0, 40, 3)) + [39],
+                         kw=dict(height=61, width=77, sigma=1.2, seed=11, flow=(1.3, 0.6))),
+    "odd_150x98_L3": dict(seq="rotzoom", frames=40, levels=3, maxflow=3.0,
+                          gamma=[4.0, 9.0, 30.0], smooth=[1, 3, 2], dump=list(range(0, 40, 3)) + [39],
+                          kw=dict(height=98, width=150, sigma=1.0, seed=12, deg_per_frame=1.5,
+                                  zoom_per_frame=1.01)),
+    "small_96x64_L2": dict(seq="bumps", frames=40, levels=2, maxflow=5.0, gamma=[2.0, 25.0],
+                           smooth=[3, 1], dump=list(range(0, 40, 3)) + [39],
+                           kw=dict(height=64, width=96, sigma=1.0, seed=13, n_bumps=3,
+                                   bump_sigma=20.0, amp=2.0, sensor_noise=2.0)),
+}
+
+FULL_LIMIT = 64 * 128  # dumps up to this many pixels are stored whole
+
+
+def stage_inputs(seed: int = 5) -> dict[str, np.ndarray]:
+    rng = np.random.default_rng(seed)
+    h, w = STAGE_H, STAGE_W
+    hc, wc = h // 2, w // 2
+    return {
+        "img_u8": rng.integers(0, 256, size=(h, w), dtype=np.uint8),
+        "img_f32": rng.uniform(0, 1, size=(h, w)).astype(np.float32),
+        "flow": (rng.normal(0, 1.5, size=(h, w, 2))).astype(np.float32),
+        "scalar": rng.uniform(0, 1, size=(h, w)).astype(np.float32),
+        "vector": (rng.normal(0, 0.8, size=(h, w, 2))).astype(np.float32),
+        "a0": rng.uniform(0, 1, size=(h, w)).astype(np.float32),
+        "grad": (rng.normal(0, 0.05, size=(h, w, 2))).astype(np.float32),
+        "a0old": rng.uniform(0, 1, size=(h, w)).astype(np.float32),
+        "coarse": (rng.normal(0, 1.0, size=(hc, wc, 2))).astype(np.float32),
+    }
+
+
+def case_frames(case: dict) -> np.ndarray:
+    return synthetic.sequence(case["seq"], frames=case["frames"], **case.get("kw", {}))
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def run(out: str) -> None:
+    os.makedirs(out, exist_ok=True)
+    sin = os.path.join(out, "stage_in")
+    sout = os.path.join(out, "stage_out")
+    os.makedirs(sin, exist_ok=True)
+    os.makedirs(sout, exist_ok=True)
+    for k, v in stage_inputs().items():
+        np.save(os.path.join(sin, k + ".npy"), v)
+    subprocess.run([DRIVER, "stages", sin, sout], check=True)
+    subprocess.run([DRIVER, "norm", os.path.join(out, "norm.npy")], check=True)
+    subprocess.run([DRIVER, "upmap", os.path.join(out, "upmap.txt"), "4200"], check=True)
+    tmp = os.environ.get("TMPDIR", "/tmp")
+    for name, case in CASES.items():
+        frames = case_frames(case)
+        fpath = os.path.join(tmp, f"frames_{name}.npy")
+        np.save(fpath, frames)
+        raw = os.path.join(tmp, f"flow_{name}.npy")
+        timing = os.path.join(out, f"timing_{name}.csv")
+        cmd = [DRIVER, "filter", fpath, raw, str(case["levels"]), repr(case["maxflow"]),
+               ",".join(repr(g) for g in case["gamma"]), ",".join(str(s) for s in case["smooth"]),
+               ",".join(str(d) for d in case["dump"]), timing]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+        flows = np.load(raw)
+        pack_flows(os.path.join(out, f"case_{name}.npz"), name, case, frames, flows)
+        os.remove(fpath)
+        os.remove(raw)
+
+
+def subsample_rows_cols(h: int, w: int) -> tuple[np.ndarray, np.ndarray]:
+    # every 5th row and 7th column, plus the last row/column so the edges are pinned
+    rows = np.unique(np.concatenate([np.arange(0, h, 5), [1, 2, h - 3, h - 2, h - 1]]))
+    cols = np.unique(np.concatenate([np.arange(0, w, 7), [1, 2, w - 3, w - 2, w - 1]]))
+    return rows, cols
+
+
+def pack_flows(path: str, name: str, case: dict, frames: np.ndarray, flows: np.ndarray) -> None:
+    t, h, w = frames.shape
+    meta = dict(case)
+    meta["name"] = name
+    meta["frames_sha256"] = sha(frames)
+    meta["flow_sha256"] = [sha(f) for f in flows]
+    arrays = {}
+    if h * w <= FULL_LIMIT:
+        arrays["flow"] = flows
+        meta["layout"] = "full"
+    else:
+        rows, cols = subsample_rows_cols(h, w)
+        arrays["rows"] = rows
+        arrays["cols"] = cols
+        arrays["flow"] = flows[:, rows][:, :, cols]
+        meta["layout"] = "subsampled"
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(path, **arrays)
+
+
+def pack(raw: str) -> None:
+    os.makedirs(GOLDEN, exist_ok=True)
+    # stage goldens: inputs are regenerated from the seed, outputs stored whole
+    sout = os.path.join(raw, "stage_out")
+    outs = {f[:-4]: np.load(os.path.join(sout, f)) for f in sorted(os.listdir(sout)) if f.endswith(".npy")}
+    ins = stage_inputs()
+    np.savez_compressed(os.path.join(GOLDEN, "ref_stages.npz"),
+                        inputs_sha256=np.frombuffer(json.dumps({k: sha(v) for k, v in ins.items()}).encode(), np.uint8),
+                        **outs)
+    np.save(os.path.join(GOLDEN, "ref_norm_u8.npy"), np.load(os.path.join(raw, "norm.npy")))
+    np.save(os.path.join(GOLDEN, "ref_upmap_detail.npy"), np.load(os.path.join(raw, "upmap.txt.detail.npy")))
+    for name in CASES:
+        src = os.path.join(raw, f"case_{name}.npz")
+        if os.path.exists(src):
+            with open(src, "rb") as fi, open(os.path.join(GOLDEN, f"ref_case_{name}.npz"), "wb") as fo:
+                fo.write(fi.read())
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    r = sub.add_parser("run")
+    r.add_argument("--out", required=True)
+    p = sub.add_parser("pack")
+    p.add_argument("--raw", required=True)
+    a = ap.parse_args()
+    if a.cmd == "run":
+        run(a.out)
+    else:
+        pack(a.raw)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,697 @@
+// CPU ORACLE for the flow-filter hot path — TEST INFRASTRUCTURE ONLY (see oracle.h).
+//
+// Reference files restated here (paths inside the reference project):
+//   src/gpu/device/pyramid_k.cu       imageDown{X,Y}_{uint8,float}_k
+//   src/gpu/device/imagemodel_k.cu    imagePrefilter_k, imageModel_k
+//   src/gpu/device/propagation_k.cu   flowPropagate{X,Y}_k, flowPropagatePayload{X,Y}_k
+//   src/gpu/device/update_k.cu        flowUpdate_k, deltaFlowUpdate_k
+//   src/gpu/device/flowsmoothing_k.cu flowSmooth{X,Y}_k
+//   src/gpu/{imagemodel,propagation,update,flowsmoothing,pyramid,flowfilter}.cu  schedule
+//   src/gpu/image.cu:292-356          texture reads: clamp addressing, point sampling
+//
+// Compiled with -ffp-contract=off: every fused multiply-add below is an explicit fma.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <thread>
+
+namespace {
+
+// Defaults pinned bit-exactly against the reference library's own stage outputs on
+// B200 (tests/golden/ref_stages.npz): nvcc fuses every propagation channel except the
+// last channel written by each kernel (flow .y of flowPropagate{X,Y}_k, vector .y of
+// flowPropagatePayload{X,Y}_k), and in the update qx = fma(g, fx, ax*Yt) but
+// qy = fma(ay, Yt, g*fy).
+int g_var[OR_V_COUNT] = {
+    1,   // OR_V_MODEL_FMA
+    61,  // OR_V_PROP_FMA: flow x (plain), flow x/y + scalar + vector x (payload)
+    7,   // OR_V_UPD_NFMA
+    3,   // OR_V_UPD_Q: qx variant 0, qy variant 1
+    0,   // OR_V_UPD_OX
+    0,   // OR_V_UPD_OY
+    1,   // OR_V_SMOOTH_FMA
+    0,   // OR_V_UPMAP
+};
+float g_norm[256];
+bool g_norm_init = false;
+int g_threads = 0;
+
+void init_norm() {
+    if (g_norm_init) return;
+    for (int v = 0; v < 256; ++v) g_norm[v] = (float)v / 255.0f;
+    g_norm_init = true;
+}
+
+inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// a*b + c with or without fusion
+inline float madd(bool fused, float a, float b, float c) {
+    if (fused) return std::fma(a, b, c);
+    float p = a * b;
+    return p + c;
+}
+
+// rows split into contiguous chunks over g_threads std::threads (serial when <= 1)
+template <typename F>
+void for_rows(int H, F&& body) {
+    const int nt = std::min(g_threads, H);
+    if (nt > 1) {
+        std::vector<std::thread> pool;
+        pool.reserve(nt);
+        for (int t = 0; t < nt; ++t) {
+            const int y0 = (int)((long)H * t / nt), y1 = (int)((long)H * (t + 1) / nt);
+            pool.emplace_back([&body, y0, y1]() {
+                for (int y = y0; y < y1; ++y) body(y);
+            });
+        }
+        for (auto& th : pool) th.join();
+        return;
+    }
+    for (int y = 0; y < H; ++y) body(y);
+}
+
+// image model masks, imagemodel_k.cu:21-22 (float constants as stored in __constant__)
+const float kSmooth[5] = {0.0625f, 0.25f, 0.375f, 0.25f, 0.0625f};
+const float kDiff[5] = {-0.125f, -0.25f, 0.0f, 0.25f, 0.125f};
+// flow smoother weights, flowsmoothing_k.cu:18-19 (0.2 as a float constant)
+const float kBox = 0.2f;
+
+// -------------------------------------------------------------- pyramid
+// imageDownX/Y: s = 0.5*c + 0.25*(m + p) evaluated in double (double literals),
+// stored as float; uint8 output is (unsigned char)(255*s) (pyramid_k.cu:33-43, 67-77).
+inline float down3(float m, float c, float p) {
+    return (float)(0.5 * (double)c + 0.25 * (double)(m + p));
+}
+
+}  // namespace
+
+extern "C" {
+
+void or_set_variant(int key, int value) {
+    if (key >= 0 && key < OR_V_COUNT) g_var[key] = value;
+}
+int or_get_variant(int key) { return (key >= 0 && key < OR_V_COUNT) ? g_var[key] : -1; }
+void or_set_norm_table(const float* t) {
+    std::memcpy(g_norm, t, sizeof(g_norm));
+    g_norm_init = true;
+}
+void or_get_norm_table(float* t) {
+    init_norm();
+    std::memcpy(t, g_norm, sizeof(g_norm));
+}
+void or_set_threads(int n) { g_threads = n; }
+
+void or_pyramid_down_u8(const uint8_t* in, int H, int W, uint8_t* out) {
+    init_norm();
+    const int Wd = W / 2, Hd = H / 2;  // integer halving, pyramid.cu:74,83
+    std::vector<uint8_t> xs((size_t)H * Wd);
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < Wd; ++x) {
+            const uint8_t* row = in + (size_t)y * W;
+            float m = g_norm[row[clampi(2 * x - 1, 0, W - 1)]];
+            float c = g_norm[row[clampi(2 * x, 0, W - 1)]];
+            float p = g_norm[row[clampi(2 * x + 1, 0, W - 1)]];
+            float s = down3(m, c, p);
+            xs[(size_t)y * Wd + x] = (uint8_t)(255.0f * s);
+        }
+    });
+    for_rows(Hd, [&](int y) {
+        for (int x = 0; x < Wd; ++x) {
+            float m = g_norm[xs[(size_t)clampi(2 * y - 1, 0, H - 1) * Wd + x]];
+            float c = g_norm[xs[(size_t)clampi(2 * y, 0, H - 1) * Wd + x]];
+            float p = g_norm[xs[(size_t)clampi(2 * y + 1, 0, H - 1) * Wd + x]];
+            float s = down3(m, c, p);
+            out[(size_t)y * Wd + x] = (uint8_t)(255.0f * s);
+        }
+    });
+}
+
+void or_pyramid_down_f32(const float* in, int H, int W, float* out) {
+    const int Wd = W / 2, Hd = H / 2;
+    std::vector<float> xs((size_t)H * Wd);
+    for_rows(H, [&](int y) {
+        const float* row = in + (size_t)y * W;
+        for (int x = 0; x < Wd; ++x)
+            xs[(size_t)y * Wd + x] = down3(row[clampi(2 * x - 1, 0, W - 1)], row[clampi(2 * x, 0, W - 1)],
+                                           row[clampi(2 * x + 1, 0, W - 1)]);
+    });
+    for_rows(Hd, [&](int y) {
+        for (int x = 0; x < Wd; ++x)
+            out[(size_t)y * Wd + x] = down3(xs[(size_t)clampi(2 * y - 1, 0, H - 1) * Wd + x],
+                                            xs[(size_t)clampi(2 * y, 0, H - 1) * Wd + x],
+                                            xs[(size_t)clampi(2 * y + 1, 0, H - 1) * Wd + x]);
+    });
+}
+
+// imagePrefilter_k (imagemodel_k.cu:31-70) then imageModel_k (:76-133).
+void or_image_model(const void* img, int item_size, int H, int W, float* a0, float* grad) {
+    init_norm();
+    const bool fz = g_var[OR_V_MODEL_FMA] != 0;
+    auto I = [&](int x, int y) -> float {
+        x = clampi(x, 0, W - 1);
+        y = clampi(y, 0, H - 1);
+        if (item_size == 1) return g_norm[((const uint8_t*)img)[(size_t)y * W + x]];
+        return ((const float*)img)[(size_t)y * W + x];
+    };
+    // prefiltered (smooth_y, smooth_x)
+    std::vector<float> pre((size_t)H * W * 2);
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            float sx = 0.0f, sy = 0.0f;
+            for (int c = -2; c <= 2; ++c) sx = madd(fz, kSmooth[c + 2], I(x + c, y), sx);
+            for (int r = -2; r <= 2; ++r) sy = madd(fz, kSmooth[r + 2], I(x, y + r), sy);
+            pre[((size_t)y * W + x) * 2 + 0] = sy;
+            pre[((size_t)y * W + x) * 2 + 1] = sx;
+        }
+    });
+    auto P = [&](int x, int y, int ch) -> float {
+        x = clampi(x, 0, W - 1);
+        y = clampi(y, 0, H - 1);
+        return pre[((size_t)y * W + x) * 2 + ch];
+    };
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            float dx = 0.0f, dy = 0.0f, sm = 0.0f;
+            for (int c = -2; c <= 2; ++c) {
+                float e = P(x + c, y, 0);
+                dx = madd(fz, kDiff[c + 2], e, dx);
+                sm = madd(fz, kSmooth[c + 2], e, sm);
+            }
+            for (int r = -2; r <= 2; ++r) dy = madd(fz, kDiff[r + 2], P(x, y + r, 1), dy);
+            grad[((size_t)y * W + x) * 2 + 0] = dx;
+            grad[((size_t)y * W + x) * 2 + 1] = dy;
+            a0[(size_t)y * W + x] = sm;
+        }
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+// one upwind sub-step of f0 with dominant velocity dv (propagation_k.cu:50-53):
+// f0 - dt*dv*(dv >= 0 ? f0 - fm : fp - f0)
+inline float upwind(bool fz, float t, float dv, float fm, float f0, float fp) {
+    float d = dv >= 0.0f ? (f0 - fm) : (fp - f0);
+    if (fz) return std::fma(-t, d, f0);
+    float p = t * d;
+    return f0 - p;
+}
+
+// dominant velocity (propagation_k.cu:37-40, 97-100)
+inline float dominant(float vm, float vp) {
+    float c = std::fabs(vp) - std::fabs(vm);
+    return c > 0.0f ? vp : vm;
+}
+
+// One direction (axis 0 = X, 1 = Y) of a propagation sub-step over the flow and the
+// optional payloads, clamp-to-edge reads, border pixels keep their input.
+void prop_pass(int axis, const float* fl, const float* sc, const float* ve, int H, int W, float dt,
+               int border, float* ofl, float* osc, float* ove) {
+    // OR_V_PROP_FMA bit mask: 1/2 flow x/y (plain kernel), 4/8 flow x/y (payload kernel),
+    // 16 scalar, 32/64 vector x/y
+    const int pv = g_var[OR_V_PROP_FMA];
+    const bool fzf[2] = {sc ? (pv & 4) != 0 : (pv & 1) != 0, sc ? (pv & 8) != 0 : (pv & 2) != 0};
+    const bool fzs = (pv & 16) != 0;
+    const bool fzv[2] = {(pv & 32) != 0, (pv & 64) != 0};
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            int xm = axis == 0 ? clampi(x - 1, 0, W - 1) : x;
+            int xp = axis == 0 ? clampi(x + 1, 0, W - 1) : x;
+            int ym = axis == 1 ? clampi(y - 1, 0, H - 1) : y;
+            int yp = axis == 1 ? clampi(y + 1, 0, H - 1) : y;
+            size_t im = (size_t)ym * W + xm, i0 = (size_t)y * W + x, ip = (size_t)yp * W + xp;
+            float vm = fl[im * 2 + axis], vp = fl[ip * 2 + axis];
+            float dv = dominant(vm, vp);
+            float t = dt * dv;
+            bool in = (x >= border && x < W - border) && (y >= border && y < H - border);
+            for (int ch = 0; ch < 2; ++ch) {
+                float r = upwind(fzf[ch], t, dv, fl[im * 2 + ch], fl[i0 * 2 + ch], fl[ip * 2 + ch]);
+                ofl[i0 * 2 + ch] = in ? r : fl[i0 * 2 + ch];
+            }
+            if (sc) {
+                float r = upwind(fzs, t, dv, sc[im], sc[i0], sc[ip]);
+                osc[i0] = in ? r : sc[i0];
+            }
+            if (ve) {
+                for (int ch = 0; ch < 2; ++ch) {
+                    float r = upwind(fzv[ch], t, dv, ve[im * 2 + ch], ve[i0 * 2 + ch], ve[ip * 2 + ch]);
+                    ove[i0 * 2 + ch] = in ? r : ve[i0 * 2 + ch];
+                }
+            }
+        }
+    });
+}
+
+// flowUpdate_k / deltaFlowUpdate_k closed-form solve (update_k.cu:43-63, 114-134)
+// OR_V_UPD_NFMA bits: 1 N00 = fma(ay,ay,g), 2 N11 = fma(ax,ax,g), 4 den = fma(ay,ay,N11)
+// OR_V_UPD_Q: qx variant + 3 * qy variant, each 0 fma(g,f,a*Yt), 1 fma(a,Yt,g*f), 2 unfused
+inline void solve2(float gamma, float ax, float ay, float yt, float fx, float fy, float& ox, float& oy) {
+    const int nf = g_var[OR_V_UPD_NFMA];
+    const int vqx = g_var[OR_V_UPD_Q] % 3, vqy = g_var[OR_V_UPD_Q] / 3;
+    const int vx = g_var[OR_V_UPD_OX], vy = g_var[OR_V_UPD_OY];
+    float ax2 = ax * ax, ay2 = ay * ay;
+    float n00 = (nf & 1) ? std::fma(ay, ay, gamma) : gamma + ay2;
+    float n11 = (nf & 2) ? std::fma(ax, ax, gamma) : gamma + ax2;
+    float den = (nf & 4) ? std::fma(ay, ay, n11) : n11 + ay2;
+    float n01 = -ax * ay;
+    float n10 = n01;
+    float gd = gamma * den;
+    float rdet = 1.0f / gd;
+    auto q = [&](int vq, float f, float a) -> float {
+        if (vq == 0) { float p = a * yt; return std::fma(gamma, f, p); }
+        if (vq == 1) { float p = gamma * f; return std::fma(a, yt, p); }
+        float p1 = gamma * f, p2 = a * yt;
+        return p1 + p2;
+    };
+    float qx = q(vqx, fx, ax), qy = q(vqy, fy, ay);
+    float ix, iy;
+    if (vx == 0) { float p = n01 * qy; ix = std::fma(n00, qx, p); }
+    else if (vx == 1) { float p = n00 * qx; ix = std::fma(n01, qy, p); }
+    else { float p1 = n00 * qx, p2 = n01 * qy; ix = p1 + p2; }
+    if (vy == 0) { float p = n11 * qy; iy = std::fma(n10, qx, p); }
+    else if (vy == 1) { float p = n10 * qx; iy = std::fma(n11, qy, p); }
+    else { float p1 = n10 * qx, p2 = n11 * qy; iy = p1 + p2; }
+    ox = ix * rdet;
+    oy = iy * rdet;
+}
+
+inline float clampf(float v, float m) { return std::fmax(-m, std::fmin(v, m)); }
+inline float sanitize(float v) { return (std::isinf(v) || std::isnan(v)) ? 0.0f : v; }
+
+}  // namespace
+
+extern "C" {
+
+// FlowPropagator::compute, propagation.cu:80-134: N x (X then Y), dt = 1/N (:146-147)
+void or_propagate(const float* flow, int H, int W, int N, int border, float* out) {
+    const float dt = 1.0f / (float)N;
+    std::vector<float> a((size_t)H * W * 2), b((size_t)H * W * 2);
+    std::memcpy(a.data(), flow, a.size() * sizeof(float));
+    for (int n = 0; n < N; ++n) {
+        prop_pass(0, a.data(), nullptr, nullptr, H, W, dt, border, b.data(), nullptr, nullptr);
+        prop_pass(1, b.data(), nullptr, nullptr, H, W, dt, border, a.data(), nullptr, nullptr);
+    }
+    std::memcpy(out, a.data(), a.size() * sizeof(float));
+}
+
+// FlowPropagatorPayload::compute, propagation.cu:324-373
+void or_propagate_payload(const float* flow, const float* scalar, const float* vector, int H, int W,
+                          int N, int border, float* oflow, float* oscalar, float* ovector) {
+    const float dt = 1.0f / (float)N;
+    const size_t P = (size_t)H * W;
+    std::vector<float> fa(flow, flow + P * 2), fb(P * 2);
+    std::vector<float> sa(scalar, scalar + P), sb(P);
+    std::vector<float> va(vector, vector + P * 2), vb(P * 2);
+    for (int n = 0; n < N; ++n) {
+        prop_pass(0, fa.data(), sa.data(), va.data(), H, W, dt, border, fb.data(), sb.data(), vb.data());
+        prop_pass(1, fb.data(), sb.data(), vb.data(), H, W, dt, border, fa.data(), sa.data(), va.data());
+    }
+    std::memcpy(oflow, fa.data(), P * 2 * sizeof(float));
+    std::memcpy(oscalar, sa.data(), P * sizeof(float));
+    std::memcpy(ovector, va.data(), P * 2 * sizeof(float));
+}
+
+// flowUpdate_k, update_k.cu:15-79
+void or_update(const float* a0, const float* grad, const float* a0old, const float* flow, int H, int W,
+               float gamma, float maxflow, float* oflow, float* oimage) {
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            float ax = grad[2 * i], ay = grad[2 * i + 1];
+            float yt = a0old[i] - a0[i];
+            float ox, oy;
+            solve2(gamma, ax, ay, yt, flow[2 * i], flow[2 * i + 1], ox, oy);
+            ox = sanitize(clampf(ox, maxflow));
+            oy = sanitize(clampf(oy, maxflow));
+            oflow[2 * i] = ox;
+            oflow[2 * i + 1] = oy;
+            oimage[i] = a0[i];
+        }
+    });
+}
+
+// texture read at normalised coordinate u = x/(W-1), point sampling, clamp
+// (update_k.cu:151-155 with the texture of update.cu:308-313).  The texture unit
+// truncates the normalised coordinate to 21 fractional bits before scaling by the
+// texel count; this was measured on B200 over every W <= 4200 and three coarse
+// widths per W on both axes (tests/golden/ref_upmap_detail.npy holds the workload sizes).
+int or_upmap_index(int x, int W, int Wc) {
+    float u = (float)x / (float)(W - 1);
+    if (!(u == u)) return 0;
+    float uq = std::floor(u * 2097152.0f);  // 2^21, exact scaling
+    long long i = ((long long)uq * (long long)Wc) >> 21;
+    if (i < 0) return 0;
+    if (i > Wc - 1) return Wc - 1;
+    return (int)i;
+}
+
+// deltaFlowUpdate_k, update_k.cu:82-173
+void or_delta_update(const float* a0, const float* grad, const float* a0old, const float* delta,
+                     const float* coarse, int Hc, int Wc, int H, int W, float gamma, float maxflow,
+                     float* oflow, float* odelta, float* oimage) {
+    std::vector<int> ix(W), iy(H);
+    for (int x = 0; x < W; ++x) ix[x] = or_upmap_index(x, W, Wc);
+    for (int y = 0; y < H; ++y) iy[y] = or_upmap_index(y, H, Hc);
+    const float hm = 0.5f * maxflow;
+    for_rows(H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            float ax = grad[2 * i], ay = grad[2 * i + 1];
+            float yt = a0old[i] - a0[i];
+            float dx, dy;
+            solve2(gamma, ax, ay, yt, delta[2 * i], delta[2 * i + 1], dx, dy);
+            dx = clampf(sanitize(dx), hm);
+            dy = clampf(sanitize(dy), hm);
+            size_t c = (size_t)iy[y] * Wc + ix[x];
+            // 2.0*fup in double, stored as float: exact doubling
+            float ux = (float)(2.0 * (double)coarse[2 * c]);
+            float uy = (float)(2.0 * (double)coarse[2 * c + 1]);
+            float fx = dx + ux, fy = dy + uy;
+            odelta[2 * i] = dx;
+            odelta[2 * i + 1] = dy;
+            oflow[2 * i] = clampf(fx, maxflow);
+            oflow[2 * i + 1] = clampf(fy, maxflow);
+            oimage[i] = a0[i];
+        }
+    });
+}
+
+// FlowSmoother::compute, flowsmoothing.cu:74-108: S x (5-tap box X then Y), weight 0.2
+void or_smooth(const float* flow, int H, int W, int S, float* out) {
+    const bool fz = g_var[OR_V_SMOOTH_FMA] != 0;
+    const size_t P = (size_t)H * W;
+    std::vector<float> a(flow, flow + P * 2), b(P * 2);
+    for (int s = 0; s < S; ++s) {
+        for_rows(H, [&](int y) {
+            for (int x = 0; x < W; ++x) {
+                float sx = 0.0f, sy = 0.0f;
+                for (int c = -2; c <= 2; ++c) {
+                    size_t j = (size_t)y * W + clampi(x + c, 0, W - 1);
+                    sx = madd(fz, kBox, a[2 * j], sx);
+                    sy = madd(fz, kBox, a[2 * j + 1], sy);
+                }
+                b[((size_t)y * W + x) * 2] = sx;
+                b[((size_t)y * W + x) * 2 + 1] = sy;
+            }
+        });
+        for_rows(H, [&](int y) {
+            for (int x = 0; x < W; ++x) {
+                float sx = 0.0f, sy = 0.0f;
+                for (int r = -2; r <= 2; ++r) {
+                    size_t j = (size_t)clampi(y + r, 0, H - 1) * W + x;
+                    sx = madd(fz, kBox, b[2 * j], sx);
+                    sy = madd(fz, kBox, b[2 * j + 1], sy);
+                }
+                a[((size_t)y * W + x) * 2] = sx;
+                a[((size_t)y * W + x) * 2 + 1] = sy;
+            }
+        });
+    }
+    std::memcpy(out, a.data(), P * 2 * sizeof(float));
+}
+
+}  // extern "C"
+
+// ====================================================================== filters
+namespace {
+
+struct Level {
+    int H = 0, W = 0;
+    int item = 1;             // input item size (1 u8, 4 f32)
+    bool delta = false;       // DeltaFlowFilter (true) or FlowFilter (false)
+    float gamma = 1.0f;       // value handed to the update stage (already scaled)
+    float maxflow = 1.0f;
+    int iters = 1;            // propagation iterations
+    int smooth = 1;
+    int border = 3;
+    bool first = true;
+    // image model outputs
+    std::vector<float> a0, grad;
+    // FlowFilter: Fp propagated flow, Fu updated flow, Iu updated image, Fs smoothed flow
+    // DeltaFlowFilter: + Ip propagated image, Dp propagated delta, Du updated delta
+    std::vector<float> Fp, Fu, Iu, Fs, Ip, Dp, Du, Fp_unused;
+    // input image (owned copy for level 0 or pyramid level)
+    const void* img = nullptr;
+    // coarse flow input of a delta level (pointer into another level's buffer)
+    const std::vector<float>* coarse = nullptr;
+    int Hc = 0, Wc = 0;
+
+    void alloc() {
+        size_t P = (size_t)H * W;
+        a0.assign(P, 0.f);
+        grad.assign(2 * P, 0.f);
+        Fp.assign(2 * P, 0.f);
+        Fu.assign(2 * P, 0.f);
+        Iu.assign(P, 0.f);
+        Fs.assign(2 * P, 0.f);
+        if (delta) {
+            Ip.assign(P, 0.f);
+            Dp.assign(2 * P, 0.f);
+            Du.assign(2 * P, 0.f);
+        }
+    }
+    void model() { or_image_model(img, item, H, W, a0.data(), grad.data()); }
+    void propagate() {
+        if (!delta) {
+            or_propagate(Fs.data(), H, W, iters, border, Fp.data());
+        } else {
+            or_propagate_payload(Fs.data(), Iu.data(), Du.data(), H, W, iters, border, Fp.data(), Ip.data(),
+                                 Dp.data());
+        }
+    }
+    void update() {
+        if (first) {  // flowfilter.cu:179-188 / 484-494
+            Iu = a0;
+            if (delta) Ip = a0;
+            first = false;
+        }
+        if (!delta) {
+            std::vector<float> old = Iu;  // update reads and writes the same image buffer
+            or_update(a0.data(), grad.data(), old.data(), Fp.data(), H, W, gamma, maxflow, Fu.data(), Iu.data());
+        } else {
+            or_delta_update(a0.data(), grad.data(), Ip.data(), Dp.data(), coarse->data(), Hc, Wc, H, W, gamma,
+                            maxflow, Fu.data(), Du.data(), Iu.data());
+        }
+        or_smooth(Fu.data(), H, W, smooth, Fs.data());
+    }
+    // FlowFilter::compute (flowfilter.cu:125-153): model, first-load copy, propagate, update, smooth
+    void compute_single() {
+        model();
+        if (first) {
+            Iu = a0;
+            if (delta) Ip = a0;
+            first = false;
+        }
+        propagate();
+        update();
+    }
+    void set_gamma(float g) { gamma = item == 1 ? g / (255.0f * 255.0f) : g; }
+    void set_maxflow(float m) {
+        maxflow = m;
+        iters = (int)std::ceil(m);
+    }
+};
+
+}  // namespace
+
+struct or_filter {
+    bool pyramidal = false;
+    int H = 0, W = 0, L = 1;
+    int item = 1;
+    std::vector<uint8_t> in8;
+    std::vector<float> in32;
+    std::vector<std::vector<uint8_t>> pyr;  // pyr[h-1] = level h image (h >= 1)
+    std::vector<Level> lv;                  // lv[h], h = 0 finest ... L-1 top
+};
+
+namespace {
+Level& top(or_filter* f) { return f->lv[f->L - 1]; }
+}  // namespace
+
+extern "C" {
+
+or_filter* or_flowfilter_create_on(int H, int W, int item_size) {
+    if (H <= 0 || W <= 0 || (item_size != 1 && item_size != 4)) return nullptr;
+    or_filter* f = new or_filter();
+    f->H = H;
+    f->W = W;
+    f->L = 1;
+    f->item = item_size;
+    if (item_size == 1) f->in8.assign((size_t)H * W, 0);
+    else f->in32.assign((size_t)H * W, 0.f);
+    f->lv.resize(1);
+    Level& l = f->lv[0];
+    l.H = H;
+    l.W = W;
+    l.item = item_size;
+    l.img = item_size == 1 ? (const void*)f->in8.data() : (const void*)f->in32.data();
+    l.alloc();
+    // configure(): FlowUpdate(..., 1.0, 1.0), FlowSmoother(.., 1), FlowPropagator(.., 1)
+    l.gamma = 1.0f;
+    l.maxflow = 1.0f;
+    l.iters = 1;
+    l.smooth = 1;
+    l.border = 3;
+    return f;
+}
+
+or_filter* or_flowfilter_create(int H, int W, int smooth, float maxflow, float gamma) {
+    or_filter* f = or_flowfilter_create_on(H, W, 1);
+    if (!f) return nullptr;
+    Level& l = f->lv[0];
+    l.set_gamma(gamma);
+    l.set_maxflow(maxflow);
+    l.smooth = smooth;
+    return f;
+}
+
+or_filter* or_pyramidal_create(int H, int W, int levels) {
+    if (H <= 0 || W <= 0 || levels <= 0) return nullptr;
+    or_filter* f = new or_filter();
+    f->pyramidal = true;
+    f->H = H;
+    f->W = W;
+    f->L = levels;
+    f->item = 1;
+    f->in8.assign((size_t)H * W, 0);
+    f->lv.resize(levels);
+    f->pyr.resize(levels > 1 ? levels - 1 : 0);
+    int h = H, w = W;
+    for (int l = 0; l < levels; ++l) {
+        Level& lv = f->lv[l];
+        if (l > 0) {
+            w /= 2;
+            h /= 2;
+            f->pyr[l - 1].assign((size_t)h * w, 0);
+        }
+        lv.H = h;
+        lv.W = w;
+        lv.item = 1;
+        lv.delta = (l < levels - 1);
+        lv.img = l == 0 ? (const void*)f->in8.data() : (const void*)f->pyr[l - 1].data();
+        lv.alloc();
+        lv.gamma = 1.0f;
+        lv.maxflow = 1.0f;
+        lv.iters = 1;
+        lv.smooth = 1;
+        lv.border = 3;
+    }
+    // coarse inputs: level L-2 reads the top level's unsmoothed flow, finer levels the
+    // next coarser level's smoothed flow (flowfilter.cu:663-672)
+    for (int l = 0; l < levels - 1; ++l) {
+        Level& lv = f->lv[l];
+        Level& up = f->lv[l + 1];
+        lv.coarse = (l == levels - 2) ? &up.Fu : &up.Fs;
+        lv.Hc = up.H;
+        lv.Wc = up.W;
+    }
+    return f;
+}
+
+void or_filter_destroy(or_filter* f) { delete f; }
+int or_filter_levels(const or_filter* f) { return f->L; }
+
+int or_filter_set_gamma(or_filter* f, int level, float gamma) {
+    if (level < 0 || level >= f->L || !(gamma > 0.0f)) return -1;
+    f->lv[level].set_gamma(gamma);
+    return 0;
+}
+float or_filter_get_gamma(const or_filter* f, int level) { return f->lv[level].gamma; }
+
+// PyramidalFlowFilter::setMaxFlow halves per level (flowfilter.cu:849-866)
+int or_filter_set_max_flow(or_filter* f, float maxflow) {
+    if (f->L == 1) {
+        f->lv[0].set_maxflow(maxflow);
+        return 0;
+    }
+    float m = maxflow;
+    for (int l = 0; l < f->L - 1; ++l) {
+        f->lv[l].set_maxflow(m);
+        m /= 2.0f;
+    }
+    f->lv[f->L - 1].set_maxflow(m);
+    return 0;
+}
+float or_filter_get_max_flow(const or_filter* f) { return f->lv[0].maxflow; }
+int or_filter_set_smooth_iterations(or_filter* f, int level, int n) {
+    if (level < 0 || level >= f->L || n <= 0) return -1;
+    f->lv[level].smooth = n;
+    return 0;
+}
+int or_filter_get_smooth_iterations(const or_filter* f, int level) { return f->lv[level].smooth; }
+int or_filter_set_propagation_border(or_filter* f, int border) {
+    if (border < 0) return -1;
+    for (auto& l : f->lv) l.border = border;
+    return 0;
+}
+int or_filter_get_propagation_iterations(const or_filter* f, int level) { return f->lv[level].iters; }
+
+void or_filter_load(or_filter* f, const void* img) {
+    if (f->item == 1) std::memcpy(f->in8.data(), img, f->in8.size());
+    else std::memcpy(f->in32.data(), img, f->in32.size() * sizeof(float));
+}
+
+// PyramidalFlowFilter::compute (flowfilter.cu:685-716) / FlowFilter::compute (:125-153)
+void or_filter_compute(or_filter* f) {
+    if (!f->pyramidal) {
+        f->lv[0].compute_single();
+        return;
+    }
+    for (int l = 1; l < f->L; ++l) {
+        const uint8_t* src = l == 1 ? f->in8.data() : f->pyr[l - 2].data();
+        Level& fine = f->lv[l - 1];
+        or_pyramid_down_u8(src, fine.H, fine.W, f->pyr[l - 1].data());
+    }
+    if (f->L == 1) {
+        f->lv[0].compute_single();
+        return;
+    }
+    Level& t = top(f);
+    t.model();
+    t.propagate();
+    for (int l = 0; l < f->L - 1; ++l) {
+        f->lv[l].model();
+        f->lv[l].propagate();
+    }
+    t.update();
+    for (int l = 0; l < f->L - 1; ++l) f->lv[l].update();
+}
+
+void or_filter_download_flow(const or_filter* f, float* out) {
+    const Level& l = f->lv[0];
+    std::memcpy(out, l.Fs.data(), l.Fs.size() * sizeof(float));
+}
+void or_filter_get_flow(const or_filter* f, float* out) {
+    const Level& l = f->lv[0];
+    const std::vector<float>& v = f->L == 1 ? l.Fu : l.Fs;
+    std::memcpy(out, v.data(), v.size() * sizeof(float));
+}
+void or_filter_download_image(const or_filter* f, float* out) {
+    const Level& l = f->lv[0];
+    std::memcpy(out, l.Iu.data(), l.Iu.size() * sizeof(float));
+}
+size_t or_filter_level_state(const or_filter* f, int level, int which, float* out) {
+    const Level& l = f->lv[level];
+    const std::vector<float>* v = nullptr;
+    switch (which) {
+        case 0: v = &l.Fs; break;
+        case 1: v = &l.Fu; break;
+        case 2: v = &l.Iu; break;
+        case 3: v = l.delta ? &l.Du : nullptr; break;
+        default: break;
+    }
+    if (!v) return 0;
+    if (out) std::memcpy(out, v->data(), v->size() * sizeof(float));
+    return v->size();
+}
+void or_filter_level_shape(const or_filter* f, int level, int* H, int* W) {
+    *H = f->lv[level].H;
+    *W = f->lv[level].W;
+}
+
+}  // extern "C"
