@@ -28,6 +28,10 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 typedef enum ff_status {
     FF_OK = 0,
     FF_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument / bare std::exception on a bad value */
@@ -109,6 +113,10 @@ ff_status ff_filter_set_propagation_border(ff_filter* f, int border);
 ff_status ff_filter_get_propagation_border(const ff_filter* f, int* border);
 ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, int* iterations);
 
+/* Select the fused per-level kernels (enabled = 1, the default) or the per-stage kernels
+ * (0).  Both give bit-identical results; the switch exists for testing and profiling. */
+ff_status ff_filter_set_fused(ff_filter* f, int enabled);
+
 /* Stream used by the blocking calls (default: a non-blocking stream owned by the filter). */
 ff_status ff_filter_set_stream(ff_filter* f, void* stream);
 
@@ -188,6 +196,10 @@ ff_status ff_stage_delta_update(const float* a0, size_t a0_pitch, const float* g
 size_t ff_stage_smooth_workspace_size(int height, int width);
 ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int width, int iterations,
                           float* out, size_t out_pitch, void* ws, void* stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

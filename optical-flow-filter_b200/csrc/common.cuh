@@ -85,15 +85,22 @@ __device__ __forceinline__ float dominant(float vm, float vp) {
     return __fsub_rn(fabsf(vp), fabsf(vm)) > 0.0f ? vp : vm;
 }
 
-// one upwind sub-step f0 - t*(dv >= 0 ? f0 - fm : fp - f0), t = dt*dv, fused as
-// fma(-t, d, f0) (propagation_k.cu:50-53)
+// One upwind sub-step f0 - t*(dv >= 0 ? f0 - fm : fp - f0), t = dt*dv
+// (propagation_k.cu:50-53, 175-207).  The reference build fuses the multiply into the
+// subtraction for every channel except the last one each kernel writes (flow .y of
+// flowPropagate{X,Y}_k, vector .y of flowPropagatePayload{X,Y}_k), so both forms exist.
 __device__ __forceinline__ float upwind(float t, float dv, float fm, float f0, float fp) {
     float d = dv >= 0.0f ? __fsub_rn(f0, fm) : __fsub_rn(fp, f0);
     return __fmaf_rn(-t, d, f0);
 }
+__device__ __forceinline__ float upwind_unfused(float t, float dv, float fm, float f0, float fp) {
+    float d = dv >= 0.0f ? __fsub_rn(f0, fm) : __fsub_rn(fp, f0);
+    return __fsub_rn(f0, __fmul_rn(t, d));
+}
 
 // closed-form 2x2 regularised solve (update_k.cu:43-63, 114-134):
-// (gamma I + a a^T)^-1 (gamma f + a Yt) = adj * q / (gamma (gamma + ax^2 + ay^2))
+// (gamma I + a a^T)^-1 (gamma f + a Yt) = adj * q / (gamma (gamma + ax^2 + ay^2)).
+// Fusion as in the reference build: qx = fma(g, fx, ax*Yt) but qy = fma(ay, Yt, g*fy).
 __device__ __forceinline__ void solve2(float gamma, float ax, float ay, float yt, float fx, float fy,
                                        float& ox, float& oy) {
     float n00 = __fmaf_rn(ay, ay, gamma);
@@ -102,7 +109,7 @@ __device__ __forceinline__ void solve2(float gamma, float ax, float ay, float yt
     float n01 = __fmul_rn(-ax, ay);
     float rdet = __frcp_rn(__fmul_rn(gamma, den));
     float qx = __fmaf_rn(gamma, fx, __fmul_rn(ax, yt));
-    float qy = __fmaf_rn(gamma, fy, __fmul_rn(ay, yt));
+    float qy = __fmaf_rn(ay, yt, __fmul_rn(gamma, fy));
     float ix = __fmaf_rn(n00, qx, __fmul_rn(n01, qy));
     float iy = __fmaf_rn(n01, qx, __fmul_rn(n11, qy));
     ox = __fmul_rn(ix, rdet);
@@ -131,10 +138,11 @@ constexpr float kS0 = 0.0625f, kS1 = 0.25f, kS2 = 0.375f;
 constexpr float kD0 = -0.125f, kD1 = -0.25f;
 constexpr float kBox = 0.2f;
 
-// 5-tap chains accumulated in tap order from 0 as the reference's loops do
-// (imagemodel_k.cu:47-50, 100-111; flowsmoothing_k.cu:38-44)
+// 5-tap chains accumulated in tap order from +0 as the reference's loops do
+// (imagemodel_k.cu:47-50, 100-111; flowsmoothing_k.cu:38-44); the first tap is
+// fma(k, a, +0), which differs from k*a only in the sign of a zero result.
 __device__ __forceinline__ float smooth5(float a, float b, float c, float d, float e) {
-    float s = __fmul_rn(kS0, a);
+    float s = __fmaf_rn(kS0, a, 0.0f);
     s = __fmaf_rn(kS1, b, s);
     s = __fmaf_rn(kS2, c, s);
     s = __fmaf_rn(kS1, d, s);
@@ -143,14 +151,14 @@ __device__ __forceinline__ float smooth5(float a, float b, float c, float d, flo
 // diff mask {-1/8, -1/4, 0, 1/4, 1/8}: the 0 tap adds 0*c, which leaves the sum unchanged
 // for finite c; it is kept so non-finite inputs propagate as in the reference
 __device__ __forceinline__ float diff5(float a, float b, float c, float d, float e) {
-    float s = __fmul_rn(kD0, a);
+    float s = __fmaf_rn(kD0, a, 0.0f);
     s = __fmaf_rn(kD1, b, s);
     s = __fmaf_rn(0.0f, c, s);
     s = __fmaf_rn(-kD1, d, s);
     return __fmaf_rn(-kD0, e, s);
 }
 __device__ __forceinline__ float box5(float a, float b, float c, float d, float e) {
-    float s = __fmul_rn(kBox, a);
+    float s = __fmaf_rn(kBox, a, 0.0f);
     s = __fmaf_rn(kBox, b, s);
     s = __fmaf_rn(kBox, c, s);
     s = __fmaf_rn(kBox, d, s);

@@ -74,7 +74,8 @@ void Level::release() {
     for (Buf* b : {&fu, &a0, &grad, &fp, &ip, &dp, &t1, &t2, &t3, &fut}) b->release();
 }
 
-Filter::Filter(Kind kind, int H, int W, int levels, int item) : kind_(kind), H_(H), W_(W), L_(levels), item_(item) {
+Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
+    : kind_(kind), H_(H), W_(W), L_(levels), item_(item) {
     if (H <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "height should be greater than zero, got: " + std::to_string(H));
     if (W <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "width should be greater than zero, got: " + std::to_string(W));
     if (levels <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "levels should be greater than zero, got: " + std::to_string(levels));
@@ -117,6 +118,11 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item) : kind_(kind), H_(
             v.H = H;
             v.W = W;
             v.item = item;
+            if (own_input) {
+                input_.alloc(H, W, item);
+                v.img = input_.p;
+                v.img_pitch = input_.pitch;
+            }
         }
         // configure() defaults: FlowUpdate/DeltaFlowUpdate(gamma 1, maxflow 1),
         // FlowSmoother(1), FlowPropagator(1), border 3 (flowfilter.cu:100-107, 393-402)
@@ -240,8 +246,8 @@ void Filter::load_device_async(const void* img, size_t pitch, cudaStream_t s) {
 void Filter::bind_device(const void* img, size_t pitch) {
     if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
     if (pitch < (size_t)W_ * item_) throw Error(FF_ERR_INVALID_ARGUMENT, "pitch smaller than a row");
-    if (((uintptr_t)img % 16) || (pitch % 16))
-        throw Error(FF_ERR_INVALID_ARGUMENT, "bound images need 16-byte aligned rows");
+    if (((uintptr_t)img % item_) || (pitch % item_))
+        throw Error(FF_ERR_INVALID_ARGUMENT, "image rows must be aligned to the item size");
     lv_[0].img = img;
     lv_[0].img_pitch = pitch;
 }

@@ -69,7 +69,8 @@ struct Level {
 
 class Filter {
 public:
-    Filter(Kind kind, int H, int W, int levels, int item);
+    // own_input: allocate the level-0 input image (FlowFilter(h, w, ...), pyramids)
+    Filter(Kind kind, int H, int W, int levels, int item, bool own_input);
     ~Filter();
     Filter(const Filter&) = delete;
     Filter& operator=(const Filter&) = delete;

@@ -85,7 +85,8 @@ __global__ void propagate_pass_k(CView<float2> fl, CView<float> sc, CView<float2
     const bool in = (x >= border && x < W - border) && (y >= border && y < H - border);
     float2 o;
     o.x = in ? upwind(t, dv, fm.x, f0.x, fp.x) : f0.x;
-    o.y = in ? upwind(t, dv, fm.y, f0.y, fp.y) : f0.y;
+    if constexpr (PAYLOAD) o.y = in ? upwind(t, dv, fm.y, f0.y, fp.y) : f0.y;
+    else o.y = in ? upwind_unfused(t, dv, fm.y, f0.y, fp.y) : f0.y;
     ofl.at(x, y) = o;
     if constexpr (PAYLOAD) {
         const float sm = sc.clamped(xm, ym), s0 = sc.clamped(x, y), sp = sc.clamped(xp, yp);
@@ -93,7 +94,7 @@ __global__ void propagate_pass_k(CView<float2> fl, CView<float> sc, CView<float2
         const float2 vm = ve.clamped(xm, ym), v0 = ve.clamped(x, y), vp = ve.clamped(xp, yp);
         float2 ov;
         ov.x = in ? upwind(t, dv, vm.x, v0.x, vp.x) : v0.x;
-        ov.y = in ? upwind(t, dv, vm.y, v0.y, vp.y) : v0.y;
+        ov.y = in ? upwind_unfused(t, dv, vm.y, v0.y, vp.y) : v0.y;
         ove.at(x, y) = ov;
     }
 }

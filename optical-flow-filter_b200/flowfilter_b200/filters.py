@@ -1,0 +1,432 @@
+"""Python filter classes mirroring the reference's Cython API.
+
+``FlowFilter`` and ``PyramidalFlowFilter`` keep the names, arguments, properties and
+error behaviour of python/flowfilter/gpu/flowfilters.pyx:15-455 (loadImage / compute /
+getFlow / getImage / elapsedTime; gamma, maxflow, smoothIterations,
+propagationIterations, propagationBorder).  Inputs may be numpy arrays (synchronous
+host upload, as in the reference) or torch tensors (CPU or CUDA).  Everything runs
+through the C ABI of libffb200.so; there is no host-side fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FFImage, call, lib
+
+__all__ = ["FlowFilter", "PyramidalFlowFilter", "DeltaFlowFilter", "device_view"]
+
+
+def _torch():
+    import torch  # imported lazily: numpy-only use does not need it
+
+    return torch
+
+
+class _CudaArray:
+    """__cuda_array_interface__ wrapper for a pitched device buffer owned by a filter."""
+
+    def __init__(self, ptr: int, shape, strides, typestr: str, owner):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(shape),
+            "strides": tuple(strides),
+            "typestr": typestr,
+            "data": (ptr, False),
+            "version": 3,
+        }
+        self._owner = owner
+
+
+def device_view(ptr: int, pitch: int, height: int, width: int, channels: int, owner=None):
+    """torch.float32 view (H, W[, C]) of a pitched device buffer (no copy)."""
+    torch = _torch()
+    if channels == 1:
+        shape, strides = (height, width), (pitch, 4)
+    else:
+        shape, strides = (height, width, channels), (pitch, 4 * channels, 4)
+    return torch.as_tensor(_CudaArray(ptr, shape, strides, "<f4", owner), device="cuda")
+
+
+def _host_image(arr: np.ndarray, depth: int) -> tuple[FFImage, np.ndarray]:
+    arr = np.ascontiguousarray(arr)
+    img = FFImage()
+    img.height = arr.shape[0]
+    img.width = arr.shape[1]
+    img.depth = depth
+    img.itemSize = arr.dtype.itemsize
+    img.pitch = arr.strides[0]
+    img.data = arr.ctypes.data_as(ctypes.c_void_p)
+    return img, arr
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+class _FilterBase:
+    _h = None
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib._lib is not None:
+            lib().ff_filter_destroy(h)
+
+    # ------------------------------------------------------------ helpers
+    def _shape(self):
+        h, w, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        call("ff_filter_shape", self._h, ctypes.byref(h), ctypes.byref(w), ctypes.byref(l))
+        return h.value, w.value, l.value
+
+    def _item(self) -> int:
+        return 1
+
+    def loadImage(self, img) -> None:
+        """Load the next frame: numpy (H, W) uint8 uploads synchronously (flowfilter.cu:218-220);
+        a CUDA tensor is copied device-to-device on the current torch stream."""
+        dtype = np.uint8 if self._item() == 1 else np.float32
+        if _is_torch(img) and img.is_cuda:
+            torch = _torch()
+            want = torch.uint8 if dtype == np.uint8 else torch.float32
+            if img.dtype != want or tuple(img.shape) != (self.height, self.width):
+                raise ValueError(f"expected a {want} tensor of shape {(self.height, self.width)}, "
+                                 f"got {img.dtype} {tuple(img.shape)}")
+            if img.stride(1) != 1:
+                img = img.contiguous()
+            stream = torch.cuda.current_stream().cuda_stream
+            call("ff_filter_load_image_device_async", self._h, ctypes.c_void_p(img.data_ptr()),
+                 img.stride(0) * img.element_size(), ctypes.c_void_p(stream))
+            self._keep_input = img
+            return
+        if _is_torch(img):
+            img = img.numpy()
+        img = np.asarray(img)
+        if img.ndim != 2:
+            raise ValueError(f"image should be 2-D (height, width), got shape {img.shape}")
+        if img.dtype != dtype:
+            raise ValueError(f"image dtype should be {np.dtype(dtype)}, got {img.dtype}")
+        fimg, keep = _host_image(img, 1)
+        call("ff_filter_load_image_host", self._h, ctypes.byref(fimg))
+
+    def compute(self) -> None:
+        """One frame; blocks until done (flowfilter.cu:125-153, 685-716)."""
+        call("ff_filter_compute", self._h)
+
+    def computeAsync(self, stream=None) -> None:
+        """Enqueue one frame on ``stream`` (default: the current torch stream)."""
+        if stream is None:
+            stream = _torch().cuda.current_stream().cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        call("ff_filter_compute_async", self._h, ctypes.c_void_p(stream))
+
+    def elapsedTime(self) -> float:
+        ms = ctypes.c_float()
+        call("ff_filter_elapsed_ms", self._h, ctypes.byref(ms))
+        return ms.value
+
+    def getFlow(self, flow: np.ndarray | None = None) -> np.ndarray:
+        """Smoothed level-0 flow as (H, W, 2) float32 (downloadFlow, flowfilter.cu:238-240)."""
+        if flow is None:
+            flow = np.zeros((self.height, self.width, 2), dtype=np.float32)
+        if flow.dtype != np.float32 or flow.shape != (self.height, self.width, 2) or not flow.flags["C_CONTIGUOUS"]:
+            raise ValueError("flow buffer should be a contiguous float32 array of shape (H, W, 2)")
+        fimg, _ = _host_image(flow, 2)
+        call("ff_filter_download_flow_host", self._h, ctypes.byref(fimg))
+        return flow
+
+    def getImage(self, image: np.ndarray | None = None) -> np.ndarray:
+        """Level-0 updated image (current a0), (H, W) float32 (downloadImage)."""
+        if image is None:
+            image = np.zeros((self.height, self.width), dtype=np.float32)
+        if image.dtype != np.float32 or image.shape != (self.height, self.width) or not image.flags["C_CONTIGUOUS"]:
+            raise ValueError("image buffer should be a contiguous float32 array of shape (H, W)")
+        fimg, _ = _host_image(image, 1)
+        call("ff_filter_download_image_host", self._h, ctypes.byref(fimg))
+        return image
+
+    def _device_result(self, which: int, channels: int):
+        p, pitch = ctypes.c_void_p(), ctypes.c_size_t()
+        call("ff_filter_device_result", self._h, which, ctypes.byref(p), ctypes.byref(pitch))
+        return device_view(p.value, pitch.value, self.height, self.width, channels, owner=self)
+
+    def getFlowDevice(self):
+        """torch view of getFlow() on the device (valid until the next compute)."""
+        return self._device_result(1, 2)
+
+    def flowTensor(self):
+        """torch view of the smoothed level-0 flow on the device (valid until the next compute)."""
+        return self._device_result(0, 2)
+
+    def imageTensor(self):
+        """torch view of the level-0 updated image on the device."""
+        return self._device_result(2, 1)
+
+    def levelState(self, level: int, which: int) -> np.ndarray:
+        """Host copy of a level's state: 0 smoothed flow, 1 unsmoothed flow (top level),
+        2 old image, 3 delta flow (delta levels)."""
+        h, w = ctypes.c_int(), ctypes.c_int()
+        call("ff_filter_level_shape", self._h, level, ctypes.byref(h), ctypes.byref(w))
+        ch = 1 if which == 2 else 2
+        out = np.zeros((h.value, w.value, ch) if ch == 2 else (h.value, w.value), np.float32)
+        call("ff_filter_level_state_host", self._h, level, which, out.ctypes.data_as(ctypes.c_void_p),
+             out.strides[0])
+        return out
+
+    def setFused(self, enabled: bool) -> None:
+        """Fused per-level kernels (default) or the per-stage kernels; results are identical."""
+        call("ff_filter_set_fused", self._h, 1 if enabled else 0)
+
+    def setStream(self, stream) -> None:
+        if hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        call("ff_filter_set_stream", self._h, ctypes.c_void_p(stream))
+
+    # ------------------------------------------------------------ properties
+    @property
+    def height(self) -> int:
+        return self._shape()[0]
+
+    @height.setter
+    def height(self, value):
+        raise RuntimeError("Filter height cannot be set after instantiation")
+
+    @property
+    def width(self) -> int:
+        return self._shape()[1]
+
+    @width.setter
+    def width(self, value):
+        raise RuntimeError("Filter width cannot be set after instantiation")
+
+    @property
+    def maxflow(self) -> float:
+        v = ctypes.c_float()
+        call("ff_filter_get_max_flow", self._h, ctypes.byref(v))
+        return v.value
+
+    @maxflow.setter
+    def maxflow(self, value: float) -> None:
+        call("ff_filter_set_max_flow", self._h, float(value))
+
+    @property
+    def propagationBorder(self) -> int:
+        v = ctypes.c_int()
+        call("ff_filter_get_propagation_border", self._h, ctypes.byref(v))
+        return v.value
+
+    @propagationBorder.setter
+    def propagationBorder(self, value: int) -> None:
+        call("ff_filter_set_propagation_border", self._h, int(value))
+
+    def _get_gamma(self, level: int) -> float:
+        v = ctypes.c_float()
+        call("ff_filter_get_gamma", self._h, level, ctypes.byref(v))
+        return v.value
+
+    def _get_smooth(self, level: int) -> int:
+        v = ctypes.c_int()
+        call("ff_filter_get_smooth_iterations", self._h, level, ctypes.byref(v))
+        return v.value
+
+    def _get_iters(self, level: int) -> int:
+        v = ctypes.c_int()
+        call("ff_filter_get_propagation_iterations", self._h, level, ctypes.byref(v))
+        return v.value
+
+
+class FlowFilter(_FilterBase):
+    """Single-level filter, flowfilters.pyx:15-200 / flowfilter.cu:45-76.
+
+    ``FlowFilter(height, width, smoothIterations=1, maxflow=1.0, gamma=1.0)`` owns a
+    uint8 input image.  ``FlowFilter.on_device(tensor)`` is FlowFilter(GPUImage): it
+    reads a caller-owned uint8 or float32 CUDA image on every compute.
+    """
+
+    def __init__(self, height: int, width: int, smoothIterations: int = 1, maxflow: float = 1.0,
+                 gamma: float = 1.0):
+        h = ctypes.c_void_p()
+        call("ff_filter_create", int(height), int(width), int(smoothIterations), float(maxflow), float(gamma),
+             ctypes.byref(h))
+        self._h = h
+        self._itemsize = 1
+
+    @classmethod
+    def on_device(cls, image) -> "FlowFilter":
+        """FlowFilter(GPUImage): configure() defaults (gamma 1 unscaled, maxflow 1, 1 smoothing)."""
+        torch = _torch()
+        if not (_is_torch(image) and image.is_cuda and image.dim() == 2):
+            raise ValueError("expected a 2-D CUDA tensor")
+        if image.dtype not in (torch.uint8, torch.float32):
+            raise ValueError("image dtype should be uint8 or float32")
+        if image.stride(1) != 1:
+            raise ValueError("image rows must be contiguous")
+        self = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        item = image.element_size()
+        call("ff_filter_create_on_device_image", ctypes.c_void_p(image.data_ptr()), image.stride(0) * item, item,
+             image.shape[0], image.shape[1], ctypes.byref(h))
+        self._h = h
+        self._itemsize = item
+        self._keep_input = image
+        return self
+
+    def _item(self) -> int:
+        return self._itemsize
+
+    def configure(self) -> None:
+        """Kept for API compatibility; the filter is configured at construction."""
+
+    def computeImageModel(self) -> None:
+        call("ff_filter_compute_image_model", self._h)
+
+    def computePropagation(self) -> None:
+        call("ff_filter_compute_propagation", self._h)
+
+    def computeUpdate(self) -> None:
+        call("ff_filter_compute_update", self._h)
+
+    @property
+    def gamma(self) -> float:
+        return self._get_gamma(0)
+
+    @gamma.setter
+    def gamma(self, value: float) -> None:
+        call("ff_filter_set_gamma", self._h, 0, float(value))
+
+    @property
+    def smoothIterations(self) -> int:
+        return self._get_smooth(0)
+
+    @smoothIterations.setter
+    def smoothIterations(self, value: int) -> None:
+        call("ff_filter_set_smooth_iterations", self._h, 0, int(value))
+
+    @property
+    def propagationIterations(self) -> int:
+        return self._get_iters(0)
+
+    @propagationIterations.setter
+    def propagationIterations(self, value):
+        raise RuntimeError("propagation iterations cannot be set, use maxflow instead")
+
+
+class DeltaFlowFilter(_FilterBase):
+    """DeltaFlowFilter(GPUImage image, GPUImage inputFlow), flowfilter.cu:349-426, over CUDA
+    tensors: ``image`` (H, W) uint8/float32 and ``coarse_flow`` (Hc, Wc, 2) float32."""
+
+    def __init__(self, image, coarse_flow):
+        torch = _torch()
+        if not (_is_torch(image) and image.is_cuda and image.dim() == 2 and image.stride(1) == 1):
+            raise ValueError("image should be a 2-D CUDA tensor with contiguous rows")
+        if image.dtype not in (torch.uint8, torch.float32):
+            raise ValueError("image dtype should be uint8 or float32")
+        if not (_is_torch(coarse_flow) and coarse_flow.is_cuda and coarse_flow.dim() == 3
+                and coarse_flow.shape[2] == 2 and coarse_flow.dtype == torch.float32
+                and coarse_flow.stride(2) == 1 and coarse_flow.stride(1) == 2):
+            raise ValueError("coarse flow should be a (Hc, Wc, 2) float32 CUDA tensor with contiguous rows")
+        h = ctypes.c_void_p()
+        item = image.element_size()
+        call("ff_delta_filter_create", ctypes.c_void_p(image.data_ptr()), image.stride(0) * item, item,
+             image.shape[0], image.shape[1], ctypes.c_void_p(coarse_flow.data_ptr()), coarse_flow.stride(0) * 4,
+             coarse_flow.shape[0], coarse_flow.shape[1], ctypes.byref(h))
+        self._h = h
+        self._itemsize = item
+        self._keep = (image, coarse_flow)
+
+    def _item(self) -> int:
+        return self._itemsize
+
+    def computeImageModel(self) -> None:
+        call("ff_filter_compute_image_model", self._h)
+
+    def computePropagation(self) -> None:
+        call("ff_filter_compute_propagation", self._h)
+
+    def computeUpdate(self) -> None:
+        call("ff_filter_compute_update", self._h)
+
+    @property
+    def gamma(self) -> float:
+        return self._get_gamma(0)
+
+    @gamma.setter
+    def gamma(self, value: float) -> None:
+        call("ff_filter_set_gamma", self._h, 0, float(value))
+
+    @property
+    def smoothIterations(self) -> int:
+        return self._get_smooth(0)
+
+    @smoothIterations.setter
+    def smoothIterations(self, value: int) -> None:
+        call("ff_filter_set_smooth_iterations", self._h, 0, int(value))
+
+    @property
+    def propagationIterations(self) -> int:
+        return self._get_iters(0)
+
+
+class PyramidalFlowFilter(_FilterBase):
+    """Pyramidal filter, flowfilters.pyx:204-455 / flowfilter.cu:621-897."""
+
+    def __init__(self, height: int, width: int, levels: int):
+        h = ctypes.c_void_p()
+        call("ff_pyramidal_create", int(height), int(width), int(levels), ctypes.byref(h))
+        self._h = h
+
+    def configure(self) -> None:
+        """Kept for API compatibility; the filter is configured at construction."""
+
+    @property
+    def levels(self) -> int:
+        return self._shape()[2]
+
+    @levels.setter
+    def levels(self, value):
+        raise RuntimeError("Filter levels cannot be set after instantiation")
+
+    @property
+    def gamma(self):
+        if self.levels == 1:
+            return self._get_gamma(0)
+        return [self._get_gamma(h) for h in range(self.levels)]
+
+    @gamma.setter
+    def gamma(self, g) -> None:
+        if self.levels == 1:
+            call("ff_filter_set_gamma", self._h, 0, float(g))
+        else:
+            for h in range(self.levels):
+                call("ff_filter_set_gamma", self._h, h, float(g[h]))
+
+    def setGamma(self, level: int, gamma: float) -> None:
+        call("ff_filter_set_gamma", self._h, int(level), float(gamma))
+
+    def getGamma(self, level: int) -> float:
+        return self._get_gamma(int(level))
+
+    @property
+    def smoothIterations(self):
+        if self.levels == 1:
+            return self._get_smooth(0)
+        return [self._get_smooth(h) for h in range(self.levels)]
+
+    @smoothIterations.setter
+    def smoothIterations(self, n) -> None:
+        if self.levels == 1:
+            call("ff_filter_set_smooth_iterations", self._h, 0, int(n))
+        else:
+            for h in range(self.levels):
+                call("ff_filter_set_smooth_iterations", self._h, h, int(n[h]))
+
+    def setSmoothIterations(self, level: int, n: int) -> None:
+        call("ff_filter_set_smooth_iterations", self._h, int(level), int(n))
+
+    def getSmoothIterations(self, level: int) -> int:
+        return self._get_smooth(int(level))
+
+    def propagationIterationsAt(self, level: int) -> int:
+        return self._get_iters(int(level))

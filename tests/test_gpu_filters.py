@@ -1,0 +1,254 @@
+"""Filters through the public API (C ABI) against the reference's own outputs and the oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_case
+from make_reference_fixtures import CASES, case_frames, sha, subsample_rows_cols
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ffb(cuda):
+    import flowfilter_b200
+
+    return flowfilter_b200
+
+
+def make_gpu_filter(ffb, case, h, w):
+    if case["levels"] == 0:
+        return ffb.FlowFilter(h, w, case["smooth"][0], case["maxflow"], case["gamma"][0])
+    f = ffb.PyramidalFlowFilter(h, w, case["levels"])
+    f.gamma = case["gamma"]
+    f.smoothIterations = case["smooth"]
+    f.maxflow = case["maxflow"]
+    return f
+
+
+def run_gpu(f, frames, dump, fused=True):
+    f.setFused(fused)
+    out = []
+    for t in range(frames.shape[0]):
+        f.loadImage(frames[t])
+        f.compute()
+        if t in dump:
+            out.append(f.getFlow())
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_reference_sequences_bit_exact(ffb, name):
+    """The GPU filter reproduces the reference library's flows bit for bit (sha256 per frame)."""
+    case = CASES[name]
+    meta, arr = golden_case(name)
+    frames = case_frames(case)
+    assert sha(frames) == meta["frames_sha256"]
+    f = make_gpu_filter(ffb, case, *frames.shape[1:])
+    flows = run_gpu(f, frames, set(case["dump"]))
+    if meta["layout"] == "full":
+        got = flows
+    else:
+        rows, cols = subsample_rows_cols(*frames.shape[1:])
+        got = flows[:, rows][:, :, cols]
+    assert np.max(np.abs(got - arr["flow"])) <= 1e-4  # the stated tolerance ...
+    assert [sha(x) for x in flows] == meta["flow_sha256"]  # ... and in fact bit-exact
+
+
+RANDOM_CASES = [
+    # (h, w, levels, maxflow, gammas, smooths, border)
+    (61, 77, 0, 2.5, [3.0], [2], 3),
+    (40, 52, 0, 6.0, [20.0], [5], 0),
+    (64, 96, 2, 5.0, [2.0, 25.0], [3, 1], 3),
+    (98, 150, 3, 3.0, [4.0, 9.0, 30.0], [1, 3, 2], 5),
+    (130, 130, 4, 8.0, [1.0, 2.0, 4.0, 8.0], [1, 1, 2, 3], 2),
+    (9, 13, 2, 1.0, [1.0, 1.0], [1, 1], 3),
+]
+
+
+def oracle_filter(case):
+    h, w, levels, maxflow, gammas, smooths, border = case
+    if levels == 0:
+        f = O.Filter.flowfilter(h, w, smooths[0], maxflow, gammas[0])
+    else:
+        f = O.Filter.pyramidal(h, w, levels)
+        f.set_gammas(gammas)
+        f.set_smooths(smooths)
+        f.set_max_flow(maxflow)
+    f.set_propagation_border(border)
+    return f
+
+
+def gpu_filter(ffb, case):
+    h, w, levels, maxflow, gammas, smooths, border = case
+    if levels == 0:
+        f = ffb.FlowFilter(h, w, smooths[0], maxflow, gammas[0])
+    else:
+        f = ffb.PyramidalFlowFilter(h, w, levels)
+        f.gamma = gammas
+        f.smoothIterations = smooths
+        f.maxflow = maxflow
+    f.propagationBorder = border
+    return f
+
+
+@pytest.mark.parametrize("case", RANDOM_CASES)
+@pytest.mark.parametrize("fused", [True, False])
+def test_against_oracle(ffb, case, fused):
+    h, w = case[:2]
+    frames = case_frames(dict(seq="bumps", frames=12, kw=dict(height=h, width=w, sigma=1.0, seed=h * w,
+                                                               n_bumps=2, bump_sigma=max(h, w) / 3, amp=2.0)))
+    of = oracle_filter(case)
+    gf = gpu_filter(ffb, case)
+    gf.setFused(fused)
+    for t in range(frames.shape[0]):
+        of.load(frames[t])
+        of.compute()
+        gf.loadImage(frames[t])
+        gf.compute()
+        np.testing.assert_array_equal(gf.getFlow(), of.flow())
+        np.testing.assert_array_equal(gf.getImage(), of.image())
+    for lv in range(max(case[2], 1)):
+        np.testing.assert_array_equal(gf.levelState(lv, 0), of.level_state(lv, 0))
+        np.testing.assert_array_equal(gf.levelState(lv, 2), of.level_state(lv, 2))
+
+
+def test_defaults_and_parameter_rules(ffb):
+    f = ffb.FlowFilter(32, 48)
+    assert f.height == 32 and f.width == 48
+    assert f.gamma == pytest.approx(1.0 / (255.0 * 255.0))  # setGamma(1) scaled for uint8
+    assert f.maxflow == 1.0 and f.propagationIterations == 1
+    assert f.smoothIterations == 1 and f.propagationBorder == 3
+    f.maxflow = 2.5
+    assert f.propagationIterations == 3
+    f.gamma = 10.0
+    assert f.gamma == pytest.approx(10.0 / 65025.0)
+    p = ffb.PyramidalFlowFilter(64, 64, 3)
+    assert p.gamma == [1.0, 1.0, 1.0]  # configure() defaults are unscaled
+    assert p.smoothIterations == [1, 1, 1]
+    p.maxflow = 4.0
+    assert [p.propagationIterationsAt(l) for l in range(3)] == [4, 2, 1]
+    p.maxflow = 3.0
+    assert [p.propagationIterationsAt(l) for l in range(3)] == [3, 2, 1]
+    assert p.maxflow == 3.0
+    with pytest.raises(RuntimeError):
+        p.levels = 2
+    with pytest.raises(RuntimeError):
+        f.propagationIterations = 2
+
+
+def test_argument_errors(ffb):
+    f = ffb.FlowFilter(16, 16)
+    with pytest.raises(ValueError):
+        f.gamma = 0.0
+    with pytest.raises(ValueError):
+        f.gamma = -1.0
+    with pytest.raises(ValueError):
+        f.maxflow = 0.0
+    with pytest.raises(ValueError):
+        f.smoothIterations = 0
+    with pytest.raises(ValueError):
+        f.propagationBorder = -1
+    with pytest.raises(ValueError):
+        f.loadImage(np.zeros((16, 15), np.uint8))
+    with pytest.raises(ValueError):
+        f.loadImage(np.zeros((16, 16), np.float32))
+    p = ffb.PyramidalFlowFilter(32, 32, 2)
+    with pytest.raises(IndexError):
+        p.setGamma(2, 1.0)
+    with pytest.raises(IndexError):
+        p.getSmoothIterations(-1)
+    with pytest.raises(ValueError):
+        ffb.PyramidalFlowFilter(4, 4, 4)  # level 3 would have zero size
+
+
+def test_getflow_semantics(ffb):
+    """Single level: getFlow() is the unsmoothed update output, downloadFlow the smoothed
+    one (flowfilter.cu:238-240, 266-268); pyramids return the smoothed flow from both."""
+    frames = case_frames(dict(seq="constant", frames=6, kw=dict(height=48, width=64, sigma=1.5, seed=3)))
+    of = O.Filter.flowfilter(48, 64, 2, 3.0, 5.0)
+    gf = ffb.FlowFilter(48, 64, 2, 3.0, 5.0)
+    for t in range(6):
+        of.load(frames[t]); of.compute()
+        gf.loadImage(frames[t]); gf.compute()
+    np.testing.assert_array_equal(gf.getFlowDevice().cpu().numpy(), of.get_flow())
+    np.testing.assert_array_equal(gf.flowTensor().cpu().numpy(), of.flow())
+    assert not np.array_equal(of.get_flow(), of.flow())
+    p = ffb.PyramidalFlowFilter(48, 64, 2)
+    p.loadImage(frames[0]); p.compute()
+    np.testing.assert_array_equal(p.getFlowDevice().cpu().numpy(), p.getFlow())
+
+
+def test_device_input_matches_host_input(ffb, cuda):
+    frames = case_frames(dict(seq="constant", frames=5, kw=dict(height=40, width=56, sigma=1.5, seed=4)))
+    a = ffb.PyramidalFlowFilter(40, 56, 2)
+    b = ffb.PyramidalFlowFilter(40, 56, 2)
+    for f in (a, b):
+        f.maxflow = 3.0
+    for t in range(5):
+        a.loadImage(frames[t]); a.compute()
+        b.loadImage(cuda.from_numpy(frames[t]).cuda()); b.compute()
+        np.testing.assert_array_equal(a.getFlow(), b.getFlow())
+    assert a.elapsedTime() > 0.0
+
+
+def test_phase_api_matches_compute(ffb):
+    frames = case_frames(dict(seq="constant", frames=5, kw=dict(height=33, width=45, sigma=1.5, seed=5)))
+    a = ffb.FlowFilter(33, 45, 2, 2.0, 4.0)
+    b = ffb.FlowFilter(33, 45, 2, 2.0, 4.0)
+    for t in range(5):
+        a.loadImage(frames[t]); a.compute()
+        b.loadImage(frames[t]); b.computeImageModel(); b.computePropagation(); b.computeUpdate()
+        np.testing.assert_array_equal(a.getFlow(), b.getFlow())
+
+
+@pytest.mark.parametrize("dtype", ["uint8", "float32"])
+def test_flowfilter_on_device_image(ffb, cuda, dtype):
+    """FlowFilter(GPUImage): configure() defaults, float input uses gamma unscaled."""
+    frames = case_frames(dict(seq="constant", frames=6, kw=dict(height=36, width=50, sigma=1.5, seed=6)))
+    if dtype == "float32":
+        frames = (frames.astype(np.float32) / 255.0).astype(np.float32)
+    img = cuda.from_numpy(frames[0]).cuda()
+    gf = ffb.FlowFilter.on_device(img)
+    of = O.Filter.flowfilter_on(36, 50, 1 if dtype == "uint8" else 4)
+    gf.gamma = 2.0
+    of.set_gamma(0, 2.0)
+    gf.maxflow = 2.0
+    of.set_max_flow(2.0)
+    for t in range(6):
+        img.copy_(cuda.from_numpy(frames[t]))
+        of.load(frames[t]); of.compute()
+        gf.compute()
+        np.testing.assert_array_equal(gf.getFlow(), of.flow())
+
+
+def test_delta_filter_standalone(ffb, cuda):
+    """DeltaFlowFilter(image, inputFlow) follows DeltaFlowFilter::compute (flowfilter.cu:429-457)."""
+    rng = np.random.default_rng(9)
+    h, w = 30, 44
+    frames = case_frames(dict(seq="constant", frames=4, kw=dict(height=h, width=w, sigma=1.5, seed=9)))
+    coarse = rng.normal(0, 0.5, (h // 2, w // 2, 2)).astype(np.float32)
+    img = cuda.from_numpy(frames[0]).cuda()
+    cf = cuda.from_numpy(coarse).cuda()
+    gf = ffb.DeltaFlowFilter(img, cf)
+    gf.gamma = 5.0
+    gf.maxflow = 2.0
+    gamma = np.float32(5.0) / np.float32(255.0 * 255.0)
+    fs = np.zeros((h, w, 2), np.float32)
+    iu = np.zeros((h, w), np.float32)
+    du = np.zeros((h, w, 2), np.float32)
+    for t in range(4):
+        img.copy_(cuda.from_numpy(frames[t]))
+        gf.compute()
+        a0, g = O.image_model(frames[t])
+        if t == 0:
+            iu = a0.copy()
+        _, ip, dp = O.propagate_payload(fs, iu, du, 2, 3)
+        if t == 0:
+            ip = a0.copy()
+        fu, du, iu = O.delta_update(a0, g, ip, dp, coarse, gamma, 2.0)
+        fs = O.smooth(fu, 1)
+        np.testing.assert_array_equal(gf.getFlow(), fs)
