@@ -46,6 +46,7 @@ struct LevelArgs {
     float gamma, maxflow;
     int border;
     int first;
+    int band;            // rows per warp band (0: chosen from the SM count)
 };
 
 // true if a fused kernel exists for this (delta, item, iterations, smoothing)
