@@ -1,0 +1,450 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the flow-filter hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+
+A step is one frame of the PyramidalFlowFilter: the frame (already resident in HBM) is
+loaded into the filter and one compute() runs (pyramid, then one fused kernel per
+level; CUDA-graph replay).  The primary workload is the reference's published
+configuration: 640x480 uint8 frames, 2 levels, gamma [10, 50], smoothing [2, 4],
+maxflow 4, on a synthetic rotation+zoom sequence (seeded) standing in for the
+reference's Blender sequence.  The 2048x1088 3-level throughput workload is reported
+beside it under "extra".
+
+Timing: every step is bracketed by CUDA events on the filter's stream and the L2 is
+flushed (a 256 MiB write) between steps outside those events, so every frame reads its
+state from HBM.  value = frames of all ranks / max over ranks of the summed step time.
+--gpus N runs N independent replicas (one process per GPU, torch.distributed for the
+barrier and the max over ranks); the path does not shard.
+
+--impl reference times the reference's CPU path restated in C++ (oracle/, the same
+arithmetic as the reference kernels) on all host cores: the reference has no CPU
+implementation of its CUDA path, and its NumPy module is a different algorithm.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "optical-flow-filter_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # the reference's published notebook configuration
+    "rotzoom_640x480_L2": dict(seq="rotzoom", H=480, W=640, levels=2, gamma=[10.0, 50.0], smooth=[2, 4],
+                               maxflow=4.0, ring=96),
+    # camera-sensor size, 3 levels (throughput / roofline run)
+    "bumps_2048x1088_L3": dict(seq="bumps", H=1088, W=2048, levels=3, gamma=[5.0, 20.0, 50.0], smooth=[1, 2, 4],
+                               maxflow=4.0, ring=24),
+}
+PRIMARY = "rotzoom_640x480_L2"
+EXTRA = "bumps_2048x1088_L3"
+METRIC = "frames/s (PyramidalFlowFilter forward, flow err <= 1e-4 px vs reference)"
+# reference notebook: 1.172 ms/frame on its textured sequence for this configuration
+# (notebooks/GPU_example.ipynb:292); 0.996 ms/frame on all-zero frames (:400)
+PUBLISHED_FPS = 1000.0 / 1.172
+FLUSH_BYTES = 256 << 20
+
+
+def level_shapes(w):
+    h, wd = w["H"], w["W"]
+    out = [(h, wd)]
+    for _ in range(1, w["levels"]):
+        h, wd = h // 2, wd // 2
+        out.append((h, wd))
+    return out
+
+
+def frame_bytes(w):
+    """Compulsory HBM bytes per frame: P0*1 + sum(delta) P_l*42 + P_top*24."""
+    shapes = level_shapes(w)
+    b = shapes[0][0] * shapes[0][1]
+    for l, (h, wd) in enumerate(shapes):
+        b += h * wd * (42 if l < len(shapes) - 1 else 24)
+    return b
+
+
+def level0_kernel_bytes(w):
+    """Algorithmic bytes of one level-0 kernel launch: the uint8 frame (1 B/px) plus the
+    delta level's state read and written and the coarse flow read (42 B/px)."""
+    h, wd = w["H"], w["W"]
+    return h * wd * (1 + (42 if w["levels"] > 1 else 24))
+
+
+def make_frames(w):
+    from flowfilter_b200 import synthetic
+
+    if w["seq"] == "rotzoom":
+        return synthetic.seq_rotzoom(frames=w["ring"], height=w["H"], width=w["W"])
+    return synthetic.seq_bumps(frames=w["ring"], height=w["H"], width=w["W"])
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name):
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    v = d.get(name)
+    return None if v is None else float(v["dram_bytes_per_launch"])
+
+
+class ClockSampler:
+    """SM clock and throttle reasons polled through NVML (read-only) every 2 ms while the
+    timed region runs (no samples are reported when NVML is unavailable)."""
+
+    # NVML clocks-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
+
+    def __init__(self, gpu_uuid: str):
+        self.uuid = gpu_uuid
+        self.sm = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByUUID(self.uuid.encode() if isinstance(self.uuid, str) else self.uuid)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self._stop.is_set():
+                    self.sm.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    bits = get_reasons(h)
+                    for b, name in self.REASONS.items():
+                        if bits & b:
+                            self.reasons.add(name)
+                    time.sleep(0.002)
+
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=2)
+
+    def summary(self):
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0, "source": "none"}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": "nvml"}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(world, value: float) -> float:
+    import torch
+
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gpu_uuid(local):
+    import torch
+
+    try:
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local]
+
+
+def make_filter(w):
+    import flowfilter_b200 as ffb
+
+    f = ffb.PyramidalFlowFilter(w["H"], w["W"], w["levels"])
+    f.gamma = w["gamma"]
+    f.smoothIterations = w["smooth"]
+    f.maxflow = w["maxflow"]
+    return f
+
+
+def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False):
+    """Device-timed frames; returns (summed step ms, per-level kernel ms or None)."""
+    import torch
+
+    f = make_filter(w)
+    f.setGraphs(graphs)
+    ring = dev_frames.shape[0]
+    for t in range(warmup):
+        f.loadImage(dev_frames[t % ring])
+        f.computeAsync()
+    torch.cuda.synchronize()
+    if profile:
+        f.setProfiling(steps)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        f.loadImage(dev_frames[(warmup + k) % ring])
+        f.computeAsync()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    total = sum(a.elapsed_time(b) for a, b in ev)
+    lv = None
+    if profile:
+        lv = [f.levelKernelTime(l) for l in range(w["levels"])]
+    return total, lv, f
+
+
+def e2e_run(w, frames, steps, warmup):
+    """loadImage(host, pinned) -> compute() -> getFlow(host, pinned), all blocking."""
+    import torch
+
+    f = make_filter(w)
+    f.setGraphs(True)
+    ring = frames.shape[0]
+    host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
+    host.copy_(torch.from_numpy(frames))
+    hnp = host.numpy()
+    out = torch.empty((w["H"], w["W"], 2), dtype=torch.float32, pin_memory=True).numpy()
+    for t in range(warmup):
+        f.loadImage(hnp[t % ring])
+        f.compute()
+        f.getFlow(out)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        f.loadImage(hnp[(warmup + k) % ring])
+        f.compute()
+        f.getFlow(out)
+    t1 = time.perf_counter()
+    return (t1 - t0) * 1000.0
+
+
+def cpu_port_fps(w, frames, seconds=10.0, max_frames=2000, threads=None):
+    """The oracle (C++ restatement of the reference path) on the host cores."""
+    import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    f = O.Filter.pyramidal(w["H"], w["W"], w["levels"])
+    f.set_gammas(w["gamma"])
+    f.set_smooths(w["smooth"])
+    f.set_max_flow(w["maxflow"])
+    ring = frames.shape[0]
+    f.load(frames[0])
+    f.compute()
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_frames and time.perf_counter() - t0 < seconds:
+        f.load(frames[(n + 1) % ring])
+        f.compute()
+        n += 1
+    dt = time.perf_counter() - t0
+    O.set_threads(0)
+    return n / dt, threads, n
+
+
+def bench_b200(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    hbm_peak, peak_kind = peaks()
+    w = WORKLOADS[PRIMARY]
+    frames = make_frames(w)
+    dev_frames = torch.from_numpy(frames).cuda()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    # ---- timed region: device time of K frames, L2 flushed between frames
+    barrier(world)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        step_ms, _, filt = device_run(w, dev_frames, args.steps, args.warmup, flush)
+        barrier(world)
+    step_ms = max_over_ranks(world, step_ms)
+    value = world * args.steps / (step_ms / 1000.0)
+
+    # ---- dominant kernel (level 0) timed live with events around its launches
+    _, lv, _ = device_run(w, dev_frames, min(args.steps, 2000), args.warmup, flush, graphs=False, profile=True)
+    l0_ms = lv[0][0] / max(lv[0][1], 1)
+    l0_bytes = level0_kernel_bytes(w)
+    achieved = l0_bytes / (l0_ms / 1000.0) / 1e9
+    traffic = ncu_traffic(PRIMARY)
+
+    # ---- end to end through the public API with host buffers
+    e2e_steps = min(args.steps, 2000)
+    e2e_ms = max_over_ranks(world, e2e_run(w, frames, e2e_steps, args.warmup))
+    e2e_fps = world * e2e_steps / (e2e_ms / 1000.0)
+
+    # ---- the throughput workload beside it
+    we = WORKLOADS[EXTRA]
+    fe = make_frames(we)
+    dfe = torch.from_numpy(fe).cuda()
+    ksteps = min(args.steps, 4000)
+    barrier(world)
+    ems, _, _ = device_run(we, dfe, ksteps, args.warmup, flush)
+    barrier(world)
+    ems = max_over_ranks(world, ems)
+    _, lve, _ = device_run(we, dfe, min(ksteps, 1000), args.warmup, flush, graphs=False, profile=True)
+    el0 = lve[0][0] / max(lve[0][1], 1)
+    eb = level0_kernel_bytes(we)
+    e_fps = world * ksteps / (ems / 1000.0)
+    extra = {
+        "workload": EXTRA, "value": e_fps, "unit": "frames/s", "steps": ksteps,
+        "ms_per_step": ems / ksteps, "mpix_per_s": e_fps * we["H"] * we["W"] / 1e6,
+        "frame_bytes": frame_bytes(we),
+        "frame_gbs": frame_bytes(we) * e_fps / world / 1e9,
+        "frame_roofline_frac": frame_bytes(we) * e_fps / world / 1e9 / hbm_peak,
+        "roofline": {"bound": "hbm", "kernel": "fused level 0 (delta, N=4, S=1)", "achieved": eb / (el0 / 1e3) / 1e9,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": eb / (el0 / 1e3) / 1e9 / hbm_peak,
+                     "traffic": ncu_traffic(EXTRA), "algorithmic_bytes": eb, "launch_ms": el0},
+    }
+
+    cpu = None
+    if rank == 0 and world == 1:
+        fps, cores, n = cpu_port_fps(w, frames)
+        cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
+               "sample": f"{n} consecutive {w['W']}x{w['H']} frames, 2 levels, oracle/ C++ port, {cores} threads"}
+
+    if rank == 0:
+        launches_per_frame = (w["levels"] - 1) + w["levels"]
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / world / PUBLISHED_FPS if world == 1 else None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": PRIMARY, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"],
+                       "gamma": w["gamma"], "smoothIterations": w["smooth"], "maxflow": w["maxflow"],
+                       "sequence": "seeded blurred noise, rotation 0.5 deg + zoom 1.004 per frame",
+                       "l2": "flushed between steps (256 MiB write outside the step events)",
+                       "step": "loadImage (device frame) + compute(), CUDA-graph replay",
+                       "parallelism": f"replicas x{world}"},
+            "mpix_per_s": value * w["H"] * w["W"] / 1e6,
+            "frame_bytes": frame_bytes(w),
+            "roofline": {"bound": "hbm", "kernel": "fused level 0 (delta, N=4, S=2)", "achieved": achieved,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                         "algorithmic_bytes": l0_bytes, "launch_ms": l0_ms, "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": w["H"] * w["W"],
+                    "d2h_bytes_per_step": w["H"] * w["W"] * 8,
+                    "path": "flowfilter_b200.PyramidalFlowFilter loadImage(pinned host) + compute() + getFlow(pinned host)"},
+            "gpu_launches": args.steps * launches_per_frame,
+            "clocks": clk.summary(),
+            "extra": extra,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def bench_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle as O
+
+    w = WORKLOADS[PRIMARY]
+    frames = make_frames(w)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    f = O.Filter.pyramidal(w["H"], w["W"], w["levels"])
+    f.set_gammas(w["gamma"])
+    f.set_smooths(w["smooth"])
+    f.set_max_flow(w["maxflow"])
+    ring = frames.shape[0]
+    for t in range(args.warmup):
+        f.load(frames[t % ring])
+        f.compute()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        f.load(frames[(args.warmup + k) % ring])
+        f.compute()
+    dt = time.perf_counter() - t0
+    fps = args.steps / dt
+    line = {
+        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1000.0 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": PRIMARY, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"],
+                   "gamma": w["gamma"], "smoothIterations": w["smooth"], "maxflow": w["maxflow"]},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} frames, reference CUDA path restated in C++ (oracle/), "
+                                   f"{threads} host threads"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_b200(args)
+
+
+if __name__ == "__main__":
+    main()

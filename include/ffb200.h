@@ -113,9 +113,22 @@ ff_status ff_filter_set_propagation_border(ff_filter* f, int border);
 ff_status ff_filter_get_propagation_border(const ff_filter* f, int* border);
 ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, int* iterations);
 
-/* Select the fused per-level kernels (enabled = 1, the default) or the per-stage kernels
- * (0).  Both give bit-identical results; the switch exists for testing and profiling. */
-ff_status ff_filter_set_fused(ff_filter* f, int enabled);
+/* Kernel selection per level: 0 per-stage kernels, 1 the fused per-level kernel wherever
+ * it is instantiated, 2 automatic (default: fused for levels of at least 200,000 pixels,
+ * where it is faster).  All modes give bit-identical results. */
+ff_status ff_filter_set_fused(ff_filter* f, int mode);
+
+/* Replay the frame step from CUDA graphs (one per state buffer parity, captured on first
+ * use and re-captured after any parameter change).  Off by default. */
+ff_status ff_filter_set_graphs(ff_filter* f, int enabled);
+/* Rows per warp band of the fused kernels (0 = chosen from the SM count). */
+ff_status ff_filter_set_band(ff_filter* f, int rows);
+/* Per-level kernel timing, in the spirit of Stage::elapsedTime (src/gpu/pipeline.cu:63-88)
+ * but without host syncs: events are recorded around each level's kernels for the
+ * next `max_frames` computes (0 disables; graphs are not used while recording).
+ * ff_filter_level_kernel_ms waits for them and returns the summed milliseconds. */
+ff_status ff_filter_set_profiling(ff_filter* f, int max_frames);
+ff_status ff_filter_level_kernel_ms(ff_filter* f, int level, float* total_ms, int* frames);
 
 /* Stream used by the blocking calls (default: a non-blocking stream owned by the filter). */
 ff_status ff_filter_set_stream(ff_filter* f, void* stream);

@@ -276,7 +276,33 @@ ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, in
 }
 
 ff_status ff_filter_set_fused(ff_filter* f, int enabled) {
-    return guard([&] { get(f)->set_fused(enabled != 0); });
+    return guard([&] {
+        if (enabled < 0 || enabled > 2) throw Error(FF_ERR_INVALID_ARGUMENT, "fused mode must be 0, 1 or 2");
+        get(f)->set_fused(enabled);
+    });
+}
+
+ff_status ff_filter_set_graphs(ff_filter* f, int enabled) {
+    return guard([&] { get(f)->set_graphs(enabled != 0); });
+}
+
+ff_status ff_filter_set_band(ff_filter* f, int rows) {
+    return guard([&] {
+        if (rows < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "band rows must be >= 0");
+        get(f)->set_band(rows);
+    });
+}
+
+ff_status ff_filter_set_profiling(ff_filter* f, int max_frames) {
+    return guard([&] { get(f)->set_profiling(max_frames); });
+}
+
+ff_status ff_filter_level_kernel_ms(ff_filter* f, int level, float* total_ms, int* frames) {
+    return guard([&] {
+        need(total_ms, "total");
+        need(frames, "frames");
+        get(f)->level_kernel_ms(level, total_ms, frames);
+    });
 }
 
 ff_status ff_filter_set_stream(ff_filter* f, void* stream) {

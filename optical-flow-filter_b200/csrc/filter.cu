@@ -21,14 +21,17 @@ void check_cuda(cudaError_t e, const char* what) {
     throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Rows are allocated with room for one extra pixel (and a 4-byte multiple), so the fused
+// kernels' aligned pair copies of columns (W-1, W) stay inside the allocation.
 void Buf::alloc(int h_, int w_, int bpp_) {
     release();
     h = h_;
     w = w_;
     bpp = bpp_;
     if (h <= 0 || w <= 0) return;
-    check_cuda(cudaMallocPitch(&p, &pitch, (size_t)w * bpp, (size_t)h), "cudaMallocPitch");
-    check_cuda(cudaMemset2D(p, pitch, 0, (size_t)w * bpp, (size_t)h), "cudaMemset2D");
+    const size_t row = ((size_t)(w + 1) * bpp + 3) & ~(size_t)3;
+    check_cuda(cudaMallocPitch(&p, &pitch, row, (size_t)h), "cudaMallocPitch");
+    check_cuda(cudaMemset2D(p, pitch, 0, row, (size_t)h), "cudaMemset2D");
 }
 
 void Buf::release() {
@@ -48,6 +51,27 @@ void Level::alloc_state() {
         if (delta) d[k].alloc(H, W, 8);
     }
     if (!delta) fu.alloc(H, W, 8);
+}
+
+// Same index as the device's upmap_index (common.cuh): u = x/(W-1) rounded to float,
+// truncated to 21 fractional bits, times the coarse size.  IEEE float division on the
+// host rounds like __fdiv_rn.
+static int upmap_index_host(int x, int W, int Wc) {
+    const float u = (float)x / (float)(W - 1);
+    if (!(u == u)) return 0;
+    const long long q = (long long)std::floor(u * 2097152.0f);
+    long long i = (q * (long long)Wc) >> 21;
+    if (i < 0) i = 0;
+    if (i > Wc - 1) i = Wc - 1;
+    return (int)i;
+}
+
+void Level::build_coarse_rows() {
+    if (!delta || Hc <= 0) return;
+    std::vector<int> t(H);
+    for (int y = 0; y < H; ++y) t[y] = upmap_index_host(y, H, Hc);
+    coarse_rows.alloc(1, H, 4);
+    check_cuda(cudaMemcpy(coarse_rows.p, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice), "coarse rows");
 }
 
 void Level::alloc_scratch() {
@@ -71,7 +95,7 @@ void Level::release() {
         io[k].release();
         d[k].release();
     }
-    for (Buf* b : {&fu, &a0, &grad, &fp, &ip, &dp, &t1, &t2, &t3, &fut}) b->release();
+    for (Buf* b : {&fu, &a0, &grad, &fp, &ip, &dp, &t1, &t2, &t3, &fut, &coarse_rows}) b->release();
 }
 
 Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
@@ -86,6 +110,11 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
         own_stream_ = true;
         check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
         check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
+        check_cuda(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (cudaEvent_t* e : {&ev_fork_, &ev_pyr_, &ev_join_, &done_})
+            check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+        check_cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
         lv_.resize(L_);
         if (kind == Kind::Pyramidal) {
             // ImagePyramid::configure: integer halving, X then Y (pyramid.cu:74-83)
@@ -107,10 +136,12 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
                 v.item = item;
                 v.img = l == 0 ? input_.p : pyr_[l - 1].p;
                 v.img_pitch = l == 0 ? input_.pitch : pyr_[l - 1].pitch;
+                v.img_owned = true;
             }
             for (int l = 0; l < L_ - 1; ++l) {
                 lv_[l].Hc = lv_[l + 1].H;
                 lv_[l].Wc = lv_[l + 1].W;
+                lv_[l].build_coarse_rows();
             }
         } else {
             Level& v = lv_[0];
@@ -122,6 +153,7 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
                 input_.alloc(H, W, item);
                 v.img = input_.p;
                 v.img_pitch = input_.pitch;
+                v.img_owned = true;
             }
         }
         // configure() defaults: FlowUpdate/DeltaFlowUpdate(gamma 1, maxflow 1),
@@ -132,22 +164,40 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
         for (Level& v : lv_) v.release();
         for (Buf& b : pyr_) b.release();
         input_.release();
-        if (ev0_) cudaEventDestroy(ev0_);
-        if (ev1_) cudaEventDestroy(ev1_);
-        if (own_stream_) cudaStreamDestroy(stream_);
+        release_runtime();
         throw;
     }
 }
 
+void Filter::release_runtime() {
+    drop_graphs();
+    for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
+    prof_ev_.clear();
+    for (cudaEvent_t* e : {&ev0_, &ev1_, &ev_fork_, &ev_pyr_, &ev_join_, &done_}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
+    if (side_) cudaStreamDestroy(side_);
+    if (cap_) cudaStreamDestroy(cap_);
+    side_ = cap_ = nullptr;
+    if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+    stream_ = nullptr;
+}
+
 Filter::~Filter() {
+    if (done_) cudaEventSynchronize(done_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (side_) cudaStreamSynchronize(side_);
+    release_runtime();
     for (Level& v : lv_) v.release();
     for (Buf& b : pyr_) b.release();
     input_.release();
-    if (ev0_) cudaEventDestroy(ev0_);
-    if (ev1_) cudaEventDestroy(ev1_);
-    if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
+
+// Every operation on the filter, on whichever stream, starts after the previous one
+// finished (event done_) and marks its own end; blocking calls use the filter's stream.
+void Filter::begin_on(cudaStream_t s) { check_cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent"); }
+void Filter::end_on(cudaStream_t s) { check_cuda(cudaEventRecord(done_, s), "cudaEventRecord"); }
 
 Level& Filter::level(int l) {
     if (l < 0 || l >= L_) throw Error(FF_ERR_OUT_OF_RANGE, "level index out of bounds: " + std::to_string(l));
@@ -161,6 +211,7 @@ const Level& Filter::level(int l) const {
 // FlowFilter::setGamma / DeltaFlowFilter::setGamma: gamma/255^2 for uint8 input
 // (flowfilter.cu:276-285, 559-568); FlowUpdate::setGamma rejects gamma <= 0 (update.cu:124-132)
 void Filter::set_gamma(int l, float g) {
+    drop_graphs();
     Level& v = level(l);
     const float eff = v.item == 1 ? g / (255.0f * 255.0f) : g;
     if (!(eff > 0.0f)) throw Error(FF_ERR_INVALID_ARGUMENT, "gamma should be greater than zero: " + std::to_string(g));
@@ -171,6 +222,7 @@ float Filter::gamma(int l) const { return level(l).gamma; }
 // setMaxFlow: iterations = int(ceilf(maxflow)) must be > 0 (propagation.cu:137-148);
 // pyramids halve per level, top = maxflow / 2^(L-1) (flowfilter.cu:849-866)
 void Filter::set_max_flow(float m) {
+    drop_graphs();
     float ml = m;
     std::vector<float> per(L_);
     if (L_ == 1) {
@@ -193,6 +245,7 @@ void Filter::set_max_flow(float m) {
 float Filter::max_flow() const { return lv_[0].maxflow; }
 
 void Filter::set_smooth(int l, int n) {
+    drop_graphs();
     Level& v = level(l);
     if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "smooth iterations should be greater than zero: " + std::to_string(n));
     v.smooth = n;
@@ -200,6 +253,7 @@ void Filter::set_smooth(int l, int n) {
 int Filter::smooth(int l) const { return level(l).smooth; }
 
 void Filter::set_border(int b) {
+    drop_graphs();
     if (b < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "border should be greater or equal zero: " + std::to_string(b));
     for (Level& v : lv_) v.border = b;
 }
@@ -207,6 +261,7 @@ int Filter::border() const { return lv_[L_ - 1].border; }
 int Filter::iterations(int l) const { return level(l).iters; }
 
 void Filter::set_stream(cudaStream_t s) {
+    check_cuda(cudaEventSynchronize(done_), "set_stream");
     if (own_stream_ && stream_) {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
@@ -228,9 +283,11 @@ void Filter::load_host(const ff_image& img) {
     if (!img.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image data");
     Level& v = lv_[0];
     if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    begin_on(stream_);
     check_cuda(cudaMemcpy2DAsync(const_cast<void*>(v.img), v.img_pitch, img.data, img.pitch, (size_t)W_ * item_,
                                  (size_t)H_, cudaMemcpyHostToDevice, stream_),
                "upload");
+    end_on(stream_);
     check_cuda(cudaStreamSynchronize(stream_), "upload");
 }
 
@@ -238,23 +295,28 @@ void Filter::load_device_async(const void* img, size_t pitch, cudaStream_t s) {
     Level& v = lv_[0];
     if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
     if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
+    begin_on(s);
     check_cuda(cudaMemcpy2DAsync(const_cast<void*>(v.img), v.img_pitch, img, pitch, (size_t)W_ * item_, (size_t)H_,
-                                 cudaMemcpyDeviceToDevice, s ? s : stream_),
+                                 cudaMemcpyDeviceToDevice, s),
                "load_device");
+    end_on(s);
 }
 
 void Filter::bind_device(const void* img, size_t pitch) {
+    drop_graphs();
     if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
     if (pitch < (size_t)W_ * item_) throw Error(FF_ERR_INVALID_ARGUMENT, "pitch smaller than a row");
     if (((uintptr_t)img % item_) || (pitch % item_))
         throw Error(FF_ERR_INVALID_ARGUMENT, "image rows must be aligned to the item size");
     lv_[0].img = img;
     lv_[0].img_pitch = pitch;
+    lv_[0].img_owned = false;
 }
 
 void Filter::set_external_image(const void* img, size_t pitch) { bind_device(img, pitch); }
 
 void Filter::set_external_coarse(const void* flow, size_t pitch, int Hc, int Wc) {
+    drop_graphs();
     if (!flow) throw Error(FF_ERR_INVALID_ARGUMENT, "null coarse flow");
     if (Hc <= 0 || Wc <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "coarse flow shape");
     if (pitch < (size_t)Wc * 8) throw Error(FF_ERR_INVALID_ARGUMENT, "coarse pitch smaller than a row");
@@ -263,6 +325,7 @@ void Filter::set_external_coarse(const void* flow, size_t pitch, int Hc, int Wc)
     v.coarse_pitch = pitch;
     v.Hc = Hc;
     v.Wc = Wc;
+    v.build_coarse_rows();
 }
 
 void Filter::coarse_of(int l, const void** p, size_t* pitch, int* Hc, int* Wc) const {
@@ -351,7 +414,21 @@ void Filter::step_level_unfused(int l, cudaStream_t s) {
 void Filter::step_level(int l, cudaStream_t s) {
     Level& v = lv_[l];
     if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
-    if (fused_ && fused_available(v.delta, v.item, v.iters, v.smooth)) {
+    // the fused kernels stage rows with 4- and 8-byte cp.async copies: the image rows must
+    // be aligned, and uint8 rows readable up to the next multiple of 4 bytes
+    const uintptr_t ib = (uintptr_t)v.img;
+    const bool img_ok = v.item == 1 ? (ib % 4 == 0 && v.img_pitch % 4 == 0 && (v.img_owned || v.W % 4 == 0))
+                                    : (ib % 8 == 0 && v.img_pitch % 8 == 0 &&
+                                       (v.img_owned || v.W % 2 == 0 || v.img_pitch >= (size_t)(v.W + 1) * 4));
+    const void* cpp = nullptr;
+    size_t cpitch = 0;
+    int chh = 0, cww = 0;
+    if (v.delta) coarse_of(l, &cpp, &cpitch, &chh, &cww);
+    const bool coarse_ok = !v.delta || ((uintptr_t)cpp % 8 == 0 && cpitch % 8 == 0);
+    // mode 2 (automatic): small levels are latency-bound in the streaming kernel (few
+    // warps, long serial rows) and run faster as per-stage kernels
+    const bool want_fused = fused_mode_ == 1 || (fused_mode_ == 2 && (long)v.H * v.W >= kFusedMinPixels);
+    if (want_fused && img_ok && coarse_ok && fused_available(v.delta, v.item, v.iters, v.smooth)) {
         const int nxt = cur_ ^ 1;
         LevelArgs a{};
         a.H = v.H;
@@ -376,6 +453,7 @@ void Filter::step_level(int l, cudaStream_t s) {
             coarse_of(l, &cp, &a.coarse_pitch, &a.Hc, &a.Wc);
             if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
             a.coarse = (const float*)cp;
+            a.coarse_rows = (const int*)v.coarse_rows.p;
         } else {
             a.fu_out = (float*)v.fu.p;
             a.fu_out_pitch = v.fu.pitch;
@@ -384,14 +462,29 @@ void Filter::step_level(int l, cudaStream_t s) {
         a.maxflow = v.maxflow;
         a.border = v.border;
         a.first = v.first ? 1 : 0;
+        a.band = band_;
         check_cuda(launch_fused_level(v.delta, v.iters, v.smooth, a, s), "fused level");
     } else {
         step_level_unfused(l, s);
     }
 }
 
-void Filter::compute_async(cudaStream_t s) {
-    if (!s) s = stream_;
+// One frame's launches on `s` for the current state parity.  Levels 0..L-3 do not
+// depend on this frame's top level, so they run on a side stream concurrently with the
+// pyramid -> top -> level L-2 chain (level 0 also without waiting for the pyramid).
+void Filter::enqueue_frame(cudaStream_t s) {
+    const bool prof = prof_count_ < prof_cap_;
+    auto level_on = [&](int l, cudaStream_t st) {
+        if (prof) check_cuda(cudaEventRecord(prof_ev_[((size_t)prof_count_ * L_ + l) * 2], st), "cudaEventRecord");
+        step_level(l, st);
+        if (prof) check_cuda(cudaEventRecord(prof_ev_[((size_t)prof_count_ * L_ + l) * 2 + 1], st), "cudaEventRecord");
+    };
+    const int side_levels = kind_ == Kind::Pyramidal && L_ > 2 ? L_ - 2 : 0;  // levels 0 .. L-3
+    if (side_levels > 0) {
+        check_cuda(cudaEventRecord(ev_fork_, s), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(side_, ev_fork_, 0), "cudaStreamWaitEvent");
+        level_on(0, side_);
+    }
     if (kind_ == Kind::Pyramidal) {
         for (int l = 1; l < L_; ++l) {
             const Level& fine = lv_[l - 1];
@@ -400,11 +493,88 @@ void Filter::compute_async(cudaStream_t s) {
                        "pyramid");
         }
     }
-    // top first (level L-2 reads its fresh unsmoothed flow), then the delta levels
-    for (int l = L_ - 1; l >= 0; --l) step_level(l, s);
+    if (side_levels > 1) {
+        check_cuda(cudaEventRecord(ev_pyr_, s), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(side_, ev_pyr_, 0), "cudaStreamWaitEvent");
+        for (int l = 1; l < side_levels; ++l) level_on(l, side_);
+    }
+    // top first (level L-2 reads its fresh unsmoothed flow)
+    for (int l = L_ - 1; l >= side_levels; --l) level_on(l, s);
+    if (side_levels > 0) {
+        check_cuda(cudaEventRecord(ev_join_, side_), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(s, ev_join_, 0), "cudaStreamWaitEvent");
+    }
+    if (prof) ++prof_count_;
+}
+
+void Filter::drop_graphs() {
+    for (int k = 0; k < 2; ++k) {
+        if (graph_exec_[k]) cudaGraphExecDestroy(graph_exec_[k]);
+        graph_exec_[k] = nullptr;
+    }
+}
+
+void Filter::compute_async(cudaStream_t s) {
+    begin_on(s);
+    bool any_first = false;
+    for (const Level& v : lv_) any_first |= v.first;
+    if (graphs_ && !any_first && prof_count_ >= prof_cap_) {
+        cudaGraphExec_t& ge = graph_exec_[cur_];
+        if (!ge) {
+            // capture this parity's frame once; the buffers it names alternate per frame
+            check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            try {
+                enqueue_frame(cap_);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(cap_, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g = nullptr;
+            check_cuda(cudaStreamEndCapture(cap_, &g), "cudaStreamEndCapture");
+            cudaError_t e = cudaGraphInstantiateWithFlags(&ge, g, 0);
+            cudaGraphDestroy(g);
+            check_cuda(e, "cudaGraphInstantiate");
+        }
+        check_cuda(cudaGraphLaunch(ge, s), "cudaGraphLaunch");
+    } else {
+        enqueue_frame(s);
+    }
+    end_on(s);
     cur_ ^= 1;
     for (Level& v : lv_) v.first = false;
     phase_ = 0;
+}
+
+void Filter::set_graphs(bool on) {
+    graphs_ = on;
+    if (!on) drop_graphs();
+}
+
+void Filter::set_profiling(int frames) {
+    if (frames < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "profiling frame count must be >= 0");
+    check_cuda(cudaStreamSynchronize(stream_), "profiling");
+    for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
+    prof_ev_.clear();
+    prof_cap_ = frames;
+    prof_count_ = 0;
+    prof_ev_.resize((size_t)frames * L_ * 2, nullptr);
+    for (auto& e : prof_ev_) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+}
+
+void Filter::level_kernel_ms(int l, float* total, int* frames) {
+    level(l);
+    float sum = 0.0f;
+    for (int k = 0; k < prof_count_; ++k) {
+        cudaEvent_t a = prof_ev_[((size_t)k * L_ + l) * 2], b = prof_ev_[((size_t)k * L_ + l) * 2 + 1];
+        check_cuda(cudaEventSynchronize(b), "cudaEventSynchronize");
+        float ms = 0.0f;
+        check_cuda(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+        sum += ms;
+    }
+    *total = sum;
+    *frames = prof_count_;
 }
 
 void Filter::compute() {
@@ -420,7 +590,9 @@ void Filter::phase_model() {
     if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
     if (!lv_[0].img) throw Error(FF_ERR_LOGIC, "input image has not been set");
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    begin_on(stream_);
     model_unfused(0, stream_);
+    end_on(stream_);
     check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     check_cuda(cudaEventSynchronize(ev1_), "computeImageModel");
     check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
@@ -430,7 +602,9 @@ void Filter::phase_model() {
 void Filter::phase_propagation() {
     if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    begin_on(stream_);
     propagate_unfused(0, stream_);
+    end_on(stream_);
     check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     check_cuda(cudaEventSynchronize(ev1_), "computePropagation");
     check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
@@ -440,7 +614,9 @@ void Filter::phase_propagation() {
 void Filter::phase_update() {
     if (kind_ == Kind::Pyramidal) throw Error(FF_ERR_UNSUPPORTED, "phase API is for single-level filters");
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    begin_on(stream_);
     update_unfused(0, stream_);
+    end_on(stream_);
     check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     check_cuda(cudaEventSynchronize(ev1_), "computeUpdate");
     check_cuda(cudaEventElapsedTime(&elapsed_, ev0_, ev1_), "cudaEventElapsedTime");
@@ -472,9 +648,11 @@ void Filter::download_flow(ff_image& out) {
                                       std::to_string(W_) + ", 2][4]");
     if (!out.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null flow buffer");
     const Buf& b = lv_[0].fs[cur_];
+    begin_on(stream_);
     check_cuda(cudaMemcpy2DAsync(out.data, out.pitch, b.p, b.pitch, b.row_bytes(), (size_t)b.h, cudaMemcpyDeviceToHost,
                                  stream_),
                "downloadFlow");
+    end_on(stream_);
     check_cuda(cudaStreamSynchronize(stream_), "downloadFlow");
 }
 
@@ -484,9 +662,11 @@ void Filter::download_image(ff_image& out) {
                                       std::to_string(W_) + ", 1][4]");
     if (!out.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image buffer");
     const Buf& b = lv_[0].io[cur_];
+    begin_on(stream_);
     check_cuda(cudaMemcpy2DAsync(out.data, out.pitch, b.p, b.pitch, b.row_bytes(), (size_t)b.h, cudaMemcpyDeviceToHost,
                                  stream_),
                "downloadImage");
+    end_on(stream_);
     check_cuda(cudaStreamSynchronize(stream_), "downloadImage");
 }
 
@@ -502,9 +682,11 @@ void Filter::level_state(int l, int which, void* dst, size_t dst_pitch) {
     }
     if (!b || !b->p) throw Error(FF_ERR_UNSUPPORTED, "level state " + std::to_string(which) + " not kept for level " + std::to_string(l));
     if (!dst) throw Error(FF_ERR_INVALID_ARGUMENT, "null destination");
+    begin_on(stream_);
     check_cuda(cudaMemcpy2DAsync(dst, dst_pitch, b->p, b->pitch, b->row_bytes(), (size_t)b->h, cudaMemcpyDeviceToHost,
                                  stream_),
                "level state");
+    end_on(stream_);
     check_cuda(cudaStreamSynchronize(stream_), "level state");
 }
 

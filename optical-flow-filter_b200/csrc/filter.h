@@ -48,6 +48,7 @@ struct Level {
     int item = 1;                // input image item size
     const void* img = nullptr;   // level image (device)
     size_t img_pitch = 0;
+    bool img_owned = false;      // image buffer allocated here (aligned, padded pitch)
     Buf fs[2], io[2], d[2];      // ping-pong state: smoothed flow, old image, delta flow
     Buf fu;                      // unsmoothed updated flow (top levels)
     // coarse flow source for delta levels
@@ -60,6 +61,8 @@ struct Level {
     int smooth = 1;
     int border = 3;
     bool first = true;
+    Buf coarse_rows;             // int per row: coarse row its update reads (delta levels)
+    void build_coarse_rows();
     // scratch of the unfused path (allocated on first use)
     Buf a0, grad, fp, ip, dp, t1, t2, t3, fut;
     void alloc_state();
@@ -118,10 +121,29 @@ public:
     void download_image(ff_image& out);
     void level_state(int level, int which, void* dst, size_t dst_pitch);
 
-    // force the unfused per-stage path (for testing both paths)
-    void set_fused(bool on) { fused_ = on; }
+    // 0: per-stage kernels only, 1: fused kernels wherever instantiated, 2: automatic
+    // (fused for levels of at least kFusedMinPixels pixels)
+    void set_fused(int mode) {
+        fused_mode_ = mode;
+        drop_graphs();
+    }
+    static constexpr long kFusedMinPixels = 200000;
+    // replay each parity's frame from a captured CUDA graph
+    void set_graphs(bool on);
+    // record per-level kernel events for the next `frames` computes
+    void set_profiling(int frames);
+    void level_kernel_ms(int level, float* total, int* frames);
+    void set_band(int rows) {
+        band_ = rows;
+        drop_graphs();
+    }
 
 private:
+    void enqueue_frame(cudaStream_t s);
+    void begin_on(cudaStream_t s);
+    void end_on(cudaStream_t s);
+    void drop_graphs();
+    void release_runtime();
     void step_level(int l, cudaStream_t s);
     void step_level_unfused(int l, cudaStream_t s);
     void model_unfused(int l, cudaStream_t s);
@@ -140,8 +162,17 @@ private:
     bool own_stream_ = false;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float elapsed_ = 0.0f;
-    bool fused_ = true;
+    int fused_mode_ = 2;
     int phase_ = 0;                // phase API progress: 0 none, 1 model, 2 propagated
+    int band_ = 0;                 // rows per warp band of the fused kernels (0 = automatic)
+    cudaStream_t side_ = nullptr;  // levels 0..L-3 run here, concurrent with the top chain
+    cudaStream_t cap_ = nullptr;   // graph capture stream
+    cudaEvent_t ev_fork_ = nullptr, ev_pyr_ = nullptr, ev_join_ = nullptr;
+    cudaEvent_t done_ = nullptr;   // end of the last operation queued on the filter
+    bool graphs_ = false;
+    cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
+    int prof_cap_ = 0, prof_count_ = 0;
+    std::vector<cudaEvent_t> prof_ev_;
 };
 
 }  // namespace ffb

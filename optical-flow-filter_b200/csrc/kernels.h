@@ -43,6 +43,7 @@ struct LevelArgs {
     float* fu_out;       size_t fu_out_pitch;  // unsmoothed flow (float2), top levels; may be null
     // coarse flow (delta levels)
     const float* coarse; size_t coarse_pitch; int Hc, Wc;
+    const int* coarse_rows;  // coarse row read by each row (upmap_index), H entries
     float gamma, maxflow;
     int border;
     int first;

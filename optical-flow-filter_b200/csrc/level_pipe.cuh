@@ -45,20 +45,16 @@ struct Ctx {
     int border;
     int first;
     float dt, gamma, maxflow, half_maxflow;
-    // X-neighbour sources for the edge path: index into {L.x, L.y, v.x, v.y, R.x, R.y}
-    // of the clamped column c+o, per pixel p and offset o in {-2, -1, +1, +2}
-    int8_t nb[2][4];
+    // edge lanes (clamp-to-edge substitution of horizontal neighbours):
+    // e_l: c0 == 0; e_r1: c1 == W-1; e_r0: c0 == W-1 (odd W); e_r2: c1 == W-2 (odd W)
+    bool e_l, e_r1, e_r0, e_r2;
+    bool freeze_cols;      // some lane of this warp lies within the propagation border
+    bool any_edge;         // some lane of this warp needs horizontal edge substitution
+    bool any_split;        // some lane's two pixels are not the loaded pair (b0, b0+1)
+    int b0;                // even base column of the lane's loaded pair
+    char* smem;            // this warp's ring: kDepth slots
+    int lane;
 };
-
-__device__ __forceinline__ float pick6(int k, float a, float b, float c, float d, float e, float f) {
-    float r = a;
-    r = (k == 1) ? b : r;
-    r = (k == 2) ? c : r;
-    r = (k == 3) ? d : r;
-    r = (k == 4) ? e : r;
-    r = (k == 5) ? f : r;
-    return r;
-}
 
 __device__ __forceinline__ float2 shfl_up2(float2 v) {
     return make_float2(__shfl_up_sync(kFull, v.x, 1), __shfl_up_sync(kFull, v.y, 1));
@@ -67,17 +63,19 @@ __device__ __forceinline__ float2 shfl_dn2(float2 v) {
     return make_float2(__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1));
 }
 
-// minus/plus neighbours (offset -1/+1) of both pixels of a pair
+// minus/plus neighbours (offset -1/+1) of both pixels of a pair.  At the image edges
+// the missing neighbour is the edge pixel itself (clamp-to-edge reads of this stage's
+// input): only the lanes holding columns 0, W-1 substitute.
 template <bool EDGE>
 __device__ __forceinline__ void nb3(const Ctx& c, float2 v, float2& m, float2& p) {
     const float ly = __shfl_up_sync(kFull, v.y, 1);
     const float rx = __shfl_down_sync(kFull, v.x, 1);
-    if (!EDGE) {
-        m = make_float2(ly, v.x);
-        p = make_float2(v.y, rx);
-    } else {
-        m = make_float2(pick6(c.nb[0][1], 0.f, ly, v.x, v.y, rx, 0.f), pick6(c.nb[1][1], 0.f, ly, v.x, v.y, rx, 0.f));
-        p = make_float2(pick6(c.nb[0][2], 0.f, ly, v.x, v.y, rx, 0.f), pick6(c.nb[1][2], 0.f, ly, v.x, v.y, rx, 0.f));
+    m = make_float2(ly, v.x);
+    p = make_float2(v.y, rx);
+    if (EDGE && c.any_edge) {  // warp-uniform
+        m.x = c.e_l ? v.x : m.x;
+        p.x = c.e_r0 ? v.x : p.x;
+        p.y = c.e_r1 ? v.y : p.y;
     }
 }
 
@@ -85,20 +83,25 @@ __device__ __forceinline__ void nb3(const Ctx& c, float2 v, float2& m, float2& p
 template <bool EDGE>
 __device__ __forceinline__ void nb5(const Ctx& c, float2 v, float2 (&t)[5]) {
     const float2 L = shfl_up2(v), R = shfl_dn2(v);
-    if (!EDGE) {
-        t[0] = make_float2(L.x, L.y);
-        t[1] = make_float2(L.y, v.x);
-        t[2] = v;
-        t[3] = make_float2(v.y, R.x);
-        t[4] = make_float2(R.x, R.y);
-    } else {
-#pragma unroll
-        for (int o = 0; o < 4; ++o) {
-            const int k = o < 2 ? o : o + 1;
-            t[k] = make_float2(pick6(c.nb[0][o], L.x, L.y, v.x, v.y, R.x, R.y),
-                               pick6(c.nb[1][o], L.x, L.y, v.x, v.y, R.x, R.y));
-        }
-        t[2] = v;
+    t[0] = make_float2(L.x, L.y);
+    t[1] = make_float2(L.y, v.x);
+    t[2] = v;
+    t[3] = make_float2(v.y, R.x);
+    t[4] = make_float2(R.x, R.y);
+    if (EDGE && c.any_edge) {  // warp-uniform
+        // left edge: columns -2, -1 read column 0
+        t[0].x = c.e_l ? v.x : t[0].x;
+        t[1].x = c.e_l ? v.x : t[1].x;
+        t[0].y = c.e_l ? v.x : t[0].y;
+        // right edge, even W: columns W, W+1 read column W-1 = v.y of the last lane
+        t[4].x = c.e_r1 ? v.y : t[4].x;
+        t[3].y = c.e_r1 ? v.y : t[3].y;
+        t[4].y = c.e_r1 ? v.y : t[4].y;
+        // right edge, odd W: the last lane holds column W-1 in v.x
+        t[3].x = c.e_r0 ? v.x : t[3].x;
+        t[4].x = c.e_r0 ? v.x : t[4].x;
+        // odd W, lane before the last: column W reads column W-1 = R.x
+        t[4].y = c.e_r2 ? R.x : t[4].y;
     }
 }
 
@@ -126,10 +129,11 @@ __device__ __forceinline__ float2 box5p(const float2 (&t)[5]) {
 // upwind step of a pair: n = vel >= 0 ? m : p; d = v - n; v - |t|*d (fused or not).
 // Equals the reference's v - t*(vel >= 0 ? v - m : p - v) bit for bit: for vel < 0,
 // t = -|t| and p - v = -(v - p) exactly.
+// fw = (vel >= 0) per pixel, at = |t| per pixel
 template <bool FUSED>
-__device__ __forceinline__ float2 upwind2(float2 v, float2 m, float2 p, float2 vel, float2 at) {
-    const float d0 = __fsub_rn(v.x, vel.x >= 0.0f ? m.x : p.x);
-    const float d1 = __fsub_rn(v.y, vel.y >= 0.0f ? m.y : p.y);
+__device__ __forceinline__ float2 upwind2(float2 v, float2 m, float2 p, bool fw0, bool fw1, float2 at) {
+    const float d0 = __fsub_rn(v.x, fw0 ? m.x : p.x);
+    const float d1 = __fsub_rn(v.y, fw1 ? m.y : p.y);
     if (FUSED) return make_float2(__fmaf_rn(-at.x, d0, v.x), __fmaf_rn(-at.y, d1, v.y));
     return make_float2(__fsub_rn(v.x, __fmul_rn(at.x, d0)), __fsub_rn(v.y, __fmul_rn(at.y, d1)));
 }
@@ -147,25 +151,39 @@ __device__ __forceinline__ T* rowp_w(void* base, size_t pitch, int y) {
     return reinterpret_cast<T*>(reinterpret_cast<char*>(base) + (size_t)y * pitch);
 }
 
+// ---------------------------------------------------------------- cp.async staging
+// Every input row a stage needs is copied into a per-warp shared-memory ring kDepth
+// rows ahead of its use (cp.async: the data is in flight without occupying registers).
+// Each lane copies and later reads only its own bytes, so no warp barrier is needed.
+constexpr int kDepth = 4;
+struct Slot {
+    static constexpr int FLOW = 0;      // 32 lanes x 16 B: (u0, v0, u1, v1) of the state row
+    static constexpr int IO = 512;      // 32 x 8 B: old image (delta: state row; top: update row)
+    static constexpr int IMG = 768;     // 32 x 8 B: image row (uint8 words or float pair)
+    static constexpr int DELTA = 1024;  // 32 x 16 B: delta flow of the state row
+    static constexpr int COARSE = 1536; // 32 x 16 B: coarse flow at the update row
+    static constexpr int TOP_BYTES = 1024, DELTA_BYTES = 2048;
+};
+
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // pair of interleaved float2 pixels (c0, c1) -> (x pair, y pair)
-__device__ __forceinline__ void load_f2pair(const Ctx& c, const float* base, size_t pitch, int y, float2& xs,
-                                            float2& ysv) {
-    const float2* row = rowp<float2>(base, pitch, y);
-    if (c.vec) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(row + c.cc0));
-        xs = make_float2(q.x, q.z);
-        ysv = make_float2(q.y, q.w);
-    } else {
-        const float2 a = __ldg(row + c.cc0), b = __ldg(row + c.cc1);
-        xs = make_float2(a.x, b.x);
-        ysv = make_float2(a.y, b.y);
-    }
-}
-__device__ __forceinline__ float2 load_f1pair(const Ctx& c, const float* base, size_t pitch, int y) {
-    const float* row = rowp<float>(base, pitch, y);
-    if (c.vec) return __ldg(reinterpret_cast<const float2*>(row + c.cc0));
-    return make_float2(__ldg(row + c.cc0), __ldg(row + c.cc1));
-}
 __device__ __forceinline__ void store_f2pair(const Ctx& c, float* base, size_t pitch, int y, float2 xs, float2 ysv) {
     float2* row = rowp_w<float2>(base, pitch, y);
     if (c.out1) {
@@ -183,17 +201,15 @@ __device__ __forceinline__ void store_f1pair(const Ctx& c, float* base, size_t p
     }
 }
 
-template <typename P>
-__device__ __forceinline__ float2 load_image(const Ctx& c, const void* img, size_t pitch, int y) {
-    const P* row = rowp<P>(img, pitch, y);
-    return make_float2(Pix<P>::get(__ldg(row + c.cc0)), Pix<P>::get(__ldg(row + c.cc1)));
-}
-
 // The pipeline of one warp.  DELTA: delta level (flow, old image and delta flow are
 // propagated; the update refines the coarse flow).  Otherwise a top level (flow is
 // propagated; old image read in place).
-template <bool DELTA, int N, int S, typename P, bool EDGE>
+// EM: edge handling compiled in.  bit 0 (EX): the window reaches the left/right image
+// edge or border (column substitution, non-adjacent lanes); bit 1 (EY): the band's rows
+// reach the top/bottom (row clamping and substitution, border rows).
+template <bool DELTA, int N, int S, typename P, int EM>
 struct Pipe {
+    static constexpr bool EX = (EM & 1) != 0, EY = (EM & 2) != 0;
     // propagated channels: U, V (flow) [, I old image, DX, DY delta flow]
     static constexpr int NC = DELTA ? 5 : 2;
     static constexpr int CU = 0, CV = 1, CI = 2, CDX = 3, CDY = 4;
@@ -224,12 +240,16 @@ struct Pipe {
 
     // border freeze (propagation_k.cu:59-65): pixels within `border` of an edge keep v
     __device__ __forceinline__ static void freeze(const Ctx& c, int q, float2 (&out)[NC], const float2 (&v)[NC]) {
-        if (!EDGE) return;
-        const bool row_ok = q >= c.border && q < c.H - c.border;
+        if (!EX && !EY) return;
+        if (EY && (q < c.border || q >= c.H - c.border)) {  // warp-uniform
 #pragma unroll
-        for (int ch = 0; ch < NC; ++ch) {
-            out[ch].x = (row_ok && c.col0) ? out[ch].x : v[ch].x;
-            out[ch].y = (row_ok && c.col1) ? out[ch].y : v[ch].y;
+            for (int ch = 0; ch < NC; ++ch) out[ch] = v[ch];
+        } else if (EX && c.freeze_cols) {  // warp-uniform
+#pragma unroll
+            for (int ch = 0; ch < NC; ++ch) {
+                out[ch].x = c.col0 ? out[ch].x : v[ch].x;
+                out[ch].y = c.col1 ? out[ch].y : v[ch].y;
+            }
         }
     }
 
@@ -237,14 +257,15 @@ struct Pipe {
     __device__ __forceinline__ static void prop_x(const Ctx& c, int q, float2 (&v)[NC]) {
         float2 m[NC], p[NC];
 #pragma unroll
-        for (int ch = 0; ch < NC; ++ch) nb3<EDGE>(c, v[ch], m[ch], p[ch]);
+        for (int ch = 0; ch < NC; ++ch) nb3<EX>(c, v[ch], m[ch], p[ch]);
         const float2 vel = make_float2(dominant(m[CU].x, p[CU].x), dominant(m[CU].y, p[CU].y));
         const float2 at = abs_t(c.dt, vel);
+        const bool fw0 = vel.x >= 0.0f, fw1 = vel.y >= 0.0f;
         float2 o[NC];
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) {
-            if (fused(ch)) o[ch] = upwind2<true>(v[ch], m[ch], p[ch], vel, at);
-            else o[ch] = upwind2<false>(v[ch], m[ch], p[ch], vel, at);
+            if (fused(ch)) o[ch] = upwind2<true>(v[ch], m[ch], p[ch], fw0, fw1, at);
+            else o[ch] = upwind2<false>(v[ch], m[ch], p[ch], fw0, fw1, at);
         }
         freeze(c, q, o, v);
 #pragma unroll
@@ -255,36 +276,113 @@ struct Pipe {
     __device__ __forceinline__ static void prop_y(const Ctx& c, int q, const float2 (&prev)[NC],
                                                   const float2 (&cur)[NC], const float2 (&next)[NC],
                                                   float2 (&o)[NC]) {
-        const bool top = EDGE && q == 0, bot = EDGE && q == c.H - 1;
         float2 m[NC], p[NC];
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) {
-            m[ch] = top ? cur[ch] : prev[ch];
-            p[ch] = bot ? cur[ch] : next[ch];
+            m[ch] = prev[ch];
+            p[ch] = next[ch];
+        }
+        if (EY && (q == 0 || q == c.H - 1)) {  // warp-uniform
+#pragma unroll
+            for (int ch = 0; ch < NC; ++ch) {
+                if (q == 0) m[ch] = cur[ch];
+                if (q == c.H - 1) p[ch] = cur[ch];
+            }
         }
         const float2 vel = make_float2(dominant(m[CV].x, p[CV].x), dominant(m[CV].y, p[CV].y));
         const float2 at = abs_t(c.dt, vel);
+        const bool fw0 = vel.x >= 0.0f, fw1 = vel.y >= 0.0f;
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) {
-            if (fused(ch)) o[ch] = upwind2<true>(cur[ch], m[ch], p[ch], vel, at);
-            else o[ch] = upwind2<false>(cur[ch], m[ch], p[ch], vel, at);
+            if (fused(ch)) o[ch] = upwind2<true>(cur[ch], m[ch], p[ch], fw0, fw1, at);
+            else o[ch] = upwind2<false>(cur[ch], m[ch], p[ch], fw0, fw1, at);
         }
         freeze(c, q, o, cur);
     }
 
-    // one streamed row
-    __device__ __forceinline__ void step(const Ctx& c, const LevelArgs& a, int i) {
+    static constexpr int SLOT = DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES;
+
+    __device__ __forceinline__ static int clampr(const Ctx& c, int r) { return EY ? min(max(r, 0), c.H - 1) : r; }
+
+    // copy every input that iteration i consumes into slot `slot`.  Each lane copies the
+    // aligned column pair (b0, b0+1) of every field; b0 = clamp(c0) rounded down to even,
+    // so one 16/8/4-byte copy per field, and rows carry at least one column of padding.
+    __device__ __forceinline__ static void issue(const Ctx& c, const LevelArgs& a, int slot, int i) {
+        char* sb = c.smem + slot * SLOT;
+        const int l = c.lane;
+        const int r = clampr(c, i);
+        cp16(sb + Slot::FLOW + 16 * l, rowp<float2>(a.fs_in, a.fs_in_pitch, r) + c.b0);
+        const int ru = clampr(c, i - N);  // update row
+        cp8(sb + Slot::IO + 8 * l, rowp<float>(a.io_in, a.io_in_pitch, DELTA ? r : ru) + c.b0);
+        if constexpr (DELTA) {
+            cp16(sb + Slot::DELTA + 16 * l, rowp<float2>(a.d_in, a.d_in_pitch, r) + c.b0);
+            // coarse row of the update row from the level's row table (upmap_index of each row)
+            const float2* crow = rowp<float2>(a.coarse, a.coarse_pitch, __ldg(a.coarse_rows + ru));
+            cp8(sb + Slot::COARSE + 16 * l, crow + c.ix0);
+            cp8(sb + Slot::COARSE + 16 * l + 8, crow + c.ix1);
+        }
+        const int rj = clampr(c, i - N + 2);  // image row
+        if constexpr (sizeof(P) == 1) {
+            // the aligned 32-bit word holding columns b0, b0+1 (image rows are 4-byte
+            // aligned and padded to a multiple of 4 bytes; see fused_available)
+            cp4(sb + Slot::IMG + 8 * l, reinterpret_cast<const uint8_t*>(rowp<P>(a.img, a.img_pitch, rj)) + (c.b0 & ~3));
+        } else {
+            cp8(sb + Slot::IMG + 8 * l, rowp<P>(a.img, a.img_pitch, rj) + c.b0);
+        }
+    }
+
+    // pixel values of the lane from a loaded pair (b0, b0+1): identity unless the lane's
+    // clamped columns are not (b0, b0+1) (lanes outside the image or at an odd right edge)
+    __device__ __forceinline__ static float2 unpair(const Ctx& c, float lo, float hi) {
+        float2 v = make_float2(lo, hi);
+        if (EX && c.any_split) {  // warp-uniform
+            v.x = c.cc0 == c.b0 ? lo : hi;
+            v.y = c.cc1 == c.b0 ? lo : hi;
+        }
+        return v;
+    }
+
+    // one streamed row; its inputs wait in slot `slot`
+    __device__ __forceinline__ void step(const Ctx& c, const LevelArgs& a, int i, int slot) {
         const int H = c.H;
+        cp_wait<kDepth - 1>();
+        const char* sb = c.smem + slot * SLOT;
+        const int l = c.lane;
         // ---- state row i
         float2 x[NC];
+        float2 io_u;  // top levels: old image at the update row
+        float2 im;    // image row i-N+2
+        float4 cf;    // delta levels: coarse flow (u0, v0, u1, v1) at the update row
         {
-            const int r = min(max(i, 0), H - 1);
-            load_f2pair(c, a.fs_in, a.fs_in_pitch, r, x[CU], x[CV]);
+            const float4 q = *reinterpret_cast<const float4*>(sb + Slot::FLOW + 16 * l);
+            x[CU] = unpair(c, q.x, q.z);
+            x[CV] = unpair(c, q.y, q.w);
+            const float2 iop = *reinterpret_cast<const float2*>(sb + Slot::IO + 8 * l);
+            const float2 io = unpair(c, iop.x, iop.y);
             if constexpr (DELTA) {
-                x[CI] = load_f1pair(c, a.io_in, a.io_in_pitch, r);
-                load_f2pair(c, a.d_in, a.d_in_pitch, r, x[CDX], x[CDY]);
+                x[CI] = io;
+                const float4 d = *reinterpret_cast<const float4*>(sb + Slot::DELTA + 16 * l);
+                x[CDX] = unpair(c, d.x, d.z);
+                x[CDY] = unpair(c, d.y, d.w);
+                cf = *reinterpret_cast<const float4*>(sb + Slot::COARSE + 16 * l);
+                io_u = make_float2(0.f, 0.f);
+            } else {
+                io_u = io;
+                cf = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if constexpr (sizeof(P) == 1) {
+                const uint32_t w = *reinterpret_cast<const uint32_t*>(sb + Slot::IMG + 8 * l);
+                const uint32_t v0 = (w >> (8 * (c.cc0 & 3))) & 0xffu;
+                const uint32_t v1 = (w >> (8 * (c.cc1 & 3))) & 0xffu;
+                im = make_float2(u8_to_unit(v0), u8_to_unit(v1));
+            } else {
+                const float2 ip = *reinterpret_cast<const float2*>(sb + Slot::IMG + 8 * l);
+                im = unpair(c, ip.x, ip.y);
             }
         }
+        // the slot is free again: stage the row needed kDepth iterations from now
+        issue(c, a, slot, i + kDepth);
+        cp_commit();
         // ---- N propagation sub-steps
 #pragma unroll
         for (int k = 0; k < N; ++k) {
@@ -303,8 +401,6 @@ struct Pipe {
         // ---- image model at row r (imagemodel_k.cu:31-133)
         float2 a0, ax, ay;
         {
-            const int j = r + 2;
-            const float2 im = load_image<P>(c, a.img, a.img_pitch, min(max(j, 0), H - 1));
             float2 t[5];
             nb5_raw(im, t);
             const float2 bx = smooth5p(t);
@@ -328,10 +424,9 @@ struct Pipe {
         float2 fu, fv;
         const bool store_r = r >= c.ys && r < c.ye;
         {
-            const int rc = min(max(r, 0), H - 1);
             float2 old;
             if constexpr (DELTA) old = x[CI];
-            else old = load_f1pair(c, a.io_in, a.io_in_pitch, rc);
+            else old = io_u;
             if (c.first) old = a0;
             float2 fx, fy;
             if constexpr (DELTA) {
@@ -348,9 +443,7 @@ struct Pipe {
                 // deltaFlowUpdate_k (update_k.cu:136-164)
                 ox = make_float2(clampm(sanitize(ox.x), c.half_maxflow), clampm(sanitize(ox.y), c.half_maxflow));
                 oy = make_float2(clampm(sanitize(oy.x), c.half_maxflow), clampm(sanitize(oy.y), c.half_maxflow));
-                const int iy = upmap_index(rc, H, a.Hc);
-                const float2* crow = rowp<float2>(a.coarse, a.coarse_pitch, iy);
-                const float2 u0 = __ldg(crow + c.ix0), u1 = __ldg(crow + c.ix1);
+                const float2 u0 = make_float2(cf.x, cf.y), u1 = make_float2(cf.z, cf.w);
                 fu = make_float2(clampm(__fadd_rn(ox.x, __fmul_rn(2.0f, u0.x)), c.maxflow),
                                  clampm(__fadd_rn(ox.y, __fmul_rn(2.0f, u1.x)), c.maxflow));
                 fv = make_float2(clampm(__fadd_rn(oy.x, __fmul_rn(2.0f, u0.y)), c.maxflow),
@@ -373,13 +466,13 @@ struct Pipe {
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             float2 tu[5], tv[5];
-            nb5<EDGE>(c, fu, tu);
-            nb5<EDGE>(c, fv, tv);
+            nb5<EX>(c, fu, tu);
+            nb5<EX>(c, fv, tv);
             const float2 sxu = box5p(tu), sxv = box5p(tv);
             const int q = r - 2 * s - 2;  // row of this Y pass
             float2 ru[5] = {sw[s][0][0], sw[s][1][0], sw[s][2][0], sw[s][3][0], sxu};
             float2 rv[5] = {sw[s][0][1], sw[s][1][1], sw[s][2][1], sw[s][3][1], sxv};
-            if (EDGE && (q < 2 || q > H - 3)) {
+            if (EY && (q < 2 || q > H - 3)) {
                 // clamp-to-edge rows: slot k holds row q-2+k
                 float2 cu[5], cv[5];
 #pragma unroll
@@ -412,17 +505,21 @@ struct Pipe {
     }
 };
 
-template <bool DELTA, int N, int S, typename P, bool EDGE>
+template <bool DELTA, int N, int S, typename P, int EM>
 __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int iters) {
-    Pipe<DELTA, N, S, P, EDGE> pipe;
+    using Pp = Pipe<DELTA, N, S, P, EM>;
+    Pp pipe;
     pipe.init();
-    // iters is a multiple of 4: windows of 2 and 4 rows rotate back in place every 4 rows
-    for (int it = 0; it < iters; it += 4) {
-        pipe.step(c, a, i0 + it);
-        pipe.step(c, a, i0 + it + 1);
-        pipe.step(c, a, i0 + it + 2);
-        pipe.step(c, a, i0 + it + 3);
+#pragma unroll
+    for (int u = 0; u < kDepth; ++u) {
+        Pp::issue(c, a, u, i0 + u);
+        cp_commit();
     }
+    // one row per iteration, not unrolled: the loop body must stay small enough for the
+    // instruction cache; the windows rotate by register moves and the slot index cycles
+#pragma unroll 1
+    for (int it = 0; it < iters; ++it) pipe.step(c, a, i0 + it, it & (kDepth - 1));
+    cp_wait<0>();
 }
 
 // halo widths of a level: columns on each side (even) and rows before the band
@@ -433,6 +530,7 @@ template <bool DELTA, int N, int S, typename P>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) level_k(LevelArgs a, int nwx, int nby, int band) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
+    extern __shared__ __align__(16) char smem_raw[];
     const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (warp >= nwx * nby) return;  // whole warps exit together
     const int lane = threadIdx.x & 31;
@@ -442,6 +540,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) level_k(LevelArgs a, int 
     Ctx c;
     c.W = W;
     c.H = H;
+    c.lane = lane;
+    c.smem = smem_raw + (threadIdx.x >> 5) * (kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES));
     const int xo = wx * OX, x0 = xo - HX;
     c.c0 = x0 + 2 * lane;
     c.c1 = c.c0 + 1;
@@ -467,40 +567,55 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) level_k(LevelArgs a, int 
     } else {
         c.ix0 = c.ix1 = 0;
     }
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-        const int cp = p == 0 ? c.c0 : c.c1;
-        const int offs[4] = {-2, -1, 1, 2};
-#pragma unroll
-        for (int o = 0; o < 4; ++o) {
-            const int src = min(max(cp + offs[o], 0), W - 1) - (c.c0 - 2);
-            c.nb[p][o] = (int8_t)min(max(src, 0), 5);
-        }
-    }
+    c.e_l = c.c0 == 0;
+    c.e_r1 = c.c1 == W - 1;
+    c.e_r0 = c.c0 == W - 1;
+    c.e_r2 = c.c1 == W - 2 && (W & 1);
+    c.freeze_cols = __any_sync(kFull, !(c.col0 && c.col1));
+    c.b0 = min(max(c.c0, 0), (W - 1) & ~1);
+    c.any_edge = __any_sync(kFull, c.e_l || c.e_r0 || c.e_r1 || c.e_r2);
+    c.any_split = __any_sync(kFull, c.cc0 != c.b0 || c.cc1 != c.b0 + 1);
     const int i0 = c.ys - lead_rows(N, S);
     const int last = c.ye - 1 + N + 2 * S;
     const int iters = (last - i0 + 1 + 3) & ~3;
     // interior warps: no clamping, substitution or border freeze can reach them
     const int m = (a.border > 2 ? a.border : 2) + 1;
     const int rlo = i0 - N - 2 * S - 2, rhi = i0 + iters + 2;
-    const bool interior = x0 >= m && x0 + 64 <= W - m && rlo >= m && rhi <= H - m;
-    if (interior) run_warp<DELTA, N, S, P, false>(a, c, i0, iters);
-    else run_warp<DELTA, N, S, P, true>(a, c, i0, iters);
+    // One code path for every warp: the edge handling costs a few selects per row, while
+    // several variants of this large loop body in one kernel thrash the instruction cache.
+    (void)m;
+    (void)rlo;
+    (void)rhi;
+    run_warp<DELTA, N, S, P, 3>(a, c, i0, iters);
 }
 
 template <bool DELTA, int N, int S, typename P>
 cudaError_t launch(const LevelArgs& a, cudaStream_t s) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
+    const int smem = kWarpsPerBlock * kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES);
+    // resident warps on this device, queried once per instantiation
+    static int resident_warps = 0;
+    if (resident_warps == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_k<DELTA, N, S, P>, kWarpsPerBlock * 32, smem);
+        resident_warps = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarpsPerBlock;
+    }
     const int nwx = (a.W + OX - 1) / OX;
-    // bands sized for about 8 resident warps per SM across 148 SMs
-    int band = a.band > 0 ? a.band : (int)(((long)a.H * nwx + 1183) / 1184);
+    // bands: as few as fill the resident warps once (every extra band restarts a pipeline)
+    int band = a.band;
+    if (band <= 0) {
+        const int bands = resident_warps / nwx > 0 ? resident_warps / nwx : 1;
+        band = (a.H + bands - 1) / bands;
+    }
     band = band < 8 ? 8 : band;
     band = band > a.H ? a.H : band;
     const int nby = (a.H + band - 1) / band;
     const int warps = nwx * nby;
     const int blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    level_k<DELTA, N, S, P><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a, nwx, nby, band);
+    level_k<DELTA, N, S, P><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a, nwx, nby, band);
     return cudaGetLastError();
 }
 

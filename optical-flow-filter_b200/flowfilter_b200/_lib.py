@@ -92,6 +92,10 @@ SIGNATURES = {
     "ff_filter_get_propagation_border": (_st, [_vp, _ip]),
     "ff_filter_get_propagation_iterations": (_st, [_vp, _i, _ip]),
     "ff_filter_set_fused": (_st, [_vp, _i]),
+    "ff_filter_set_graphs": (_st, [_vp, _i]),
+    "ff_filter_set_band": (_st, [_vp, _i]),
+    "ff_filter_set_profiling": (_st, [_vp, _i]),
+    "ff_filter_level_kernel_ms": (_st, [_vp, _i, _fp, _ip]),
     "ff_filter_set_stream": (_st, [_vp, _vp]),
     "ff_filter_load_image_host": (_st, [_vp, ctypes.POINTER(FFImage)]),
     "ff_filter_load_image_device_async": (_st, [_vp, _vp, _sz, _vp]),

@@ -175,9 +175,28 @@ class _FilterBase:
              out.strides[0])
         return out
 
-    def setFused(self, enabled: bool) -> None:
-        """Fused per-level kernels (default) or the per-stage kernels; results are identical."""
-        call("ff_filter_set_fused", self._h, 1 if enabled else 0)
+    def setFused(self, mode) -> None:
+        """Kernel selection: False/0 per-stage kernels, True/1 fused per-level kernels, 2 automatic
+        (the default: fused for levels of at least 200,000 pixels).  Results are identical."""
+        call("ff_filter_set_fused", self._h, int(mode))
+
+    def setGraphs(self, enabled: bool) -> None:
+        """Replay the frame step from captured CUDA graphs (one per state parity)."""
+        call("ff_filter_set_graphs", self._h, 1 if enabled else 0)
+
+    def setBand(self, rows: int) -> None:
+        """Rows per warp band of the fused kernels (0 = automatic)."""
+        call("ff_filter_set_band", self._h, int(rows))
+
+    def setProfiling(self, max_frames: int) -> None:
+        """Record per-level kernel events for the next ``max_frames`` computes."""
+        call("ff_filter_set_profiling", self._h, int(max_frames))
+
+    def levelKernelTime(self, level: int) -> tuple[float, int]:
+        """(summed milliseconds, frames) of the level's kernels since setProfiling."""
+        ms, n = ctypes.c_float(), ctypes.c_int()
+        call("ff_filter_level_kernel_ms", self._h, int(level), ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
 
     def setStream(self, stream) -> None:
         if hasattr(stream, "cuda_stream"):

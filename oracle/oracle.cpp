@@ -17,6 +17,9 @@
 #include <cstring>
 #include <vector>
 
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 
 namespace {
@@ -55,20 +58,81 @@ inline float madd(bool fused, float a, float b, float c) {
     return p + c;
 }
 
-// rows split into contiguous chunks over g_threads std::threads (serial when <= 1)
+// Persistent worker pool: rows split into contiguous chunks over g_threads threads
+// (serial when <= 1).  Workers are created once and woken per parallel loop.
+class Pool {
+public:
+    void run(int H, int nt, const std::function<void(int)>& body) {
+        std::unique_lock<std::mutex> lk(m_);
+        resize(nt - 1);
+        body_ = &body;
+        H_ = H;
+        nt_ = nt;
+        pending_ = nt - 1;
+        ++gen_;
+        lk.unlock();
+        cv_.notify_all();
+        chunk(0, body);
+        lk.lock();
+        done_.wait(lk, [&] { return pending_ == 0; });
+        body_ = nullptr;
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+private:
+    void chunk(int t, const std::function<void(int)>& body) {
+        const int y0 = (int)((long)H_ * t / nt_), y1 = (int)((long)H_ * (t + 1) / nt_);
+        for (int y = y0; y < y1; ++y) body(y);
+    }
+    void resize(int n) {
+        while ((int)workers_.size() < n) {
+            const int id = (int)workers_.size() + 1;
+            workers_.emplace_back([this, id] { loop(id); });
+        }
+    }
+    void loop(int id) {
+        unsigned long seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (stop_) return;
+            if (id >= nt_ || !body_) continue;
+            const std::function<void(int)>* body = body_;
+            lk.unlock();
+            chunk(id, *body);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    std::vector<std::thread> workers_;
+    const std::function<void(int)>* body_ = nullptr;
+    int H_ = 0, nt_ = 1, pending_ = 0;
+    unsigned long gen_ = 0;
+    bool stop_ = false;
+};
+
+Pool& pool() {
+    static Pool p;
+    return p;
+}
+
 template <typename F>
 void for_rows(int H, F&& body) {
     const int nt = std::min(g_threads, H);
     if (nt > 1) {
-        std::vector<std::thread> pool;
-        pool.reserve(nt);
-        for (int t = 0; t < nt; ++t) {
-            const int y0 = (int)((long)H * t / nt), y1 = (int)((long)H * (t + 1) / nt);
-            pool.emplace_back([&body, y0, y1]() {
-                for (int y = y0; y < y1; ++y) body(y);
-            });
-        }
-        for (auto& th : pool) th.join();
+        std::function<void(int)> fn = [&body](int y) { body(y); };
+        pool().run(H, nt, fn);
         return;
     }
     for (int y = 0; y < H; ++y) body(y);

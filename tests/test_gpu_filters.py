@@ -252,3 +252,31 @@ def test_delta_filter_standalone(ffb, cuda):
         fu, du, iu = O.delta_update(a0, g, ip, dp, coarse, gamma, 2.0)
         fs = O.smooth(fu, 1)
         np.testing.assert_array_equal(gf.getFlow(), fs)
+
+
+@pytest.mark.parametrize("levels", [1, 2, 3, 4])
+def test_graphs_side_streams_and_profiling(ffb, cuda, levels):
+    """CUDA-graph replay (one graph per state parity), the side stream that runs levels
+    0..L-3 concurrently, and the profiling events all leave results unchanged."""
+    h, w = 96, 160
+    frames = case_frames(dict(seq="bumps", frames=9, kw=dict(height=h, width=w, sigma=1.0, seed=21, n_bumps=2,
+                                                              bump_sigma=40.0, amp=2.0)))
+    ref = ffb.PyramidalFlowFilter(h, w, levels)
+    g = ffb.PyramidalFlowFilter(h, w, levels)
+    for f in (ref, g):
+        f.maxflow = 4.0
+        f.smoothIterations = [2] * levels if levels > 1 else 2
+    g.setGraphs(True)
+    dev = cuda.from_numpy(frames).cuda()
+    for t in range(9):
+        if t == 4:
+            g.setProfiling(3)
+        if t == 6:
+            g.maxflow = 3.0  # parameter change re-captures the graphs
+            ref.maxflow = 3.0
+        ref.loadImage(frames[t]); ref.compute()
+        g.loadImage(dev[t]); g.computeAsync()
+        cuda.cuda.synchronize()
+        np.testing.assert_array_equal(g.getFlow(), ref.getFlow())
+    ms, n = g.levelKernelTime(0)
+    assert n == 3 and ms > 0.0
