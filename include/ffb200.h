@@ -121,6 +121,17 @@ ff_status ff_filter_set_fused(ff_filter* f, int mode);
 /* Replay the frame step from CUDA graphs (one per state buffer parity, captured on first
  * use and re-captured after any parameter change).  Off by default. */
 ff_status ff_filter_set_graphs(ff_filter* f, int enabled);
+/* Autotuner: on the current inputs, time each level's per-stage kernels and its fused
+ * kernel at several band heights (`repetitions` runs each) and keep the fastest per
+ * level, used while the mode is 2.  Needs one computed frame; results are unchanged
+ * because every candidate writes bit-identical outputs.  Parameter changes reset it. */
+ff_status ff_filter_autotune(ff_filter* f, int repetitions);
+/* Read or set one level's kernel choice (path: -1 untuned, 0 per-stage, 1 fused; band rows
+ * of the fused kernel, 0 automatic), e.g. to reuse a saved autotuning result. */
+ff_status ff_filter_get_level_tuning(const ff_filter* f, int level, int* path, int* band);
+ff_status ff_filter_set_level_tuning(ff_filter* f, int level, int path, int band);
+/* Human-readable summary of the tuned choice per level (NUL-terminated, truncated to len). */
+ff_status ff_filter_tuning(const ff_filter* f, char* buf, size_t len);
 /* Rows per warp band of the fused kernels (0 = chosen from the SM count). */
 ff_status ff_filter_set_band(ff_filter* f, int rows);
 /* Per-level kernel timing, in the spirit of Stage::elapsedTime (src/gpu/pipeline.cu:63-88)
@@ -129,6 +140,13 @@ ff_status ff_filter_set_band(ff_filter* f, int rows);
  * ff_filter_level_kernel_ms waits for them and returns the summed milliseconds. */
 ff_status ff_filter_set_profiling(ff_filter* f, int max_frames);
 ff_status ff_filter_level_kernel_ms(ff_filter* f, int level, float* total_ms, int* frames);
+
+/* Device time of one level's step in its current kernel configuration: the step is
+ * captured as a CUDA graph and launched `reps` times on the filter's stream, each launch
+ * bracketed by events; when `flush` is non-NULL, `flush_bytes` of it are overwritten
+ * before every launch, outside the events (evicting the L2).  Re-running a step rewrites
+ * bit-identical outputs; needs one computed frame.  *total_ms is the sum over launches. */
+ff_status ff_filter_time_level(ff_filter* f, int level, int reps, void* flush, size_t flush_bytes, float* total_ms);
 
 /* Stream used by the blocking calls (default: a non-blocking stream owned by the filter). */
 ff_status ff_filter_set_stream(ff_filter* f, void* stream);

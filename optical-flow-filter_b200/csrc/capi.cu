@@ -286,6 +286,39 @@ ff_status ff_filter_set_graphs(ff_filter* f, int enabled) {
     return guard([&] { get(f)->set_graphs(enabled != 0); });
 }
 
+ff_status ff_filter_autotune(ff_filter* f, int repetitions) {
+    return guard([&] { get(f)->autotune(repetitions); });
+}
+
+ff_status ff_filter_get_level_tuning(const ff_filter* f, int level, int* path, int* band) {
+    return guard([&] {
+        need(path, "path");
+        need(band, "band");
+        const ffb::Level& v = cget(f)->level(level);
+        *path = v.tuned_path;
+        *band = v.tuned_band;
+    });
+}
+
+ff_status ff_filter_set_level_tuning(ff_filter* f, int level, int path, int band) {
+    return guard([&] {
+        if (path < -1 || path > 1) throw Error(FF_ERR_INVALID_ARGUMENT, "path must be -1, 0 or 1");
+        if (band < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "band rows must be >= 0");
+        get(f)->set_level_tuning(level, path, band);
+    });
+}
+
+ff_status ff_filter_tuning(const ff_filter* f, char* buf, size_t len) {
+    return guard([&] {
+        need(buf, "buffer");
+        const std::string t = cget(f)->tuning();
+        if (len == 0) throw Error(FF_ERR_INVALID_ARGUMENT, "empty buffer");
+        const size_t n = t.size() < len - 1 ? t.size() : len - 1;
+        std::memcpy(buf, t.data(), n);
+        buf[n] = 0;
+    });
+}
+
 ff_status ff_filter_set_band(ff_filter* f, int rows) {
     return guard([&] {
         if (rows < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "band rows must be >= 0");
@@ -302,6 +335,13 @@ ff_status ff_filter_level_kernel_ms(ff_filter* f, int level, float* total_ms, in
         need(total_ms, "total");
         need(frames, "frames");
         get(f)->level_kernel_ms(level, total_ms, frames);
+    });
+}
+
+ff_status ff_filter_time_level(ff_filter* f, int level, int reps, void* flush, size_t flush_bytes, float* total_ms) {
+    return guard([&] {
+        need(total_ms, "total");
+        *total_ms = get(f)->time_level(level, reps, flush, flush_bytes);
     });
 }
 

@@ -223,6 +223,7 @@ float Filter::gamma(int l) const { return level(l).gamma; }
 // pyramids halve per level, top = maxflow / 2^(L-1) (flowfilter.cu:849-866)
 void Filter::set_max_flow(float m) {
     drop_graphs();
+    for (Level& v : lv_) v.tuned_path = -1;
     float ml = m;
     std::vector<float> per(L_);
     if (L_ == 1) {
@@ -246,6 +247,7 @@ float Filter::max_flow() const { return lv_[0].maxflow; }
 
 void Filter::set_smooth(int l, int n) {
     drop_graphs();
+    for (Level& v : lv_) v.tuned_path = -1;
     Level& v = level(l);
     if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "smooth iterations should be greater than zero: " + std::to_string(n));
     v.smooth = n;
@@ -411,62 +413,236 @@ void Filter::step_level_unfused(int l, cudaStream_t s) {
     update_unfused(l, s);
 }
 
-void Filter::step_level(int l, cudaStream_t s) {
-    Level& v = lv_[l];
-    if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+// can the fused kernel run this level (instantiated, aligned image rows, coarse flow)?
+bool Filter::fused_ok(int l) const {
+    const Level& v = lv_[l];
     // the fused kernels stage rows with 4- and 8-byte cp.async copies: the image rows must
     // be aligned, and uint8 rows readable up to the next multiple of 4 bytes
     const uintptr_t ib = (uintptr_t)v.img;
     const bool img_ok = v.item == 1 ? (ib % 4 == 0 && v.img_pitch % 4 == 0 && (v.img_owned || v.W % 4 == 0))
                                     : (ib % 8 == 0 && v.img_pitch % 8 == 0 &&
                                        (v.img_owned || v.W % 2 == 0 || v.img_pitch >= (size_t)(v.W + 1) * 4));
-    const void* cpp = nullptr;
-    size_t cpitch = 0;
-    int chh = 0, cww = 0;
-    if (v.delta) coarse_of(l, &cpp, &cpitch, &chh, &cww);
-    const bool coarse_ok = !v.delta || ((uintptr_t)cpp % 8 == 0 && cpitch % 8 == 0);
-    // mode 2 (automatic): small levels are latency-bound in the streaming kernel (few
-    // warps, long serial rows) and run faster as per-stage kernels
-    const bool want_fused = fused_mode_ == 1 || (fused_mode_ == 2 && (long)v.H * v.W >= kFusedMinPixels);
-    if (want_fused && img_ok && coarse_ok && fused_available(v.delta, v.item, v.iters, v.smooth)) {
-        const int nxt = cur_ ^ 1;
-        LevelArgs a{};
-        a.H = v.H;
-        a.W = v.W;
-        a.item = v.item;
-        a.img = v.img;
-        a.img_pitch = v.img_pitch;
-        a.fs_in = (const float*)v.fs[cur_].p;
-        a.fs_in_pitch = v.fs[cur_].pitch;
-        a.io_in = (const float*)v.io[cur_].p;
-        a.io_in_pitch = v.io[cur_].pitch;
-        a.fs_out = (float*)v.fs[nxt].p;
-        a.fs_out_pitch = v.fs[nxt].pitch;
-        a.io_out = (float*)v.io[nxt].p;
-        a.io_out_pitch = v.io[nxt].pitch;
-        if (v.delta) {
-            a.d_in = (const float*)v.d[cur_].p;
-            a.d_in_pitch = v.d[cur_].pitch;
-            a.d_out = (float*)v.d[nxt].p;
-            a.d_out_pitch = v.d[nxt].pitch;
-            const void* cp;
-            coarse_of(l, &cp, &a.coarse_pitch, &a.Hc, &a.Wc);
-            if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
-            a.coarse = (const float*)cp;
-            a.coarse_rows = (const int*)v.coarse_rows.p;
-        } else {
-            a.fu_out = (float*)v.fu.p;
-            a.fu_out_pitch = v.fu.pitch;
-        }
-        a.gamma = v.gamma;
-        a.maxflow = v.maxflow;
-        a.border = v.border;
-        a.first = v.first ? 1 : 0;
-        a.band = band_;
-        check_cuda(launch_fused_level(v.delta, v.iters, v.smooth, a, s), "fused level");
-    } else {
-        step_level_unfused(l, s);
+    bool coarse_ok = true;
+    if (v.delta) {
+        const void* cpp = nullptr;
+        size_t cpitch = 0;
+        int chh = 0, cww = 0;
+        coarse_of(l, &cpp, &cpitch, &chh, &cww);
+        coarse_ok = cpp && (uintptr_t)cpp % 8 == 0 && cpitch % 8 == 0;
     }
+    return img_ok && coarse_ok && fused_available(v.delta, v.item, v.iters, v.smooth);
+}
+
+void Filter::launch_fused(int l, int band, cudaStream_t s) {
+    Level& v = lv_[l];
+    const int nxt = cur_ ^ 1;
+    LevelArgs a{};
+    a.H = v.H;
+    a.W = v.W;
+    a.item = v.item;
+    a.img = v.img;
+    a.img_pitch = v.img_pitch;
+    a.fs_in = (const float*)v.fs[cur_].p;
+    a.fs_in_pitch = v.fs[cur_].pitch;
+    a.io_in = (const float*)v.io[cur_].p;
+    a.io_in_pitch = v.io[cur_].pitch;
+    a.fs_out = (float*)v.fs[nxt].p;
+    a.fs_out_pitch = v.fs[nxt].pitch;
+    a.io_out = (float*)v.io[nxt].p;
+    a.io_out_pitch = v.io[nxt].pitch;
+    if (v.delta) {
+        a.d_in = (const float*)v.d[cur_].p;
+        a.d_in_pitch = v.d[cur_].pitch;
+        a.d_out = (float*)v.d[nxt].p;
+        a.d_out_pitch = v.d[nxt].pitch;
+        const void* cp;
+        coarse_of(l, &cp, &a.coarse_pitch, &a.Hc, &a.Wc);
+        a.coarse = (const float*)cp;
+        a.coarse_rows = (const int*)v.coarse_rows.p;
+    } else {
+        a.fu_out = (float*)v.fu.p;
+        a.fu_out_pitch = v.fu.pitch;
+    }
+    a.gamma = v.gamma;
+    a.maxflow = v.maxflow;
+    a.border = v.border;
+    a.first = v.first ? 1 : 0;
+    a.band = band;
+    check_cuda(launch_fused_level(v.delta, v.iters, v.smooth, a, s), "fused level");
+}
+
+void Filter::step_level(int l, cudaStream_t s) {
+    Level& v = lv_[l];
+    if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
+    if (v.delta) {
+        const void* cp;
+        size_t cpitch;
+        int hc, wc;
+        coarse_of(l, &cp, &cpitch, &hc, &wc);
+        if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
+    }
+    int band = band_;
+    if (uses_fused(l, &band)) launch_fused(l, band, s);
+    else step_level_unfused(l, s);
+}
+
+bool Filter::uses_fused(int l, int* band) const {
+    const Level& v = lv_[l];
+    if (v.tuned_path >= 0 && fused_mode_ == 2) {
+        if (band && v.tuned_band > 0) *band = v.tuned_band;
+        return v.tuned_path == 1 && fused_ok(l);
+    }
+    // mode 2 without tuning: small levels are latency-bound in the streaming kernel
+    // (few warps, long serial rows) and run faster as per-stage kernels
+    const bool want = fused_mode_ == 1 || (fused_mode_ == 2 && (long)v.H * v.W >= kFusedMinPixels);
+    return want && fused_ok(l);
+}
+
+void Filter::autotune(int reps) {
+    if (reps < 1) throw Error(FF_ERR_INVALID_ARGUMENT, "autotune repetitions must be >= 1");
+    for (const Level& v : lv_)
+        if (v.first) throw Error(FF_ERR_LOGIC, "autotune needs at least one computed frame");
+    check_cuda(cudaEventSynchronize(done_), "autotune");
+    drop_graphs();
+    // the top level's unsmoothed flow is a result (getFlow) and an input of level L-2:
+    // keep this frame's copy and restore it afterwards
+    Buf keep;
+    Level& top = lv_[L_ - 1];
+    if (!top.delta && top.fu.p) {
+        keep.alloc(top.fu.h, top.fu.w, top.fu.bpp);
+        check_cuda(cudaMemcpy2DAsync(keep.p, keep.pitch, top.fu.p, top.fu.pitch, top.fu.row_bytes(), top.fu.h,
+                                     cudaMemcpyDeviceToDevice, stream_), "autotune");
+    }
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    // candidates are timed as captured graphs of `reps` level steps, as the frame step
+    // replays them, so launch gaps do not penalise the multi-kernel per-stage path
+    auto time_it = [&](auto&& run) {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        try {
+            for (int k = 0; k < reps; ++k) run(cap_);
+        } catch (...) {
+            cudaStreamEndCapture(cap_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        check_cuda(cudaStreamEndCapture(cap_, &g), "cudaStreamEndCapture");
+        cudaError_t e = cudaGraphInstantiateWithFlags(&ge, g, 0);
+        cudaGraphDestroy(g);
+        check_cuda(e, "cudaGraphInstantiate");
+        check_cuda(cudaGraphLaunch(ge, stream_), "cudaGraphLaunch");  // warm-up
+        check_cuda(cudaEventRecord(e0, stream_), "cudaEventRecord");
+        check_cuda(cudaGraphLaunch(ge, stream_), "cudaGraphLaunch");
+        check_cuda(cudaEventRecord(e1, stream_), "cudaEventRecord");
+        check_cuda(cudaEventSynchronize(e1), "autotune");
+        cudaGraphExecDestroy(ge);
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+        return ms;
+    };
+    // top level first: level L-2 reads its unsmoothed flow
+    for (int l = L_ - 1; l >= 0; --l) {
+        Level& v = lv_[l];
+        v.alloc_scratch();  // allocations cannot happen inside a capture
+        float best = time_it([&](cudaStream_t st) { step_level_unfused(l, st); });
+        int path = 0, band = 0;
+        if (fused_ok(l)) {
+            const int auto_rows = 0;
+            const int rows[] = {auto_rows, 8, 16, 24, 32, 48, 64, 96, 128};
+            for (int b : rows) {
+                if (b > v.H) continue;
+                const float t = time_it([&](cudaStream_t st) { launch_fused(l, b, st); });
+                if (t < best) {
+                    best = t;
+                    path = 1;
+                    band = b;
+                }
+            }
+        }
+        v.tuned_path = path;
+        v.tuned_band = band;
+    }
+    if (keep.p) {
+        check_cuda(cudaMemcpy2DAsync(top.fu.p, top.fu.pitch, keep.p, keep.pitch, top.fu.row_bytes(), top.fu.h,
+                                     cudaMemcpyDeviceToDevice, stream_), "autotune");
+    }
+    check_cuda(cudaStreamSynchronize(stream_), "autotune");
+    keep.release();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    end_on(stream_);
+}
+
+float Filter::time_level(int l, int reps, void* flush, size_t flush_bytes) {
+    level(l);
+    if (reps < 1) throw Error(FF_ERR_INVALID_ARGUMENT, "repetitions must be >= 1");
+    for (const Level& v : lv_)
+        if (v.first) throw Error(FF_ERR_LOGIC, "timing a level needs at least one computed frame");
+    check_cuda(cudaEventSynchronize(done_), "time_level");
+    Level& top = lv_[L_ - 1];
+    Buf keep;
+    if (!top.delta && top.fu.p) {  // getFlow() result / coarse input: restored afterwards
+        keep.alloc(top.fu.h, top.fu.w, top.fu.bpp);
+        check_cuda(cudaMemcpy2DAsync(keep.p, keep.pitch, top.fu.p, top.fu.pitch, top.fu.row_bytes(), top.fu.h,
+                                     cudaMemcpyDeviceToDevice, stream_), "time_level");
+    }
+    if (!uses_fused(l, nullptr)) lv_[l].alloc_scratch();
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        step_level(l, cap_);
+    } catch (...) {
+        cudaStreamEndCapture(cap_, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(cap_, &g), "cudaStreamEndCapture");
+    cudaError_t e = cudaGraphInstantiateWithFlags(&ge, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(e, "cudaGraphInstantiate");
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps);
+    for (auto& x : ev) check_cuda(cudaEventCreate(&x), "cudaEventCreate");
+    check_cuda(cudaGraphLaunch(ge, stream_), "cudaGraphLaunch");  // warm-up
+    for (int k = 0; k < reps; ++k) {
+        if (flush && flush_bytes) check_cuda(cudaMemsetAsync(flush, k & 0xff, flush_bytes, stream_), "flush");
+        check_cuda(cudaEventRecord(ev[2 * k], stream_), "cudaEventRecord");
+        check_cuda(cudaGraphLaunch(ge, stream_), "cudaGraphLaunch");
+        check_cuda(cudaEventRecord(ev[2 * k + 1], stream_), "cudaEventRecord");
+    }
+    check_cuda(cudaEventSynchronize(ev.back()), "time_level");
+    float total = 0.f;
+    for (int k = 0; k < reps; ++k) {
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]), "cudaEventElapsedTime");
+        total += ms;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    cudaGraphExecDestroy(ge);
+    if (keep.p)
+        check_cuda(cudaMemcpy2DAsync(top.fu.p, top.fu.pitch, keep.p, keep.pitch, top.fu.row_bytes(), top.fu.h,
+                                     cudaMemcpyDeviceToDevice, stream_), "time_level");
+    check_cuda(cudaStreamSynchronize(stream_), "time_level");
+    keep.release();
+    end_on(stream_);
+    return total;
+}
+
+std::string Filter::tuning() const {
+    std::string out;
+    for (int l = 0; l < L_; ++l) {
+        const Level& v = lv_[l];
+        out += "level " + std::to_string(l) + ": " +
+               (v.tuned_path < 0 ? std::string("untuned")
+                                 : v.tuned_path == 0 ? std::string("per-stage")
+                                                     : "fused band " + (v.tuned_band ? std::to_string(v.tuned_band)
+                                                                                     : std::string("auto"))) +
+               (l + 1 < L_ ? "; " : "");
+    }
+    return out;
 }
 
 // One frame's launches on `s` for the current state parity.  Levels 0..L-3 do not
@@ -521,6 +697,9 @@ void Filter::compute_async(cudaStream_t s) {
     if (graphs_ && !any_first && prof_count_ >= prof_cap_) {
         cudaGraphExec_t& ge = graph_exec_[cur_];
         if (!ge) {
+            // per-stage levels need their scratch before the capture (no allocation inside it)
+            for (int l = 0; l < L_; ++l)
+                if (!uses_fused(l, nullptr)) lv_[l].alloc_scratch();
             // capture this parity's frame once; the buffers it names alternate per frame
             check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
             try {

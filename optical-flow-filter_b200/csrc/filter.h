@@ -61,6 +61,8 @@ struct Level {
     int smooth = 1;
     int border = 3;
     bool first = true;
+    int tuned_path = -1;         // autotuned: -1 not tuned, 0 per-stage, 1 fused
+    int tuned_band = 0;          // autotuned band rows of the fused kernel (0 automatic)
     Buf coarse_rows;             // int per row: coarse row its update reads (delta levels)
     void build_coarse_rows();
     // scratch of the unfused path (allocated on first use)
@@ -128,6 +130,17 @@ public:
         drop_graphs();
     }
     static constexpr long kFusedMinPixels = 200000;
+    // time every candidate kernel configuration of each level on the current inputs and
+    // keep the fastest (re-running a level step rewrites bit-identical outputs)
+    void autotune(int reps);
+    float time_level(int l, int reps, void* flush, size_t flush_bytes);
+    std::string tuning() const;
+    void set_level_tuning(int l, int path, int band) {
+        Level& v = level(l);
+        v.tuned_path = path;
+        v.tuned_band = band;
+        drop_graphs();
+    }
     // replay each parity's frame from a captured CUDA graph
     void set_graphs(bool on);
     // record per-level kernel events for the next `frames` computes
@@ -145,6 +158,9 @@ private:
     void drop_graphs();
     void release_runtime();
     void step_level(int l, cudaStream_t s);
+    bool fused_ok(int l) const;
+    bool uses_fused(int l, int* band) const;
+    void launch_fused(int l, int band, cudaStream_t s);
     void step_level_unfused(int l, cudaStream_t s);
     void model_unfused(int l, cudaStream_t s);
     void propagate_unfused(int l, cudaStream_t s);

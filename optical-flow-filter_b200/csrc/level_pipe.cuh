@@ -31,6 +31,13 @@ namespace lvl {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerBlock = 4;
+#ifndef FFB_ROW_UNROLL
+#define FFB_ROW_UNROLL 1  // rows per loop body (2 saves the 2-row window moves, doubles code)
+#endif
+#ifndef FFB_BLOCKS_PER_SM
+#define FFB_BLOCKS_PER_SM 2
+#endif
+constexpr int kBlocksPerSM = FFB_BLOCKS_PER_SM;  // resident blocks per SM the register budget targets
 
 // lane-constant geometry and arguments of one warp
 struct Ctx {
@@ -517,8 +524,16 @@ __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int
     }
     // one row per iteration, not unrolled: the loop body must stay small enough for the
     // instruction cache; the windows rotate by register moves and the slot index cycles
+#if FFB_ROW_UNROLL == 2
+#pragma unroll 1
+    for (int it = 0; it < iters; it += 2) {
+        pipe.step(c, a, i0 + it, it & (kDepth - 1));
+        pipe.step(c, a, i0 + it + 1, (it + 1) & (kDepth - 1));
+    }
+#else
 #pragma unroll 1
     for (int it = 0; it < iters; ++it) pipe.step(c, a, i0 + it, it & (kDepth - 1));
+#endif
     cp_wait<0>();
 }
 
@@ -527,7 +542,7 @@ __host__ __device__ constexpr int halo_x(int N, int S) { return ((2 * S + (N > 2
 __host__ __device__ constexpr int lead_rows(int N, int S) { return 2 * S + (N > 4 - N ? N : 4 - N); }
 
 template <bool DELTA, int N, int S, typename P>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) level_k(LevelArgs a, int nwx, int nby, int band) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int nby, int band) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
     extern __shared__ __align__(16) char smem_raw[];
@@ -577,7 +592,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) level_k(LevelArgs a, int 
     c.any_split = __any_sync(kFull, c.cc0 != c.b0 || c.cc1 != c.b0 + 1);
     const int i0 = c.ys - lead_rows(N, S);
     const int last = c.ye - 1 + N + 2 * S;
-    const int iters = (last - i0 + 1 + 3) & ~3;
+    const int iters = (last - i0 + 1 + 1) & ~1;  // even: the loop body holds two rows
     // interior warps: no clamping, substitution or border freeze can reach them
     const int m = (a.border > 2 ? a.border : 2) + 1;
     const int rlo = i0 - N - 2 * S - 2, rhi = i0 + iters + 2;

@@ -94,8 +94,13 @@ SIGNATURES = {
     "ff_filter_set_fused": (_st, [_vp, _i]),
     "ff_filter_set_graphs": (_st, [_vp, _i]),
     "ff_filter_set_band": (_st, [_vp, _i]),
+    "ff_filter_autotune": (_st, [_vp, _i]),
+    "ff_filter_tuning": (_st, [_vp, ctypes.c_char_p, _sz]),
+    "ff_filter_get_level_tuning": (_st, [_vp, _i, _ip, _ip]),
+    "ff_filter_set_level_tuning": (_st, [_vp, _i, _i, _i]),
     "ff_filter_set_profiling": (_st, [_vp, _i]),
     "ff_filter_level_kernel_ms": (_st, [_vp, _i, _fp, _ip]),
+    "ff_filter_time_level": (_st, [_vp, _i, _i, _vp, _sz, _fp]),
     "ff_filter_set_stream": (_st, [_vp, _vp]),
     "ff_filter_load_image_host": (_st, [_vp, ctypes.POINTER(FFImage)]),
     "ff_filter_load_image_device_async": (_st, [_vp, _vp, _sz, _vp]),

@@ -184,6 +184,39 @@ class _FilterBase:
         """Replay the frame step from captured CUDA graphs (one per state parity)."""
         call("ff_filter_set_graphs", self._h, 1 if enabled else 0)
 
+    def autotune(self, repetitions: int = 5) -> str:
+        """Time each level's kernel choices on the current inputs and keep the fastest;
+        returns the choice per level.  Needs one computed frame; results are unchanged."""
+        call("ff_filter_autotune", self._h, int(repetitions))
+        return self.tuning()
+
+    def tuningState(self) -> list:
+        """[(path, band)] per level: path -1 untuned, 0 per-stage, 1 fused."""
+        out = []
+        for l in range(self._shape()[2]):
+            p, b = ctypes.c_int(), ctypes.c_int()
+            call("ff_filter_get_level_tuning", self._h, l, ctypes.byref(p), ctypes.byref(b))
+            out.append((p.value, b.value))
+        return out
+
+    def setTuningState(self, state) -> None:
+        for l, (p, b) in enumerate(state):
+            call("ff_filter_set_level_tuning", self._h, l, int(p), int(b))
+
+    def tuning(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        call("ff_filter_tuning", self._h, buf, 512)
+        return buf.value.decode()
+
+    def timeLevel(self, level: int, reps: int = 100, flush=None) -> float:
+        """Mean device milliseconds of one level step in its current configuration, replayed
+        as a captured graph; ``flush`` (a CUDA tensor) is overwritten before every launch."""
+        ms = ctypes.c_float()
+        fp = ctypes.c_void_p(flush.data_ptr()) if flush is not None else None
+        nb = flush.numel() * flush.element_size() if flush is not None else 0
+        call("ff_filter_time_level", self._h, int(level), int(reps), fp, nb, ctypes.byref(ms))
+        return ms.value / reps
+
     def setBand(self, rows: int) -> None:
         """Rows per warp band of the fused kernels (0 = automatic)."""
         call("ff_filter_set_band", self._h, int(rows))

@@ -280,3 +280,49 @@ def test_graphs_side_streams_and_profiling(ffb, cuda, levels):
         np.testing.assert_array_equal(g.getFlow(), ref.getFlow())
     ms, n = g.levelKernelTime(0)
     assert n == 3 and ms > 0.0
+
+
+def test_autotune_keeps_results(ffb, cuda):
+    """Autotuning re-runs level steps on live data; the sequence is unchanged by it."""
+    h, w = 272, 512
+    frames = case_frames(dict(seq="bumps", frames=7, kw=dict(height=h, width=w, sigma=1.0, seed=31, n_bumps=3,
+                                                              bump_sigma=60.0, amp=2.0)))
+    ref = ffb.PyramidalFlowFilter(h, w, 3)
+    tun = ffb.PyramidalFlowFilter(h, w, 3)
+    for f in (ref, tun):
+        f.gamma = [5.0, 20.0, 50.0]
+        f.smoothIterations = [1, 2, 4]
+        f.maxflow = 4.0
+    ref.setFused(0)
+    for t in range(7):
+        ref.loadImage(frames[t]); ref.compute()
+        tun.loadImage(frames[t]); tun.compute()
+        if t == 2:
+            with pytest.raises(ValueError):
+                tun.autotune(0)
+            choice = tun.autotune(2)
+            assert choice.count("level") == 3 and "untuned" not in choice
+            tun.setGraphs(True)
+        np.testing.assert_array_equal(tun.getFlow(), ref.getFlow())
+        np.testing.assert_array_equal(tun.getFlowDevice().cpu().numpy(), ref.getFlowDevice().cpu().numpy())
+    fresh = ffb.PyramidalFlowFilter(h, w, 3)
+    with pytest.raises(RuntimeError):
+        fresh.autotune(1)  # needs one computed frame
+
+
+def test_time_level_keeps_results(ffb, cuda):
+    h, w = 96, 128
+    frames = case_frames(dict(seq="bumps", frames=6, kw=dict(height=h, width=w, sigma=1.0, seed=41, n_bumps=2,
+                                                              bump_sigma=30.0, amp=2.0)))
+    ref = ffb.PyramidalFlowFilter(h, w, 3)
+    tim = ffb.PyramidalFlowFilter(h, w, 3)
+    for f in (ref, tim):
+        f.maxflow = 4.0
+    flush = cuda.empty(1 << 20, dtype=cuda.uint8, device="cuda")
+    for t in range(6):
+        ref.loadImage(frames[t]); ref.compute()
+        tim.loadImage(frames[t]); tim.compute()
+        if t >= 1:
+            for lv in range(3):
+                assert tim.timeLevel(lv, 3, flush if lv == 0 else None) > 0.0
+        np.testing.assert_array_equal(tim.getFlow(), ref.getFlow())
