@@ -227,6 +227,18 @@ ff_status ff_stage_delta_update(const float* a0, size_t a0_pitch, const float* g
 size_t ff_stage_smooth_workspace_size(int height, int width);
 ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int width, int iterations,
                           float* out, size_t out_pitch, void* ws, void* stream);
+/* ff_stage_smooth without a workspace and without any allocation (no counterpart in the
+ * reference, whose FlowSmoother allocates its X-pass scratch image in configure(),
+ * flowsmoothing.cu:59-62). The X-pass scratch is a 32 MiB static device array of the
+ * library, so flows of up to 32 MiB of 512-byte-aligned float2 rows (2048x2048) are
+ * accepted; larger ones fail with FF_ERR_INVALID_ARGUMENT. The scratch needs no initial
+ * contents. It is one array per device: calls that overlap on one device (two streams, or
+ * two threads) race on it; calls queued on one stream do not. Make each device's first
+ * call outside stream capture (it looks the array's address up once per device). For
+ * callers that may not allocate: code running under a frame deadline, where cudaMalloc
+ * would synchronise the device, and hosts whose memory belongs to their own allocator. */
+ff_status ff_stage_smooth_noalloc(const float* flow, size_t flow_pitch, int height, int width, int iterations,
+                                  float* out, size_t out_pitch, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -555,6 +556,65 @@ ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int 
         ffb::check_cuda(ffb::launch_smooth(flow, flow_pitch, height, width, iterations, out, out_pitch, (float*)ws,
                                            ws_pitch(width, 8), (cudaStream_t)stream),
                         "smooth");
+    });
+}
+
+}  // extern "C"
+
+// ---- smoothing on a static device scratch (ff_stage_smooth_noalloc)
+//
+// The X pass of every smoothing iteration writes its float2 field into this module-scope
+// array and the Y pass reads it back, so the entry point needs neither a caller workspace
+// nor an allocation. The array needs no initial contents: every element a Y pass reads
+// was written by the X pass just before it, on the same stream.
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;  // a 2048x2048 float2 field
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_smooth_scratch[kStaticScratchBytes];
+
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_smooth_scratch on the current device, looked up once per device.
+// The first lookup may load this module onto the device, which is not allowed while a
+// stream is being captured, so each device's first call belongs before any capture.
+void* static_scratch() {
+    int dev = 0;
+    ffb::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) throw Error(FF_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        ffb::check_cuda(cudaGetSymbolAddress(&p, g_smooth_scratch), "cudaGetSymbolAddress(static scratch)");
+        if (!p) throw Error(FF_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+        g_scratch_ptr[dev] = p;
+    }
+    return g_scratch_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+ff_status ff_stage_smooth_noalloc(const float* flow, size_t flow_pitch, int height, int width, int iterations,
+                                  float* out, size_t out_pitch, void* stream) {
+    return guard([&] {
+        need(flow, "flow");
+        need(out, "output");
+        check_stage_dims(height, width);
+        if (iterations <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "iterations should be greater than zero");
+        const size_t bytes = ws_pitch(width, 8) * (size_t)height;
+        if (bytes > kStaticScratchBytes)
+            throw Error(FF_ERR_INVALID_ARGUMENT,
+                        "ff_stage_smooth_noalloc: a " + std::to_string(height) + "x" + std::to_string(width) +
+                            " flow needs " + std::to_string(bytes) + " bytes of scratch, above the static " +
+                            std::to_string(kStaticScratchBytes) + " bytes (use ff_stage_smooth with a workspace)");
+        float* tmp = (float*)static_scratch();
+        ffb::check_cuda(ffb::launch_smooth(flow, flow_pitch, height, width, iterations, out, out_pitch, tmp,
+                                           ws_pitch(width, 8), (cudaStream_t)stream),
+                        "smooth (static scratch)");
     });
 }
 

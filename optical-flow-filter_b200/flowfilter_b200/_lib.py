@@ -127,6 +127,7 @@ SIGNATURES = {
                                     _vp, _sz, _vp, _sz, _vp]),
     "ff_stage_smooth_workspace_size": (_sz, [_i, _i]),
     "ff_stage_smooth": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp, _vp]),
+    "ff_stage_smooth_noalloc": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp]),
 }
 
 _lib = None
