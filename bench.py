@@ -2,6 +2,7 @@
 """Throughput benchmark of the flow-filter hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+    python bench.py --profile WORKLOAD --steps K --warmup W     (profiler target only)
 
 A step is one frame of the PyramidalFlowFilter: the frame (already resident in HBM) is
 loaded into the filter and one compute() runs (pyramid, then one fused kernel per
@@ -263,8 +264,10 @@ def tuned(f, w, key=None):
         json.dump(cache, fh, indent=1)
 
 
-def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, tune=True):
-    """Device-timed frames; returns (summed step ms, per-level kernel ms or None, filter)."""
+def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, tune=True, label="timed"):
+    """Device-timed frames; returns (summed step ms, per-level kernel ms or None, filter).
+
+    The timed frames sit inside the NVTX range `label`, so a profiler can select them."""
     import torch
 
     f = make_filter(w)
@@ -279,6 +282,7 @@ def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, 
     if profile:
         f.setProfiling(steps)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.nvtx.range_push(label)
     for k in range(steps):
         flush.zero_()
         ev[k][0].record()
@@ -286,6 +290,7 @@ def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, 
         f.computeAsync()
         ev[k][1].record()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     total = sum(a.elapsed_time(b) for a, b in ev)
     lv = None
     if profile:
@@ -379,7 +384,7 @@ def bench_b200(args):
     dfe = torch.from_numpy(fe).cuda()
     ksteps = min(args.steps, 4000)
     barrier(world)
-    ems, _, efilt = device_run(we, dfe, ksteps, args.warmup, flush)
+    ems, _, efilt = device_run(we, dfe, ksteps, args.warmup, flush, label="timed_extra")
     barrier(world)
     ems = max_over_ranks(world, ems)
     el0 = efilt.timeLevel(0, min(ksteps, 1000), flush)
@@ -476,16 +481,47 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_case(args):
+    """A profiler target: the tuned filter of one workload runs --warmup untimed frames, then
+    --steps frames inside the NVTX range "timed" (L2 flushed before each), and nothing else."""
+    import torch
+
+    w = dict(WORKLOADS[args.profile])
+    w["ring"] = 4
+    frames = make_frames(w)
+    dev = torch.from_numpy(frames).cuda()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    f = make_filter(w)
+    for t in range(args.warmup):
+        f.loadImage(dev[t % 4])
+        f.computeAsync()
+        if t == 1:
+            tuned(f, w)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    for t in range(args.steps):
+        flush.zero_()
+        f.loadImage(dev[t % 4])
+        f.computeAsync()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": args.profile, "frames": args.steps, "kernels": f.tuning()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
+                    help="profiler target: run --steps frames of one workload in the NVTX range 'timed' (no JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.impl == "reference":
+    if args.profile:
+        profile_case(args)
+    elif args.impl == "reference":
         bench_reference(args)
     else:
         bench_b200(args)
