@@ -84,8 +84,9 @@ def level0_kernel_bytes(w):
 
 
 def kernels_per_frame(w, tuning: str) -> int:
-    """Kernel launches of one frame: L-1 pyramid steps, then per level one fused kernel or
-    the per-stage kernels (model, 2N propagation passes, update, 2S smoothing passes)."""
+    """Kernel launches of one frame: L-1 pyramid steps, then per level one fused kernel
+    (streaming or tile) or the per-stage kernels (model, 2N propagation passes, update,
+    2S smoothing passes)."""
     L = w["levels"]
     n = L - 1
     parts = [p.strip() for p in tuning.split(";")]
@@ -93,7 +94,7 @@ def kernels_per_frame(w, tuning: str) -> int:
         m = w["maxflow"] / (2 ** min(l, L - 1))
         N = int(np.ceil(np.float32(m)))
         S = w["smooth"][l]
-        fused = l < len(parts) and "fused" in parts[l]
+        fused = l < len(parts) and ("fused" in parts[l] or "tile" in parts[l])
         n += 1 if fused else 2 + 2 * N + 2 * S
     return n
 

@@ -113,21 +113,24 @@ ff_status ff_filter_set_propagation_border(ff_filter* f, int border);
 ff_status ff_filter_get_propagation_border(const ff_filter* f, int* border);
 ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, int* iterations);
 
-/* Kernel selection per level: 0 per-stage kernels, 1 the fused per-level kernel wherever
- * it is instantiated, 2 automatic (default: fused for levels of at least 200,000 pixels,
- * where it is faster).  All modes give bit-identical results. */
+/* Kernel selection per level: 0 per-stage kernels, 1 the streaming fused per-level kernel
+ * wherever it is instantiated, 2 automatic (default: the autotuned choice, else the
+ * streaming kernel for levels of at least 200,000 pixels and the tile-fused kernel below),
+ * 3 the tile-fused kernel wherever it fits in shared memory.  All modes give bit-identical
+ * results. */
 ff_status ff_filter_set_fused(ff_filter* f, int mode);
 
 /* Replay the frame step from CUDA graphs (one per state buffer parity, captured on first
  * use and re-captured after any parameter change).  Off by default. */
 ff_status ff_filter_set_graphs(ff_filter* f, int enabled);
-/* Autotuner: on the current inputs, time each level's per-stage kernels and its fused
- * kernel at several band heights (`repetitions` runs each) and keep the fastest per
- * level, used while the mode is 2.  Needs one computed frame; results are unchanged
+/* Autotuner: on the current inputs, time each level's per-stage kernels, its streaming
+ * fused kernel at several band heights and its tile-fused kernel at several tile shapes
+ * (`repetitions` runs each) and keep the fastest per level, used while the mode is 2.  Needs one computed frame; results are unchanged
  * because every candidate writes bit-identical outputs.  Parameter changes reset it. */
 ff_status ff_filter_autotune(ff_filter* f, int repetitions);
-/* Read or set one level's kernel choice (path: -1 untuned, 0 per-stage, 1 fused; band rows
- * of the fused kernel, 0 automatic), e.g. to reuse a saved autotuning result. */
+/* Read or set one level's kernel choice (path: -1 untuned, 0 per-stage, 1 streaming fused,
+ * 2 tile-fused; band: rows of a streaming band or the tile-shape index, 0 automatic), e.g.
+ * to reuse a saved autotuning result. */
 ff_status ff_filter_get_level_tuning(const ff_filter* f, int level, int* path, int* band);
 ff_status ff_filter_set_level_tuning(ff_filter* f, int level, int path, int band);
 /* Human-readable summary of the tuned choice per level (NUL-terminated, truncated to len). */

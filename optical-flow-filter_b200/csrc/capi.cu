@@ -278,7 +278,7 @@ ff_status ff_filter_get_propagation_iterations(const ff_filter* f, int level, in
 
 ff_status ff_filter_set_fused(ff_filter* f, int enabled) {
     return guard([&] {
-        if (enabled < 0 || enabled > 2) throw Error(FF_ERR_INVALID_ARGUMENT, "fused mode must be 0, 1 or 2");
+        if (enabled < 0 || enabled > 3) throw Error(FF_ERR_INVALID_ARGUMENT, "fused mode must be 0, 1, 2 or 3");
         get(f)->set_fused(enabled);
     });
 }
@@ -303,8 +303,10 @@ ff_status ff_filter_get_level_tuning(const ff_filter* f, int level, int* path, i
 
 ff_status ff_filter_set_level_tuning(ff_filter* f, int level, int path, int band) {
     return guard([&] {
-        if (path < -1 || path > 1) throw Error(FF_ERR_INVALID_ARGUMENT, "path must be -1, 0 or 1");
+        if (path < -1 || path > 2) throw Error(FF_ERR_INVALID_ARGUMENT, "path must be -1, 0, 1 or 2");
         if (band < 0) throw Error(FF_ERR_INVALID_ARGUMENT, "band rows must be >= 0");
+        if (path == 2 && band >= ffb::tile_config_count())
+            throw Error(FF_ERR_INVALID_ARGUMENT, "tile shape index must be below " + std::to_string(ffb::tile_config_count()));
         get(f)->set_level_tuning(level, path, band);
     });
 }

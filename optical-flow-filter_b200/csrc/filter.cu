@@ -433,8 +433,21 @@ bool Filter::fused_ok(int l) const {
     return img_ok && coarse_ok && fused_available(v.delta, v.item, v.iters, v.smooth);
 }
 
-void Filter::launch_fused(int l, int band, cudaStream_t s) {
-    Level& v = lv_[l];
+bool Filter::tile_ok(int l, int cfg) const {
+    const Level& v = lv_[l];
+    if (v.delta) {
+        const void* cpp = nullptr;
+        size_t cpitch = 0;
+        int chh = 0, cww = 0;
+        coarse_of(l, &cpp, &cpitch, &chh, &cww);
+        if (!cpp || (uintptr_t)cpp % 8 != 0 || cpitch % 8 != 0) return false;
+    }
+    if (v.item == 4 && ((uintptr_t)v.img % 4 != 0 || v.img_pitch % 4 != 0)) return false;
+    return tile_available(v.delta, v.iters, v.smooth, v.W, v.H, cfg);
+}
+
+LevelArgs Filter::level_args(int l) const {
+    const Level& v = lv_[l];
     const int nxt = cur_ ^ 1;
     LevelArgs a{};
     a.H = v.H;
@@ -467,8 +480,19 @@ void Filter::launch_fused(int l, int band, cudaStream_t s) {
     a.maxflow = v.maxflow;
     a.border = v.border;
     a.first = v.first ? 1 : 0;
+    return a;
+}
+
+void Filter::launch_fused(int l, int band, cudaStream_t s) {
+    const Level& v = lv_[l];
+    LevelArgs a = level_args(l);
     a.band = band;
     check_cuda(launch_fused_level(v.delta, v.iters, v.smooth, a, s), "fused level");
+}
+
+void Filter::launch_tile(int l, int cfg, cudaStream_t s) {
+    const Level& v = lv_[l];
+    check_cuda(launch_tile_level(v.delta, v.iters, v.smooth, level_args(l), cfg, s), "tile level");
 }
 
 void Filter::step_level(int l, cudaStream_t s) {
@@ -481,21 +505,46 @@ void Filter::step_level(int l, cudaStream_t s) {
         coarse_of(l, &cp, &cpitch, &hc, &wc);
         if (!cp) throw Error(FF_ERR_LOGIC, "DeltaFlowFilter: input flow not set");
     }
-    int band = band_;
-    if (uses_fused(l, &band)) launch_fused(l, band, s);
-    else step_level_unfused(l, s);
+    int param = 0;
+    switch (path_of(l, &param)) {
+        case kStream: launch_fused(l, param, s); break;
+        case kTile: launch_tile(l, param, s); break;
+        default: step_level_unfused(l, s);
+    }
 }
 
-bool Filter::uses_fused(int l, int* band) const {
+// the path a level step takes now; *param = band rows (streaming) or tile shape (tile)
+int Filter::path_of(int l, int* param) const {
     const Level& v = lv_[l];
-    if (v.tuned_path >= 0 && fused_mode_ == 2) {
-        if (band && v.tuned_band > 0) *band = v.tuned_band;
-        return v.tuned_path == 1 && fused_ok(l);
+    int dummy = 0;
+    int& p = param ? *param : dummy;
+    p = 0;
+    switch (fused_mode_) {
+        case 0: return kPerStage;
+        case 1:
+            p = band_;
+            return fused_ok(l) ? kStream : kPerStage;
+        case 3: return tile_ok(l, 0) ? kTile : kPerStage;
+        default: break;
     }
-    // mode 2 without tuning: small levels are latency-bound in the streaming kernel
-    // (few warps, long serial rows) and run faster as per-stage kernels
-    const bool want = fused_mode_ == 1 || (fused_mode_ == 2 && (long)v.H * v.W >= kFusedMinPixels);
-    return want && fused_ok(l);
+    if (v.tuned_path == kStream && fused_ok(l)) {
+        p = v.tuned_band > 0 ? v.tuned_band : band_;
+        return kStream;
+    }
+    if (v.tuned_path == kTile && tile_ok(l, v.tuned_band)) {
+        p = v.tuned_band;
+        return kTile;
+    }
+    if (v.tuned_path == kPerStage) return kPerStage;
+    // untuned: the streaming kernel keeps large levels in one pass over HBM; below
+    // kFusedMinPixels its warps are few and latency-bound, and the tile kernel spreads
+    // each stage over whole CTAs instead
+    if ((long)v.H * v.W >= kFusedMinPixels && fused_ok(l)) {
+        p = band_;
+        return kStream;
+    }
+    if (tile_ok(l, 0)) return kTile;
+    return kPerStage;
 }
 
 void Filter::autotune(int reps) {
@@ -548,7 +597,7 @@ void Filter::autotune(int reps) {
         Level& v = lv_[l];
         v.alloc_scratch();  // allocations cannot happen inside a capture
         float best = time_it([&](cudaStream_t st) { step_level_unfused(l, st); });
-        int path = 0, band = 0;
+        int path = kPerStage, band = 0;
         if (fused_ok(l)) {
             const int auto_rows = 0;
             const int rows[] = {auto_rows, 8, 16, 24, 32, 48, 64, 96, 128};
@@ -557,9 +606,18 @@ void Filter::autotune(int reps) {
                 const float t = time_it([&](cudaStream_t st) { launch_fused(l, b, st); });
                 if (t < best) {
                     best = t;
-                    path = 1;
+                    path = kStream;
                     band = b;
                 }
+            }
+        }
+        for (int c = 0; c < tile_config_count(); ++c) {
+            if (!tile_ok(l, c)) continue;
+            const float t = time_it([&](cudaStream_t st) { launch_tile(l, c, st); });
+            if (t < best) {
+                best = t;
+                path = kTile;
+                band = c;
             }
         }
         v.tuned_path = path;
@@ -589,7 +647,7 @@ float Filter::time_level(int l, int reps, void* flush, size_t flush_bytes) {
         check_cuda(cudaMemcpy2DAsync(keep.p, keep.pitch, top.fu.p, top.fu.pitch, top.fu.row_bytes(), top.fu.h,
                                      cudaMemcpyDeviceToDevice, stream_), "time_level");
     }
-    if (!uses_fused(l, nullptr)) lv_[l].alloc_scratch();
+    if (path_of(l, nullptr) == kPerStage) lv_[l].alloc_scratch();
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -635,12 +693,20 @@ std::string Filter::tuning() const {
     std::string out;
     for (int l = 0; l < L_; ++l) {
         const Level& v = lv_[l];
-        out += "level " + std::to_string(l) + ": " +
-               (v.tuned_path < 0 ? std::string("untuned")
-                                 : v.tuned_path == 0 ? std::string("per-stage")
-                                                     : "fused band " + (v.tuned_band ? std::to_string(v.tuned_band)
-                                                                                     : std::string("auto"))) +
-               (l + 1 < L_ ? "; " : "");
+        int param = 0;
+        const int path = path_of(l, &param);
+        std::string what;
+        if (path == kStream) {
+            what = "fused band " + (param ? std::to_string(param) : std::string("auto"));
+        } else if (path == kTile) {
+            int tw = 0, th = 0;
+            tile_shape(v.delta, v.iters, v.smooth, v.W, v.H, param, &tw, &th);
+            what = "tile " + std::to_string(tw) + "x" + std::to_string(th);
+        } else {
+            what = "per-stage";
+        }
+        if (v.tuned_path < 0 && fused_mode_ == 2) what += " (untuned)";
+        out += "level " + std::to_string(l) + ": " + what + (l + 1 < L_ ? "; " : "");
     }
     return out;
 }
@@ -699,7 +765,7 @@ void Filter::compute_async(cudaStream_t s) {
         if (!ge) {
             // per-stage levels need their scratch before the capture (no allocation inside it)
             for (int l = 0; l < L_; ++l)
-                if (!uses_fused(l, nullptr)) lv_[l].alloc_scratch();
+                if (path_of(l, nullptr) == kPerStage) lv_[l].alloc_scratch();
             // capture this parity's frame once; the buffers it names alternate per frame
             check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
             try {

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "ffb200.h"
+#include "kernels.h"
 
 namespace ffb {
 
@@ -42,6 +43,9 @@ struct Buf {
 
 enum class Kind { Single = 0, Delta = 1, Pyramidal = 2 };
 
+// how one level step runs
+enum Path { kPerStage = 0, kStream = 1, kTile = 2 };
+
 struct Level {
     bool delta = false;
     int H = 0, W = 0;
@@ -61,8 +65,8 @@ struct Level {
     int smooth = 1;
     int border = 3;
     bool first = true;
-    int tuned_path = -1;         // autotuned: -1 not tuned, 0 per-stage, 1 fused
-    int tuned_band = 0;          // autotuned band rows of the fused kernel (0 automatic)
+    int tuned_path = -1;         // autotuned: -1 not tuned, else a Path
+    int tuned_band = 0;          // streaming kernel: band rows; tile kernel: tile shape (0 automatic)
     Buf coarse_rows;             // int per row: coarse row its update reads (delta levels)
     void build_coarse_rows();
     // scratch of the unfused path (allocated on first use)
@@ -123,8 +127,9 @@ public:
     void download_image(ff_image& out);
     void level_state(int level, int which, void* dst, size_t dst_pitch);
 
-    // 0: per-stage kernels only, 1: fused kernels wherever instantiated, 2: automatic
-    // (fused for levels of at least kFusedMinPixels pixels)
+    // 0: per-stage kernels only, 1: streaming fused kernel wherever instantiated,
+    // 2: automatic (the autotuned choice, else the streaming kernel for levels of at least
+    // kFusedMinPixels pixels and the tile kernel below), 3: tile-fused kernel wherever it fits
     void set_fused(int mode) {
         fused_mode_ = mode;
         drop_graphs();
@@ -159,8 +164,11 @@ private:
     void release_runtime();
     void step_level(int l, cudaStream_t s);
     bool fused_ok(int l) const;
-    bool uses_fused(int l, int* band) const;
+    bool tile_ok(int l, int cfg) const;
+    int path_of(int l, int* param) const;
+    LevelArgs level_args(int l) const;
     void launch_fused(int l, int band, cudaStream_t s);
+    void launch_tile(int l, int cfg, cudaStream_t s);
     void step_level_unfused(int l, cudaStream_t s);
     void model_unfused(int l, cudaStream_t s);
     void propagate_unfused(int l, cudaStream_t s);

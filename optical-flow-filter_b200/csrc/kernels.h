@@ -54,4 +54,10 @@ struct LevelArgs {
 bool fused_available(bool delta, int item, int N, int S);
 cudaError_t launch_fused_level(bool delta, int N, int S, const LevelArgs& a, cudaStream_t s);
 
+// ---- tile-fused per-level kernels (tile_level.cu); cfg 0 = automatic tile shape
+int tile_config_count();
+bool tile_available(bool delta, int N, int S, int W, int H, int cfg);
+void tile_shape(bool delta, int N, int S, int W, int H, int cfg, int* tw, int* th);
+cudaError_t launch_tile_level(bool delta, int N, int S, const LevelArgs& a, int cfg, cudaStream_t s);
+
 }  // namespace ffb

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace ffb {
 namespace lvl {
@@ -546,6 +547,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(Lev
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
     extern __shared__ __align__(16) char smem_raw[];
+    grid_dep_wait();
+    grid_dep_launch();
     const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (warp >= nwx * nby) return;  // whole warps exit together
     const int lane = threadIdx.x & 31;
@@ -630,8 +633,7 @@ cudaError_t launch(const LevelArgs& a, cudaStream_t s) {
     const int nby = (a.H + band - 1) / band;
     const int warps = nwx * nby;
     const int blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    level_k<DELTA, N, S, P><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a, nwx, nby, band);
-    return cudaGetLastError();
+    return launch_k(level_k<DELTA, N, S, P>, dim3(blocks), dim3(kWarpsPerBlock * 32), smem, s, a, nwx, nby, band);
 }
 
 }  // namespace lvl

@@ -4,8 +4,11 @@
 // (ff_stage_*), the phase API of the filters (computeImageModel / Propagation /
 // Update) and every (iterations, smoothing) combination the fused level kernels are
 // not instantiated for.  Results are identical, bit for bit, to the fused kernels.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace ffb {
 
@@ -19,6 +22,8 @@ inline dim3 grid_for(int w, int h) { return dim3((w + BX - 1) / BX, (h + BY - 1)
 // in registers (pyramid_k.cu:14-145).  Output (H/2) x (W/2).
 template <typename P>
 __global__ void pyramid_down_k(CView<P> in, View<P> out) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= out.w || y >= out.h) return;
@@ -42,6 +47,8 @@ __global__ void pyramid_down_k(CView<P> in, View<P> out) {
 // bY = Y-blur, bX = X-blur of the input; a0 = X-blur(bY), ax = X-diff(bY), ay = Y-diff(bX).
 template <typename P>
 __global__ void image_model_k(CView<P> img, View<float> a0, View<float2> grad) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a0.w || y >= a0.h) return;
@@ -73,6 +80,8 @@ __global__ void image_model_k(CView<P> img, View<float> a0, View<float2> grad) {
 template <int AXIS, bool PAYLOAD>
 __global__ void propagate_pass_k(CView<float2> fl, CView<float> sc, CView<float2> ve, View<float2> ofl,
                                  View<float> osc, View<float2> ove, float dt, int border) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int W = ofl.w, H = ofl.h;
@@ -104,6 +113,8 @@ __global__ void propagate_pass_k(CView<float2> fl, CView<float> sc, CView<float2
 // when each pixel is read before it is written (true here: one thread per pixel).
 __global__ void update_k(CView<float> a0, CView<float2> grad, CView<float> a0_old, CView<float2> flow,
                          View<float2> out_flow, View<float> out_image, float gamma, float maxflow, int first) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= out_flow.w || y >= out_flow.h) return;
@@ -121,6 +132,8 @@ __global__ void update_k(CView<float> a0, CView<float2> grad, CView<float> a0_ol
 __global__ void delta_update_k(CView<float> a0, CView<float2> grad, CView<float> a0_old, CView<float2> delta,
                                CView<float2> coarse, View<float2> out_flow, View<float2> out_delta,
                                View<float> out_image, float gamma, float maxflow, int first) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int W = out_flow.w, H = out_flow.h;
@@ -145,6 +158,8 @@ __global__ void delta_update_k(CView<float> a0, CView<float2> grad, CView<float>
 // flowSmooth{X,Y}_k (flowsmoothing_k.cu:21-87)
 template <int AXIS>
 __global__ void smooth_pass_k(CView<float2> in, View<float2> out) {
+    grid_dep_wait();
+    grid_dep_launch();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= out.w || y >= out.h) return;
@@ -163,16 +178,24 @@ CView<T> cv(const View<T>& v) {
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("FFB_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 cudaError_t launch_pyramid_down(const void* in, size_t in_pitch, int item, int H, int W, void* out,
                                 size_t out_pitch, cudaStream_t s) {
     const int h = H / 2, w = W / 2;
     if (h <= 0 || w <= 0) return cudaSuccess;
     if (item == 1) {
-        pyramid_down_k<uint8_t><<<grid_for(w, h), dim3(BX, BY), 0, s>>>(
-            CView<uint8_t>{(const uint8_t*)in, in_pitch, H, W}, View<uint8_t>{(uint8_t*)out, out_pitch, h, w});
+        return launch_k(pyramid_down_k<uint8_t>, grid_for(w, h), dim3(BX, BY), 0, s,
+                        CView<uint8_t>{(const uint8_t*)in, in_pitch, H, W}, View<uint8_t>{(uint8_t*)out, out_pitch, h, w});
     } else {
-        pyramid_down_k<float><<<grid_for(w, h), dim3(BX, BY), 0, s>>>(
-            CView<float>{(const float*)in, in_pitch, H, W}, View<float>{(float*)out, out_pitch, h, w});
+        return launch_k(pyramid_down_k<float>, grid_for(w, h), dim3(BX, BY), 0, s,
+                        CView<float>{(const float*)in, in_pitch, H, W}, View<float>{(float*)out, out_pitch, h, w});
     }
     return cudaGetLastError();
 }
@@ -182,10 +205,10 @@ cudaError_t launch_image_model(const void* img, size_t pitch, int item, int H, i
     View<float> A{a0, a0p, H, W};
     View<float2> G{(float2*)grad, gp, H, W};
     if (item == 1)
-        image_model_k<uint8_t><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(CView<uint8_t>{(const uint8_t*)img, pitch, H, W}, A, G);
-    else
-        image_model_k<float><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(CView<float>{(const float*)img, pitch, H, W}, A, G);
-    return cudaGetLastError();
+        return launch_k(image_model_k<uint8_t>, grid_for(W, H), dim3(BX, BY), 0, s,
+                        CView<uint8_t>{(const uint8_t*)img, pitch, H, W}, A, G);
+    return launch_k(image_model_k<float>, grid_for(W, H), dim3(BX, BY), 0, s,
+                    CView<float>{(const float*)img, pitch, H, W}, A, G);
 }
 
 // N sub-steps ping-ponging between `out` and the workspace `tmp` (same shape as out):
@@ -200,11 +223,15 @@ cudaError_t launch_propagate(const float* flow, size_t fp, int H, int W, int N, 
     View<float2> O{(float2*)out, op, H, W}, T{(float2*)tmp, tp, H, W};
     CView<float2> src{(const float2*)flow, fp, H, W};
     for (int n = 0; n < N; ++n) {
-        propagate_pass_k<0, false><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(src, nsc, nve, T, nosc, nove, dt, border);
-        propagate_pass_k<1, false><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(cv(T), nsc, nve, O, nosc, nove, dt, border);
+        cudaError_t e = launch_k(propagate_pass_k<0, false>, grid_for(W, H), dim3(BX, BY), 0, s, src, nsc, nve, T,
+                                 nosc, nove, dt, border);
+        if (e != cudaSuccess) return e;
+        e = launch_k(propagate_pass_k<1, false>, grid_for(W, H), dim3(BX, BY), 0, s, cv(T), nsc, nve, O, nosc, nove,
+                     dt, border);
+        if (e != cudaSuccess) return e;
         src = cv(O);
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 cudaError_t launch_propagate_payload(const float* flow, size_t fp, const float* sc, size_t sp, const float* ve,
@@ -219,35 +246,37 @@ cudaError_t launch_propagate_payload(const float* flow, size_t fp, const float* 
     CView<float> ss{sc, sp, H, W};
     CView<float2> sv{(const float2*)ve, vp, H, W};
     for (int n = 0; n < N; ++n) {
-        propagate_pass_k<0, true><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(sf, ss, sv, TF, TS, TV, dt, border);
-        propagate_pass_k<1, true><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(cv(TF), cv(TS), cv(TV), OF, OS, OV, dt, border);
+        cudaError_t e = launch_k(propagate_pass_k<0, true>, grid_for(W, H), dim3(BX, BY), 0, s, sf, ss, sv, TF, TS, TV,
+                                 dt, border);
+        if (e != cudaSuccess) return e;
+        e = launch_k(propagate_pass_k<1, true>, grid_for(W, H), dim3(BX, BY), 0, s, cv(TF), cv(TS), cv(TV), OF, OS,
+                     OV, dt, border);
+        if (e != cudaSuccess) return e;
         sf = cv(OF);
         ss = cv(OS);
         sv = cv(OV);
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 cudaError_t launch_update(const float* a0, size_t a0p, const float* grad, size_t gp, const float* old, size_t olp,
                           const float* flow, size_t fp, int H, int W, float gamma, float maxflow, float* of,
                           size_t ofp, float* oi, size_t oip, int first, cudaStream_t s) {
-    update_k<<<grid_for(W, H), dim3(BX, BY), 0, s>>>(
-        CView<float>{a0, a0p, H, W}, CView<float2>{(const float2*)grad, gp, H, W}, CView<float>{old, olp, H, W},
+    return launch_k(
+        update_k, grid_for(W, H), dim3(BX, BY), 0, s, CView<float>{a0, a0p, H, W}, CView<float2>{(const float2*)grad, gp, H, W}, CView<float>{old, olp, H, W},
         CView<float2>{(const float2*)flow, fp, H, W}, View<float2>{(float2*)of, ofp, H, W}, View<float>{oi, oip, H, W},
         gamma, maxflow, first);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_delta_update(const float* a0, size_t a0p, const float* grad, size_t gp, const float* old,
                                 size_t olp, const float* delta, size_t dp, const float* coarse, size_t cp, int Hc,
                                 int Wc, int H, int W, float gamma, float maxflow, float* of, size_t ofp, float* od,
                                 size_t odp, float* oi, size_t oip, int first, cudaStream_t s) {
-    delta_update_k<<<grid_for(W, H), dim3(BX, BY), 0, s>>>(
-        CView<float>{a0, a0p, H, W}, CView<float2>{(const float2*)grad, gp, H, W}, CView<float>{old, olp, H, W},
+    return launch_k(
+        delta_update_k, grid_for(W, H), dim3(BX, BY), 0, s, CView<float>{a0, a0p, H, W}, CView<float2>{(const float2*)grad, gp, H, W}, CView<float>{old, olp, H, W},
         CView<float2>{(const float2*)delta, dp, H, W}, CView<float2>{(const float2*)coarse, cp, Hc, Wc},
         View<float2>{(float2*)of, ofp, H, W}, View<float2>{(float2*)od, odp, H, W}, View<float>{oi, oip, H, W}, gamma,
         maxflow, first);
-    return cudaGetLastError();
 }
 
 // S iterations: X: in -> tmp, Y: tmp -> out, X: out -> tmp, ...
@@ -256,11 +285,13 @@ cudaError_t launch_smooth(const float* flow, size_t fp, int H, int W, int S, flo
     View<float2> O{(float2*)out, op, H, W}, T{(float2*)tmp, tp, H, W};
     CView<float2> src{(const float2*)flow, fp, H, W};
     for (int k = 0; k < S; ++k) {
-        smooth_pass_k<0><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(src, T);
-        smooth_pass_k<1><<<grid_for(W, H), dim3(BX, BY), 0, s>>>(cv(T), O);
+        cudaError_t e = launch_k(smooth_pass_k<0>, grid_for(W, H), dim3(BX, BY), 0, s, src, T);
+        if (e != cudaSuccess) return e;
+        e = launch_k(smooth_pass_k<1>, grid_for(W, H), dim3(BX, BY), 0, s, cv(T), O);
+        if (e != cudaSuccess) return e;
         src = cv(O);
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 }  // namespace ffb

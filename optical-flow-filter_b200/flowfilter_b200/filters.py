@@ -176,8 +176,10 @@ class _FilterBase:
         return out
 
     def setFused(self, mode) -> None:
-        """Kernel selection: False/0 per-stage kernels, True/1 fused per-level kernels, 2 automatic
-        (the default: fused for levels of at least 200,000 pixels).  Results are identical."""
+        """Kernel selection: False/0 per-stage kernels, True/1 streaming fused per-level kernels,
+        2 automatic (the default: the autotuned choice, else the streaming kernel for levels
+        of at least 200,000 pixels and the tile-fused kernel below), 3 tile-fused kernels.
+        Results are identical."""
         call("ff_filter_set_fused", self._h, int(mode))
 
     def setGraphs(self, enabled: bool) -> None:
@@ -191,7 +193,8 @@ class _FilterBase:
         return self.tuning()
 
     def tuningState(self) -> list:
-        """[(path, band)] per level: path -1 untuned, 0 per-stage, 1 fused."""
+        """[(path, band)] per level: path -1 untuned, 0 per-stage, 1 streaming fused (band =
+        rows per band, 0 automatic), 2 tile-fused (band = tile-shape index, 0 automatic)."""
         out = []
         for l in range(self._shape()[2]):
             p, b = ctypes.c_int(), ctypes.c_int()

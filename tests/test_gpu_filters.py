@@ -29,7 +29,7 @@ def make_gpu_filter(ffb, case, h, w):
     return f
 
 
-def run_gpu(f, frames, dump, fused=True):
+def run_gpu(f, frames, dump, fused=1):
     f.setFused(fused)
     out = []
     for t in range(frames.shape[0]):
@@ -40,15 +40,17 @@ def run_gpu(f, frames, dump, fused=True):
     return np.stack(out)
 
 
+@pytest.mark.parametrize("mode", [1, 3])
 @pytest.mark.parametrize("name", list(CASES))
-def test_reference_sequences_bit_exact(ffb, name):
-    """The GPU filter reproduces the reference library's flows bit for bit (sha256 per frame)."""
+def test_reference_sequences_bit_exact(ffb, name, mode):
+    """The GPU filter reproduces the reference library's flows bit for bit (sha256 per frame),
+    with the streaming fused kernel (mode 1) and with the tile-fused kernel (mode 3)."""
     case = CASES[name]
     meta, arr = golden_case(name)
     frames = case_frames(case)
     assert sha(frames) == meta["frames_sha256"]
     f = make_gpu_filter(ffb, case, *frames.shape[1:])
-    flows = run_gpu(f, frames, set(case["dump"]))
+    flows = run_gpu(f, frames, set(case["dump"]), mode)
     if meta["layout"] == "full":
         got = flows
     else:
@@ -96,7 +98,7 @@ def gpu_filter(ffb, case):
 
 
 @pytest.mark.parametrize("case", RANDOM_CASES)
-@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("fused", [1, 0, 3])
 def test_against_oracle(ffb, case, fused):
     h, w = case[:2]
     frames = case_frames(dict(seq="bumps", frames=12, kw=dict(height=h, width=w, sigma=1.0, seed=h * w,
@@ -326,3 +328,57 @@ def test_time_level_keeps_results(ffb, cuda):
             for lv in range(3):
                 assert tim.timeLevel(lv, 3, flush if lv == 0 else None) > 0.0
         np.testing.assert_array_equal(tim.getFlow(), ref.getFlow())
+
+
+TILE_CASES = [
+    # (kind, h, w, item, maxflow, smooth, border)
+    ("single", 37, 53, 1, 4.0, 2, 3),
+    ("single", 120, 200, 4, 3.0, 4, 0),
+    ("single", 5, 3, 1, 1.0, 1, 3),
+    ("delta", 66, 90, 1, 4.0, 1, 3),
+    ("delta", 97, 131, 4, 6.0, 3, 2),
+    ("delta", 240, 320, 1, 2.0, 4, 3),
+]
+
+
+@pytest.mark.parametrize("case", TILE_CASES)
+def test_tile_kernel_matches_per_stage(ffb, cuda, case):
+    """The tile-fused kernel against the per-stage kernels, every tile shape, on FlowFilter
+    and standalone DeltaFlowFilter over uint8 and float images."""
+    kind, h, w, item, maxflow, smooth, border = case
+    rng = np.random.default_rng(h * w + item)
+    frames = case_frames(dict(seq="bumps", frames=5, kw=dict(height=h, width=w, sigma=1.0, seed=h + w, n_bumps=2,
+                                                              bump_sigma=max(h, w) / 3, amp=2.0)))
+    if item == 4:
+        frames = (frames.astype(np.float32) / 255.0).astype(np.float32)
+    coarse = cuda.from_numpy(rng.normal(0, 0.7, (max(h // 2, 1), max(w // 2, 1), 2)).astype(np.float32)).cuda()
+    imgs = [cuda.from_numpy(frames[0]).cuda() for _ in range(2)]
+
+    def make(img):
+        f = ffb.DeltaFlowFilter(img, coarse) if kind == "delta" else ffb.FlowFilter.on_device(img)
+        f.gamma = 10.0
+        f.maxflow = maxflow
+        f.smoothIterations = smooth
+        f.propagationBorder = border
+        return f
+
+    ref = make(imgs[0])
+    ref.setFused(0)
+    tiles = []
+    for c in range(64):  # every tile-shape index the library accepts
+        f = make(imgs[1])
+        try:
+            f.setTuningState([(2, c)])
+        except ValueError:
+            break
+        tiles.append((c, f))
+    assert len(tiles) > 3
+    for t in range(frames.shape[0]):
+        for img in imgs:
+            img.copy_(cuda.from_numpy(frames[t]))
+        ref.compute()
+        want = ref.getFlow()
+        for c, f in tiles:
+            f.compute()
+            np.testing.assert_array_equal(f.getFlow(), want, err_msg=f"tile shape {c} frame {t} ({f.tuning()})")
+            np.testing.assert_array_equal(f.getImage(), ref.getImage())
