@@ -80,11 +80,15 @@ __device__ __forceinline__ T* growm(void* base, size_t pitch, int y) {
 // in an array of row stride `stride` whose (xa, ya) element is k0.  load(x, y, k) reads a
 // pixel's inputs and done(x, y, k, in) computes and stores; two rows are visited per
 // iteration with both loads issued before either store, so their latencies overlap.
+// Every loop bound is uniform across the warp: in the last column chunk the lanes past
+// xb repeat column xb - 1, computing and storing the same value as the lane that owns it,
+// so no lane diverges.
 template <typename Load, typename Done>
 __device__ __forceinline__ void walk(int xa, int xb, int ya, int yb, int stride, int k0, Load&& load, Done&& done) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int dk = nw * stride;
-    for (int x = xa + lane; x < xb; x += 32) {
+    for (int cx = xa; cx < xb; cx += 32) {
+        const int x = min(cx + lane, xb - 1);
         int y = ya + w;
         int k = k0 + (x - xa) + w * stride;
         for (; y + nw < yb; y += 2 * nw, k += 2 * dk) {
@@ -162,6 +166,23 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
     const int ox = x0 - g.R, oy = y0 - g.R;  // state region origin (may lie outside the image)
     const int SW = g.SW, NS = g.SW * g.SH;
     const int B = a.border;
+    // kernel parameters used per pixel, held in registers
+    const float2* __restrict__ fs_in = reinterpret_cast<const float2*>(a.fs_in);
+    const float2* __restrict__ d_in = reinterpret_cast<const float2*>(a.d_in);
+    const float* __restrict__ io_in = a.io_in;
+    const size_t fs_in_p = a.fs_in_pitch, d_in_p = a.d_in_pitch, io_in_p = a.io_in_pitch;
+    const P* __restrict__ img_in = reinterpret_cast<const P*>(a.img);
+    const size_t img_p = a.img_pitch;
+    const float2* __restrict__ coarse = reinterpret_cast<const float2*>(a.coarse);
+    const size_t coarse_p = a.coarse_pitch;
+    const int* __restrict__ coarse_rows = a.coarse_rows;
+    float* const d_out = a.d_out;
+    float* const io_out = a.io_out;
+    float* const fu_out = a.fu_out;
+    float* const fs_out = a.fs_out;
+    const size_t d_out_p = a.d_out_pitch, io_out_p = a.io_out_pitch, fu_out_p = a.fu_out_pitch,
+                 fs_out_p = a.fs_out_pitch;
+    const bool first = a.first != 0;
 
     float2* fA = reinterpret_cast<float2*>(sm);
     float2* fB = reinterpret_cast<float2*>(sm + g.offB);
@@ -189,10 +210,10 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
             xa(g.R), xb(g.R), ya(g.R), yb(g.R), SW, sidx(xa(g.R), ya(g.R)),
             [&](int x, int y, int) {
                 In v;
-                v.f = __ldg(grow<float2>(a.fs_in, a.fs_in_pitch, y) + x);
+                v.f = __ldg(grow<float2>(fs_in, fs_in_p, y) + x);
                 if constexpr (DELTA) {
-                    v.d = __ldg(grow<float2>(a.d_in, a.d_in_pitch, y) + x);
-                    v.i = __ldg(grow<float>(a.io_in, a.io_in_pitch, y) + x);
+                    v.d = __ldg(grow<float2>(d_in, d_in_p, y) + x);
+                    v.i = __ldg(grow<float>(io_in, io_in_p, y) + x);
                 }
                 return v;
             },
@@ -248,7 +269,7 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
     auto iidx = [&](int x, int y) { return (y - y0 + rI) * IW + (x - x0 + rI); };
     walk(
         xa(rI), xb(rI), ya(rI), yb(rI), IW, iidx(xa(rI), ya(rI)),
-        [&](int x, int y, int) { return __ldg(grow<P>(a.img, a.img_pitch, y) + x); },
+        [&](int x, int y, int) { return __ldg(grow<P>(img_in, img_p, y) + x); },
         [&](int, int, int k, P v) { img[k] = Pix<P>::get(v); });
     if constexpr (DELTA) {
         for (int x = xa(S2) + (int)threadIdx.x; x < xb(S2); x += blockDim.x) ccol[x - x0 + S2] = upmap_index(x, W, a.Wc);
@@ -317,10 +338,10 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
                 if constexpr (DELTA) {
                     u.old = iA[k];
                     u.f = dA[k];
-                    const int cr = __ldg(a.coarse_rows + y);
-                    u.up = __ldg(grow<float2>(a.coarse, a.coarse_pitch, cr) + ccol[x - x0 + S2]);
+                    const int cr = __ldg(coarse_rows + y);
+                    u.up = __ldg(grow<float2>(coarse, coarse_p, cr) + ccol[x - x0 + S2]);
                 } else {
-                    u.old = __ldg(grow<float>(a.io_in, a.io_in_pitch, y) + x);
+                    u.old = __ldg(grow<float>(io_in, io_in_p, y) + x);
                     u.f = fA[k];
                 }
                 return u;
@@ -329,7 +350,7 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
                 const float c = smooth5(u.b0, u.b1, u.b2, u.b3, u.b4);
                 const float ax = diff5(u.b0, u.b1, u.b2, u.b3, u.b4);
                 const float ay = diff5(u.c0, u.c1, u.c2, u.c3, u.c4);
-                const float old = a.first ? c : u.old;
+                const float old = first ? c : u.old;
                 const bool out = x >= x0 && x < x1 && y >= y0 && y < y1;
                 float fx, fy;
                 solve2(gamma, ax, ay, __fsub_rn(old, c), u.f.x, u.f.y, fx, fy);
@@ -342,16 +363,16 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
                     const float gy = __fadd_rn(dy, __fmul_rn(2.0f, u.up.y));
                     fA[k] = make_float2(clampm(gx, maxflow), clampm(gy, maxflow));
                     if (out) {
-                        growm<float2>(a.d_out, a.d_out_pitch, y)[x] = make_float2(dx, dy);
-                        growm<float>(a.io_out, a.io_out_pitch, y)[x] = c;
+                        growm<float2>(d_out, d_out_p, y)[x] = make_float2(dx, dy);
+                        growm<float>(io_out, io_out_p, y)[x] = c;
                     }
                 } else {
                     // flowUpdate_k (update_k.cu:15-79); the old image is the previous frame's a0
                     const float2 o = make_float2(sanitize(clampm(fx, maxflow)), sanitize(clampm(fy, maxflow)));
                     fA[k] = o;
                     if (out) {
-                        if (a.fu_out) growm<float2>(a.fu_out, a.fu_out_pitch, y)[x] = o;
-                        growm<float>(a.io_out, a.io_out_pitch, y)[x] = c;
+                        if (fu_out) growm<float2>(fu_out, fu_out_p, y)[x] = o;
+                        growm<float>(io_out, io_out_p, y)[x] = c;
                     }
                 }
             });
@@ -390,7 +411,7 @@ __global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
             },
             [&](int x, int y, int k, const Five& f) {
                 const float2 o = box5_2(f);
-                if (last) growm<float2>(a.fs_out, a.fs_out_pitch, y)[x] = o;
+                if (last) growm<float2>(fs_out, fs_out_p, y)[x] = o;
                 else fA[k] = o;
             });
         if (!last) __syncthreads();
