@@ -1,0 +1,528 @@
+// C++ drop-in classes (include/flowfilter/...) over the C ABI of libffb200.so.
+//
+// Each class keeps the reference's names, arguments and error types; all device work is
+// done by the ff_* entry points.  Built as libflowfilter_gpu.so, the library name the
+// reference's callers link against.
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <stdexcept>
+#include <string>
+
+#include "ffb200.h"
+#include "flowfilter/gpu/flowfilter.h"
+#include "flowfilter/gpu/image.h"
+#include "flowfilter/gpu/imagemodel.h"
+#include "flowfilter/gpu/pipeline.h"
+
+// flowfilter::image_t is passed to the C ABI as an ff_image: same fields, same layout
+static_assert(sizeof(flowfilter::image_t) == sizeof(ff_image), "image_t / ff_image size");
+static_assert(offsetof(flowfilter::image_t, height) == offsetof(ff_image, height), "image_t.height");
+static_assert(offsetof(flowfilter::image_t, width) == offsetof(ff_image, width), "image_t.width");
+static_assert(offsetof(flowfilter::image_t, depth) == offsetof(ff_image, depth), "image_t.depth");
+static_assert(offsetof(flowfilter::image_t, pitch) == offsetof(ff_image, pitch), "image_t.pitch");
+static_assert(offsetof(flowfilter::image_t, itemSize) == offsetof(ff_image, itemSize), "image_t.itemSize");
+static_assert(offsetof(flowfilter::image_t, data) == offsetof(ff_image, data), "image_t.data");
+
+namespace flowfilter {
+namespace gpu {
+
+namespace {
+
+// ff_status -> the exception type the reference throws for the same condition
+void check(ff_status s, const char* where) {
+    if (s == FF_OK) return;
+    const std::string msg = std::string(where) + ": " + ff_last_error();
+    switch (s) {
+        case FF_ERR_INVALID_ARGUMENT:
+        case FF_ERR_SHAPE: throw std::invalid_argument(msg);
+        case FF_ERR_OUT_OF_RANGE: throw std::out_of_range(msg);
+        case FF_ERR_LOGIC: throw std::logic_error(msg);
+        default: throw std::runtime_error(msg);
+    }
+}
+
+ff_image* as_ff(flowfilter::image_t& img) { return reinterpret_cast<ff_image*>(&img); }
+
+void require(ff_filter* f, const char* where) {
+    if (!f) throw std::logic_error(std::string(where) + ": the filter has not been configured");
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ GPUImage
+GPUImage::GPUImage() = default;
+
+GPUImage::GPUImage(const int height, const int width, const int depth, const int itemSize) {
+    if (height <= 0 || width <= 0 || depth <= 0 || itemSize <= 0)
+        throw std::invalid_argument("GPUImage: height, width, depth and itemSize must be positive");
+    h_ = (std::size_t)height;
+    w_ = (std::size_t)width;
+    depth_ = (std::size_t)depth;
+    item_ = (std::size_t)itemSize;
+    void* p = nullptr;
+    check(ff_malloc_pitch(&p, &pitch_, w_ * depth_ * item_, h_), "GPUImage");
+    buf_ = std::shared_ptr<void>(p, [](void* q) { ff_free(q); });
+    clear();
+}
+
+GPUImage::~GPUImage() = default;
+
+int GPUImage::height() const { return (int)h_; }
+int GPUImage::width() const { return (int)w_; }
+int GPUImage::depth() const { return (int)depth_; }
+int GPUImage::pitch() const { return (int)pitch_; }
+int GPUImage::itemSize() const { return (int)item_; }
+void* GPUImage::data() { return buf_.get(); }
+std::shared_ptr<void> GPUImage::getDeviceBuffer() { return buf_; }
+
+bool GPUImage::compareShape(const flowfilter::image_t& img) const {
+    return (std::size_t)img.height == h_ && (std::size_t)img.width == w_ && (std::size_t)img.depth == depth_ &&
+           img.itemSize == item_;
+}
+
+bool GPUImage::compareShapeGPU(const flowfilter::gpu::GPUImage& img) const {
+    return img.h_ == h_ && img.w_ == w_ && img.depth_ == depth_ && img.item_ == item_;
+}
+
+void GPUImage::upload(flowfilter::image_t& img) {
+    if (!compareShape(img)) throw std::invalid_argument("GPUImage::upload(): shapes do not match");
+    check(ff_memcpy2d(buf_.get(), pitch_, img.data, img.pitch, w_ * depth_ * item_, h_, 0), "GPUImage::upload");
+}
+
+void GPUImage::download(flowfilter::image_t& img) const {
+    if (!compareShape(img)) throw std::invalid_argument("GPUImage::download(): shapes do not match");
+    check(ff_memcpy2d(img.data, img.pitch, buf_.get(), pitch_, w_ * depth_ * item_, h_, 1), "GPUImage::download");
+}
+
+void GPUImage::copyFrom(flowfilter::gpu::GPUImage& img) {
+    if (!compareShapeGPU(img)) throw std::invalid_argument("GPUImage::copyFrom(): shapes do not match");
+    check(ff_memcpy2d(buf_.get(), pitch_, img.buf_.get(), img.pitch_, w_ * depth_ * item_, h_, 2),
+          "GPUImage::copyFrom");
+}
+
+void GPUImage::clear() {
+    if (buf_) check(ff_memset2d(buf_.get(), pitch_, 0, w_ * depth_ * item_, h_), "GPUImage::clear");
+}
+
+// ------------------------------------------------------------------ Stage
+struct Stage::Events {
+    cudaEvent_t start = nullptr, stop = nullptr;
+    ~Events() {
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+    }
+};
+
+Stage::Stage() = default;
+Stage::Stage(void* stream) : stream_(stream) {}
+Stage::~Stage() = default;
+
+void Stage::startTiming() {
+    if (!events_) {
+        auto e = std::make_shared<Events>();
+        if (cudaEventCreate(&e->start) != cudaSuccess || cudaEventCreate(&e->stop) != cudaSuccess)
+            throw std::runtime_error("Stage: cudaEventCreate failed");
+        events_ = e;
+    }
+    if (cudaEventRecord(events_->start, (cudaStream_t)stream_) != cudaSuccess)
+        throw std::runtime_error("Stage::startTiming(): cudaEventRecord failed");
+}
+
+void Stage::stopTiming() {
+    if (!events_) throw std::logic_error("Stage::stopTiming(): startTiming() was not called");
+    if (cudaEventRecord(events_->stop, (cudaStream_t)stream_) != cudaSuccess ||
+        cudaEventSynchronize(events_->stop) != cudaSuccess ||
+        cudaEventElapsedTime(&elapsed_, events_->start, events_->stop) != cudaSuccess)
+        throw std::runtime_error("Stage::stopTiming(): CUDA event failure");
+}
+
+float Stage::elapsedTime() const { return elapsed_; }
+
+EmptyStage::EmptyStage() = default;
+void EmptyStage::configure() {}
+void EmptyStage::compute() {
+    startTiming();
+    stopTiming();
+}
+
+// ------------------------------------------------------------------ ImageModel
+ImageModel::ImageModel() = default;
+
+ImageModel::ImageModel(GPUImage inputImage) {
+    setInputImage(inputImage);
+    configure();
+}
+
+ImageModel::~ImageModel() = default;
+
+void ImageModel::setInputImage(GPUImage img) {
+    if (img.depth() != 1) throw std::invalid_argument("ImageModel::setInputImage(): input image should have depth 1");
+    if (img.itemSize() != 1 && img.itemSize() != 4)
+        throw std::invalid_argument("ImageModel::setInputImage(): item size should be 1 or 4");
+    input_ = img;
+    configured_ = false;
+}
+
+void ImageModel::configure() {
+    if (!input_.data()) throw std::logic_error("ImageModel::configure(): input image has not been set");
+    constant_ = GPUImage(input_.height(), input_.width(), 1, sizeof(float));
+    gradient_ = GPUImage(input_.height(), input_.width(), 2, sizeof(float));
+    configured_ = true;
+}
+
+void ImageModel::compute() {
+    if (!configured_) throw std::logic_error("ImageModel::compute(): stage not configured");
+    startTiming();
+    check(ff_stage_image_model(input_.data(), input_.pitch(), input_.itemSize(), input_.height(), input_.width(),
+                               (float*)constant_.data(), constant_.pitch(), (float*)gradient_.data(),
+                               gradient_.pitch(), stream_),
+          "ImageModel::compute");
+    stopTiming();
+}
+
+GPUImage ImageModel::getImageConstant() { return constant_; }
+GPUImage ImageModel::getImageGradient() { return gradient_; }
+
+// ------------------------------------------------------------------ FilterHandle
+FilterHandle::~FilterHandle() { reset(nullptr); }
+
+ff_filter* FilterHandle::get() const { return f_; }
+
+void FilterHandle::reset(ff_filter* f) {
+    if (f_) ff_filter_destroy(f_);
+    f_ = f;
+    for (int k = 0; k < 3; ++k) {
+        has_alias_[k] = false;
+        alias_[k] = GPUImage();
+    }
+}
+
+GPUImage FilterHandle::alias(int which, int depth) {
+    if (!has_alias_[which]) {
+        int h = 0, w = 0, l = 0;
+        check(ff_filter_shape(f_, &h, &w, &l), "getFlow");
+        alias_[which] = GPUImage(h, w, depth, sizeof(float));
+        has_alias_[which] = true;
+        refresh();
+    }
+    return alias_[which];
+}
+
+// the filter's current results live in buffers that alternate between frames; the
+// GPUImages handed out keep their own buffer and are brought up to date here
+void FilterHandle::refresh() {
+    for (int k = 0; k < 3; ++k) {
+        if (!has_alias_[k]) continue;
+        void* p = nullptr;
+        std::size_t pitch = 0;
+        check(ff_filter_device_result(f_, k, &p, &pitch), "getFlow");
+        GPUImage& a = alias_[k];
+        check(ff_memcpy2d(a.data(), a.pitch(), p, pitch, (std::size_t)a.width() * a.depth() * a.itemSize(),
+                          a.height(), 2),
+              "getFlow");
+    }
+}
+
+// ------------------------------------------------------------------ FlowFilter
+FlowFilter::FlowFilter() = default;
+
+FlowFilter::FlowFilter(GPUImage inputImage) {
+    setInputImage(inputImage);
+    configure();
+}
+
+FlowFilter::FlowFilter(const int height, const int width) : FlowFilter(height, width, 1, 1.0f, 1.0f) {}
+
+FlowFilter::FlowFilter(const int height, const int width, const int smoothIterations, const float maxflow,
+                       const float gamma) {
+    ff_filter* f = nullptr;
+    check(ff_filter_create(height, width, smoothIterations, maxflow, gamma, &f), "FlowFilter::FlowFilter");
+    h_.reset(f);
+    height_ = height;
+    width_ = width;
+}
+
+FlowFilter::~FlowFilter() = default;
+
+ff_filter* FlowFilter::handle() const {
+    require(h_.get(), "FlowFilter");
+    return h_.get();
+}
+
+void FlowFilter::setInputImage(GPUImage inputImage) {
+    if (inputImage.depth() != 1)
+        throw std::invalid_argument("FlowFilter::setInputImage(): input image should have depth 1, got: " +
+                                    std::to_string(inputImage.depth()));
+    if (inputImage.itemSize() != 1 && inputImage.itemSize() != 4)
+        throw std::invalid_argument("FlowFilter::setInputImage(): item size should be 1 or 4: " +
+                                    std::to_string(inputImage.itemSize()));
+    input_ = inputImage;
+}
+
+void FlowFilter::configure() {
+    if (!input_.data()) {
+        if (h_.get()) return;  // FlowFilter(h, w, ...) owns its input and is configured
+        throw std::logic_error("FlowFilter::configure(): input image has not been set");
+    }
+    ff_filter* f = nullptr;
+    check(ff_filter_create_on_device_image(input_.data(), input_.pitch(), input_.itemSize(), input_.height(),
+                                           input_.width(), &f),
+          "FlowFilter::configure");
+    h_.reset(f);
+    height_ = input_.height();
+    width_ = input_.width();
+}
+
+void FlowFilter::compute() {
+    check(ff_filter_compute(handle()), "FlowFilter::compute");
+    check(ff_filter_elapsed_ms(handle(), &elapsed_), "FlowFilter::compute");
+    h_.refresh();
+}
+
+void FlowFilter::computeImageModel() { check(ff_filter_compute_image_model(handle()), "FlowFilter::computeImageModel"); }
+void FlowFilter::computePropagation() {
+    check(ff_filter_compute_propagation(handle()), "FlowFilter::computePropagation");
+}
+void FlowFilter::computeUpdate() {
+    check(ff_filter_compute_update(handle()), "FlowFilter::computeUpdate");
+    h_.refresh();
+}
+
+GPUImage FlowFilter::getFlow() { return h_.alias(1, 2); }
+
+void FlowFilter::loadImage(flowfilter::image_t& image) {
+    check(ff_filter_load_image_host(handle(), as_ff(image)), "FlowFilter::loadImage");
+}
+void FlowFilter::downloadFlow(flowfilter::image_t& flow) {
+    check(ff_filter_download_flow_host(handle(), as_ff(flow)), "FlowFilter::downloadFlow");
+}
+void FlowFilter::downloadImage(flowfilter::image_t& image) {
+    check(ff_filter_download_image_host(handle(), as_ff(image)), "FlowFilter::downloadImage");
+}
+
+float FlowFilter::getGamma() const {
+    float g = 0.f;
+    check(ff_filter_get_gamma(handle(), 0, &g), "FlowFilter::getGamma");
+    return g;
+}
+void FlowFilter::setGamma(const float gamma) { check(ff_filter_set_gamma(handle(), 0, gamma), "FlowFilter::setGamma"); }
+float FlowFilter::getMaxFlow() const {
+    float m = 0.f;
+    check(ff_filter_get_max_flow(handle(), &m), "FlowFilter::getMaxFlow");
+    return m;
+}
+void FlowFilter::setMaxFlow(const float maxflow) {
+    check(ff_filter_set_max_flow(handle(), maxflow), "FlowFilter::setMaxFlow");
+}
+int FlowFilter::getSmoothIterations() const {
+    int n = 0;
+    check(ff_filter_get_smooth_iterations(handle(), 0, &n), "FlowFilter::getSmoothIterations");
+    return n;
+}
+void FlowFilter::setSmoothIterations(const int N) {
+    check(ff_filter_set_smooth_iterations(handle(), 0, N), "FlowFilter::setSmoothIterations");
+}
+void FlowFilter::setPropagationBorder(const int border) {
+    check(ff_filter_set_propagation_border(handle(), border), "FlowFilter::setPropagationBorder");
+}
+int FlowFilter::getPropagationBorder() const {
+    int b = 0;
+    check(ff_filter_get_propagation_border(handle(), &b), "FlowFilter::getPropagationBorder");
+    return b;
+}
+int FlowFilter::getPropagationIterations() const {
+    int n = 0;
+    check(ff_filter_get_propagation_iterations(handle(), 0, &n), "FlowFilter::getPropagationIterations");
+    return n;
+}
+int FlowFilter::height() const { return height_; }
+int FlowFilter::width() const { return width_; }
+
+// ------------------------------------------------------------------ DeltaFlowFilter
+DeltaFlowFilter::DeltaFlowFilter() = default;
+
+DeltaFlowFilter::DeltaFlowFilter(GPUImage inputImage, GPUImage inputFlow) {
+    setInputImage(inputImage);
+    setInputFlow(inputFlow);
+    configure();
+}
+
+DeltaFlowFilter::~DeltaFlowFilter() = default;
+
+ff_filter* DeltaFlowFilter::handle() const {
+    require(h_.get(), "DeltaFlowFilter");
+    return h_.get();
+}
+
+void DeltaFlowFilter::setInputImage(GPUImage inputImage) {
+    if (inputImage.depth() != 1) throw std::invalid_argument("DeltaFlowFilter::setInputImage(): depth should be 1");
+    if (inputImage.itemSize() != 1 && inputImage.itemSize() != 4)
+        throw std::invalid_argument("DeltaFlowFilter::setInputImage(): item size should be 1 or 4");
+    input_ = inputImage;
+}
+
+void DeltaFlowFilter::setInputFlow(GPUImage inputFlow) {
+    if (inputFlow.depth() != 2 || inputFlow.itemSize() != 4)
+        throw std::invalid_argument("DeltaFlowFilter::setInputFlow(): the flow should be 2 float channels");
+    flow_ = inputFlow;
+}
+
+void DeltaFlowFilter::configure() {
+    if (!input_.data()) throw std::logic_error("DeltaFlowFilter::configure(): input image has not been set");
+    if (!flow_.data()) throw std::logic_error("DeltaFlowFilter::configure(): input flow has not been set");
+    ff_filter* f = nullptr;
+    check(ff_delta_filter_create(input_.data(), input_.pitch(), input_.itemSize(), input_.height(), input_.width(),
+                                 flow_.data(), flow_.pitch(), flow_.height(), flow_.width(), &f),
+          "DeltaFlowFilter::configure");
+    h_.reset(f);
+}
+
+void DeltaFlowFilter::compute() {
+    check(ff_filter_compute(handle()), "DeltaFlowFilter::compute");
+    check(ff_filter_elapsed_ms(handle(), &elapsed_), "DeltaFlowFilter::compute");
+    h_.refresh();
+}
+void DeltaFlowFilter::computeImageModel() {
+    check(ff_filter_compute_image_model(handle()), "DeltaFlowFilter::computeImageModel");
+}
+void DeltaFlowFilter::computePropagation() {
+    check(ff_filter_compute_propagation(handle()), "DeltaFlowFilter::computePropagation");
+}
+void DeltaFlowFilter::computeUpdate() {
+    check(ff_filter_compute_update(handle()), "DeltaFlowFilter::computeUpdate");
+    h_.refresh();
+}
+
+GPUImage DeltaFlowFilter::getFlow() { return h_.alias(1, 2); }
+GPUImage DeltaFlowFilter::getImage() { return h_.alias(2, 1); }
+
+float DeltaFlowFilter::getGamma() const {
+    float g = 0.f;
+    check(ff_filter_get_gamma(handle(), 0, &g), "DeltaFlowFilter::getGamma");
+    return g;
+}
+void DeltaFlowFilter::setGamma(const float gamma) {
+    check(ff_filter_set_gamma(handle(), 0, gamma), "DeltaFlowFilter::setGamma");
+}
+float DeltaFlowFilter::getMaxFlow() const {
+    float m = 0.f;
+    check(ff_filter_get_max_flow(handle(), &m), "DeltaFlowFilter::getMaxFlow");
+    return m;
+}
+void DeltaFlowFilter::setMaxFlow(const float maxflow) {
+    check(ff_filter_set_max_flow(handle(), maxflow), "DeltaFlowFilter::setMaxFlow");
+}
+int DeltaFlowFilter::getSmoothIterations() const {
+    int n = 0;
+    check(ff_filter_get_smooth_iterations(handle(), 0, &n), "DeltaFlowFilter::getSmoothIterations");
+    return n;
+}
+void DeltaFlowFilter::setSmoothIterations(const int N) {
+    check(ff_filter_set_smooth_iterations(handle(), 0, N), "DeltaFlowFilter::setSmoothIterations");
+}
+void DeltaFlowFilter::setPropagationBorder(const int border) {
+    check(ff_filter_set_propagation_border(handle(), border), "DeltaFlowFilter::setPropagationBorder");
+}
+int DeltaFlowFilter::getPropagationBorder() const {
+    int b = 0;
+    check(ff_filter_get_propagation_border(handle(), &b), "DeltaFlowFilter::getPropagationBorder");
+    return b;
+}
+int DeltaFlowFilter::getPropagationIterations() const {
+    int n = 0;
+    check(ff_filter_get_propagation_iterations(handle(), 0, &n), "DeltaFlowFilter::getPropagationIterations");
+    return n;
+}
+int DeltaFlowFilter::height() const { return input_.height(); }
+int DeltaFlowFilter::width() const { return input_.width(); }
+
+// ------------------------------------------------------------------ PyramidalFlowFilter
+PyramidalFlowFilter::PyramidalFlowFilter() = default;
+
+PyramidalFlowFilter::PyramidalFlowFilter(const int height, const int width, const int levels) {
+    ff_filter* f = nullptr;
+    check(ff_pyramidal_create(height, width, levels, &f), "PyramidalFlowFilter::PyramidalFlowFilter");
+    h_.reset(f);
+    height_ = height;
+    width_ = width;
+    levels_ = levels;
+}
+
+PyramidalFlowFilter::~PyramidalFlowFilter() = default;
+
+ff_filter* PyramidalFlowFilter::handle() const {
+    require(h_.get(), "PyramidalFlowFilter");
+    return h_.get();
+}
+
+void PyramidalFlowFilter::configure() { handle(); }
+
+void PyramidalFlowFilter::compute() {
+    check(ff_filter_compute(handle()), "PyramidalFlowFilter::compute");
+    check(ff_filter_elapsed_ms(handle(), &elapsed_), "PyramidalFlowFilter::compute");
+    h_.refresh();
+}
+
+GPUImage PyramidalFlowFilter::getFlow() { return h_.alias(1, 2); }
+
+void PyramidalFlowFilter::loadImage(flowfilter::image_t& image) {
+    check(ff_filter_load_image_host(handle(), as_ff(image)), "PyramidalFlowFilter::loadImage");
+}
+void PyramidalFlowFilter::downloadFlow(flowfilter::image_t& flow) {
+    check(ff_filter_download_flow_host(handle(), as_ff(flow)), "PyramidalFlowFilter::downloadFlow");
+}
+void PyramidalFlowFilter::downloadImage(flowfilter::image_t& image) {
+    check(ff_filter_download_image_host(handle(), as_ff(image)), "PyramidalFlowFilter::downloadImage");
+}
+
+float PyramidalFlowFilter::getGamma(const int level) const {
+    float g = 0.f;
+    check(ff_filter_get_gamma(handle(), level, &g), "PyramidalFlowFilter::getGamma");
+    return g;
+}
+void PyramidalFlowFilter::setGamma(const int level, const float gamma) {
+    check(ff_filter_set_gamma(handle(), level, gamma), "PyramidalFlowFilter::setGamma");
+}
+void PyramidalFlowFilter::setGamma(const std::vector<float>& gamma) {
+    if ((int)gamma.size() != levels_)
+        throw std::invalid_argument("PyramidalFlowFilter::setGamma(): gamma vector should be size " +
+                                    std::to_string(levels_) + ", got: " + std::to_string(gamma.size()));
+    for (int l = 0; l < levels_; ++l) setGamma(l, gamma[l]);
+}
+float PyramidalFlowFilter::getMaxFlow() const {
+    float m = 0.f;
+    check(ff_filter_get_max_flow(handle(), &m), "PyramidalFlowFilter::getMaxFlow");
+    return m;
+}
+void PyramidalFlowFilter::setMaxFlow(const float maxflow) {
+    check(ff_filter_set_max_flow(handle(), maxflow), "PyramidalFlowFilter::setMaxFlow");
+}
+int PyramidalFlowFilter::getSmoothIterations(const int level) const {
+    int n = 0;
+    check(ff_filter_get_smooth_iterations(handle(), level, &n), "PyramidalFlowFilter::getSmoothIterations");
+    return n;
+}
+void PyramidalFlowFilter::setSmoothIterations(const int level, const int N) {
+    check(ff_filter_set_smooth_iterations(handle(), level, N), "PyramidalFlowFilter::setSmoothIterations");
+}
+void PyramidalFlowFilter::setSmoothIterations(const std::vector<int>& iterations) {
+    if ((int)iterations.size() != levels_)
+        throw std::invalid_argument("PyramidalFlowFilter::setSmoothIterations(): vector should be size " +
+                                    std::to_string(levels_) + ", got: " + std::to_string(iterations.size()));
+    for (int l = 0; l < levels_; ++l) setSmoothIterations(l, iterations[l]);
+}
+void PyramidalFlowFilter::setPropagationBorder(const int border) {
+    check(ff_filter_set_propagation_border(handle(), border), "PyramidalFlowFilter::setPropagationBorder");
+}
+int PyramidalFlowFilter::getPropagationBorder() const {
+    int b = 0;
+    check(ff_filter_get_propagation_border(handle(), &b), "PyramidalFlowFilter::getPropagationBorder");
+    return b;
+}
+int PyramidalFlowFilter::height() const { return height_; }
+int PyramidalFlowFilter::width() const { return width_; }
+int PyramidalFlowFilter::levels() const { return levels_; }
+
+}  // namespace gpu
+}  // namespace flowfilter

@@ -94,3 +94,31 @@ def test_memcpy_kind_checked():
     a = np.zeros(4, np.uint8)
     p = a.ctypes.data_as(ctypes.c_void_p)
     assert L.ff_memcpy2d(p, 4, p, 4, 4, 1, 7) == _lib.FF_ERR_INVALID_ARGUMENT
+
+
+def test_cpp_dropin_library_exports_the_reference_classes():
+    """libflowfilter_gpu.so carries the flowfilter::gpu classes the reference's callers link."""
+    import subprocess
+
+    lib = os.path.join(ROOT, "optical-flow-filter_b200", "flowfilter_b200", "libflowfilter_gpu.so")
+    assert os.path.exists(lib)
+    syms = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    for name in ["flowfilter::gpu::GPUImage::upload(", "flowfilter::gpu::GPUImage::download(",
+                 "flowfilter::gpu::ImageModel::getImageGradient()", "flowfilter::gpu::FlowFilter::FlowFilter(int, int)",
+                 "flowfilter::gpu::FlowFilter::FlowFilter(flowfilter::gpu::GPUImage)",
+                 "flowfilter::gpu::FlowFilter::getFlow()", "flowfilter::gpu::FlowFilter::computeUpdate()",
+                 "flowfilter::gpu::DeltaFlowFilter::DeltaFlowFilter(flowfilter::gpu::GPUImage, flowfilter::gpu::GPUImage)",
+                 "flowfilter::gpu::PyramidalFlowFilter::PyramidalFlowFilter(int, int, int)",
+                 "flowfilter::gpu::PyramidalFlowFilter::setGamma(std::vector<float, std::allocator<float> > const&)",
+                 "flowfilter::gpu::PyramidalFlowFilter::setSmoothIterations(int, int)",
+                 "flowfilter::gpu::Stage::elapsedTime() const"]:
+        assert name in syms, name
+
+
+def test_cpp_dropin_headers_compile(tmp_path):
+    import subprocess
+
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "flowfilter/gpu/flowfilter.h"\n#include "flowfilter/gpu/imagemodel.h"\n'
+                   "int main() { flowfilter::image_t t{}; (void)t; return 0; }\n")
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)], check=True)

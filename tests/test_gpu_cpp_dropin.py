@@ -1,0 +1,60 @@
+"""The C++ drop-in classes (include/flowfilter/gpu/*.h, libflowfilter_gpu.so) driven by a
+C++ program the way the reference's demos use the reference classes, against the oracle."""
+
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT
+from make_reference_fixtures import case_frames
+
+pytestmark = pytest.mark.gpu
+
+PKG = os.path.join(ROOT, "optical-flow-filter_b200", "flowfilter_b200")
+
+
+@pytest.fixture(scope="module")
+def program(cuda, tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("dropin") / "dropin_sequence")
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "dropin_sequence.cpp"), "-o", out,
+           "-L", PKG, "-lflowfilter_gpu", "-Wl,-rpath," + PKG]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+@pytest.mark.parametrize("h,w,levels", [(45, 61, 0), (96, 128, 2), (98, 150, 3)])
+def test_cpp_dropin_sequence_matches_oracle(program, tmp_path, h, w, levels):
+    t = 6
+    frames = case_frames(dict(seq="bumps", frames=t, kw=dict(height=h, width=w, sigma=1.0, seed=h + w, n_bumps=2,
+                                                              bump_sigma=max(h, w) / 3, amp=2.0)))
+    fin, fout = tmp_path / "frames.u8", tmp_path / "out.f32"
+    frames.tofile(fin)
+    r = subprocess.run([program, str(fin), str(h), str(w), str(t), str(levels), str(fout)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    got = np.fromfile(fout, np.float32)
+    if levels == 0:
+        of = O.Filter.flowfilter(h, w, 2, 4.0, 10.0)
+    else:
+        of = O.Filter.pyramidal(h, w, levels)
+        of.set_gammas([5.0 * 2 ** l for l in range(levels)])
+        of.set_smooths([1 + l % 3 for l in range(levels)])
+        of.set_max_flow(4.0)
+    n2, n1 = h * w * 2, h * w
+    off = 0
+    for k in range(t):
+        of.load(frames[k])
+        of.compute()
+        np.testing.assert_array_equal(got[off:off + n2].reshape(h, w, 2), of.flow()); off += n2
+        np.testing.assert_array_equal(got[off:off + n2].reshape(h, w, 2), of.get_flow()); off += n2
+        np.testing.assert_array_equal(got[off:off + n1].reshape(h, w), of.image()); off += n1
+    a0, grad = O.image_model(frames[-1])
+    np.testing.assert_array_equal(got[off:off + n1].reshape(h, w), a0); off += n1
+    np.testing.assert_array_equal(got[off:off + n2].reshape(h, w, 2), grad); off += n2
+    assert off == got.size
