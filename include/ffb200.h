@@ -230,6 +230,24 @@ ff_status ff_stage_delta_update(const float* a0, size_t a0_pitch, const float* g
 size_t ff_stage_smooth_workspace_size(int height, int width);
 ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int width, int iterations,
                           float* out, size_t out_pitch, void* ws, void* stream);
+/* ------------------------------------------------------------ batched streams
+ * No counterpart in the reference: many independent PyramidalFlowFilter streams of
+ * different sizes, levels and parameters advanced together.  Stream i's frame is read from
+ * a packed uint8 device buffer at the offset ff_batch_frame_layout gives (rows of width
+ * bytes, no padding); one step runs a fixed number of kernel launches (ff_batch_launches)
+ * whatever the number of streams, and every stream's results equal those of the same
+ * stream filtered alone.  Each stream is an ff_filter owned by the batch (ff_batch_stream):
+ * set its parameters and read its results with the ff_filter_* calls; do not destroy it. */
+typedef struct ff_batch ff_batch;
+ff_status ff_batch_create(int n, const int* heights, const int* widths, const int* levels, ff_batch** batch);
+ff_status ff_batch_destroy(ff_batch* batch);
+ff_status ff_batch_size(const ff_batch* batch, int* n);
+ff_status ff_batch_stream(ff_batch* batch, int index, ff_filter** filter);
+ff_status ff_batch_frame_layout(const ff_batch* batch, size_t* offsets, size_t* total_bytes);
+ff_status ff_batch_launches(const ff_batch* batch, int* launches);
+/* frames: 16-byte aligned device buffer of total_bytes; stream: cudaStream_t (NULL = legacy) */
+ff_status ff_batch_step(ff_batch* batch, const void* frames, void* stream);
+
 /* ff_stage_smooth without a workspace and without any allocation (no counterpart in the
  * reference, whose FlowSmoother allocates its X-pass scratch image in configure(),
  * flowsmoothing.cu:59-62). The X-pass scratch is a 32 MiB static device array of the

@@ -6,9 +6,11 @@
 
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include <new>
 #include <string>
 
+#include "batch.h"
 #include "ffb200.h"
 #include "filter.h"
 #include "kernels.h"
@@ -20,6 +22,13 @@ using ffb::Kind;
 struct ff_filter {
     Filter* impl;
     int device;
+    bool borrowed = false;  // a stream of an ff_batch: owned and destroyed by the batch
+};
+
+struct ff_batch {
+    ffb::Batch* impl;
+    int device;
+    std::vector<ff_filter> streams;
 };
 
 namespace {
@@ -203,6 +212,7 @@ ff_status ff_pyramidal_create(int height, int width, int levels, ff_filter** out
 ff_status ff_filter_destroy(ff_filter* f) {
     return guard([&] {
         if (!f) return;
+        if (f->borrowed) throw Error(FF_ERR_LOGIC, "this filter is a stream of a batch; destroy the batch instead");
         cudaSetDevice(f->device);
         delete f->impl;
         delete f;
@@ -558,6 +568,87 @@ ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int 
         ffb::check_cuda(ffb::launch_smooth(flow, flow_pitch, height, width, iterations, out, out_pitch, (float*)ws,
                                            ws_pitch(width, 8), (cudaStream_t)stream),
                         "smooth");
+    });
+}
+
+}  // extern "C"
+
+// ---- batched step over many streams (batch.h)
+extern "C" {
+
+ff_status ff_batch_create(int n, const int* heights, const int* widths, const int* levels, ff_batch** out) {
+    return guard([&] {
+        need(out, "output handle");
+        *out = nullptr;
+        int dev = 0;
+        ffb::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        ff_batch* b = new ff_batch;
+        try {
+            b->impl = new ffb::Batch(n, heights, widths, levels);
+        } catch (...) {
+            delete b;
+            throw;
+        }
+        b->device = dev;
+        b->streams.resize(n);
+        for (int i = 0; i < n; ++i) {
+            b->streams[i].impl = &b->impl->stream(i);
+            b->streams[i].device = dev;
+            b->streams[i].borrowed = true;
+        }
+        *out = b;
+    });
+}
+
+ff_status ff_batch_destroy(ff_batch* b) {
+    return guard([&] {
+        if (!b) return;
+        cudaSetDevice(b->device);
+        delete b->impl;
+        delete b;
+    });
+}
+
+ff_status ff_batch_size(const ff_batch* b, int* n) {
+    return guard([&] {
+        need(b, "batch");
+        need(n, "count");
+        *n = b->impl->size();
+    });
+}
+
+ff_status ff_batch_stream(ff_batch* b, int i, ff_filter** f) {
+    return guard([&] {
+        need(b, "batch");
+        need(f, "output handle");
+        if (i < 0 || i >= b->impl->size())
+            throw Error(FF_ERR_OUT_OF_RANGE, "batch stream index out of bounds: " + std::to_string(i));
+        *f = &b->streams[i];
+    });
+}
+
+ff_status ff_batch_frame_layout(const ff_batch* b, size_t* offsets, size_t* total) {
+    return guard([&] {
+        need(b, "batch");
+        if (offsets)
+            for (int i = 0; i < b->impl->size(); ++i) offsets[i] = b->impl->frame_offset(i);
+        if (total) *total = b->impl->frame_bytes();
+    });
+}
+
+ff_status ff_batch_launches(const ff_batch* b, int* launches) {
+    return guard([&] {
+        need(b, "batch");
+        need(launches, "count");
+        *launches = b->impl->launches_per_step();
+    });
+}
+
+ff_status ff_batch_step(ff_batch* b, const void* frames, void* stream) {
+    return guard([&] {
+        need(b, "batch");
+        ffb::check_cuda(cudaSetDevice(b->device), "cudaSetDevice");
+        b->impl->step(frames, (cudaStream_t)stream);
     });
 }
 

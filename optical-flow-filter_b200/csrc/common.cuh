@@ -80,6 +80,26 @@ __device__ __forceinline__ uint8_t quantize_u8(float s) {
     return (uint8_t)__float2uint_rz(__fmul_rn(255.0f, s));
 }
 
+// One pixel of the next pyramid level: imageDownX then imageDownY (pyramid_k.cu:14-145),
+// the X-pass value at (2x+k, 2y+j) recomputed in registers.  out is (H/2) x (W/2) of in.
+template <typename P>
+__device__ __forceinline__ void pyramid_px(const CView<P>& in, const View<P>& out, int x, int y) {
+    float xs[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int sy = min(max(2 * y - 1 + j, 0), in.h - 1);  // X-pass image height = in.h
+        float m = Pix<P>::get(in.clamped(2 * x - 1, sy));
+        float c = Pix<P>::get(in.clamped(2 * x, sy));
+        float p = Pix<P>::get(in.clamped(2 * x + 1, sy));
+        float s = down3(m, c, p);
+        if constexpr (sizeof(P) == 1) xs[j] = u8_to_unit(quantize_u8(s));
+        else xs[j] = s;
+    }
+    float s = down3(xs[0], xs[1], xs[2]);
+    if constexpr (sizeof(P) == 1) out.at(x, y) = quantize_u8(s);
+    else out.at(x, y) = s;
+}
+
 // dominant velocity: |v+| - |v-| > 0 ? v+ : v-   (propagation_k.cu:37-40)
 __device__ __forceinline__ float dominant(float vm, float vp) {
     return __fsub_rn(fabsf(vp), fabsf(vm)) > 0.0f ? vp : vm;

@@ -197,7 +197,30 @@ Filter::~Filter() {
 // Every operation on the filter, on whichever stream, starts after the previous one
 // finished (event done_) and marks its own end; blocking calls use the filter's stream.
 void Filter::begin_on(cudaStream_t s) { check_cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent"); }
-void Filter::end_on(cudaStream_t s) { check_cuda(cudaEventRecord(done_, s), "cudaEventRecord"); }
+void Filter::end_on(cudaStream_t s) {
+    check_cuda(cudaEventRecord(done_, s), "cudaEventRecord");
+    ++ops_;
+}
+
+void Filter::wait_done() const { check_cuda(cudaEventSynchronize(done_), "wait"); }
+
+bool Filter::any_first() const {
+    for (const Level& v : lv_)
+        if (v.first) return true;
+    return false;
+}
+
+void Filter::batch_begin(cudaStream_t s) {
+    if (ops_ != batch_seen_) begin_on(s);
+}
+
+void Filter::batch_end(cudaStream_t s) {
+    end_on(s);
+    batch_seen_ = ops_;
+    cur_ ^= 1;
+    for (Level& v : lv_) v.first = false;
+    phase_ = 0;
+}
 
 Level& Filter::level(int l) {
     if (l < 0 || l >= L_) throw Error(FF_ERR_OUT_OF_RANGE, "level index out of bounds: " + std::to_string(l));
@@ -750,6 +773,7 @@ void Filter::enqueue_frame(cudaStream_t s) {
 }
 
 void Filter::drop_graphs() {
+    ++config_gen_;
     for (int k = 0; k < 2; ++k) {
         if (graph_exec_[k]) cudaGraphExecDestroy(graph_exec_[k]);
         graph_exec_[k] = nullptr;

@@ -156,6 +156,20 @@ public:
         drop_graphs();
     }
 
+    // ---- stepping by a Batch (batch.cu), which launches this filter's level steps itself
+    // kernel arguments of level l for the next frame (state copy cur -> cur ^ 1)
+    LevelArgs level_args(int l) const;
+    bool any_first() const;
+    int parity() const { return cur_; }
+    // block until everything queued on the filter so far has finished
+    void wait_done() const;
+    // changes whenever a parameter that shapes the level steps changes
+    unsigned long long config_generation() const { return config_gen_; }
+    // order stream s after this filter's own work queued since the last batch step
+    void batch_begin(cudaStream_t s);
+    // a batch finished this filter's frame on s: record it and advance the state parity
+    void batch_end(cudaStream_t s);
+
 private:
     void enqueue_frame(cudaStream_t s);
     void begin_on(cudaStream_t s);
@@ -166,7 +180,6 @@ private:
     bool fused_ok(int l) const;
     bool tile_ok(int l, int cfg) const;
     int path_of(int l, int* param) const;
-    LevelArgs level_args(int l) const;
     void launch_fused(int l, int band, cudaStream_t s);
     void launch_tile(int l, int cfg, cudaStream_t s);
     void step_level_unfused(int l, cudaStream_t s);
@@ -194,6 +207,9 @@ private:
     cudaEvent_t ev_fork_ = nullptr, ev_pyr_ = nullptr, ev_join_ = nullptr;
     cudaEvent_t done_ = nullptr;   // end of the last operation queued on the filter
     bool graphs_ = false;
+    unsigned long long config_gen_ = 0;  // bumped by drop_graphs (every parameter change)
+    unsigned long long ops_ = 0;         // bumped by end_on
+    unsigned long long batch_seen_ = 0;  // ops_ after the last batch step
     cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
     int prof_cap_ = 0, prof_count_ = 0;
     std::vector<cudaEvent_t> prof_ev_;

@@ -18,8 +18,7 @@ constexpr int BX = 32, BY = 8;
 
 inline dim3 grid_for(int w, int h) { return dim3((w + BX - 1) / BX, (h + BY - 1) / BY); }
 
-// imageDownX then imageDownY fused: the X-pass value at (2x+k, 2y+j) is recomputed
-// in registers (pyramid_k.cu:14-145).  Output (H/2) x (W/2).
+// imageDownX then imageDownY fused (pyramid_px, common.cuh).  Output (H/2) x (W/2).
 template <typename P>
 __global__ void pyramid_down_k(CView<P> in, View<P> out) {
     grid_dep_wait();
@@ -27,20 +26,7 @@ __global__ void pyramid_down_k(CView<P> in, View<P> out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= out.w || y >= out.h) return;
-    float xs[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        const int sy = min(max(2 * y - 1 + j, 0), in.h - 1);  // X-pass image height = in.h
-        float m = Pix<P>::get(in.clamped(2 * x - 1, sy));
-        float c = Pix<P>::get(in.clamped(2 * x, sy));
-        float p = Pix<P>::get(in.clamped(2 * x + 1, sy));
-        float s = down3(m, c, p);
-        if constexpr (sizeof(P) == 1) xs[j] = u8_to_unit(quantize_u8(s));
-        else xs[j] = s;
-    }
-    float s = down3(xs[0], xs[1], xs[2]);
-    if constexpr (sizeof(P) == 1) out.at(x, y) = quantize_u8(s);
-    else out.at(x, y) = s;
+    pyramid_px(in, out, x, y);
 }
 
 // imagePrefilter_k + imageModel_k fused per pixel (imagemodel_k.cu:31-133):

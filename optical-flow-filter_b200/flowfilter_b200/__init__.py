@@ -1,17 +1,19 @@
 """flowfilter_b200 — the Adarve–Mahony optical flow filter's per-frame hot path on B200.
 
 Python face of libffb200.so (include/ffb200.h).  ``FlowFilter``,
-``PyramidalFlowFilter`` and ``DeltaFlowFilter`` mirror the reference's classes; the
+``PyramidalFlowFilter`` and ``DeltaFlowFilter`` mirror the reference's classes;
+``BatchFlowFilter`` advances many independent streams together; the
 ``stages`` module exposes the individual stages on CUDA tensors.
 """
 
 from ._lib import FFError, FFIndexError, FFLogicError, FFValueError, lib  # noqa: F401
-from .filters import DeltaFlowFilter, FlowFilter, PyramidalFlowFilter, device_view  # noqa: F401
+from .filters import BatchFlowFilter, DeltaFlowFilter, FlowFilter, PyramidalFlowFilter, device_view  # noqa: F401
 
 __all__ = [
     "FlowFilter",
     "PyramidalFlowFilter",
     "DeltaFlowFilter",
+    "BatchFlowFilter",
     "FFError",
     "FFValueError",
     "FFIndexError",

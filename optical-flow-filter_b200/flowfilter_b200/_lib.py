@@ -128,6 +128,13 @@ SIGNATURES = {
     "ff_stage_smooth_workspace_size": (_sz, [_i, _i]),
     "ff_stage_smooth": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp, _vp]),
     "ff_stage_smooth_noalloc": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp]),
+    "ff_batch_create": (_st, [_i, _ip, _ip, _ip, _vpp]),
+    "ff_batch_destroy": (_st, [_vp]),
+    "ff_batch_size": (_st, [_vp, _ip]),
+    "ff_batch_stream": (_st, [_vp, _i, _vpp]),
+    "ff_batch_frame_layout": (_st, [_vp, _szp, _szp]),
+    "ff_batch_launches": (_st, [_vp, _ip]),
+    "ff_batch_step": (_st, [_vp, _vp, _vp]),
 }
 
 _lib = None

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import FFImage, call, lib
 
-__all__ = ["FlowFilter", "PyramidalFlowFilter", "DeltaFlowFilter", "device_view"]
+__all__ = ["FlowFilter", "PyramidalFlowFilter", "DeltaFlowFilter", "BatchFlowFilter", "device_view"]
 
 
 def _torch():
@@ -485,3 +485,94 @@ class PyramidalFlowFilter(_FilterBase):
 
     def propagationIterationsAt(self, level: int) -> int:
         return self._get_iters(int(level))
+
+
+class _BatchStream(PyramidalFlowFilter):
+    """One stream of a BatchFlowFilter: a PyramidalFlowFilter owned by the batch."""
+
+    def __init__(self, handle, batch):
+        self._h = handle
+        self._batch = batch  # keeps the batch (and so this stream) alive
+
+    def __del__(self):
+        self._h = None  # the batch destroys its streams
+
+
+class BatchFlowFilter:
+    """Many independent pyramidal streams advanced together (no reference counterpart).
+
+    ``BatchFlowFilter([(height, width, levels), ...])``.  ``stream(i)`` is stream i as a
+    PyramidalFlowFilter (set gamma / smoothIterations / maxflow / propagationBorder, read
+    getFlow() / getFlowDevice()); ``step(frames)`` advances every stream by one frame, where
+    ``frames`` is one uint8 CUDA tensor of ``frameBytes()`` bytes holding stream i's frame
+    at ``frameOffsets()[i]`` (``pack()`` builds it from a list of (H, W) tensors).  A step
+    runs ``launches()`` kernels whatever the number of streams; every stream's results
+    equal those of the same stream filtered alone.
+    """
+
+    def __init__(self, shapes):
+        shapes = [tuple(int(v) for v in s) for s in shapes]
+        n = len(shapes)
+        if n == 0:
+            raise ValueError("a batch needs at least one stream")
+        arr = (ctypes.c_int * n)
+        hs, ws, ls = arr(*[s[0] for s in shapes]), arr(*[s[1] for s in shapes]), arr(*[s[2] for s in shapes])
+        h = ctypes.c_void_p()
+        call("ff_batch_create", n, hs, ws, ls, ctypes.byref(h))
+        self._h = h
+        self.shapes = shapes
+        offs = (ctypes.c_size_t * n)()
+        total = ctypes.c_size_t()
+        call("ff_batch_frame_layout", self._h, offs, ctypes.byref(total))
+        self._offsets = list(offs)
+        self._total = total.value
+        self._streams = []
+        for i in range(n):
+            fh = ctypes.c_void_p()
+            call("ff_batch_stream", self._h, i, ctypes.byref(fh))
+            self._streams.append(_BatchStream(fh, self))
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib._lib is not None:
+            lib().ff_batch_destroy(h)
+
+    def __len__(self) -> int:
+        return len(self.shapes)
+
+    def stream(self, i: int) -> PyramidalFlowFilter:
+        return self._streams[i]
+
+    def frameOffsets(self) -> list:
+        return list(self._offsets)
+
+    def frameBytes(self) -> int:
+        return self._total
+
+    def launches(self) -> int:
+        n = ctypes.c_int()
+        call("ff_batch_launches", self._h, ctypes.byref(n))
+        return n.value
+
+    def pack(self, frames, out=None):
+        """Pack one (H, W) uint8 CUDA tensor per stream into a step buffer (device copies)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self._total, dtype=torch.uint8, device="cuda")
+        for (hh, ww, _), off, f in zip(self.shapes, self._offsets, frames):
+            if tuple(f.shape) != (hh, ww) or f.dtype != torch.uint8:
+                raise ValueError(f"stream frame should be a uint8 tensor of shape {(hh, ww)}")
+            out[off:off + hh * ww].view(hh, ww).copy_(f)
+        return out
+
+    def step(self, frames, stream=None) -> None:
+        """Advance every stream by one frame (enqueued on ``stream``, default the current one)."""
+        torch = _torch()
+        if not (_is_torch(frames) and frames.is_cuda and frames.dtype == torch.uint8 and frames.is_contiguous()
+                and frames.numel() >= self._total):
+            raise ValueError(f"frames should be a contiguous uint8 CUDA tensor of {self._total} bytes")
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        call("ff_batch_step", self._h, ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(stream))

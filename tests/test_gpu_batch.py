@@ -1,0 +1,83 @@
+"""Batched multi-stream step (BatchFlowFilter / ff_batch_*) against each stream filtered alone."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from make_reference_fixtures import case_frames
+
+pytestmark = pytest.mark.gpu
+
+# (height, width, levels, gamma per level, smooth per level, maxflow, border)
+STREAMS = [
+    (48, 64, 1, [7.0], [2], 3.0, 3),
+    (61, 77, 2, [4.0, 30.0], [1, 3], 4.0, 3),
+    (96, 128, 3, [5.0, 20.0, 50.0], [1, 2, 4], 4.0, 2),
+    (120, 160, 2, [10.0, 50.0], [2, 4], 6.0, 3),
+    (33, 45, 1, [2.0], [4], 1.0, 0),
+    (130, 130, 4, [1.0, 2.0, 4.0, 8.0], [1, 1, 2, 3], 8.0, 3),
+]
+
+
+def configure(f, s):
+    h, w, levels, gamma, smooth, maxflow, border = s
+    f.gamma = gamma if levels > 1 else gamma[0]
+    f.smoothIterations = smooth if levels > 1 else smooth[0]
+    f.maxflow = maxflow
+    f.propagationBorder = border
+
+
+@pytest.fixture(scope="module")
+def ffb(cuda):
+    import flowfilter_b200
+
+    return flowfilter_b200
+
+
+def test_batch_matches_streams_alone(ffb, cuda):
+    t_frames = 8
+    seqs = [case_frames(dict(seq="bumps", frames=t_frames, kw=dict(height=s[0], width=s[1], sigma=1.0, seed=11 + i,
+                                                                    n_bumps=2, bump_sigma=max(s[0], s[1]) / 3,
+                                                                    amp=2.0)))
+            for i, s in enumerate(STREAMS)]
+    alone = [ffb.PyramidalFlowFilter(s[0], s[1], s[2]) for s in STREAMS]
+    batch = ffb.BatchFlowFilter([s[:3] for s in STREAMS])
+    for f, b, s in zip(alone, [batch.stream(i) for i in range(len(STREAMS))], STREAMS):
+        configure(f, s)
+        configure(b, s)
+    assert batch.launches() == 1 + (4 - 1) + 2
+    dev = [cuda.from_numpy(q).cuda() for q in seqs]
+    buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
+    for t in range(t_frames):
+        if t == 5:  # a parameter change rebuilds the batch's job tables
+            for f in (alone[2], batch.stream(2)):
+                f.setGamma(1, 7.5)
+            for f in (alone[4], batch.stream(4)):
+                f.maxflow = 2.0
+        batch.pack([d[t] for d in dev], out=buf)
+        batch.step(buf)
+        cuda.cuda.synchronize()
+        for i, f in enumerate(alone):
+            f.loadImage(seqs[i][t])
+            f.compute()
+            np.testing.assert_array_equal(batch.stream(i).getFlow(), f.getFlow(), err_msg=f"stream {i} frame {t}")
+            np.testing.assert_array_equal(batch.stream(i).getImage(), f.getImage(), err_msg=f"stream {i} frame {t}")
+
+
+def test_batch_frame_layout_and_errors(ffb, cuda):
+    from flowfilter_b200 import _lib
+
+    batch = ffb.BatchFlowFilter([(10, 20, 1), (30, 17, 2)])
+    offs = batch.frameOffsets()
+    assert offs[0] == 0 and offs[1] == 256 and batch.frameBytes() == 256 + (30 * 17 + 255) // 256 * 256
+    with pytest.raises(ValueError):
+        batch.step(cuda.empty(batch.frameBytes() - 1, dtype=cuda.uint8, device="cuda"))
+    st = _lib.lib().ff_filter_destroy(batch.stream(0)._h)
+    assert st == _lib.FF_ERR_LOGIC  # streams belong to the batch
+    h = ctypes.c_void_p()
+    assert _lib.lib().ff_batch_stream(batch._h, 2, ctypes.byref(h)) == _lib.FF_ERR_OUT_OF_RANGE
+    with pytest.raises(ValueError):
+        ffb.BatchFlowFilter([])
