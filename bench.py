@@ -10,7 +10,8 @@ level; CUDA-graph replay).  The primary workload is the reference's published
 configuration: 640x480 uint8 frames, 2 levels, gamma [10, 50], smoothing [2, 4],
 maxflow 4, on a synthetic rotation+zoom sequence (seeded) standing in for the
 reference's Blender sequence.  The 2048x1088 3-level throughput workload is reported
-beside it under "extra".
+beside it under "extra", and the 64-stream mixed-size batched step (BatchFlowFilter,
+against the same 64 streams looped as single filters) under "batched".
 
 Timing: every step is bracketed by CUDA events on the filter's stream and the L2 is
 flushed (a 256 MiB write) between steps outside those events, so every frame reads its
@@ -349,6 +350,86 @@ def cpu_port_fps(w, frames, seconds=10.0, max_frames=2000, threads=None):
     O.set_threads(0)
     return n / dt, threads, n
 
+BATCH_SIZES = [(240, 320), (480, 640), (720, 1280), (1080, 1920)]
+BATCH_PER_SIZE = 16
+BATCH_RING = 3
+
+
+def batched_streams(seed=100):
+    """64 streams, 16 at each size: levels in {1,2,3}, gamma log-uniform in [2, 100] per
+    level, smoothing in {1..4} per level, maxflow 4 (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, (h, w) in enumerate(BATCH_SIZES):
+        for _ in range(BATCH_PER_SIZE):
+            levels = int(rng.integers(1, 4))
+            gamma = [float(np.exp(rng.uniform(np.log(2.0), np.log(100.0)))) for _ in range(levels)]
+            smooth = [int(rng.integers(1, 5)) for _ in range(levels)]
+            out.append(dict(H=h, W=w, levels=levels, gamma=gamma, smooth=smooth, maxflow=4.0, size=k))
+    return out
+
+
+def configure_stream(f, s):
+    f.gamma = s["gamma"] if s["levels"] > 1 else s["gamma"][0]
+    f.smoothIterations = s["smooth"] if s["levels"] > 1 else s["smooth"][0]
+    f.maxflow = s["maxflow"]
+
+
+def bench_batched(steps, warmup):
+    """The 64-stream mixed-size step: one BatchFlowFilter step against a loop that runs the
+    64 streams one after another as single-stream filters (graph replay each), both over
+    frames already in HBM.  The 64 streams' state (~1 GB) exceeds L2, so no flush."""
+    import torch
+    from flowfilter_b200 import BatchFlowFilter, PyramidalFlowFilter, synthetic
+
+    streams = batched_streams()
+    seqs = [torch.from_numpy(synthetic.seq_bumps(frames=BATCH_RING, height=h, width=w, seed=100 + k)).cuda()
+            for k, (h, w) in enumerate(BATCH_SIZES)]
+    batch = BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
+    for i, s in enumerate(streams):
+        configure_stream(batch.stream(i), s)
+    packed = [batch.pack([seqs[s["size"]][r] for s in streams]) for r in range(BATCH_RING)]
+
+    def timed(run):
+        for t in range(warmup):
+            run(t)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for t in range(steps):
+            run(warmup + t)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    b_ms = timed(lambda t: batch.step(packed[t % BATCH_RING]))
+    loop = []
+    for s in streams:
+        f = PyramidalFlowFilter(s["H"], s["W"], s["levels"])
+        configure_stream(f, s)
+        loop.append(f)
+
+    def loop_step(t):
+        for s, f in zip(streams, loop):
+            f.loadImage(seqs[s["size"]][t % BATCH_RING])
+            f.computeAsync()
+            if t == 0:
+                f.setGraphs(True)
+
+    l_ms = timed(loop_step)
+    px = sum(s["H"] * s["W"] for s in streams)
+    n = len(streams)
+    return {
+        "workload": f"{n} streams: {BATCH_PER_SIZE} each at " + ", ".join(f"{w}x{h}" for h, w in BATCH_SIZES)
+                    + "; levels 1-3, gamma log-uniform [2,100], smoothing 1-4, maxflow 4 (seed 100)",
+        "value": n * steps / (b_ms / 1e3), "unit": "stream-frames/s", "steps": steps,
+        "ms_per_step": b_ms / steps, "mpix_per_s": px * steps / (b_ms / 1e3) / 1e6,
+        "launches_per_step": batch.launches(),
+        "loop_value": n * steps / (l_ms / 1e3), "loop_ms_per_step": l_ms / steps,
+        "speedup_vs_loop": l_ms / b_ms,
+        "data": "synthetic: one seeded bump-flow sequence per size (seed 100 + size index), shared by that size's streams",
+    }
+
 
 def bench_b200(args):
     import torch
@@ -403,6 +484,11 @@ def bench_b200(args):
                      "traffic": ncu_traffic(EXTRA), "algorithmic_bytes": eb, "launch_ms": el0},
     }
 
+    # ---- the 64-stream batched step (each rank its own batch: replicas)
+    barrier(world)
+    batched = bench_batched(min(args.steps, 200), max(args.warmup, 3))
+    barrier(world)
+
     cpu = None
     if rank == 0 and world == 1:
         fps, cores, n = cpu_port_fps(w, frames)
@@ -435,6 +521,7 @@ def bench_b200(args):
             "gpu_launches": args.steps * launches_per_frame,
             "clocks": clk.summary(),
             "extra": extra,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
