@@ -248,6 +248,45 @@ ff_status ff_batch_launches(const ff_batch* batch, int* launches);
 /* frames: 16-byte aligned device buffer of total_bytes; stream: cudaStream_t (NULL = legacy) */
 ff_status ff_batch_step(ff_batch* batch, const void* frames, void* stream);
 
+/* ------------------------------------------------------------ differentiable stages
+ * No counterpart in the reference: the float-input filter's stages as forward and adjoint
+ * kernels for training (flowfilter_b200.diff builds torch.autograd Functions on them).
+ * dtype 0 = float32, 1 = float64; B images per call, dense [B][H][W] scalar and
+ * [B][H][W][2] vector layouts; gamma and the 5 smoothing weights are device scalars of the
+ * same dtype.  The float32 forward equals the stage kernels above (with weights 0.2, the
+ * reference's box).  Backward calls ADD into their gradient outputs (zero them first) and
+ * take the stage's forward inputs; the upwind, dominant-velocity and clamp branches follow
+ * the forward (zero gradient through a clamped or sanitised value). */
+ff_status ff_diff_pyramid(int dtype, int B, int H, int W, const void* in, void* out, void* stream);
+ff_status ff_diff_pyramid_bwd(int dtype, int B, int H, int W, const void* gout, void* gin, void* stream);
+ff_status ff_diff_model(int dtype, int B, int H, int W, const void* img, void* a0, void* grad, void* stream);
+/* gby, gbx: scratch of B*H*W elements each (cleared here) */
+ff_status ff_diff_model_bwd(int dtype, int B, int H, int W, const void* ga0, const void* ggrad, void* gby, void* gbx,
+                            void* gimg, void* stream);
+/* one sub-step along axis (0 = X, 1 = Y); payload: also advect scalar s and vector v */
+ff_status ff_diff_propagate(int dtype, int B, int H, int W, int axis, int payload, double dt, int border,
+                            const void* f, const void* s, const void* v, void* fo, void* so, void* vo, void* stream);
+ff_status ff_diff_propagate_bwd(int dtype, int B, int H, int W, int axis, int payload, double dt, int border,
+                                const void* f, const void* s, const void* v, const void* gfo, const void* gso,
+                                const void* gvo, void* gf, void* gs, void* gv, void* stream);
+ff_status ff_diff_update(int dtype, int B, int H, int W, const void* a0, const void* grad, const void* old,
+                         const void* fhat, const void* gamma, double maxflow, void* out, void* stream);
+ff_status ff_diff_update_bwd(int dtype, int B, int H, int W, const void* a0, const void* grad, const void* old,
+                             const void* fhat, const void* gamma, double maxflow, const void* gout, void* ga0,
+                             void* ggrad, void* gold, void* gfhat, void* ggamma, void* stream);
+ff_status ff_diff_delta_update(int dtype, int B, int H, int W, int Hc, int Wc, const void* a0, const void* grad,
+                               const void* old, const void* dhat, const void* coarse, const void* gamma,
+                               double maxflow, void* flow, void* delta, void* stream);
+ff_status ff_diff_delta_update_bwd(int dtype, int B, int H, int W, int Hc, int Wc, const void* a0, const void* grad,
+                                   const void* old, const void* dhat, const void* coarse, const void* gamma,
+                                   double maxflow, const void* gflow, const void* gdelta, void* ga0, void* ggrad,
+                                   void* gold, void* gdhat, void* gcoarse, void* ggamma, void* stream);
+/* one weighted 5-tap pass along axis over a vector field (weights w5[0..4]) */
+ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w5, const void* in, void* out,
+                         void* stream);
+ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
+                             const void* gout, void* gin, void* gw5, void* stream);
+
 /* ff_stage_smooth without a workspace and without any allocation (no counterpart in the
  * reference, whose FlowSmoother allocates its X-pass scratch image in configure(),
  * flowsmoothing.cu:59-62). The X-pass scratch is a 32 MiB static device array of the

@@ -86,6 +86,9 @@ void check_stage_dims(int h, int w) {
 
 }  // namespace
 
+// last-error setter for entry points defined in other files (diff_kernels.cu)
+void ffb_set_last_error(const std::string& msg) { g_last_error = msg; }
+
 extern "C" {
 
 const char* ff_last_error(void) { return g_last_error.c_str(); }

@@ -1,0 +1,747 @@
+// Differentiable stages: forward and adjoint (backward) kernels of every stage of the
+// float-input filter, in float and in double, over a batch of B images (no reference
+// counterpart; the forward recurrence is the reference's, float path).
+//
+// Layout: dense arrays, scalar fields [B][H][W], two-channel fields [B][H][W][2].  The float
+// forward kernels repeat the per-stage kernels' arithmetic operation for operation
+// (stage_kernels.cu), so with the default 0.2 smoothing weights the float forward equals the
+// reference.  The smoothing weights (5 per level) and gamma (1 per level) are device
+// scalars, so they can be trained without a host round trip.
+//
+// Backward kernels take the forward inputs (the forward is recomputed locally), follow the
+// branch the forward took at every upwind, dominant-velocity and clamp decision (the
+// gradient of a clamped or sanitised value is zero) and ADD into the input gradients with
+// atomics: gradient buffers start at zero (or hold earlier contributions).  Gradients of the
+// per-level scalars are reduced per block, then added once per block.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "common.cuh"
+#include "ffb200.h"
+#include "kernels.h"
+#include "launch.cuh"
+
+namespace ffb {
+namespace diff {
+
+// ------------------------------------------------------------------ arithmetic per type
+template <typename T>
+struct Ar;
+template <>
+struct Ar<float> {
+    __device__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ static float rcp(float a) { return __frcp_rn(a); }
+    __device__ static bool finite(float a) { return isfinite(a); }
+};
+template <>
+struct Ar<double> {
+    __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ static double rcp(double a) { return __drcp_rn(a); }
+    __device__ static bool finite(double a) { return isfinite(a); }
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+template <typename T>
+__device__ __forceinline__ T down3(T m, T c, T p) {
+    return Ar<T>::fma(T(0.5), c, Ar<T>::mul(T(0.25), Ar<T>::add(m, p)));
+}
+template <typename T>
+__device__ __forceinline__ T chain5(const T* k, T a, T b, T c, T d, T e) {
+    T s = Ar<T>::fma(k[0], a, T(0));
+    s = Ar<T>::fma(k[1], b, s);
+    s = Ar<T>::fma(k[2], c, s);
+    s = Ar<T>::fma(k[3], d, s);
+    return Ar<T>::fma(k[4], e, s);
+}
+template <typename T>
+struct Masks {
+    T s[5], d[5];
+    __device__ Masks() {
+        s[0] = T(0.0625); s[1] = T(0.25); s[2] = T(0.375); s[3] = T(0.25); s[4] = T(0.0625);
+        d[0] = T(-0.125); d[1] = T(-0.25); d[2] = T(0); d[3] = T(0.25); d[4] = T(0.125);
+    }
+};
+template <typename T>
+__device__ __forceinline__ T dominant(T vm, T vp) {
+    return Ar<T>::sub(fabs(vp), fabs(vm)) > T(0) ? vp : vm;
+}
+template <typename T>
+__device__ __forceinline__ T upwind(T t, T dv, T fm, T f0, T fp) {
+    T d = dv >= T(0) ? Ar<T>::sub(f0, fm) : Ar<T>::sub(fp, f0);
+    return Ar<T>::fma(-t, d, f0);
+}
+template <typename T>
+__device__ __forceinline__ T upwind_unfused(T t, T dv, T fm, T f0, T fp) {
+    T d = dv >= T(0) ? Ar<T>::sub(f0, fm) : Ar<T>::sub(fp, f0);
+    return Ar<T>::sub(f0, Ar<T>::mul(t, d));
+}
+template <typename T>
+__device__ __forceinline__ T clampm(T v, T m) {
+    return fmax(-m, fmin(v, m));
+}
+template <typename T>
+__device__ __forceinline__ T sanitize(T v) {
+    return Ar<T>::finite(v) ? v : T(0);
+}
+
+// the 2x2 solve with its intermediates (update_k.cu:43-63)
+template <typename T>
+struct Solve {
+    T n00, n11, n01, rdet, ox, oy;
+    __device__ Solve(T g, T ax, T ay, T yt, T fx, T fy) {
+        n00 = Ar<T>::fma(ay, ay, g);
+        n11 = Ar<T>::fma(ax, ax, g);
+        const T den = Ar<T>::fma(ay, ay, n11);
+        n01 = Ar<T>::mul(-ax, ay);
+        rdet = Ar<T>::rcp(Ar<T>::mul(g, den));
+        const T qx = Ar<T>::fma(g, fx, Ar<T>::mul(ax, yt));
+        const T qy = Ar<T>::fma(ay, yt, Ar<T>::mul(g, fy));
+        const T ix = Ar<T>::fma(n00, qx, Ar<T>::mul(n01, qy));
+        const T iy = Ar<T>::fma(n01, qx, Ar<T>::mul(n11, qy));
+        ox = Ar<T>::mul(ix, rdet);
+        oy = Ar<T>::mul(iy, rdet);
+    }
+};
+
+// adjoint of o = (g I + a a^T)^-1 (g f + a yt) for the output gradient (gx, gy)
+template <typename T>
+struct SolveGrad {
+    T gfx, gfy, gyt, gax, gay, gg;
+    __device__ SolveGrad(const Solve<T>& s, T g, T ax, T ay, T yt, T fx, T fy, T gx, T gy) {
+        const T lx = s.rdet * (s.n00 * gx + s.n01 * gy);
+        const T ly = s.rdet * (s.n01 * gx + s.n11 * gy);
+        gfx = g * lx;
+        gfy = g * ly;
+        gyt = ax * lx + ay * ly;
+        const T oa = s.ox * ax + s.oy * ay, la = lx * ax + ly * ay;
+        gax = yt * lx - lx * oa - s.ox * la;
+        gay = yt * ly - ly * oa - s.oy * la;
+        gg = (fx * lx + fy * ly) - (lx * s.ox + ly * s.oy);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ void atomic_add(T* p, T v) {
+    atomicAdd(p, v);
+}
+
+// block-wide sum of one value per thread, added once per block into *dst
+template <typename T>
+__device__ __forceinline__ void block_add(T v, T* dst) {
+    __shared__ T part[32];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (warp == 0) {
+        T s = lane < nw ? part[lane] : T(0);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) atomicAdd(dst, s);
+    }
+}
+
+#define PIX_SETUP                                              \
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;       \
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;       \
+    const size_t b = blockIdx.z;                               \
+    const bool live = x < W && y < H;
+
+// ------------------------------------------------------------------ pyramid (float path)
+template <typename T>
+__global__ void pyr_fwd_k(const T* __restrict__ in, T* __restrict__ out, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    const int h = H / 2, w = W / 2;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const size_t b = blockIdx.z;
+    if (x >= w || y >= h) return;
+    const T* I = in + b * H * W;
+    T xs[3];
+    for (int j = 0; j < 3; ++j) {
+        const int sy = clampi(2 * y - 1 + j, 0, H - 1);
+        xs[j] = down3(I[sy * W + clampi(2 * x - 1, 0, W - 1)], I[sy * W + clampi(2 * x, 0, W - 1)],
+                      I[sy * W + clampi(2 * x + 1, 0, W - 1)]);
+    }
+    out[(b * h + y) * w + x] = down3(xs[0], xs[1], xs[2]);
+}
+
+template <typename T>
+__global__ void pyr_bwd_k(const T* __restrict__ gout, T* gin, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    const int h = H / 2, w = W / 2;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const size_t b = blockIdx.z;
+    if (x >= w || y >= h) return;
+    const T g = gout[(b * h + y) * w + x];
+    const T wt[3] = {T(0.25), T(0.5), T(0.25)};
+    T* G = gin + b * H * W;
+    for (int j = 0; j < 3; ++j) {
+        const int sy = clampi(2 * y - 1 + j, 0, H - 1);
+        for (int k = 0; k < 3; ++k) atomic_add(&G[sy * W + clampi(2 * x - 1 + k, 0, W - 1)], g * wt[j] * wt[k]);
+    }
+}
+
+// ------------------------------------------------------------------ image model
+template <typename T>
+__global__ void model_fwd_k(const T* __restrict__ img, T* __restrict__ a0, T* __restrict__ grad, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const Masks<T> M;
+    const T* I = img + b * H * W;
+    T by[5], bx[5];
+    for (int c = 0; c < 5; ++c) {
+        const int xc = clampi(x + c - 2, 0, W - 1);
+        T v[5];
+        for (int r = 0; r < 5; ++r) v[r] = I[clampi(y + r - 2, 0, H - 1) * W + xc];
+        by[c] = chain5(M.s, v[0], v[1], v[2], v[3], v[4]);
+    }
+    for (int r = 0; r < 5; ++r) {
+        const int yr = clampi(y + r - 2, 0, H - 1);
+        T v[5];
+        for (int c = 0; c < 5; ++c) v[c] = I[yr * W + clampi(x + c - 2, 0, W - 1)];
+        bx[r] = chain5(M.s, v[0], v[1], v[2], v[3], v[4]);
+    }
+    const size_t k = (b * H + y) * W + x;
+    a0[k] = chain5(M.s, by[0], by[1], by[2], by[3], by[4]);
+    grad[2 * k] = chain5(M.d, by[0], by[1], by[2], by[3], by[4]);
+    grad[2 * k + 1] = chain5(M.d, bx[0], bx[1], bx[2], bx[3], bx[4]);
+}
+
+// step 1: gradients of the Y blur (by, at (x', y)) and of the X blur (bx, at (x, y'))
+template <typename T>
+__global__ void model_bwd1_k(const T* __restrict__ ga0, const T* __restrict__ ggrad, T* gby, T* gbx, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const Masks<T> M;
+    const size_t k = (b * H + y) * W + x;
+    const T g0 = ga0[k], gx = ggrad[2 * k], gy = ggrad[2 * k + 1];
+    T* BY = gby + b * H * W;
+    T* BX = gbx + b * H * W;
+    for (int c = 0; c < 5; ++c) atomic_add(&BY[y * W + clampi(x + c - 2, 0, W - 1)], M.s[c] * g0 + M.d[c] * gx);
+    for (int r = 0; r < 5; ++r) atomic_add(&BX[clampi(y + r - 2, 0, H - 1) * W + x], M.d[r] * gy);
+}
+
+// step 2: by = Y blur of the image, bx = X blur of the image
+template <typename T>
+__global__ void model_bwd2_k(const T* __restrict__ gby, const T* __restrict__ gbx, T* gimg, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const Masks<T> M;
+    const size_t k = (b * H + y) * W + x;
+    const T a = gby[k], c0 = gbx[k];
+    T* G = gimg + b * H * W;
+    for (int r = 0; r < 5; ++r) atomic_add(&G[clampi(y + r - 2, 0, H - 1) * W + x], M.s[r] * a);
+    for (int c = 0; c < 5; ++c) atomic_add(&G[y * W + clampi(x + c - 2, 0, W - 1)], M.s[c] * c0);
+}
+
+// ------------------------------------------------------------------ propagation sub-step
+template <typename T, int AXIS, bool PAYLOAD>
+__global__ void prop_fwd_k(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v, T* __restrict__ fo,
+                           T* __restrict__ so, T* __restrict__ vo, int H, int W, T dt, int border) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const int xm = AXIS == 0 ? max(x - 1, 0) : x, xp = AXIS == 0 ? min(x + 1, W - 1) : x;
+    const int ym = AXIS == 1 ? max(y - 1, 0) : y, yp = AXIS == 1 ? min(y + 1, H - 1) : y;
+    const size_t k = (b * H + y) * W + x, km = (b * H + ym) * W + xm, kp = (b * H + yp) * W + xp;
+    const T fmx = f[2 * km], fmy = f[2 * km + 1], f0x = f[2 * k], f0y = f[2 * k + 1], fpx = f[2 * kp], fpy = f[2 * kp + 1];
+    const T dv = AXIS == 0 ? dominant(fmx, fpx) : dominant(fmy, fpy);
+    const T t = Ar<T>::mul(dt, dv);
+    const bool in = x >= border && x < W - border && y >= border && y < H - border;
+    fo[2 * k] = in ? upwind(t, dv, fmx, f0x, fpx) : f0x;
+    fo[2 * k + 1] = in ? (PAYLOAD ? upwind(t, dv, fmy, f0y, fpy) : upwind_unfused(t, dv, fmy, f0y, fpy)) : f0y;
+    if constexpr (PAYLOAD) {
+        so[k] = in ? upwind(t, dv, s[km], s[k], s[kp]) : s[k];
+        vo[2 * k] = in ? upwind(t, dv, v[2 * km], v[2 * k], v[2 * kp]) : v[2 * k];
+        vo[2 * k + 1] = in ? upwind_unfused(t, dv, v[2 * km + 1], v[2 * k + 1], v[2 * kp + 1]) : v[2 * k + 1];
+    }
+}
+
+// adjoint of one upwind channel: out = g0 - t*(dv >= 0 ? g0 - gm : gp - g0); returns d out / d dv
+template <typename T>
+__device__ __forceinline__ T upwind_grad(T go, T t, T dt, T dv, T gm, T g0, T gp, T* Gm, T* G0, T* Gp) {
+    if (dv >= T(0)) {
+        atomic_add(G0, go * (T(1) - t));
+        atomic_add(Gm, go * t);
+        return -go * dt * (g0 - gm);
+    }
+    atomic_add(G0, go * (T(1) + t));
+    atomic_add(Gp, -go * t);
+    return -go * dt * (gp - g0);
+}
+
+template <typename T, int AXIS, bool PAYLOAD>
+__global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v,
+                           const T* __restrict__ gfo, const T* __restrict__ gso, const T* __restrict__ gvo, T* gf, T* gs,
+                           T* gv, int H, int W, T dt, int border) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const int xm = AXIS == 0 ? max(x - 1, 0) : x, xp = AXIS == 0 ? min(x + 1, W - 1) : x;
+    const int ym = AXIS == 1 ? max(y - 1, 0) : y, yp = AXIS == 1 ? min(y + 1, H - 1) : y;
+    const size_t k = (b * H + y) * W + x, km = (b * H + ym) * W + xm, kp = (b * H + yp) * W + xp;
+    const bool in = x >= border && x < W - border && y >= border && y < H - border;
+    if (!in) {
+        atomic_add(&gf[2 * k], gfo[2 * k]);
+        atomic_add(&gf[2 * k + 1], gfo[2 * k + 1]);
+        if constexpr (PAYLOAD) {
+            atomic_add(&gs[k], gso[k]);
+            atomic_add(&gv[2 * k], gvo[2 * k]);
+            atomic_add(&gv[2 * k + 1], gvo[2 * k + 1]);
+        }
+        return;
+    }
+    const T fmx = f[2 * km], fmy = f[2 * km + 1], f0x = f[2 * k], f0y = f[2 * k + 1], fpx = f[2 * kp], fpy = f[2 * kp + 1];
+    const T vm_ = AXIS == 0 ? fmx : fmy, vp_ = AXIS == 0 ? fpx : fpy;
+    const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
+    const T dv = take_p ? vp_ : vm_;
+    const T t = Ar<T>::mul(dt, dv);
+    T gdv = upwind_grad(gfo[2 * k], t, dt, dv, fmx, f0x, fpx, &gf[2 * km], &gf[2 * k], &gf[2 * kp]);
+    gdv += upwind_grad(gfo[2 * k + 1], t, dt, dv, fmy, f0y, fpy, &gf[2 * km + 1], &gf[2 * k + 1], &gf[2 * kp + 1]);
+    if constexpr (PAYLOAD) {
+        gdv += upwind_grad(gso[k], t, dt, dv, s[km], s[k], s[kp], &gs[km], &gs[k], &gs[kp]);
+        gdv += upwind_grad(gvo[2 * k], t, dt, dv, v[2 * km], v[2 * k], v[2 * kp], &gv[2 * km], &gv[2 * k], &gv[2 * kp]);
+        gdv += upwind_grad(gvo[2 * k + 1], t, dt, dv, v[2 * km + 1], v[2 * k + 1], v[2 * kp + 1], &gv[2 * km + 1],
+                           &gv[2 * k + 1], &gv[2 * kp + 1]);
+    }
+    // the dominant velocity is the chosen neighbour's AXIS component
+    atomic_add(&gf[2 * (take_p ? kp : km) + AXIS], gdv);
+}
+
+// ------------------------------------------------------------------ update (top level)
+template <typename T>
+__global__ void update_fwd_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                             const T* __restrict__ fh, const T* __restrict__ gamma, T* __restrict__ out, int H, int W,
+                             T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const size_t k = (b * H + y) * W + x;
+    const T g = *gamma, c = a0[k];
+    const Solve<T> s(g, grad[2 * k], grad[2 * k + 1], Ar<T>::sub(old[k], c), fh[2 * k], fh[2 * k + 1]);
+    out[2 * k] = sanitize(clampm(s.ox, maxflow));
+    out[2 * k + 1] = sanitize(clampm(s.oy, maxflow));
+}
+
+template <typename T>
+__device__ __forceinline__ bool passes(T o, T m) {
+    return Ar<T>::finite(o) && o < m && o > -m;
+}
+
+template <typename T>
+__global__ void update_bwd_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                             const T* __restrict__ fh, const T* __restrict__ gamma, const T* __restrict__ gout, T* ga0,
+                             T* ggrad, T* gold, T* gfh, T* ggamma, int H, int W, T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    T gg = T(0);
+    if (live) {
+        const size_t k = (b * H + y) * W + x;
+        const T g = *gamma, c = a0[k], ax = grad[2 * k], ay = grad[2 * k + 1], yt = Ar<T>::sub(old[k], c);
+        const T fx = fh[2 * k], fy = fh[2 * k + 1];
+        const Solve<T> s(g, ax, ay, yt, fx, fy);
+        const T gx = passes(s.ox, maxflow) ? gout[2 * k] : T(0);
+        const T gy = passes(s.oy, maxflow) ? gout[2 * k + 1] : T(0);
+        const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
+        atomic_add(&gfh[2 * k], d.gfx);
+        atomic_add(&gfh[2 * k + 1], d.gfy);
+        atomic_add(&gold[k], d.gyt);
+        atomic_add(&ga0[k], -d.gyt);
+        atomic_add(&ggrad[2 * k], d.gax);
+        atomic_add(&ggrad[2 * k + 1], d.gay);
+        gg = d.gg;
+    }
+    block_add(gg, ggamma);
+}
+
+// ------------------------------------------------------------------ delta update
+template <typename T>
+__global__ void dupdate_fwd_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                              const T* __restrict__ dh, const T* __restrict__ coarse, const T* __restrict__ gamma,
+                              T* __restrict__ flow, T* __restrict__ delta, int H, int W, int Hc, int Wc, T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    const size_t k = (b * H + y) * W + x;
+    const T g = *gamma, c = a0[k];
+    const Solve<T> s(g, grad[2 * k], grad[2 * k + 1], Ar<T>::sub(old[k], c), dh[2 * k], dh[2 * k + 1]);
+    const T hm = Ar<T>::mul(T(0.5), maxflow);
+    const T dx = clampm(sanitize(s.ox), hm), dy = clampm(sanitize(s.oy), hm);
+    const size_t kc = (b * Hc + upmap_index(y, H, Hc)) * Wc + upmap_index(x, W, Wc);
+    delta[2 * k] = dx;
+    delta[2 * k + 1] = dy;
+    flow[2 * k] = clampm(Ar<T>::add(dx, Ar<T>::mul(T(2), coarse[2 * kc])), maxflow);
+    flow[2 * k + 1] = clampm(Ar<T>::add(dy, Ar<T>::mul(T(2), coarse[2 * kc + 1])), maxflow);
+}
+
+template <typename T>
+__global__ void dupdate_bwd_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                              const T* __restrict__ dh, const T* __restrict__ coarse, const T* __restrict__ gamma,
+                              const T* __restrict__ gflow, const T* __restrict__ gdelta, T* ga0, T* ggrad, T* gold,
+                              T* gdh, T* gcoarse, T* ggamma, int H, int W, int Hc, int Wc, T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    T gg = T(0);
+    if (live) {
+        const size_t k = (b * H + y) * W + x;
+        const T g = *gamma, c = a0[k], ax = grad[2 * k], ay = grad[2 * k + 1], yt = Ar<T>::sub(old[k], c);
+        const T fx = dh[2 * k], fy = dh[2 * k + 1];
+        const Solve<T> s(g, ax, ay, yt, fx, fy);
+        const T hm = Ar<T>::mul(T(0.5), maxflow);
+        const T dx = clampm(sanitize(s.ox), hm), dy = clampm(sanitize(s.oy), hm);
+        const size_t kc = (b * Hc + upmap_index(y, H, Hc)) * Wc + upmap_index(x, W, Wc);
+        const T ux = Ar<T>::add(dx, Ar<T>::mul(T(2), coarse[2 * kc]));
+        const T uy = Ar<T>::add(dy, Ar<T>::mul(T(2), coarse[2 * kc + 1]));
+        const T gux = passes(ux, maxflow) ? gflow[2 * k] : T(0);
+        const T guy = passes(uy, maxflow) ? gflow[2 * k + 1] : T(0);
+        atomic_add(&gcoarse[2 * kc], T(2) * gux);
+        atomic_add(&gcoarse[2 * kc + 1], T(2) * guy);
+        const T gx = passes(s.ox, hm) ? gdelta[2 * k] + gux : T(0);
+        const T gy = passes(s.oy, hm) ? gdelta[2 * k + 1] + guy : T(0);
+        const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
+        atomic_add(&gdh[2 * k], d.gfx);
+        atomic_add(&gdh[2 * k + 1], d.gfy);
+        atomic_add(&gold[k], d.gyt);
+        atomic_add(&ga0[k], -d.gyt);
+        atomic_add(&ggrad[2 * k], d.gax);
+        atomic_add(&ggrad[2 * k + 1], d.gay);
+        gg = d.gg;
+    }
+    block_add(gg, ggamma);
+}
+
+// ------------------------------------------------------------------ weighted smoothing pass
+template <typename T, int AXIS>
+__global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in, T* __restrict__ out, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    if (!live) return;
+    T w[5];
+    for (int i = 0; i < 5; ++i) w[i] = w5[i];
+    size_t kk[5];
+    for (int i = 0; i < 5; ++i)
+        kk[i] = AXIS == 0 ? (b * H + y) * W + clampi(x + i - 2, 0, W - 1) : (b * H + clampi(y + i - 2, 0, H - 1)) * W + x;
+    const size_t k = (b * H + y) * W + x;
+    for (int ch = 0; ch < 2; ++ch)
+        out[2 * k + ch] = chain5(w, in[2 * kk[0] + ch], in[2 * kk[1] + ch], in[2 * kk[2] + ch], in[2 * kk[3] + ch],
+                                 in[2 * kk[4] + ch]);
+}
+
+template <typename T, int AXIS>
+__global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in, const T* __restrict__ gout, T* gin,
+                             T* gw5, int H, int W) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    T gw[5] = {T(0), T(0), T(0), T(0), T(0)};
+    if (live) {
+        const size_t k = (b * H + y) * W + x;
+        for (int i = 0; i < 5; ++i) {
+            const size_t ki = AXIS == 0 ? (b * H + y) * W + clampi(x + i - 2, 0, W - 1)
+                                        : (b * H + clampi(y + i - 2, 0, H - 1)) * W + x;
+            for (int ch = 0; ch < 2; ++ch) {
+                const T go = gout[2 * k + ch];
+                atomic_add(&gin[2 * ki + ch], w5[i] * go);
+                gw[i] += go * in[2 * ki + ch];
+            }
+        }
+    }
+    for (int i = 0; i < 5; ++i) {
+        block_add(gw[i], &gw5[i]);
+        __syncthreads();
+    }
+}
+
+inline dim3 grid3(int w, int h, int B) { return dim3((w + 31) / 32, (h + 7) / 8, B); }
+const dim3 kBlock(32, 8);
+
+template <typename T>
+cudaError_t pyramid(bool bwd, int B, int H, int W, const void* a, void* o, cudaStream_t s) {
+    const int h = H / 2, w = W / 2;
+    if (h <= 0 || w <= 0) return cudaSuccess;
+    if (bwd) return launch_k(pyr_bwd_k<T>, grid3(w, h, B), kBlock, 0, s, (const T*)a, (T*)o, H, W);
+    return launch_k(pyr_fwd_k<T>, grid3(w, h, B), kBlock, 0, s, (const T*)a, (T*)o, H, W);
+}
+
+}  // namespace diff
+}  // namespace ffb
+
+// ------------------------------------------------------------------ C ABI
+void ffb_set_last_error(const std::string& msg);  // capi.cu
+
+using namespace ffb;
+using namespace ffb::diff;
+
+namespace {
+
+template <typename F>
+ff_status run(int dtype, F&& f) {
+    if (dtype != 0 && dtype != 1) {
+        ffb_set_last_error("dtype must be 0 (float32) or 1 (float64)");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    cudaError_t e = f();
+    if (e != cudaSuccess) {
+        ffb_set_last_error(std::string("CUDA: ") + cudaGetErrorString(e));
+        return FF_ERR_CUDA;
+    }
+    return FF_OK;
+}
+
+ff_status check_shape(int B, int H, int W) {
+    if (B <= 0 || H <= 0 || W <= 0) {
+        ffb_set_last_error("batch, height and width must be positive");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    return FF_OK;
+}
+
+}  // namespace
+
+#define SHAPE_OR_RETURN(B, H, W)                   \
+    do {                                           \
+        ff_status st_ = check_shape(B, H, W);      \
+        if (st_ != FF_OK) return st_;              \
+    } while (0)
+
+extern "C" {
+
+ff_status ff_diff_pyramid(int dtype, int B, int H, int W, const void* in, void* out, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    return run(dtype, [&] {
+        return dtype ? pyramid<double>(false, B, H, W, in, out, (cudaStream_t)stream)
+                     : pyramid<float>(false, B, H, W, in, out, (cudaStream_t)stream);
+    });
+}
+
+ff_status ff_diff_pyramid_bwd(int dtype, int B, int H, int W, const void* gout, void* gin, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    return run(dtype, [&] {
+        return dtype ? pyramid<double>(true, B, H, W, gout, gin, (cudaStream_t)stream)
+                     : pyramid<float>(true, B, H, W, gout, gin, (cudaStream_t)stream);
+    });
+}
+
+ff_status ff_diff_model(int dtype, int B, int H, int W, const void* img, void* a0, void* grad, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        if (dtype) return launch_k(model_fwd_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)img, (double*)a0,
+                                   (double*)grad, H, W);
+        return launch_k(model_fwd_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)img, (float*)a0, (float*)grad,
+                        H, W);
+    });
+}
+
+ff_status ff_diff_model_bwd(int dtype, int B, int H, int W, const void* ga0, const void* ggrad, void* gby, void* gbx,
+                            void* gimg, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = (size_t)B * H * W * (dtype ? 8 : 4);
+    return run(dtype, [&] {
+        cudaError_t e = cudaMemsetAsync(gby, 0, bytes, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(gbx, 0, bytes, s);
+        if (e != cudaSuccess) return e;
+        if (dtype) {
+            e = launch_k(model_bwd1_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)ga0, (const double*)ggrad,
+                         (double*)gby, (double*)gbx, H, W);
+            if (e == cudaSuccess)
+                e = launch_k(model_bwd2_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)gby,
+                             (const double*)gbx, (double*)gimg, H, W);
+            return e;
+        }
+        e = launch_k(model_bwd1_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)ga0, (const float*)ggrad,
+                     (float*)gby, (float*)gbx, H, W);
+        if (e == cudaSuccess)
+            e = launch_k(model_bwd2_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)gby, (const float*)gbx,
+                         (float*)gimg, H, W);
+        return e;
+    });
+}
+
+ff_status ff_diff_propagate(int dtype, int B, int H, int W, int axis, int payload, double dt, int border,
+                            const void* f, const void* sc, const void* v, void* fo, void* so, void* vo,
+                            void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    if ((axis != 0 && axis != 1) || border < 0) {
+        ffb_set_last_error("axis must be 0 or 1 and border >= 0");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        const dim3 g = grid3(W, H, B);
+#define PROP_F(T, A, P)                                                                                          \
+    launch_k(prop_fwd_k<T, A, P>, g, kBlock, 0, s, (const T*)f, (const T*)sc, (const T*)v, (T*)fo, (T*)so, (T*)vo, H, \
+             W, (T)dt, border)
+        if (dtype) {
+            if (axis == 0) return payload ? PROP_F(double, 0, true) : PROP_F(double, 0, false);
+            return payload ? PROP_F(double, 1, true) : PROP_F(double, 1, false);
+        }
+        if (axis == 0) return payload ? PROP_F(float, 0, true) : PROP_F(float, 0, false);
+        return payload ? PROP_F(float, 1, true) : PROP_F(float, 1, false);
+#undef PROP_F
+    });
+}
+
+ff_status ff_diff_propagate_bwd(int dtype, int B, int H, int W, int axis, int payload, double dt, int border,
+                                const void* f, const void* sc, const void* v, const void* gfo, const void* gso,
+                                const void* gvo, void* gf, void* gs, void* gv, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    if ((axis != 0 && axis != 1) || border < 0) {
+        ffb_set_last_error("axis must be 0 or 1 and border >= 0");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        const dim3 g = grid3(W, H, B);
+#define PROP_B(T, A, P)                                                                                         \
+    launch_k(prop_bwd_k<T, A, P>, g, kBlock, 0, s, (const T*)f, (const T*)sc, (const T*)v, (const T*)gfo,        \
+             (const T*)gso, (const T*)gvo, (T*)gf, (T*)gs, (T*)gv, H, W, (T)dt, border)
+        if (dtype) {
+            if (axis == 0) return payload ? PROP_B(double, 0, true) : PROP_B(double, 0, false);
+            return payload ? PROP_B(double, 1, true) : PROP_B(double, 1, false);
+        }
+        if (axis == 0) return payload ? PROP_B(float, 0, true) : PROP_B(float, 0, false);
+        return payload ? PROP_B(float, 1, true) : PROP_B(float, 1, false);
+#undef PROP_B
+    });
+}
+
+ff_status ff_diff_update(int dtype, int B, int H, int W, const void* a0, const void* grad, const void* old,
+                         const void* fhat, const void* gamma, double maxflow, void* out, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        if (dtype)
+            return launch_k(update_fwd_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)a0, (const double*)grad,
+                            (const double*)old, (const double*)fhat, (const double*)gamma, (double*)out, H, W,
+                            maxflow);
+        return launch_k(update_fwd_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)a0, (const float*)grad,
+                        (const float*)old, (const float*)fhat, (const float*)gamma, (float*)out, H, W, (float)maxflow);
+    });
+}
+
+ff_status ff_diff_update_bwd(int dtype, int B, int H, int W, const void* a0, const void* grad, const void* old,
+                             const void* fhat, const void* gamma, double maxflow, const void* gout, void* ga0,
+                             void* ggrad, void* gold, void* gfhat, void* ggamma, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        if (dtype)
+            return launch_k(update_bwd_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)a0, (const double*)grad,
+                            (const double*)old, (const double*)fhat, (const double*)gamma, (const double*)gout,
+                            (double*)ga0, (double*)ggrad, (double*)gold, (double*)gfhat, (double*)ggamma, H, W,
+                            maxflow);
+        return launch_k(update_bwd_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)a0, (const float*)grad,
+                        (const float*)old, (const float*)fhat, (const float*)gamma, (const float*)gout, (float*)ga0,
+                        (float*)ggrad, (float*)gold, (float*)gfhat, (float*)ggamma, H, W, (float)maxflow);
+    });
+}
+
+ff_status ff_diff_delta_update(int dtype, int B, int H, int W, int Hc, int Wc, const void* a0, const void* grad,
+                               const void* old, const void* dhat, const void* coarse, const void* gamma,
+                               double maxflow, void* flow, void* delta, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    SHAPE_OR_RETURN(B, Hc, Wc);
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        if (dtype)
+            return launch_k(dupdate_fwd_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)a0,
+                            (const double*)grad, (const double*)old, (const double*)dhat, (const double*)coarse,
+                            (const double*)gamma, (double*)flow, (double*)delta, H, W, Hc, Wc, maxflow);
+        return launch_k(dupdate_fwd_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)a0, (const float*)grad,
+                        (const float*)old, (const float*)dhat, (const float*)coarse, (const float*)gamma, (float*)flow,
+                        (float*)delta, H, W, Hc, Wc, (float)maxflow);
+    });
+}
+
+ff_status ff_diff_delta_update_bwd(int dtype, int B, int H, int W, int Hc, int Wc, const void* a0, const void* grad,
+                                   const void* old, const void* dhat, const void* coarse, const void* gamma,
+                                   double maxflow, const void* gflow, const void* gdelta, void* ga0, void* ggrad,
+                                   void* gold, void* gdhat, void* gcoarse, void* ggamma, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    SHAPE_OR_RETURN(B, Hc, Wc);
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        if (dtype)
+            return launch_k(dupdate_bwd_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)a0,
+                            (const double*)grad, (const double*)old, (const double*)dhat, (const double*)coarse,
+                            (const double*)gamma, (const double*)gflow, (const double*)gdelta, (double*)ga0,
+                            (double*)ggrad, (double*)gold, (double*)gdhat, (double*)gcoarse, (double*)ggamma, H, W, Hc,
+                            Wc, maxflow);
+        return launch_k(dupdate_bwd_k<float>, grid3(W, H, B), kBlock, 0, s, (const float*)a0, (const float*)grad,
+                        (const float*)old, (const float*)dhat, (const float*)coarse, (const float*)gamma,
+                        (const float*)gflow, (const float*)gdelta, (float*)ga0, (float*)ggrad, (float*)gold,
+                        (float*)gdhat, (float*)gcoarse, (float*)ggamma, H, W, Hc, Wc, (float)maxflow);
+    });
+}
+
+ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w5, const void* in, void* out,
+                         void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    if (axis != 0 && axis != 1) {
+        ffb_set_last_error("axis must be 0 or 1");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        const dim3 g = grid3(W, H, B);
+        if (dtype)
+            return axis == 0 ? launch_k(smooth_fwd_k<double, 0>, g, kBlock, 0, s, (const double*)w5,
+                                        (const double*)in, (double*)out, H, W)
+                             : launch_k(smooth_fwd_k<double, 1>, g, kBlock, 0, s, (const double*)w5,
+                                        (const double*)in, (double*)out, H, W);
+        return axis == 0 ? launch_k(smooth_fwd_k<float, 0>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
+                                    (float*)out, H, W)
+                         : launch_k(smooth_fwd_k<float, 1>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
+                                    (float*)out, H, W);
+    });
+}
+
+ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
+                             const void* gout, void* gin, void* gw5, void* stream) {
+    SHAPE_OR_RETURN(B, H, W);
+    if (axis != 0 && axis != 1) {
+        ffb_set_last_error("axis must be 0 or 1");
+        return FF_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return run(dtype, [&] {
+        const dim3 g = grid3(W, H, B);
+        if (dtype)
+            return axis == 0 ? launch_k(smooth_bwd_k<double, 0>, g, kBlock, 0, s, (const double*)w5,
+                                        (const double*)in, (const double*)gout, (double*)gin, (double*)gw5, H, W)
+                             : launch_k(smooth_bwd_k<double, 1>, g, kBlock, 0, s, (const double*)w5,
+                                        (const double*)in, (const double*)gout, (double*)gin, (double*)gw5, H, W);
+        return axis == 0 ? launch_k(smooth_bwd_k<float, 0>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
+                                    (const float*)gout, (float*)gin, (float*)gw5, H, W)
+                         : launch_k(smooth_bwd_k<float, 1>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
+                                    (const float*)gout, (float*)gin, (float*)gw5, H, W);
+    });
+}
+
+}  // extern "C"

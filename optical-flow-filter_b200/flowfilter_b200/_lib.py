@@ -135,6 +135,18 @@ SIGNATURES = {
     "ff_batch_frame_layout": (_st, [_vp, _szp, _szp]),
     "ff_batch_launches": (_st, [_vp, _ip]),
     "ff_batch_step": (_st, [_vp, _vp, _vp]),
+    "ff_diff_pyramid": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),
+    "ff_diff_pyramid_bwd": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),
+    "ff_diff_model": (_st, [_i, _i, _i, _i, _vp, _vp, _vp, _vp]),
+    "ff_diff_model_bwd": (_st, [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ff_diff_propagate": (_st, [_i, _i, _i, _i, _i, _i, ctypes.c_double, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ff_diff_propagate_bwd": (_st, [_i, _i, _i, _i, _i, _i, ctypes.c_double, _i] + [_vp] * 10),
+    "ff_diff_update": (_st, [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp]),
+    "ff_diff_update_bwd": (_st, [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, ctypes.c_double] + [_vp] * 7),
+    "ff_diff_delta_update": (_st, [_i, _i, _i, _i, _i, _i] + [_vp] * 6 + [ctypes.c_double, _vp, _vp, _vp]),
+    "ff_diff_delta_update_bwd": (_st, [_i, _i, _i, _i, _i, _i] + [_vp] * 6 + [ctypes.c_double] + [_vp] * 9),
+    "ff_diff_smooth": (_st, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp]),
+    "ff_diff_smooth_bwd": (_st, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
