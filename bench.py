@@ -11,7 +11,8 @@ configuration: 640x480 uint8 frames, 2 levels, gamma [10, 50], smoothing [2, 4],
 maxflow 4, on a synthetic rotation+zoom sequence (seeded) standing in for the
 reference's Blender sequence.  The 2048x1088 3-level throughput workload is reported
 beside it under "extra", and the 64-stream mixed-size batched step (BatchFlowFilter,
-against the same 64 streams looped as single filters) under "batched".
+against the same 64 streams looped as single filters) under "batched", and the
+differentiable filter's forward and forward+backward time under "differentiable".
 
 Timing: every step is bracketed by CUDA events on the filter's stream and the L2 is
 flushed (a 256 MiB write) between steps outside those events, so every frame reads its
@@ -431,6 +432,54 @@ def bench_batched(steps, warmup):
     }
 
 
+def bench_differentiable(steps):
+    """The differentiable filter on 16 sequences of 256x256 float frames, 32 frames each,
+    2 levels (gamma [10, 50], smoothing [2, 4], maxflow 4, checkpoint every 8 frames):
+    device time of the forward pass alone and of forward + backward of the mean endpoint
+    error over frames 8-31 against the known flow."""
+    import torch
+    from flowfilter_b200 import diff, synthetic
+
+    B, T, H, W = 16, 32, 256, 256
+    seqs = [synthetic.seq_bumps_float(frames=T, height=H, width=W, seed=200 + b, n_bumps=8, bump_sigma=40.0,
+                                      amp=2.0) for b in range(B)]
+    frames = torch.from_numpy(np.stack([q[0] for q in seqs])).cuda()
+    truth = torch.from_numpy(np.stack([np.stack([q[1], q[2]], -1) for q in seqs])).cuda()[:, None]
+    f = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=8)
+
+    def fwd():
+        with torch.no_grad():
+            return f(frames)
+
+    def fwd_bwd():
+        loss = diff.endpoint_error(f(frames), truth.expand(B, T, H, W, 2), first=8)
+        loss.backward()
+        return loss
+
+    def timed(fn, n):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    n = max(1, min(steps, 5))
+    t_f = timed(fwd, n)
+    t_fb = timed(fwd_bwd, n)
+    return {
+        "workload": f"{B} sequences x {T} frames of {W}x{H} float32, 2 levels, gamma [10, 50], smoothing [2, 4], "
+                    "maxflow 4, loss = mean endpoint error over frames 8-31, checkpoint every 8 frames",
+        "fwd_ms": t_f, "fwd_bwd_ms": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
+        "fwd_frames_per_s": B * T / (t_f / 1e3), "fwd_bwd_frames_per_s": B * T / (t_fb / 1e3),
+        "dtype": "f32", "data": "synthetic: seeded bump flows (seed 200 + b), known flow",
+    }
+
+
 def bench_b200(args):
     import torch
 
@@ -489,6 +538,8 @@ def bench_b200(args):
     batched = bench_batched(min(args.steps, 200), max(args.warmup, 3))
     barrier(world)
 
+    differentiable = bench_differentiable(args.steps)
+
     cpu = None
     if rank == 0 and world == 1:
         fps, cores, n = cpu_port_fps(w, frames)
@@ -522,6 +573,7 @@ def bench_b200(args):
             "clocks": clk.summary(),
             "extra": extra,
             "batched": batched,
+            "differentiable": differentiable,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

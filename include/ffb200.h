@@ -256,11 +256,12 @@ ff_status ff_batch_step(ff_batch* batch, const void* frames, void* stream);
  * same dtype.  The float32 forward equals the stage kernels above (with weights 0.2, the
  * reference's box).  Backward calls ADD into their gradient outputs (zero them first) and
  * take the stage's forward inputs; the upwind, dominant-velocity and clamp branches follow
- * the forward (zero gradient through a clamped or sanitised value). */
+ * the forward (zero gradient through a clamped or sanitised value).  Stencil adjoints are
+ * gathers (deterministic); the coarse-flow gradient of the delta update uses atomics. */
 ff_status ff_diff_pyramid(int dtype, int B, int H, int W, const void* in, void* out, void* stream);
 ff_status ff_diff_pyramid_bwd(int dtype, int B, int H, int W, const void* gout, void* gin, void* stream);
 ff_status ff_diff_model(int dtype, int B, int H, int W, const void* img, void* a0, void* grad, void* stream);
-/* gby, gbx: scratch of B*H*W elements each (cleared here) */
+/* gby, gbx: scratch of B*H*W elements each (overwritten) */
 ff_status ff_diff_model_bwd(int dtype, int B, int H, int W, const void* ga0, const void* ggrad, void* gby, void* gbx,
                             void* gimg, void* stream);
 /* one sub-step along axis (0 = X, 1 = Y); payload: also advect scalar s and vector v */

@@ -10,9 +10,12 @@
 //
 // Backward kernels take the forward inputs (the forward is recomputed locally), follow the
 // branch the forward took at every upwind, dominant-velocity and clamp decision (the
-// gradient of a clamped or sanitised value is zero) and ADD into the input gradients with
-// atomics: gradient buffers start at zero (or hold earlier contributions).  Gradients of the
-// per-level scalars are reduced per block, then added once per block.
+// gradient of a clamped or sanitised value is zero) and ADD into the input gradients:
+// gradient buffers start at zero (or hold earlier contributions).  Stencil adjoints are in
+// gather form (each input pixel collects from the outputs that read it, clamps included), so
+// they need no atomics and are deterministic; only the coarse-flow gradient of the delta
+// update is scattered with atomics.  Gradients of the per-level scalars are reduced per
+// block, then added once per block.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -175,21 +178,31 @@ __global__ void pyr_fwd_k(const T* __restrict__ in, T* __restrict__ out, int H, 
     out[(b * h + y) * w + x] = down3(xs[0], xs[1], xs[2]);
 }
 
+// gather form: input pixel (X, Y) sums the contributions of the outputs whose 3x3 stencil
+// (after clamping) reads it; outputs x in [X/2 - 1, X/2 + 1] cover every case
 template <typename T>
 __global__ void pyr_bwd_k(const T* __restrict__ gout, T* gin, int H, int W) {
     grid_dep_wait();
     grid_dep_launch();
     const int h = H / 2, w = W / 2;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    const size_t b = blockIdx.z;
-    if (x >= w || y >= h) return;
-    const T g = gout[(b * h + y) * w + x];
+    PIX_SETUP
+    if (!live) return;
     const T wt[3] = {T(0.25), T(0.5), T(0.25)};
-    T* G = gin + b * H * W;
-    for (int j = 0; j < 3; ++j) {
-        const int sy = clampi(2 * y - 1 + j, 0, H - 1);
-        for (int k = 0; k < 3; ++k) atomic_add(&G[sy * W + clampi(2 * x - 1 + k, 0, W - 1)], g * wt[j] * wt[k]);
+    const T* G = gout + b * h * w;
+    T acc = T(0);
+    for (int yo = max(y / 2 - 1, 0); yo <= min(y / 2 + 1, h - 1); ++yo) {
+        T wy = T(0);
+        for (int j = 0; j < 3; ++j)
+            if (clampi(2 * yo - 1 + j, 0, H - 1) == y) wy += wt[j];
+        if (wy == T(0)) continue;
+        for (int xo = max(x / 2 - 1, 0); xo <= min(x / 2 + 1, w - 1); ++xo) {
+            T wx = T(0);
+            for (int k = 0; k < 3; ++k)
+                if (clampi(2 * xo - 1 + k, 0, W - 1) == x) wx += wt[k];
+            if (wx != T(0)) acc += G[yo * w + xo] * wy * wx;
+        }
     }
+    gin[(b * H + y) * W + x] += acc;
 }
 
 // ------------------------------------------------------------------ image model
@@ -220,7 +233,18 @@ __global__ void model_fwd_k(const T* __restrict__ img, T* __restrict__ a0, T* __
     grad[2 * k + 1] = chain5(M.d, bx[0], bx[1], bx[2], bx[3], bx[4]);
 }
 
-// step 1: gradients of the Y blur (by, at (x', y)) and of the X blur (bx, at (x, y'))
+// weight of tap k of a clamped 5-tap stencil centred at output i that lands on index j
+// (several taps land on the edge index at the borders), summed over taps
+template <typename T>
+__device__ __forceinline__ T tap_weight(const T* w, int i, int j, int n) {
+    T acc = T(0);
+    for (int k = 0; k < 5; ++k)
+        if (clampi(i + k - 2, 0, n - 1) == j) acc += w[k];
+    return acc;
+}
+
+// step 1 (gather): gradients of the Y blur by (used by a0 and ax along X) and of the X blur
+// bx (used by ay along Y) at this pixel
 template <typename T>
 __global__ void model_bwd1_k(const T* __restrict__ ga0, const T* __restrict__ ggrad, T* gby, T* gbx, int H, int W) {
     grid_dep_wait();
@@ -228,15 +252,19 @@ __global__ void model_bwd1_k(const T* __restrict__ ga0, const T* __restrict__ gg
     PIX_SETUP
     if (!live) return;
     const Masks<T> M;
-    const size_t k = (b * H + y) * W + x;
-    const T g0 = ga0[k], gx = ggrad[2 * k], gy = ggrad[2 * k + 1];
-    T* BY = gby + b * H * W;
-    T* BX = gbx + b * H * W;
-    for (int c = 0; c < 5; ++c) atomic_add(&BY[y * W + clampi(x + c - 2, 0, W - 1)], M.s[c] * g0 + M.d[c] * gx);
-    for (int r = 0; r < 5; ++r) atomic_add(&BX[clampi(y + r - 2, 0, H - 1) * W + x], M.d[r] * gy);
+    const size_t row = (b * H + y) * W;
+    T aby = T(0), abx = T(0);
+    for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) {
+        const T ws = tap_weight(M.s, i, x, W), wd = tap_weight(M.d, i, x, W);
+        aby += ws * ga0[row + i] + wd * ggrad[2 * (row + i)];
+    }
+    for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i)
+        abx += tap_weight(M.d, i, y, H) * ggrad[2 * ((b * H + i) * W + x) + 1];
+    gby[row + x] = aby;
+    gbx[row + x] = abx;
 }
 
-// step 2: by = Y blur of the image, bx = X blur of the image
+// step 2 (gather): by = Y blur of the image, bx = X blur of the image
 template <typename T>
 __global__ void model_bwd2_k(const T* __restrict__ gby, const T* __restrict__ gbx, T* gimg, int H, int W) {
     grid_dep_wait();
@@ -244,11 +272,11 @@ __global__ void model_bwd2_k(const T* __restrict__ gby, const T* __restrict__ gb
     PIX_SETUP
     if (!live) return;
     const Masks<T> M;
-    const size_t k = (b * H + y) * W + x;
-    const T a = gby[k], c0 = gbx[k];
-    T* G = gimg + b * H * W;
-    for (int r = 0; r < 5; ++r) atomic_add(&G[clampi(y + r - 2, 0, H - 1) * W + x], M.s[r] * a);
-    for (int c = 0; c < 5; ++c) atomic_add(&G[y * W + clampi(x + c - 2, 0, W - 1)], M.s[c] * c0);
+    T acc = T(0);
+    for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i) acc += tap_weight(M.s, i, y, H) * gby[(b * H + i) * W + x];
+    const size_t row = (b * H + y) * W;
+    for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) acc += tap_weight(M.s, i, x, W) * gbx[row + i];
+    gimg[row + x] += acc;
 }
 
 // ------------------------------------------------------------------ propagation sub-step
@@ -275,19 +303,9 @@ __global__ void prop_fwd_k(const T* __restrict__ f, const T* __restrict__ s, con
     }
 }
 
-// adjoint of one upwind channel: out = g0 - t*(dv >= 0 ? g0 - gm : gp - g0); returns d out / d dv
-template <typename T>
-__device__ __forceinline__ T upwind_grad(T go, T t, T dt, T dv, T gm, T g0, T gp, T* Gm, T* G0, T* Gp) {
-    if (dv >= T(0)) {
-        atomic_add(G0, go * (T(1) - t));
-        atomic_add(Gm, go * t);
-        return -go * dt * (g0 - gm);
-    }
-    atomic_add(G0, go * (T(1) + t));
-    atomic_add(Gp, -go * t);
-    return -go * dt * (gp - g0);
-}
-
+// Gather-form adjoint of one upwind sub-step: input pixel j (index along AXIS) collects
+// from the outputs i in {j-1, j, j+1} whose clamped stencil (i-1, i, i+1) reads it,
+// recomputing each output's dominant velocity, upwind branch and border freeze.
 template <typename T, int AXIS, bool PAYLOAD>
 __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v,
                            const T* __restrict__ gfo, const T* __restrict__ gso, const T* __restrict__ gvo, T* gf, T* gs,
@@ -296,35 +314,61 @@ __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, con
     grid_dep_launch();
     PIX_SETUP
     if (!live) return;
-    const int xm = AXIS == 0 ? max(x - 1, 0) : x, xp = AXIS == 0 ? min(x + 1, W - 1) : x;
-    const int ym = AXIS == 1 ? max(y - 1, 0) : y, yp = AXIS == 1 ? min(y + 1, H - 1) : y;
-    const size_t k = (b * H + y) * W + x, km = (b * H + ym) * W + xm, kp = (b * H + yp) * W + xp;
-    const bool in = x >= border && x < W - border && y >= border && y < H - border;
-    if (!in) {
-        atomic_add(&gf[2 * k], gfo[2 * k]);
-        atomic_add(&gf[2 * k + 1], gfo[2 * k + 1]);
-        if constexpr (PAYLOAD) {
-            atomic_add(&gs[k], gso[k]);
-            atomic_add(&gv[2 * k], gvo[2 * k]);
-            atomic_add(&gv[2 * k + 1], gvo[2 * k + 1]);
+    const int n = AXIS == 0 ? W : H;
+    const int j = AXIS == 0 ? x : y;
+    // linear index of position p along the axis, on this pixel's line
+    auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
+    const bool line_in = AXIS == 0 ? (y >= border && y < H - border) : (x >= border && x < W - border);
+    constexpr int NC = PAYLOAD ? 5 : 2;  // channels: flow x, flow y [, scalar, vector x, vector y]
+    auto chan = [&](size_t k, int c) -> T {
+        return c < 2 ? f[2 * k + c] : (c == 2 ? s[k] : v[2 * k + (c - 3)]);
+    };
+    auto gchan = [&](size_t k, int c) -> T {
+        return c < 2 ? gfo[2 * k + c] : (c == 2 ? gso[k] : gvo[2 * k + (c - 3)]);
+    };
+    T acc[NC];
+    for (int c = 0; c < NC; ++c) acc[c] = T(0);
+    for (int i = max(j - 1, 0); i <= min(j + 1, n - 1); ++i) {
+        const size_t ki = at(i);
+        const bool in = line_in && i >= border && i < n - border;
+        if (!in) {
+            if (i == j)
+                for (int c = 0; c < NC; ++c) acc[c] += gchan(ki, c);
+            continue;
         }
-        return;
+        const int im = max(i - 1, 0), ip = min(i + 1, n - 1);
+        const size_t km = at(im), kp = at(ip);
+        const T vm_ = f[2 * km + AXIS], vp_ = f[2 * kp + AXIS];
+        const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
+        const T dv = take_p ? vp_ : vm_;
+        const T t = dt * dv;
+        T gdv = T(0);
+        for (int c = 0; c < NC; ++c) {
+            const T go = gchan(ki, c);
+            const T g0 = chan(ki, c);
+            if (dv >= T(0)) {
+                const T gm = chan(km, c);
+                if (i == j) acc[c] += go * (T(1) - t);
+                if (im == j) acc[c] += go * t;
+                gdv -= go * dt * (g0 - gm);
+            } else {
+                const T gp = chan(kp, c);
+                if (i == j) acc[c] += go * (T(1) + t);
+                if (ip == j) acc[c] -= go * t;
+                gdv -= go * dt * (gp - g0);
+            }
+        }
+        // the dominant velocity is the chosen neighbour's AXIS component
+        if ((take_p ? ip : im) == j) acc[AXIS] += gdv;
     }
-    const T fmx = f[2 * km], fmy = f[2 * km + 1], f0x = f[2 * k], f0y = f[2 * k + 1], fpx = f[2 * kp], fpy = f[2 * kp + 1];
-    const T vm_ = AXIS == 0 ? fmx : fmy, vp_ = AXIS == 0 ? fpx : fpy;
-    const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
-    const T dv = take_p ? vp_ : vm_;
-    const T t = Ar<T>::mul(dt, dv);
-    T gdv = upwind_grad(gfo[2 * k], t, dt, dv, fmx, f0x, fpx, &gf[2 * km], &gf[2 * k], &gf[2 * kp]);
-    gdv += upwind_grad(gfo[2 * k + 1], t, dt, dv, fmy, f0y, fpy, &gf[2 * km + 1], &gf[2 * k + 1], &gf[2 * kp + 1]);
+    const size_t kj = at(j);
+    gf[2 * kj] += acc[0];
+    gf[2 * kj + 1] += acc[1];
     if constexpr (PAYLOAD) {
-        gdv += upwind_grad(gso[k], t, dt, dv, s[km], s[k], s[kp], &gs[km], &gs[k], &gs[kp]);
-        gdv += upwind_grad(gvo[2 * k], t, dt, dv, v[2 * km], v[2 * k], v[2 * kp], &gv[2 * km], &gv[2 * k], &gv[2 * kp]);
-        gdv += upwind_grad(gvo[2 * k + 1], t, dt, dv, v[2 * km + 1], v[2 * k + 1], v[2 * kp + 1], &gv[2 * km + 1],
-                           &gv[2 * k + 1], &gv[2 * kp + 1]);
+        gs[kj] += acc[2];
+        gv[2 * kj] += acc[3];
+        gv[2 * kj + 1] += acc[4];
     }
-    // the dominant velocity is the chosen neighbour's AXIS component
-    atomic_add(&gf[2 * (take_p ? kp : km) + AXIS], gdv);
 }
 
 // ------------------------------------------------------------------ update (top level)
@@ -364,12 +408,13 @@ __global__ void update_bwd_k(const T* __restrict__ a0, const T* __restrict__ gra
         const T gx = passes(s.ox, maxflow) ? gout[2 * k] : T(0);
         const T gy = passes(s.oy, maxflow) ? gout[2 * k + 1] : T(0);
         const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
-        atomic_add(&gfh[2 * k], d.gfx);
-        atomic_add(&gfh[2 * k + 1], d.gfy);
-        atomic_add(&gold[k], d.gyt);
-        atomic_add(&ga0[k], -d.gyt);
-        atomic_add(&ggrad[2 * k], d.gax);
-        atomic_add(&ggrad[2 * k + 1], d.gay);
+        // one thread per pixel writes these: plain adds
+        gfh[2 * k] += d.gfx;
+        gfh[2 * k + 1] += d.gfy;
+        gold[k] += d.gyt;
+        ga0[k] -= d.gyt;
+        ggrad[2 * k] += d.gax;
+        ggrad[2 * k + 1] += d.gay;
         gg = d.gg;
     }
     block_add(gg, ggamma);
@@ -422,12 +467,13 @@ __global__ void dupdate_bwd_k(const T* __restrict__ a0, const T* __restrict__ gr
         const T gx = passes(s.ox, hm) ? gdelta[2 * k] + gux : T(0);
         const T gy = passes(s.oy, hm) ? gdelta[2 * k + 1] + guy : T(0);
         const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
-        atomic_add(&gdh[2 * k], d.gfx);
-        atomic_add(&gdh[2 * k + 1], d.gfy);
-        atomic_add(&gold[k], d.gyt);
-        atomic_add(&ga0[k], -d.gyt);
-        atomic_add(&ggrad[2 * k], d.gax);
-        atomic_add(&ggrad[2 * k + 1], d.gay);
+        // one thread per pixel writes these: plain adds (the coarse flow above needs atomics)
+        gdh[2 * k] += d.gfx;
+        gdh[2 * k + 1] += d.gfy;
+        gold[k] += d.gyt;
+        ga0[k] -= d.gyt;
+        ggrad[2 * k] += d.gax;
+        ggrad[2 * k + 1] += d.gay;
         gg = d.gg;
     }
     block_add(gg, ggamma);
@@ -459,15 +505,27 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
     PIX_SETUP
     T gw[5] = {T(0), T(0), T(0), T(0), T(0)};
     if (live) {
-        const size_t k = (b * H + y) * W + x;
-        for (int i = 0; i < 5; ++i) {
-            const size_t ki = AXIS == 0 ? (b * H + y) * W + clampi(x + i - 2, 0, W - 1)
-                                        : (b * H + clampi(y + i - 2, 0, H - 1)) * W + x;
-            for (int ch = 0; ch < 2; ++ch) {
-                const T go = gout[2 * k + ch];
-                atomic_add(&gin[2 * ki + ch], w5[i] * go);
-                gw[i] += go * in[2 * ki + ch];
+        T w[5];
+        for (int i = 0; i < 5; ++i) w[i] = w5[i];
+        const int n = AXIS == 0 ? W : H;
+        const int j = AXIS == 0 ? x : y;
+        auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
+        // input gradient at this pixel: outputs i in [j-2, j+2] whose clamped taps land on j
+        T a0 = T(0), a1 = T(0);
+        for (int i = max(j - 2, 0); i <= min(j + 2, n - 1); ++i) {
+            const T wt = tap_weight(w, i, j, n);
+            if (wt != T(0)) {
+                a0 += wt * gout[2 * at(i)];
+                a1 += wt * gout[2 * at(i) + 1];
             }
+        }
+        gin[2 * at(j)] += a0;
+        gin[2 * at(j) + 1] += a1;
+        // weight gradient: this pixel as an output
+        const T g0 = gout[2 * at(j)], g1 = gout[2 * at(j) + 1];
+        for (int k = 0; k < 5; ++k) {
+            const size_t kk = at(clampi(j + k - 2, 0, n - 1));
+            gw[k] = g0 * in[2 * kk] + g1 * in[2 * kk + 1];
         }
     }
     for (int i = 0; i < 5; ++i) {
@@ -483,7 +541,8 @@ template <typename T>
 cudaError_t pyramid(bool bwd, int B, int H, int W, const void* a, void* o, cudaStream_t s) {
     const int h = H / 2, w = W / 2;
     if (h <= 0 || w <= 0) return cudaSuccess;
-    if (bwd) return launch_k(pyr_bwd_k<T>, grid3(w, h, B), kBlock, 0, s, (const T*)a, (T*)o, H, W);
+    // the adjoint runs one thread per INPUT pixel (gather), the forward one per output pixel
+    if (bwd) return launch_k(pyr_bwd_k<T>, grid3(W, H, B), kBlock, 0, s, (const T*)a, (T*)o, H, W);
     return launch_k(pyr_fwd_k<T>, grid3(w, h, B), kBlock, 0, s, (const T*)a, (T*)o, H, W);
 }
 
@@ -561,11 +620,8 @@ ff_status ff_diff_model_bwd(int dtype, int B, int H, int W, const void* ga0, con
                             void* gimg, void* stream) {
     SHAPE_OR_RETURN(B, H, W);
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t bytes = (size_t)B * H * W * (dtype ? 8 : 4);
     return run(dtype, [&] {
-        cudaError_t e = cudaMemsetAsync(gby, 0, bytes, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(gbx, 0, bytes, s);
-        if (e != cudaSuccess) return e;
+        cudaError_t e;
         if (dtype) {
             e = launch_k(model_bwd1_k<double>, grid3(W, H, B), kBlock, 0, s, (const double*)ga0, (const double*)ggrad,
                          (double*)gby, (double*)gbx, H, W);

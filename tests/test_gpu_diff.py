@@ -98,10 +98,12 @@ def test_stage_adjoints_gradcheck(dm, cuda):
         return cuda.tensor(rng.normal(offset, scale, shape), dtype=cuda.float64, device=dev, requires_grad=True)
 
     B, H, W = 2, 9, 11
-    assert gc(lambda x: F["Pyramid"].apply(x), (t(B, H, W),), eps=1e-6, atol=1e-8)
+    for ph, pw in [(9, 11), (20, 28), (35, 70)]:  # odd and even sizes; grids wider than one block
+        assert gc(lambda x: F["Pyramid"].apply(x), (t(B, ph, pw),), eps=1e-6, atol=1e-8)
     assert gc(lambda x: F["Model"].apply(x), (t(B, H, W),), eps=1e-6, atol=1e-8)
     for axis in (0, 1):
         assert gc(lambda f: F["PropFlow"].apply(f, axis, 0.25, 2), (t(B, H, W, 2),), eps=1e-6, atol=1e-8)
+        assert gc(lambda f: F["PropFlow"].apply(f, axis, 0.5, 0), (t(1, 12, 40, 2),), eps=1e-6, atol=1e-8)
         assert gc(lambda f, s, v: F["PropPayload"].apply(f, s, v, axis, 0.5, 1),
                   (t(B, H, W, 2), t(B, H, W), t(B, H, W, 2)), eps=1e-6, atol=1e-8)
         w5 = cuda.tensor([0.1, 0.25, 0.3, 0.2, 0.15], dtype=cuda.float64, device=dev, requires_grad=True)
@@ -228,5 +230,26 @@ def test_fitting_gamma_lowers_endpoint_error(dm, cuda):
         opt.zero_grad()
         loss.backward()
         opt.step()
-        losses.append(float(loss))
+        losses.append(float(loss.detach()))
     assert losses[-1] < losses[0]
+
+
+@pytest.mark.parametrize("levels", [1, 2, 3])
+def test_frame_node_matches_per_stage_nodes(dm, cuda, levels):
+    """The single autograd node per frame gives the per-stage nodes' flows and gradients."""
+    B, T, H, W = 2, 5, 26, 34
+    frames = cuda.from_numpy(float_frames(B, T, H, W, 23).astype(np.float64)).cuda()
+    proj = cuda.from_numpy(np.random.default_rng(5).normal(0, 1, (B, T, H, W, 2))).cuda()
+    res = []
+    for per_stage in (False, True):
+        f = dm.DiffPyramidalFlowFilter(H, W, levels, [3.0, 12.0, 40.0][:levels], [1, 2, 1][:levels], maxflow=4.0,
+                                       dtype=cuda.float64, checkpoint_every=2)
+        f.per_stage = per_stage
+        x = frames.clone().requires_grad_(True)
+        flows = f(x)
+        sequence_loss(flows, proj).backward()
+        res.append((flows.detach().cpu().numpy(), f.gamma.grad.cpu().numpy(), f.weights.grad.cpu().numpy(),
+                    x.grad.cpu().numpy()))
+    np.testing.assert_array_equal(res[0][0], res[1][0])
+    for a, b in zip(res[0][1:], res[1][1:]):
+        np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-13)
