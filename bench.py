@@ -302,28 +302,27 @@ def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, 
 
 
 def e2e_run(w, frames, steps, warmup):
-    """loadImage(host, pinned) -> compute() -> getFlow(host, pinned), all blocking."""
+    """End to end through the public API with host buffers: every step uploads its frame from
+    pinned host memory, computes, and downloads the smoothed flow into pinned host memory
+    (PyramidalFlowFilter.processAsync: the three overlap across consecutive frames); the
+    clock stops after synchronize() has delivered the last flow.  Wall-clock time."""
     import torch
 
     f = make_filter(w)
     ring = frames.shape[0]
-    host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
-    host.copy_(torch.from_numpy(frames))
-    hnp = host.numpy()
-    out = torch.empty((w["H"], w["W"], 2), dtype=torch.float32, pin_memory=True).numpy()
+    host = torch.from_numpy(frames).pin_memory()
+    outs = [torch.empty((w["H"], w["W"], 2), dtype=torch.float32).pin_memory() for _ in range(4)]
     for t in range(warmup):
-        f.loadImage(hnp[t % ring])
-        f.compute()
-        f.getFlow(out)
+        f.processAsync(host[t % ring], outs[t % 4])
         if t == 1:
+            f.synchronize()
             tuned(f, w)
     f.setGraphs(True)
-    torch.cuda.synchronize()
+    f.synchronize()
     t0 = time.perf_counter()
     for k in range(steps):
-        f.loadImage(hnp[(warmup + k) % ring])
-        f.compute()
-        f.getFlow(out)
+        f.processAsync(host[(warmup + k) % ring], outs[k % 4])
+    f.synchronize()
     t1 = time.perf_counter()
     return (t1 - t0) * 1000.0
 
@@ -568,7 +567,8 @@ def bench_b200(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": w["H"] * w["W"],
                     "d2h_bytes_per_step": w["H"] * w["W"] * 8,
-                    "path": "flowfilter_b200.PyramidalFlowFilter loadImage(pinned host) + compute() + getFlow(pinned host)"},
+                    "path": "flowfilter_b200.PyramidalFlowFilter.processAsync(pinned host frame -> pinned host flow), "
+                            "synchronize() at the end; wall clock"},
             "gpu_launches": args.steps * launches_per_frame,
             "clocks": clk.summary(),
             "extra": extra,

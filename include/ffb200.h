@@ -169,6 +169,15 @@ ff_status ff_filter_compute(ff_filter* f);
 /* Enqueue one frame on `stream` without blocking (elapsed time not updated). */
 ff_status ff_filter_compute_async(ff_filter* f, void* stream);
 /* Phase API of FlowFilter / DeltaFlowFilter (flowfilter.cu:155-197, 460-503). */
+/* Pipelined host processing (no reference counterpart; replaces the loadImage ->
+ * compute -> downloadFlow loop of a host-fed caller): uploads `in` on a copy stream,
+ * computes on `stream` (NULL = legacy default), downloads the smoothed level-0 flow into
+ * `out` on a second copy stream, and returns without waiting, so the copies of one frame
+ * overlap the computation of its neighbours.  `in` and `out` (pinned host memory for
+ * overlap) must stay untouched until ff_filter_synchronize; results equal those of the
+ * blocking loop.  Needs a filter that owns its input image. */
+ff_status ff_filter_process_host_async(ff_filter* f, const ff_image* in, ff_image* out, void* stream);
+ff_status ff_filter_synchronize(ff_filter* f);
 ff_status ff_filter_compute_image_model(ff_filter* f);
 ff_status ff_filter_compute_propagation(ff_filter* f);
 ff_status ff_filter_compute_update(ff_filter* f);

@@ -386,6 +386,16 @@ ff_status ff_filter_compute(ff_filter* f) {
 ff_status ff_filter_compute_async(ff_filter* f, void* stream) {
     return guard([&] { get(f)->compute_async((cudaStream_t)stream); });
 }
+ff_status ff_filter_process_host_async(ff_filter* f, const ff_image* in, ff_image* out, void* stream) {
+    return guard([&] {
+        need(in, "input image");
+        need(out, "flow buffer");
+        get(f)->process_host_async(*in, *out, (cudaStream_t)stream);
+    });
+}
+ff_status ff_filter_synchronize(ff_filter* f) {
+    return guard([&] { get(f)->synchronize(); });
+}
 ff_status ff_filter_compute_image_model(ff_filter* f) {
     return guard([&] { get(f)->phase_model(); });
 }

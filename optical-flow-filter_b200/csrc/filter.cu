@@ -169,7 +169,98 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
     }
 }
 
+Filter::HostPipe::~HostPipe() {
+    if (out) cudaStreamSynchronize(out);
+    if (in) cudaStreamSynchronize(in);
+    for (int k = 0; k < 2; ++k) {
+        for (cudaEvent_t e : {h2d[k], computed[k], d2h[k]})
+            if (e) cudaEventDestroy(e);
+        staging[k].release();
+    }
+    if (last_d2h) cudaEventDestroy(last_d2h);
+    if (in) cudaStreamDestroy(in);
+    if (out) cudaStreamDestroy(out);
+}
+
+void Filter::leave_pipe_mode() {
+    if (!pipe_mode_) return;
+    lv_[0].img = input_.p;
+    lv_[0].img_pitch = input_.pitch;
+    pipe_mode_ = false;
+    drop_graphs();
+}
+
+void Filter::synchronize() {
+    check_cuda(cudaEventSynchronize(done_), "synchronize");
+    if (pipe_) {
+        check_cuda(cudaStreamSynchronize(pipe_->out), "synchronize");
+        check_cuda(cudaStreamSynchronize(pipe_->in), "synchronize");
+        pipe_->pending = false;
+    }
+}
+
+void Filter::process_host_async(const ff_image& in, ff_image& out, cudaStream_t s) {
+    if (!input_.p || lv_[0].img_owned == false)
+        throw Error(FF_ERR_UNSUPPORTED, "pipelined host processing needs a filter that owns its input image");
+    check_image_shape(in.height, in.width, in.depth, (int)in.itemSize);
+    if (!in.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image data");
+    if (out.height != H_ || out.width != W_ || out.depth != 2 || out.itemSize != 4)
+        throw Error(FF_ERR_SHAPE, "flow buffer should be [" + std::to_string(H_) + ", " + std::to_string(W_) + ", 2][4]");
+    if (!out.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null flow buffer");
+    if (!pipe_) {
+        std::unique_ptr<HostPipe> p(new HostPipe);
+        check_cuda(cudaStreamCreateWithFlags(&p->in, cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaStreamCreateWithFlags(&p->out, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (int k = 0; k < 2; ++k) {
+            p->staging[k].alloc(H_, W_, item_);
+            for (cudaEvent_t* e : {&p->h2d[k], &p->computed[k], &p->d2h[k]}) {
+                check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+                check_cuda(cudaEventRecord(*e, stream_), "cudaEventRecord");
+            }
+        }
+        check_cuda(cudaEventCreateWithFlags(&p->last_d2h, cudaEventDisableTiming), "cudaEventCreate");
+        pipe_ = std::move(p);
+    }
+    HostPipe& P = *pipe_;
+    if (!pipe_mode_) {
+        drop_graphs();
+        pipe_mode_ = true;
+    }
+    const int p = cur_;
+    // upload into this parity's staging image once the frame two steps back stopped reading it
+    check_cuda(cudaStreamWaitEvent(P.in, P.computed[p], 0), "cudaStreamWaitEvent");
+    check_cuda(cudaMemcpy2DAsync(P.staging[p].p, P.staging[p].pitch, in.data, in.pitch, (size_t)W_ * item_, (size_t)H_,
+                                 cudaMemcpyHostToDevice, P.in),
+               "upload");
+    check_cuda(cudaEventRecord(P.h2d[p], P.in), "cudaEventRecord");
+    // compute: after the upload, and after the download of the frame two steps back, whose
+    // result buffer this frame overwrites
+    lv_[0].img = P.staging[p].p;
+    lv_[0].img_pitch = P.staging[p].pitch;
+    check_cuda(cudaStreamWaitEvent(s, P.h2d[p], 0), "cudaStreamWaitEvent");
+    check_cuda(cudaStreamWaitEvent(s, P.d2h[p], 0), "cudaStreamWaitEvent");
+    in_pipe_ = true;
+    try {
+        compute_async(s);
+    } catch (...) {
+        in_pipe_ = false;
+        throw;
+    }
+    in_pipe_ = false;
+    check_cuda(cudaEventRecord(P.computed[p], s), "cudaEventRecord");
+    // download the smoothed level-0 flow of this frame
+    const Buf& r = lv_[0].fs[cur_];
+    check_cuda(cudaStreamWaitEvent(P.out, P.computed[p], 0), "cudaStreamWaitEvent");
+    check_cuda(cudaMemcpy2DAsync(out.data, out.pitch, r.p, r.pitch, r.row_bytes(), (size_t)r.h, cudaMemcpyDeviceToHost,
+                                 P.out),
+               "download");
+    check_cuda(cudaEventRecord(P.d2h[p], P.out), "cudaEventRecord");
+    check_cuda(cudaEventRecord(P.last_d2h, P.out), "cudaEventRecord");
+    P.pending = true;
+}
+
 void Filter::release_runtime() {
+    pipe_.reset();
     drop_graphs();
     for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
     prof_ev_.clear();
@@ -196,7 +287,14 @@ Filter::~Filter() {
 
 // Every operation on the filter, on whichever stream, starts after the previous one
 // finished (event done_) and marks its own end; blocking calls use the filter's stream.
-void Filter::begin_on(cudaStream_t s) { check_cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent"); }
+void Filter::begin_on(cudaStream_t s) {
+    check_cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
+    // work outside the pipelined path must not overwrite a result still being downloaded
+    if (pipe_ && pipe_->pending && !in_pipe_) {
+        check_cuda(cudaStreamWaitEvent(s, pipe_->last_d2h, 0), "cudaStreamWaitEvent");
+        pipe_->pending = false;
+    }
+}
 void Filter::end_on(cudaStream_t s) {
     check_cuda(cudaEventRecord(done_, s), "cudaEventRecord");
     ++ops_;
@@ -304,6 +402,7 @@ void Filter::check_image_shape(int h, int w, int depth, int item) const {
 }
 
 void Filter::load_host(const ff_image& img) {
+    leave_pipe_mode();
     check_image_shape(img.height, img.width, img.depth, (int)img.itemSize);
     if (!img.data) throw Error(FF_ERR_INVALID_ARGUMENT, "null image data");
     Level& v = lv_[0];
@@ -317,6 +416,7 @@ void Filter::load_host(const ff_image& img) {
 }
 
 void Filter::load_device_async(const void* img, size_t pitch, cudaStream_t s) {
+    leave_pipe_mode();
     Level& v = lv_[0];
     if (!v.img) throw Error(FF_ERR_LOGIC, "input image has not been set");
     if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
@@ -328,6 +428,7 @@ void Filter::load_device_async(const void* img, size_t pitch, cudaStream_t s) {
 }
 
 void Filter::bind_device(const void* img, size_t pitch) {
+    pipe_mode_ = false;
     drop_graphs();
     if (!img) throw Error(FF_ERR_INVALID_ARGUMENT, "null image pointer");
     if (pitch < (size_t)W_ * item_) throw Error(FF_ERR_INVALID_ARGUMENT, "pitch smaller than a row");

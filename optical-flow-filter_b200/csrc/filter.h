@@ -14,6 +14,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "ffb200.h"
@@ -115,6 +116,12 @@ public:
 
     // compute
     void compute();                       // blocking, records elapsed time
+    // Pipelined host processing: upload `in` (host) on a copy stream, compute on s, and
+    // download the smoothed level-0 flow into `out` (host) on a second copy stream, so
+    // consecutive frames overlap.  Host buffers must stay valid until synchronize().
+    void process_host_async(const ff_image& in, ff_image& out, cudaStream_t s);
+    // block until every operation queued on the filter (pipelined copies included) is done
+    void synchronize();
     void compute_async(cudaStream_t s);   // enqueue only
     void phase_model();
     void phase_propagation();
@@ -213,6 +220,20 @@ private:
     cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
     int prof_cap_ = 0, prof_count_ = 0;
     std::vector<cudaEvent_t> prof_ev_;
+    // pipelined host processing: per state parity a staging input image and the events of
+    // its upload, its compute and the download of its result
+    struct HostPipe {
+        Buf staging[2];
+        cudaStream_t in = nullptr, out = nullptr;
+        cudaEvent_t h2d[2] = {nullptr, nullptr}, computed[2] = {nullptr, nullptr}, d2h[2] = {nullptr, nullptr};
+        cudaEvent_t last_d2h = nullptr;
+        bool pending = false;  // downloads queued that later non-pipelined work must wait for
+        ~HostPipe();
+    };
+    std::unique_ptr<HostPipe> pipe_;
+    bool pipe_mode_ = false;  // level 0 reads the staging images (graphs captured that way)
+    bool in_pipe_ = false;
+    void leave_pipe_mode();
 };
 
 }  // namespace ffb

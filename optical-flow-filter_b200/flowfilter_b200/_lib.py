@@ -107,6 +107,8 @@ SIGNATURES = {
     "ff_filter_bind_image_device": (_st, [_vp, _vp, _sz]),
     "ff_filter_compute": (_st, [_vp]),
     "ff_filter_compute_async": (_st, [_vp, _vp]),
+    "ff_filter_process_host_async": (_st, [_vp, ctypes.POINTER(FFImage), ctypes.POINTER(FFImage), _vp]),
+    "ff_filter_synchronize": (_st, [_vp]),
     "ff_filter_compute_image_model": (_st, [_vp]),
     "ff_filter_compute_propagation": (_st, [_vp]),
     "ff_filter_compute_update": (_st, [_vp]),

@@ -66,6 +66,21 @@ def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
 
 
+def _torch_cuda() -> bool:
+    try:
+        return _torch().cuda.is_available()
+    except ImportError:
+        return False
+
+
+def _host_array(x, dtype, shape) -> np.ndarray:
+    """A C-contiguous numpy view of a host buffer (numpy array or CPU tensor), no copy."""
+    arr = x.numpy() if _is_torch(x) else x
+    if not isinstance(arr, np.ndarray) or arr.dtype != dtype or arr.shape != shape or not arr.flags["C_CONTIGUOUS"]:
+        raise ValueError(f"expected a contiguous host {np.dtype(dtype).name} buffer of shape {shape}")
+    return arr
+
+
 class _FilterBase:
     _h = None
 
@@ -121,6 +136,27 @@ class _FilterBase:
         elif hasattr(stream, "cuda_stream"):
             stream = stream.cuda_stream
         call("ff_filter_compute_async", self._h, ctypes.c_void_p(stream))
+
+    def processAsync(self, frame, flow, stream=None) -> None:
+        """Pipelined loadImage + compute + downloadFlow for host buffers: ``frame`` (H, W) and
+        ``flow`` (H, W, 2) float32 are numpy arrays or CPU tensors (pinned for overlap); the
+        call returns at once and ``flow`` is filled once ``synchronize()`` returns.  Keep
+        both buffers untouched until then."""
+        dtype = np.uint8 if self._item() == 1 else np.float32
+        fin = _host_array(frame, dtype, (self.height, self.width))
+        fout = _host_array(flow, np.float32, (self.height, self.width, 2))
+        img_in, _ = _host_image(fin, 1)
+        img_out, _ = _host_image(fout, 2)
+        if stream is None:
+            stream = _torch().cuda.current_stream().cuda_stream if _torch_cuda() else 0
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        call("ff_filter_process_host_async", self._h, ctypes.byref(img_in), ctypes.byref(img_out),
+             ctypes.c_void_p(stream))
+
+    def synchronize(self) -> None:
+        """Wait for everything queued on the filter, pipelined copies included."""
+        call("ff_filter_synchronize", self._h)
 
     def elapsedTime(self) -> float:
         ms = ctypes.c_float()

@@ -382,3 +382,41 @@ def test_tile_kernel_matches_per_stage(ffb, cuda, case):
             f.compute()
             np.testing.assert_array_equal(f.getFlow(), want, err_msg=f"tile shape {c} frame {t} ({f.tuning()})")
             np.testing.assert_array_equal(f.getImage(), ref.getImage())
+
+
+@pytest.mark.parametrize("levels", [0, 2, 3])
+def test_pipelined_host_processing_matches_blocking_loop(ffb, cuda, levels):
+    """processAsync (upload, compute and download overlapped on three streams) gives the
+    blocking loadImage/compute/downloadFlow results, also with graphs and when the caller
+    returns to the blocking calls afterwards."""
+    h, w, t = 120, 160, 9
+    frames = case_frames(dict(seq="bumps", frames=t, kw=dict(height=h, width=w, sigma=1.0, seed=51, n_bumps=2,
+                                                              bump_sigma=40.0, amp=2.0)))
+
+    def make():
+        if levels == 0:
+            return ffb.FlowFilter(h, w, 2, 4.0, 10.0)
+        f = ffb.PyramidalFlowFilter(h, w, levels)
+        f.maxflow = 4.0
+        f.smoothIterations = [1, 2, 4][:levels]
+        return f
+
+    ref, pip = make(), make()
+    want = []
+    for k in range(t):
+        ref.loadImage(frames[k])
+        ref.compute()
+        want.append(ref.flowTensor().cpu().numpy())
+    hin = cuda.from_numpy(frames).pin_memory()
+    outs = [cuda.empty((h, w, 2), dtype=cuda.float32).pin_memory() for _ in range(t)]
+    for k in range(6):
+        if k == 3:
+            pip.setGraphs(True)
+        pip.processAsync(hin[k], outs[k])
+    pip.synchronize()
+    for k in range(6):
+        np.testing.assert_array_equal(outs[k].numpy(), want[k], err_msg=f"frame {k}")
+    for k in range(6, t):  # back to the blocking path
+        pip.loadImage(frames[k])
+        pip.compute()
+        np.testing.assert_array_equal(pip.flowTensor().cpu().numpy(), want[k], err_msg=f"frame {k}")
