@@ -180,6 +180,13 @@ class ClockSampler:
                 "samples": len(self.sm), "source": "nvml"}
 
 
+def dist_backend() -> str:
+    """NCCL between GPU ranks; gloo when there is no GPU (the CPU tests of the N>1 path)."""
+    import torch
+
+    return os.environ.get("FFB_DIST_BACKEND") or ("nccl" if torch.cuda.is_available() else "gloo")
+
+
 def dist_setup():
     import torch
 
@@ -191,9 +198,13 @@ def dist_setup():
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        backend = dist_backend()
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     elif torch.cuda.is_available():
         torch.cuda.set_device(local)
     return world, rank, local
@@ -206,7 +217,8 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(world, value: float) -> float:
@@ -216,9 +228,15 @@ def max_over_ranks(world, value: float) -> float:
         return value
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: int, max_ms: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1000.0)
 
 
 def gpu_uuid(local):
@@ -495,7 +513,7 @@ def bench_b200(args):
         step_ms, _, filt = device_run(w, dev_frames, args.steps, args.warmup, flush)
         barrier(world)
     step_ms = max_over_ranks(world, step_ms)
-    value = world * args.steps / (step_ms / 1000.0)
+    value = aggregate_rate(world, args.steps, step_ms)
 
     # ---- dominant kernel step (level 0) timed live: its captured graph, L2 flushed before each
     l0_ms = filt.timeLevel(0, min(args.steps, 1000), flush)
@@ -506,7 +524,7 @@ def bench_b200(args):
     # ---- end to end through the public API with host buffers
     e2e_steps = min(args.steps, 2000)
     e2e_ms = max_over_ranks(world, e2e_run(w, frames, e2e_steps, args.warmup))
-    e2e_fps = world * e2e_steps / (e2e_ms / 1000.0)
+    e2e_fps = aggregate_rate(world, e2e_steps, e2e_ms)
 
     # ---- the throughput workload beside it
     we = WORKLOADS[EXTRA]
@@ -519,7 +537,7 @@ def bench_b200(args):
     ems = max_over_ranks(world, ems)
     el0 = efilt.timeLevel(0, min(ksteps, 1000), flush)
     eb = level0_kernel_bytes(we)
-    e_fps = world * ksteps / (ems / 1000.0)
+    e_fps = aggregate_rate(world, ksteps, ems)
     extra = {
         "workload": EXTRA, "value": e_fps, "unit": "frames/s", "steps": ksteps,
         "ms_per_step": ems / ksteps, "mpix_per_s": e_fps * we["H"] * we["W"] / 1e6,
