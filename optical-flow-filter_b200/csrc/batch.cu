@@ -267,6 +267,10 @@ void Batch::build(Table& t) {
             j.g = batch_geom(v.delta, v.iters, v.smooth, v.W, v.H, &smem);
             const int tiles = j.g.tiles_x * ((v.H + j.g.TH - 1) / j.g.TH);
             const bool late = L >= 2 && l == L - 2;
+            // launch B follows launch A (which holds every top level): its jobs wait for A only
+            // before their update, and A lets B's blocks start at once
+            j.a.pdl_late_wait = late ? 1 : 0;
+            j.a.pdl_early_trigger = late ? 0 : 1;
             if (late) {
                 j.first_block = blocks_b;
                 blocks_b += tiles;

@@ -616,7 +616,17 @@ void Filter::launch_fused(int l, int band, cudaStream_t s) {
 
 void Filter::launch_tile(int l, int cfg, cudaStream_t s) {
     const Level& v = lv_[l];
-    check_cuda(launch_tile_level(v.delta, v.iters, v.smooth, level_args(l), cfg, s), "tile level");
+    LevelArgs a = level_args(l);
+    // In a pyramid frame the top level's tile kernel is followed on the same stream by level
+    // L-2's, which reads the top's output only from its update on: the top lets it start at
+    // once, and it waits only before its update (so its propagation overlaps the top level).
+    if (kind_ == Kind::Pyramidal && L_ >= 2 && pdl_chain_) {
+        int p_top = 0, p_next = 0;
+        const bool top_tile = path_of(L_ - 1, &p_top) == kTile, next_tile = path_of(L_ - 2, &p_next) == kTile;
+        if (l == L_ - 1 && next_tile) a.pdl_early_trigger = 1;
+        if (l == L_ - 2 && top_tile) a.pdl_late_wait = 1;
+    }
+    check_cuda(launch_tile_level(v.delta, v.iters, v.smooth, a, cfg, s), "tile level");
 }
 
 void Filter::step_level(int l, cudaStream_t s) {
@@ -864,8 +874,11 @@ void Filter::enqueue_frame(cudaStream_t s) {
         check_cuda(cudaStreamWaitEvent(side_, ev_pyr_, 0), "cudaStreamWaitEvent");
         for (int l = 1; l < side_levels; ++l) level_on(l, side_);
     }
-    // top first (level L-2 reads its fresh unsmoothed flow)
+    // top first (level L-2 reads its fresh unsmoothed flow); with profiling events between
+    // the launches there is no programmatic edge to exploit
+    pdl_chain_ = !prof;
     for (int l = L_ - 1; l >= side_levels; --l) level_on(l, s);
+    pdl_chain_ = false;
     if (side_levels > 0) {
         check_cuda(cudaEventRecord(ev_join_, side_), "cudaEventRecord");
         check_cuda(cudaStreamWaitEvent(s, ev_join_, 0), "cudaStreamWaitEvent");

@@ -233,6 +233,7 @@ private:
     std::unique_ptr<HostPipe> pipe_;
     bool pipe_mode_ = false;  // level 0 reads the staging images (graphs captured that way)
     bool in_pipe_ = false;
+    bool pdl_chain_ = false;  // set while enqueue_frame launches the top -> L-2 chain
     void leave_pipe_mode();
 };
 

@@ -48,6 +48,11 @@ struct LevelArgs {
     int border;
     int first;
     int band;            // rows per warp band (0: chosen from the SM count)
+    // programmatic dependent launch (tile kernel): wait for the preceding kernel only before
+    // the update (its stages before need nothing that kernel writes), and let the next
+    // kernel's blocks start right after this kernel's own wait
+    int pdl_late_wait;
+    int pdl_early_trigger;
 };
 
 // true if a fused kernel exists for this (delta, item, iterations, smoothing)

@@ -161,7 +161,14 @@ __device__ __forceinline__ float2 box5_2(const Five& f) {
 // described by (a, g), in the dynamic shared memory `sm`.
 template <bool DELTA, typename P>
 __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int tile, unsigned char* sm) {
-    grid_dep_wait();
+    // Ordering with the preceding kernel (PDL): by default wait for it before anything.  With
+    // pdl_late_wait (a delta level launched right after its top level) the state load,
+    // propagation and image model read only the previous frame's state and an image that
+    // was complete before the preceding kernel passed its own wait, so the wait moves to
+    // just before the update, the first stage that reads the coarse flow.
+    const bool late_wait = a.pdl_late_wait != 0;
+    if (!late_wait) grid_dep_wait();
+    if (a.pdl_early_trigger) grid_dep_launch();
     const int W = a.W, H = a.H;
     const int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
     const int x0 = tx * g.TW, y0 = ty * g.TH;
@@ -313,6 +320,8 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
     }
     __syncthreads();
 
+    if (late_wait) grid_dep_wait();
+
     // ---- update over radius 2S: the new flow goes to A's flow field in place
     {
         const float gamma = a.gamma, maxflow = a.maxflow;
@@ -400,7 +409,7 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
         __syncthreads();
         const bool last = s == g.S;
         // the next kernel in the stream may start scheduling its blocks from here on
-        if (last) grid_dep_launch();
+        if (last && !a.pdl_early_trigger) grid_dep_launch();
         walk(
             xa(r), xb(r), ya(r), yb(r), SW, sidx(xa(r), ya(r)),
             [&](int, int y, int k) {
