@@ -6,10 +6,10 @@
 // then runs every stage of the level there, each stage over a region one stencil radius
 // smaller than the one before:
 //
-//   N x (upwind X sub-step, upwind Y sub-step)    radius R     -> 2S   (ping-pong A <-> B)
-//   image model of the new frame                  radius 2S + 2 -> 2S  (in B)
-//   update (2x2 solve, clamps, coarse upsample)   radius 2S            (in place in A)
-//   S x (5-tap box X, 5-tap box Y)                radius 2S    -> 0    (A <-> B, last pass to HBM)
+//   N x (upwind X sub-step, upwind Y sub-step)    radius R     -> 2S   (one pass per pair, A <-> B)
+//   image model of the new frame                  radius 2S + 2 -> 2S  (in the spare buffer)
+//   update (2x2 solve, clamps, coarse upsample)   radius 2S            (in place)
+//   S x (5-tap box X, 5-tap box Y)                radius 2S    -> 0    (ping-pong, last pass to HBM)
 //
 // Reads outside the image are clamped to the edge, as the reference's textures do
 // (cudaAddressModeClamp), so a region that touches the image border simply stops there.
@@ -40,9 +40,9 @@ struct Geom {
 };
 
 // Shared-memory bytes of one tile.  Buffers A and B each hold the state fields over the
-// state region: float2 flow, then for delta levels float2 delta and float old image.  B
-// also hosts the image model (the image, its Y blur and its X blur) between the last
-// propagation sub-step and the update.
+// state region: float2 flow, then for delta levels float2 delta and float old image.  The
+// buffer that does not hold the propagated state hosts the image model (the image, its Y
+// blur and its X blur) between the propagation and the update.
 struct Layout {
     size_t a, b, c, total;
 };
@@ -54,8 +54,10 @@ inline Layout layout(bool delta, int N, int S, int tw, int th) {
     const size_t iw = tw + 2 * rI, ih = th + 2 * rI;
     const size_t model = (iw * ih + (th + 4 * (size_t)S) * iw + ih * (tw + 4 * (size_t)S)) * 4;
     Layout L;
-    L.a = (ns * fb + 15) / 16 * 16;
-    L.b = (std::max(ns * fb, model) + 15) / 16 * 16;
+    // the propagated state ends in A or in B (one swap per sub-step pair), and the image
+    // model then lives in the other buffer: both are sized for either use
+    L.a = (std::max(ns * fb, model) + 15) / 16 * 16;
+    L.b = L.a;
     L.c = delta ? ((size_t)tw + 4 * (size_t)S) * 4 : 0;
     L.total = L.a + L.b + L.c;
     return L;
@@ -130,24 +132,28 @@ __device__ __forceinline__ PropIn prop_load(const float2* fs, const float2* ds, 
     return p;
 }
 
+// the state fields of one pixel
+struct PropOut {
+    float2 f;
+    float s;
+    float2 v;
+};
+
 // One upwind sub-step at one pixel: propagate_pass_k<AXIS, DELTA> (stage_kernels.cu).
 template <int AXIS, bool DELTA>
-__device__ __forceinline__ void prop_store(const PropIn& p, float2* fd, float2* dd, float* id, int k, float dt,
-                                           bool in) {
+__device__ __forceinline__ PropOut prop_eval(const PropIn& p, float dt, bool in) {
     const float dv = AXIS == 0 ? dominant(p.fm.x, p.fp.x) : dominant(p.fm.y, p.fp.y);
     const float t = __fmul_rn(dt, dv);
-    float2 o;
-    o.x = in ? upwind(t, dv, p.fm.x, p.f0.x, p.fp.x) : p.f0.x;
-    if constexpr (DELTA) o.y = in ? upwind(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
-    else o.y = in ? upwind_unfused(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
-    fd[k] = o;
+    PropOut o;
+    o.f.x = in ? upwind(t, dv, p.fm.x, p.f0.x, p.fp.x) : p.f0.x;
+    if constexpr (DELTA) o.f.y = in ? upwind(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
+    else o.f.y = in ? upwind_unfused(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
     if constexpr (DELTA) {
-        id[k] = in ? upwind(t, dv, p.sm, p.s0, p.sp) : p.s0;
-        float2 ov;
-        ov.x = in ? upwind(t, dv, p.vm.x, p.v0.x, p.vp.x) : p.v0.x;
-        ov.y = in ? upwind_unfused(t, dv, p.vm.y, p.v0.y, p.vp.y) : p.v0.y;
-        dd[k] = ov;
+        o.s = in ? upwind(t, dv, p.sm, p.s0, p.sp) : p.s0;
+        o.v.x = in ? upwind(t, dv, p.vm.x, p.v0.x, p.vp.x) : p.v0.x;
+        o.v.y = in ? upwind_unfused(t, dv, p.vm.y, p.v0.y, p.vp.y) : p.v0.y;
     }
+    return o;
 }
 
 struct Five {
@@ -237,42 +243,76 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
     }
     __syncthreads();
 
-    // ---- propagation: N x (X, Y) sub-steps, dt = 1/N (propagation.cu:146-147)
+    // ---- propagation: N x (X, Y) sub-steps, dt = 1/N (propagation.cu:146-147).  Each X/Y
+    // pair is one pass: a warp takes a 32-column chunk and a band of rows, computes the X
+    // sub-step for rows y-1, y, y+1 into a rolling register window and the Y sub-step from
+    // it, so the X result never goes through shared memory (one barrier per pair).
     const float dt = 1.0f / (float)g.N;
     float2 *fs = fA, *fd = fB, *ds = dA, *dd = dB;
     float *is = iA, *id = iB;
-    for (int j = 1; j <= g.N; ++j) {
-        const int rx = g.R - j, ry = g.R - j + 1;
-        walk(
-            xa(rx), xb(rx), ya(ry), yb(ry), SW, sidx(xa(rx), ya(ry)),
-            [&](int x, int, int k) { return prop_load<DELTA>(fs, ds, is, k, k - (x > 0), k + (x < W - 1)); },
-            [&](int x, int y, int k, const PropIn& p) {
-                prop_store<0, DELTA>(p, fd, dd, id, k, dt, col_in(x) && row_in(y));
-            });
-        __syncthreads();
-        swap2(fs, fd);
-        swap2(ds, dd);
-        swap2(is, id);
-        walk(
-            xa(rx), xb(rx), ya(rx), yb(rx), SW, sidx(xa(rx), ya(rx)),
-            [&](int, int y, int k) {
-                return prop_load<DELTA>(fs, ds, is, k, y > 0 ? k - SW : k, y < H - 1 ? k + SW : k);
-            },
-            [&](int x, int y, int k, const PropIn& p) {
-                prop_store<1, DELTA>(p, fd, dd, id, k, dt, col_in(x) && row_in(y));
-            });
-        __syncthreads();
-        swap2(fs, fd);
-        swap2(ds, dd);
-        swap2(is, id);
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int j = 1; j <= g.N; ++j) {
+            const int r = g.R - j;  // output radius of this pair; its X sub-step reads radius r + 1
+            const int cxa = xa(r), cxb = xb(r), rya = ya(r), ryb = yb(r);
+            const int nc = (cxb - cxa + 31) >> 5;
+            const int nb = max(1, nw / nc);
+            const int K = (ryb - rya + nb - 1) / nb;
+            for (int item = warp; item < nc * nb; item += nw) {
+                const int band = item / nc, c = item - band * nc;
+                const int x = min(cxa + c * 32 + lane, cxb - 1);  // spare lanes repeat the last column
+                const int by0 = rya + band * K, by1 = min(by0 + K, ryb);
+                if (by0 >= by1) continue;
+                const int kc = x - ox;
+                const int dxm = x > 0 ? 1 : 0, dxp = x < W - 1 ? 1 : 0;
+                const bool cin = col_in(x);
+                auto xstep = [&](int row) {
+                    const int k = (row - oy) * SW + kc;
+                    return prop_eval<0, DELTA>(prop_load<DELTA>(fs, ds, is, k, k - dxm, k + dxp), dt,
+                                               cin && row_in(row));
+                };
+                PropOut cur = xstep(by0);
+                PropOut prev = by0 > 0 ? xstep(by0 - 1) : cur;  // row -1 clamps to row 0
+                for (int y = by0; y < by1; ++y) {
+                    const PropOut nxt = y + 1 < H ? xstep(y + 1) : cur;  // row H clamps to H - 1
+                    PropIn q;
+                    q.fm = prev.f;
+                    q.f0 = cur.f;
+                    q.fp = nxt.f;
+                    if constexpr (DELTA) {
+                        q.sm = prev.s;
+                        q.s0 = cur.s;
+                        q.sp = nxt.s;
+                        q.vm = prev.v;
+                        q.v0 = cur.v;
+                        q.vp = nxt.v;
+                    }
+                    const PropOut o = prop_eval<1, DELTA>(q, dt, cin && row_in(y));
+                    const int k = (y - oy) * SW + kc;
+                    fd[k] = o.f;
+                    if constexpr (DELTA) {
+                        id[k] = o.s;
+                        dd[k] = o.v;
+                    }
+                    prev = cur;
+                    cur = nxt;
+                }
+            }
+            __syncthreads();
+            swap2(fs, fd);
+            swap2(ds, dd);
+            swap2(is, id);
+        }
     }
-    // 2N swaps: the propagated state is in A again
+    // the propagated state is in fs/is/ds (buffer A for even N, B for odd N); the image model
+    // goes to the other buffer
+    unsigned char* const spare = reinterpret_cast<unsigned char*>(fd);
 
     // ---- image model of the new frame (imagemodel_k.cu:31-133) over radius 2S, in B
     const int S2 = 2 * g.S, rI = S2 + 2;
     const int IW = g.TW + 2 * rI, BXW = g.TW + 2 * S2;
     const int IH = g.TH + 2 * rI;
-    float* img = reinterpret_cast<float*>(sm + g.offB);  // origin (x0 - rI, y0 - rI), IW x IH
+    float* img = reinterpret_cast<float*>(spare);        // origin (x0 - rI, y0 - rI), IW x IH
     float* byv = img + IW * IH;                          // Y blur, origin (x0 - rI, y0 - 2S), IW wide
     float* bxv = byv + (g.TH + 2 * S2) * IW;             // X blur, origin (x0 - 2S, y0 - rI), BXW wide
     int* ccol = reinterpret_cast<int*>(sm + g.offC);     // coarse column of each column, origin x0 - 2S
@@ -322,7 +362,7 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
 
     if (late_wait) grid_dep_wait();
 
-    // ---- update over radius 2S: the new flow goes to A's flow field in place
+    // ---- update over radius 2S: the new flow goes to the propagated flow field in place
     {
         const float gamma = a.gamma, maxflow = a.maxflow;
         struct UpdIn {
@@ -348,13 +388,13 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
                 u.c3 = bxv[kx + min(H - 1 - y, 1) * BXW];
                 u.c4 = bxv[kx + min(H - 1 - y, 2) * BXW];
                 if constexpr (DELTA) {
-                    u.old = iA[k];
-                    u.f = dA[k];
+                    u.old = is[k];
+                    u.f = ds[k];
                     const int cr = __ldg(coarse_rows + y);
                     u.up = __ldg(grow<float2>(coarse, coarse_p, cr) + ccol[x - x0 + S2]);
                 } else {
                     u.old = __ldg(grow<float>(io_in, io_in_p, y) + x);
-                    u.f = fA[k];
+                    u.f = fs[k];
                 }
                 return u;
             },
@@ -373,7 +413,7 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
                     const float dy = clampm(sanitize(fy), hm);
                     const float gx = __fadd_rn(dx, __fmul_rn(2.0f, u.up.x));
                     const float gy = __fadd_rn(dy, __fmul_rn(2.0f, u.up.y));
-                    fA[k] = make_float2(clampm(gx, maxflow), clampm(gy, maxflow));
+                    fs[k] = make_float2(clampm(gx, maxflow), clampm(gy, maxflow));
                     if (out) {
                         growm<float2>(d_out, d_out_p, y)[x] = make_float2(dx, dy);
                         growm<float>(io_out, io_out_p, y)[x] = c;
@@ -381,7 +421,7 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
                 } else {
                     // flowUpdate_k (update_k.cu:15-79); the old image is the previous frame's a0
                     const float2 o = make_float2(sanitize(clampm(fx, maxflow)), sanitize(clampm(fy, maxflow)));
-                    fA[k] = o;
+                    fs[k] = o;
                     if (out) {
                         if (fu_out) growm<float2>(fu_out, fu_out_p, y)[x] = o;
                         growm<float>(io_out, io_out_p, y)[x] = c;
@@ -398,14 +438,14 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
             xa(r), xb(r), ya(r + 2), yb(r + 2), SW, sidx(xa(r), ya(r + 2)),
             [&](int x, int, int k) {
                 Five f;
-                f.v0 = fA[k - min(x, 2)];
-                f.v1 = fA[k - min(x, 1)];
-                f.v2 = fA[k];
-                f.v3 = fA[k + min(W - 1 - x, 1)];
-                f.v4 = fA[k + min(W - 1 - x, 2)];
+                f.v0 = fs[k - min(x, 2)];
+                f.v1 = fs[k - min(x, 1)];
+                f.v2 = fs[k];
+                f.v3 = fs[k + min(W - 1 - x, 1)];
+                f.v4 = fs[k + min(W - 1 - x, 2)];
                 return f;
             },
-            [&](int, int, int k, const Five& f) { fB[k] = box5_2(f); });
+            [&](int, int, int k, const Five& f) { fd[k] = box5_2(f); });
         __syncthreads();
         const bool last = s == g.S;
         // the next kernel in the stream may start scheduling its blocks from here on
@@ -414,17 +454,17 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
             xa(r), xb(r), ya(r), yb(r), SW, sidx(xa(r), ya(r)),
             [&](int, int y, int k) {
                 Five f;
-                f.v0 = fB[k - min(y, 2) * SW];
-                f.v1 = fB[k - min(y, 1) * SW];
-                f.v2 = fB[k];
-                f.v3 = fB[k + min(H - 1 - y, 1) * SW];
-                f.v4 = fB[k + min(H - 1 - y, 2) * SW];
+                f.v0 = fd[k - min(y, 2) * SW];
+                f.v1 = fd[k - min(y, 1) * SW];
+                f.v2 = fd[k];
+                f.v3 = fd[k + min(H - 1 - y, 1) * SW];
+                f.v4 = fd[k + min(H - 1 - y, 2) * SW];
                 return f;
             },
             [&](int x, int y, int k, const Five& f) {
                 const float2 o = box5_2(f);
                 if (last) growm<float2>(fs_out, fs_out_p, y)[x] = o;
-                else fA[k] = o;
+                else fs[k] = o;
             });
         if (!last) __syncthreads();
     }

@@ -10,7 +10,7 @@ namespace ffb {
 namespace tile {
 
 template <bool DELTA, typename P>
-__global__ void __launch_bounds__(512, 2) tile_k(LevelArgs a, Geom g) {
+__global__ void __launch_bounds__(1024) tile_k(LevelArgs a, Geom g) {
     extern __shared__ __align__(16) unsigned char sm[];
     tile_body<DELTA, P>(a, g, blockIdx.x, sm);
 }
@@ -35,14 +35,16 @@ DeviceInfo device_info() {
     return d;
 }
 
-// A tile-shape choice is a tile width and a number of tiles resident per SM; the tile
-// height follows so that the tiles fill whole waves of the GPU (as few as fit in shared
-// memory).  Index 0 is the automatic choice.
+// A tile-shape choice is a tile width, a number of tiles resident per SM and the threads of
+// a tile; the tile height follows so that the tiles fill whole waves of the GPU (as few as
+// fit in shared memory).  Index 0 is the automatic choice.
 struct Choice {
-    int tw, per_sm;
+    int tw, per_sm, threads;
 };
-constexpr Choice kChoices[] = {{0, 0},  {32, 1}, {32, 2}, {32, 3}, {48, 1}, {48, 2}, {48, 3},
-                               {64, 1}, {64, 2}, {64, 3}, {96, 1}, {96, 2}, {128, 1}};
+constexpr Choice kChoices[] = {{0, 0, 0},     {32, 1, 512},  {32, 2, 512},  {32, 3, 256},  {48, 1, 512},
+                               {48, 2, 512},  {48, 3, 256},  {64, 1, 512},  {64, 2, 512},  {64, 3, 256},
+                               {96, 1, 512},  {96, 2, 512},  {128, 1, 512}, {32, 1, 1024}, {48, 1, 1024},
+                               {64, 1, 1024}, {96, 1, 1024}, {128, 1, 1024}};
 constexpr int kNumChoices = sizeof(kChoices) / sizeof(kChoices[0]);
 constexpr size_t kSmemPerSM = 228 * 1024;  // B200 shared memory per SM
 constexpr size_t kSmemReserve = 1024;      // per resident block
@@ -55,7 +57,7 @@ Cfg shape_of(Choice c, bool delta, int N, int S, int W, int H) {
     Cfg out;
     if (c.tw <= 0) return out;
     const DeviceInfo d = device_info();
-    const int threads = c.per_sm >= 3 ? 256 : 512;
+    const int threads = c.threads;
     if (threads * c.per_sm > 2048) return out;
     const int tiles_x = (W + c.tw - 1) / c.tw;
     for (int waves = 1; waves <= 256; ++waves) {
