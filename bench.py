@@ -90,8 +90,9 @@ def kernels_per_frame(w, tuning: str) -> int:
     (streaming or tile) or the per-stage kernels (model, 2N propagation passes, update,
     2S smoothing passes)."""
     L = w["levels"]
-    n = L - 1
     parts = [p.strip() for p in tuning.split(";")]
+    # a two-level pyramid whose top level runs the tile kernel makes level 1 inside it
+    n = 0 if (L == 2 and len(parts) > 1 and "tile" in parts[1]) else L - 1
     for l in range(L):
         m = w["maxflow"] / (2 ** min(l, L - 1))
         N = int(np.ceil(np.float32(m)))

@@ -81,9 +81,10 @@ __device__ __forceinline__ uint8_t quantize_u8(float s) {
 }
 
 // One pixel of the next pyramid level: imageDownX then imageDownY (pyramid_k.cu:14-145),
-// the X-pass value at (2x+k, 2y+j) recomputed in registers.  out is (H/2) x (W/2) of in.
+// the X-pass value at (2x+k, 2y+j) recomputed in registers; the next level is
+// (H/2) x (W/2) of in.
 template <typename P>
-__device__ __forceinline__ void pyramid_px(const CView<P>& in, const View<P>& out, int x, int y) {
+__device__ __forceinline__ P pyramid_val(const CView<P>& in, int x, int y) {
     float xs[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
@@ -96,8 +97,12 @@ __device__ __forceinline__ void pyramid_px(const CView<P>& in, const View<P>& ou
         else xs[j] = s;
     }
     float s = down3(xs[0], xs[1], xs[2]);
-    if constexpr (sizeof(P) == 1) out.at(x, y) = quantize_u8(s);
-    else out.at(x, y) = s;
+    if constexpr (sizeof(P) == 1) return quantize_u8(s);
+    else return s;
+}
+template <typename P>
+__device__ __forceinline__ void pyramid_px(const CView<P>& in, const View<P>& out, int x, int y) {
+    out.at(x, y) = pyramid_val(in, x, y);
 }
 
 // dominant velocity: |v+| - |v-| > 0 ? v+ : v-   (propagation_k.cu:37-40)

@@ -626,6 +626,13 @@ void Filter::launch_tile(int l, int cfg, cudaStream_t s) {
         if (l == L_ - 1 && next_tile) a.pdl_early_trigger = 1;
         if (l == L_ - 2 && top_tile) a.pdl_late_wait = 1;
     }
+    if (fuse_pyramid_ && l == L_ - 1) {
+        const Level& fine = lv_[0];
+        a.pyr_src = fine.img;
+        a.pyr_src_pitch = fine.img_pitch;
+        a.pyr_src_H = fine.H;
+        a.pyr_src_W = fine.W;
+    }
     check_cuda(launch_tile_level(v.delta, v.iters, v.smooth, a, cfg, s), "tile level");
 }
 
@@ -861,7 +868,11 @@ void Filter::enqueue_frame(cudaStream_t s) {
         check_cuda(cudaStreamWaitEvent(side_, ev_fork_, 0), "cudaStreamWaitEvent");
         level_on(0, side_);
     }
-    if (kind_ == Kind::Pyramidal) {
+    // a two-level pyramid whose top level runs the tile kernel computes its level image
+    // inside that kernel (the pyramid step needs no launch of its own)
+    int p_top = 0;
+    fuse_pyramid_ = kind_ == Kind::Pyramidal && L_ == 2 && path_of(1, &p_top) == kTile;
+    if (kind_ == Kind::Pyramidal && !fuse_pyramid_) {
         for (int l = 1; l < L_; ++l) {
             const Level& fine = lv_[l - 1];
             check_cuda(launch_pyramid_down(fine.img, fine.img_pitch, item_, fine.H, fine.W, pyr_[l - 1].p,
@@ -879,6 +890,7 @@ void Filter::enqueue_frame(cudaStream_t s) {
     pdl_chain_ = !prof;
     for (int l = L_ - 1; l >= side_levels; --l) level_on(l, s);
     pdl_chain_ = false;
+    fuse_pyramid_ = false;
     if (side_levels > 0) {
         check_cuda(cudaEventRecord(ev_join_, side_), "cudaEventRecord");
         check_cuda(cudaStreamWaitEvent(s, ev_join_, 0), "cudaStreamWaitEvent");

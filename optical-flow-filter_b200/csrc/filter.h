@@ -234,6 +234,7 @@ private:
     bool pipe_mode_ = false;  // level 0 reads the staging images (graphs captured that way)
     bool in_pipe_ = false;
     bool pdl_chain_ = false;  // set while enqueue_frame launches the top -> L-2 chain
+    bool fuse_pyramid_ = false;  // set while enqueue_frame runs a frame whose top kernel makes level 1
     void leave_pipe_mode();
 };
 

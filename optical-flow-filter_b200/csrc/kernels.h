@@ -53,6 +53,10 @@ struct LevelArgs {
     // kernel's blocks start right after this kernel's own wait
     int pdl_late_wait;
     int pdl_early_trigger;
+    // tile kernel of a two-level pyramid's top level: compute this level's image from the
+    // finer image (the pyramid step) instead of reading it, and store the tile's pixels of
+    // it to img (so every other reader still finds the level image); null otherwise
+    const void* pyr_src; size_t pyr_src_pitch; int pyr_src_H, pyr_src_W;
 };
 
 // true if a fused kernel exists for this (delta, item, iterations, smoothing)

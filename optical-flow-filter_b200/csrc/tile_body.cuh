@@ -317,10 +317,22 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
     float* bxv = byv + (g.TH + 2 * S2) * IW;             // X blur, origin (x0 - 2S, y0 - rI), BXW wide
     int* ccol = reinterpret_cast<int*>(sm + g.offC);     // coarse column of each column, origin x0 - 2S
     auto iidx = [&](int x, int y) { return (y - y0 + rI) * IW + (x - x0 + rI); };
-    walk(
-        xa(rI), xb(rI), ya(rI), yb(rI), IW, iidx(xa(rI), ya(rI)),
-        [&](int x, int y, int) { return __ldg(grow<P>(img_in, img_p, y) + x); },
-        [&](int, int, int k, P v) { img[k] = Pix<P>::get(v); });
+    if (a.pyr_src) {
+        // fused pyramid step: this level's image from the finer one (pyramid_down_k)
+        const CView<P> fine{reinterpret_cast<const P*>(a.pyr_src), a.pyr_src_pitch, a.pyr_src_H, a.pyr_src_W};
+        walk(
+            xa(rI), xb(rI), ya(rI), yb(rI), IW, iidx(xa(rI), ya(rI)),
+            [&](int x, int y, int) { return pyramid_val(fine, x, y); },
+            [&](int x, int y, int k, P v) {
+                img[k] = Pix<P>::get(v);
+                if (x >= x0 && x < x1 && y >= y0 && y < y1) growm<P>(const_cast<void*>(a.img), img_p, y)[x] = v;
+            });
+    } else {
+        walk(
+            xa(rI), xb(rI), ya(rI), yb(rI), IW, iidx(xa(rI), ya(rI)),
+            [&](int x, int y, int) { return __ldg(grow<P>(img_in, img_p, y) + x); },
+            [&](int, int, int k, P v) { img[k] = Pix<P>::get(v); });
+    }
     if constexpr (DELTA) {
         for (int x = xa(S2) + (int)threadIdx.x; x < xb(S2); x += blockDim.x) ccol[x - x0 + S2] = upmap_index(x, W, a.Wc);
     }
