@@ -22,6 +22,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -250,6 +251,9 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
     const float dt = 1.0f / (float)g.N;
     float2 *fs = fA, *fd = fB, *ds = dA, *dd = dB;
     float *is = iA, *id = iB;
+    // A tile whose whole state region lies inside the propagation border (x, y in [B, size-B))
+    // has no frozen pixel: its sub-steps skip the border test and its selects.
+    const bool interior = x0 - g.R >= B && x1 + g.R <= W - B && y0 - g.R >= B && y1 + g.R <= H - B;
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         for (int j = 1; j <= g.N; ++j) {
@@ -266,37 +270,45 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
                 const int kc = x - ox;
                 const int dxm = x > 0 ? 1 : 0, dxp = x < W - 1 ? 1 : 0;
                 const bool cin = col_in(x);
-                auto xstep = [&](int row) {
-                    const int k = (row - oy) * SW + kc;
-                    return prop_eval<0, DELTA>(prop_load<DELTA>(fs, ds, is, k, k - dxm, k + dxp), dt,
-                                               cin && row_in(row));
+                // one band of rows: X sub-step into a rolling window of rows y-1, y, y+1, then
+                // the Y sub-step from it; FREE = no pixel of the tile is frozen at the border
+                auto band_pass = [&](auto free_tag) {
+                    constexpr bool FREE = decltype(free_tag)::value;
+                    auto xstep = [&](int row) {
+                        const int k = (row - oy) * SW + kc;
+                        const PropIn p = prop_load<DELTA>(fs, ds, is, k, k - dxm, k + dxp);
+                        return FREE ? prop_eval<0, DELTA>(p, dt, true) : prop_eval<0, DELTA>(p, dt, cin && row_in(row));
+                    };
+                    PropOut cur = xstep(by0);
+                    PropOut prev = by0 > 0 ? xstep(by0 - 1) : cur;  // row -1 clamps to row 0
+                    for (int y = by0; y < by1; ++y) {
+                        const PropOut nxt = y + 1 < H ? xstep(y + 1) : cur;  // row H clamps to H - 1
+                        PropIn q;
+                        q.fm = prev.f;
+                        q.f0 = cur.f;
+                        q.fp = nxt.f;
+                        if constexpr (DELTA) {
+                            q.sm = prev.s;
+                            q.s0 = cur.s;
+                            q.sp = nxt.s;
+                            q.vm = prev.v;
+                            q.v0 = cur.v;
+                            q.vp = nxt.v;
+                        }
+                        const PropOut o =
+                            FREE ? prop_eval<1, DELTA>(q, dt, true) : prop_eval<1, DELTA>(q, dt, cin && row_in(y));
+                        const int k = (y - oy) * SW + kc;
+                        fd[k] = o.f;
+                        if constexpr (DELTA) {
+                            id[k] = o.s;
+                            dd[k] = o.v;
+                        }
+                        prev = cur;
+                        cur = nxt;
+                    }
                 };
-                PropOut cur = xstep(by0);
-                PropOut prev = by0 > 0 ? xstep(by0 - 1) : cur;  // row -1 clamps to row 0
-                for (int y = by0; y < by1; ++y) {
-                    const PropOut nxt = y + 1 < H ? xstep(y + 1) : cur;  // row H clamps to H - 1
-                    PropIn q;
-                    q.fm = prev.f;
-                    q.f0 = cur.f;
-                    q.fp = nxt.f;
-                    if constexpr (DELTA) {
-                        q.sm = prev.s;
-                        q.s0 = cur.s;
-                        q.sp = nxt.s;
-                        q.vm = prev.v;
-                        q.v0 = cur.v;
-                        q.vp = nxt.v;
-                    }
-                    const PropOut o = prop_eval<1, DELTA>(q, dt, cin && row_in(y));
-                    const int k = (y - oy) * SW + kc;
-                    fd[k] = o.f;
-                    if constexpr (DELTA) {
-                        id[k] = o.s;
-                        dd[k] = o.v;
-                    }
-                    prev = cur;
-                    cur = nxt;
-                }
+                if (interior) band_pass(std::true_type{});
+                else band_pass(std::false_type{});
             }
             __syncthreads();
             swap2(fs, fd);
