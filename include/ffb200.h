@@ -297,6 +297,34 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
 ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
                              const void* gout, void* gin, void* gw5, void* stream);
 
+/* One frame of the differentiable pyramidal filter, and its adjoint, as single calls that
+ * launch every stage kernel (the schedule of PyramidalFlowFilter::compute on float input,
+ * src/gpu/flowfilter.cu:685-716: pyramid, top level, then delta levels L-2 .. 0).  State per
+ * level: smoothed flow [B][H][W][2], old image [B][H][W], delta flow [B][H][W][2] (3 pointers
+ * per level, level 0 first; inputs and outputs must not overlap).  The forward writes the
+ * new state and keeps every intermediate the adjoint needs in `tape`
+ * (ff_diff_frame_tape_bytes); `fu_out` (optional) receives the top level's unsmoothed flow.
+ * The backward ADDS the gradients of the frame, gamma (L), weights (L x 5) and the input
+ * state into its outputs; absent output gradients may be NULL; `scratch` is
+ * ff_diff_frame_scratch_bytes of device memory.  Sizes return 0 for a bad geometry. */
+#define FF_DIFF_MAX_LEVELS 8
+typedef struct ff_diff_geom {
+    int batch, levels, border;
+    int height[FF_DIFF_MAX_LEVELS], width[FF_DIFF_MAX_LEVELS];
+    int iterations[FF_DIFF_MAX_LEVELS], smooth[FF_DIFF_MAX_LEVELS];
+    double maxflow[FF_DIFF_MAX_LEVELS];
+} ff_diff_geom;
+size_t ff_diff_frame_tape_bytes(int dtype, const ff_diff_geom* geom);
+size_t ff_diff_frame_scratch_bytes(int dtype, const ff_diff_geom* geom);
+ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                                const void* weights, const void* const* state_in, void* const* state_out,
+                                void* fu_out, void* tape, void* stream);
+ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                                 const void* weights, const void* const* state_in, const void* const* state_out,
+                                 const void* tape, const void* const* grad_state_out, const void* grad_fu,
+                                 void* grad_frame, void* grad_gamma, void* grad_weights, void* const* grad_state_in,
+                                 void* scratch, void* stream);
+
 /* ff_stage_smooth without a workspace and without any allocation (no counterpart in the
  * reference, whose FlowSmoother allocates its X-pass scratch image in configure(),
  * flowsmoothing.cu:59-62). The X-pass scratch is a 32 MiB static device array of the

@@ -18,7 +18,10 @@
 // block, then added once per block.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "ffb200.h"
@@ -534,6 +537,15 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
     }
 }
 
+// dst += src over n elements
+template <typename T>
+__global__ void add_k(T* __restrict__ dst, const T* __restrict__ src, size_t n) {
+    grid_dep_wait();
+    grid_dep_launch();
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+
 inline dim3 grid3(int w, int h, int B) { return dim3((w + 31) / 32, (h + 7) / 8, B); }
 const dim3 kBlock(32, 8);
 
@@ -797,6 +809,426 @@ ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const voi
                                     (const float*)gout, (float*)gin, (float*)gw5, H, W)
                          : launch_k(smooth_bwd_k<float, 1>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
                                     (const float*)gout, (float*)gin, (float*)gw5, H, W);
+    });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ frame driver
+// One frame of the differentiable pyramidal filter (and its adjoint) as one host call that
+// launches every stage kernel itself: the same recurrence as flowfilter_b200.diff composes
+// from the stage Functions (pyramid, then the top level, then the delta levels from L-2
+// down to 0), with every intermediate the adjoint needs kept in a caller-provided tape.
+namespace ffb {
+namespace diff {
+namespace {
+
+struct Geo {
+    int B, L, border;
+    int H[FF_DIFF_MAX_LEVELS], W[FF_DIFF_MAX_LEVELS], N[FF_DIFF_MAX_LEVELS], S[FF_DIFF_MAX_LEVELS];
+    double maxflow[FF_DIFF_MAX_LEVELS];
+    size_t n1(int l) const { return (size_t)B * H[l] * W[l]; }
+};
+
+Geo geo_of(const ff_diff_geom* g) {
+    if (!g || g->levels < 1 || g->levels > FF_DIFF_MAX_LEVELS || g->batch < 1 || g->border < 0)
+        throw std::invalid_argument("bad differentiable-filter geometry");
+    Geo o{};
+    o.B = g->batch;
+    o.L = g->levels;
+    o.border = g->border;
+    for (int l = 0; l < o.L; ++l) {
+        o.H[l] = g->height[l];
+        o.W[l] = g->width[l];
+        o.N[l] = g->iterations[l];
+        o.S[l] = g->smooth[l];
+        o.maxflow[l] = g->maxflow[l];
+        if (o.H[l] < 1 || o.W[l] < 1 || o.N[l] < 1 || o.S[l] < 0) throw std::invalid_argument("bad level geometry");
+        if (l > 0 && (o.H[l] != o.H[l - 1] / 2 || o.W[l] != o.W[l - 1] / 2))
+            throw std::invalid_argument("level sizes must halve");
+    }
+    return o;
+}
+
+// offsets (in elements of T) of everything the adjoint reads, laid out in one tape
+struct Tape {
+    size_t img[FF_DIFF_MAX_LEVELS] = {};                // level images, l >= 1
+    size_t grad[FF_DIFF_MAX_LEVELS] = {};               // image gradients
+    std::vector<size_t> prop[FF_DIFF_MAX_LEVELS];       // outputs of sub-steps 0..2N-1
+    std::vector<size_t> sm[FF_DIFF_MAX_LEVELS];         // inputs of smoothing passes (sm[0] = update output)
+    size_t total = 0;
+    Tape(const Geo& g) {
+        auto take = [&](size_t n) {
+            size_t at = total;
+            total += (n + 31) / 32 * 32;
+            return at;
+        };
+        for (int l = 0; l < g.L; ++l) {
+            const size_t n1 = g.n1(l), n2 = 2 * n1;
+            const bool delta = l < g.L - 1;
+            const size_t state = delta ? n2 + n1 + n2 : n2;  // (f, s, v) or f
+            if (l > 0) img[l] = take(n1);
+            grad[l] = take(n2);
+            for (int k = 1; k <= 2 * g.N[l]; ++k) prop[l].push_back(take(state));
+            for (int k = 0; k < std::max(2 * g.S[l], 1); ++k) sm[l].push_back(take(n2));
+        }
+    }
+};
+
+// backward scratch (elements of T)
+struct Scratch {
+    size_t gimg[FF_DIFF_MAX_LEVELS] = {};
+    size_t ga0, gg, gold, gh, gfu, gby, gbx, pa, pb, sa, sb, zero;
+    size_t total = 0;
+    Scratch(const Geo& g) {
+        auto take = [&](size_t n) {
+            size_t at = total;
+            total += (n + 31) / 32 * 32;
+            return at;
+        };
+        size_t n1m = 0;
+        for (int l = 0; l < g.L; ++l) {
+            gimg[l] = take(g.n1(l));
+            n1m = std::max(n1m, g.n1(l));
+        }
+        const size_t n2m = 2 * n1m, st = n2m + n1m + n2m;
+        ga0 = take(n1m);
+        gg = take(n2m);
+        gold = take(n1m);
+        gh = take(n2m);
+        gfu = take(2 * g.n1(g.L - 1));
+        gby = take(n1m);
+        gbx = take(n1m);
+        pa = take(st);
+        pb = take(st);
+        sa = take(n2m);
+        sb = take(n2m);
+        zero = take(st);  // zeros standing in for absent output gradients
+    }
+};
+
+template <typename T>
+struct Driver {
+    const Geo& g;
+    cudaStream_t s;
+    Driver(const Geo& g_, cudaStream_t s_) : g(g_), s(s_) {}
+    void ok(cudaError_t e) const {
+        if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+    }
+    dim3 grid(int l) const { return grid3(g.W[l], g.H[l], g.B); }
+    void zero(T* p, size_t n) const { ok(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void add(T* dst, const T* src, size_t n) const {
+        ok(launch_k(add_k<T>, dim3((unsigned)std::min<size_t>((n + 255) / 256, 4096)), dim3(256), 0, s, dst, src, n));
+    }
+    void prop(int l, int axis, bool payload, const T* f, const T* sc, const T* v, T* fo, T* so, T* vo) const {
+        const T dt = (T)(1.0 / g.N[l]);
+        const int H = g.H[l], W = g.W[l], b = g.border;
+        cudaError_t e;
+        if (payload) {
+            e = axis == 0 ? launch_k(prop_fwd_k<T, 0, true>, grid(l), kBlock, 0, s, f, sc, v, fo, so, vo, H, W, dt, b)
+                          : launch_k(prop_fwd_k<T, 1, true>, grid(l), kBlock, 0, s, f, sc, v, fo, so, vo, H, W, dt, b);
+        } else {
+            e = axis == 0 ? launch_k(prop_fwd_k<T, 0, false>, grid(l), kBlock, 0, s, f, sc, v, fo, so, vo, H, W, dt, b)
+                          : launch_k(prop_fwd_k<T, 1, false>, grid(l), kBlock, 0, s, f, sc, v, fo, so, vo, H, W, dt, b);
+        }
+        ok(e);
+    }
+    void prop_bwd(int l, int axis, bool payload, const T* f, const T* sc, const T* v, const T* gfo, const T* gso,
+                  const T* gvo, T* gf, T* gs, T* gv) const {
+        const T dt = (T)(1.0 / g.N[l]);
+        const int H = g.H[l], W = g.W[l], b = g.border;
+        cudaError_t e;
+        if (payload) {
+            e = axis == 0 ? launch_k(prop_bwd_k<T, 0, true>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs, gv,
+                                     H, W, dt, b)
+                          : launch_k(prop_bwd_k<T, 1, true>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs, gv,
+                                     H, W, dt, b);
+        } else {
+            e = axis == 0 ? launch_k(prop_bwd_k<T, 0, false>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
+                                     gv, H, W, dt, b)
+                          : launch_k(prop_bwd_k<T, 1, false>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
+                                     gv, H, W, dt, b);
+        }
+        ok(e);
+    }
+    void smooth(int l, int axis, const T* w5, const T* in, T* out) const {
+        ok(axis == 0 ? launch_k(smooth_fwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l])
+                     : launch_k(smooth_fwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l]));
+    }
+    void smooth_bwd(int l, int axis, const T* w5, const T* in, const T* go, T* gi, T* gw5) const {
+        ok(axis == 0 ? launch_k(smooth_bwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, go, gi, gw5, g.H[l], g.W[l])
+                     : launch_k(smooth_bwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, go, gi, gw5, g.H[l], g.W[l]));
+    }
+    void model(int l, const T* img, T* a0, T* grad) const {
+        ok(launch_k(model_fwd_k<T>, grid(l), kBlock, 0, s, img, a0, grad, g.H[l], g.W[l]));
+    }
+    void model_bwd(int l, const T* ga0, const T* ggrad, T* gby, T* gbx, T* gimg) const {
+        ok(launch_k(model_bwd1_k<T>, grid(l), kBlock, 0, s, ga0, ggrad, gby, gbx, g.H[l], g.W[l]));
+        ok(launch_k(model_bwd2_k<T>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l], g.W[l]));
+    }
+
+    // ---- forward
+    void forward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in, T* const* out,
+                 T* fu_out, T* tp) const {
+        const Tape tape(g);
+        const int L = g.L, top = L - 1;
+        auto img = [&](int l) -> const T* { return l == 0 ? frame : tp + tape.img[l]; };
+        for (int l = 1; l < L; ++l)
+            ok(launch_k(pyr_fwd_k<T>, grid3(g.W[l], g.H[l], g.B), kBlock, 0, s, img(l - 1), tp + tape.img[l],
+                        g.H[l - 1], g.W[l - 1]));
+        // top level: flow propagation, update, smoothing
+        {
+            const int l = top;
+            const size_t n2 = 2 * g.n1(l);
+            T* a0 = out[3 * l + 1];
+            T* grad = tp + tape.grad[l];
+            model(l, img(l), a0, grad);
+            const T* f = in[3 * l];
+            for (int k = 0; k < 2 * g.N[l]; ++k) {
+                T* fo = tp + tape.prop[l][k];
+                prop(l, k % 2, false, f, nullptr, nullptr, fo, nullptr, nullptr);
+                f = fo;
+            }
+            const T* old = first ? a0 : in[3 * l + 1];
+            T* fu = tp + tape.sm[l][0];
+            ok(launch_k(update_fwd_k<T>, grid(l), kBlock, 0, s, (const T*)a0, (const T*)grad, old, f, gamma + l, fu,
+                        g.H[l], g.W[l], (T)g.maxflow[l]));
+            if (fu_out) ok(cudaMemcpyAsync(fu_out, fu, n2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l]);
+            ok(cudaMemcpyAsync(out[3 * l + 2], in[3 * l + 2], n2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        }
+        // delta levels, L-2 down to 0
+        for (int l = L - 2; l >= 0; --l) {
+            const size_t n1 = g.n1(l), n2 = 2 * n1;
+            T* a0 = out[3 * l + 1];
+            T* grad = tp + tape.grad[l];
+            model(l, img(l), a0, grad);
+            const T *f = in[3 * l], *sc = in[3 * l + 1], *v = in[3 * l + 2];
+            for (int k = 0; k < 2 * g.N[l]; ++k) {
+                T* base = tp + tape.prop[l][k];
+                prop(l, k % 2, true, f, sc, v, base, base + n2, base + n2 + n1);
+                f = base;
+                sc = base + n2;
+                v = base + n2 + n1;
+            }
+            const T* old = first ? a0 : sc;
+            const T* coarse = l == L - 2 ? tp + tape.sm[top][0] : in[3 * (l + 1)];
+            T* flow = tp + tape.sm[l][0];
+            ok(launch_k(dupdate_fwd_k<T>, grid(l), kBlock, 0, s, (const T*)a0, (const T*)grad, old, v, coarse,
+                        gamma + l, flow, out[3 * l + 2], g.H[l], g.W[l], g.H[l + 1], g.W[l + 1], (T)g.maxflow[l]));
+            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l]);
+        }
+    }
+    // 2S passes from tape.sm[l][0]; pass j writes tape.sm[l][j+1], the last writes `last`
+    void smooth_chain(int l, const T* w5, const Tape& tape, T* tp, T* last) const {
+        const int n = 2 * g.S[l];
+        if (n == 0) ok(cudaMemcpyAsync(last, tp + tape.sm[l][0], 2 * g.n1(l) * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        for (int j = 0; j < n; ++j) smooth(l, j % 2, w5, tp + tape.sm[l][j], j + 1 < n ? tp + tape.sm[l][j + 1] : last);
+    }
+
+    // ---- backward: gradients of the outputs -> gradients of the inputs (all accumulated)
+    void backward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in,
+                  const T* const* out, const T* tp, const T* const* gout, const T* gfu_out, T* gframe, T* ggamma,
+                  T* gweights, T* const* gin, T* sc_) const {
+        const Tape tape(g);
+        const Scratch S_(g);
+        const int L = g.L, top = L - 1;
+        T* gimg[FF_DIFF_MAX_LEVELS];
+        for (int l = 0; l < L; ++l) {
+            gimg[l] = sc_ + S_.gimg[l];
+            zero(gimg[l], g.n1(l));
+        }
+        T* const zbuf = sc_ + S_.zero;
+        size_t n1m = 0;
+        for (int l = 0; l < L; ++l) n1m = std::max(n1m, g.n1(l));
+        zero(zbuf, 5 * n1m);
+        auto gz = [&](const T* p) { return p ? p : (const T*)zbuf; };
+        T* gfu = sc_ + S_.gfu;
+        zero(gfu, 2 * g.n1(top));
+        if (gfu_out) add(gfu, gfu_out, 2 * g.n1(top));
+        T *ga0 = sc_ + S_.ga0, *ggr = sc_ + S_.gg, *gold = sc_ + S_.gold, *gh = sc_ + S_.gh;
+        T *pa = sc_ + S_.pa, *pb = sc_ + S_.pb, *sa = sc_ + S_.sa, *sb = sc_ + S_.sb;
+        T *gby = sc_ + S_.gby, *gbx = sc_ + S_.gbx;
+        // smoothing chain adjoint: returns the gradient of tape.sm[l][0]
+        auto smooth_back = [&](int l, const T* g_last) -> const T* {
+            const int n = 2 * g.S[l];
+            const size_t n2 = 2 * g.n1(l);
+            const T* gcur = gz(g_last);
+            T* bufs[2] = {sa, sb};
+            for (int j = n - 1; j >= 0; --j) {
+                T* dst = bufs[j % 2];
+                zero(dst, n2);
+                smooth_bwd(l, j % 2, weights + 5 * l, tp + tape.sm[l][j], gcur, dst, gweights + 5 * l);
+                gcur = dst;
+            }
+            return gcur;
+        };
+        for (int l = 0; l <= L - 2; ++l) {
+            const size_t n1 = g.n1(l), n2 = 2 * n1;
+            const T* a0 = out[3 * l + 1];
+            const T* grad = tp + tape.grad[l];
+            const int last = 2 * g.N[l] - 1;
+            const T* fh_base = tp + tape.prop[l][last];
+            const T* sh = fh_base + n2;
+            const T* vh = fh_base + n2 + n1;
+            const T* old = first ? a0 : sh;
+            const T* coarse = l == L - 2 ? tp + tape.sm[top][0] : in[3 * (l + 1)];
+            const T* gflow = smooth_back(l, gout[3 * l]);
+            zero(ga0, n1);
+            zero(ggr, n2);
+            zero(gold, n1);
+            zero(gh, n2);
+            T* gco = l == L - 2 ? gfu : gin[3 * (l + 1)];
+            ok(launch_k(dupdate_bwd_k<T>, grid(l), kBlock, 0, s, a0, grad, old, vh, coarse, gamma + l, gflow,
+                        gz(gout[3 * l + 2]), ga0, ggr, gold, gh, gco, ggamma + l, g.H[l], g.W[l], g.H[l + 1],
+                        g.W[l + 1], (T)g.maxflow[l]));
+            if (gout[3 * l + 1]) add(ga0, gout[3 * l + 1], n1);
+            // gradient of the propagated (f, s, v): f none, s = old (unless first), v = gh
+            T* cur = pa;
+            zero(cur, n2 + n1 + n2);
+            if (first) add(ga0, gold, n1);
+            else add(cur + n2, gold, n1);
+            add(cur + n2 + n1, gh, n2);
+            for (int k = last; k >= 0; --k) {
+                const T *f, *sc, *v;
+                if (k == 0) {
+                    f = in[3 * l];
+                    sc = in[3 * l + 1];
+                    v = in[3 * l + 2];
+                } else {
+                    const T* b = tp + tape.prop[l][k - 1];
+                    f = b;
+                    sc = b + n2;
+                    v = b + n2 + n1;
+                }
+                T* nxt = cur == pa ? pb : pa;
+                zero(nxt, n2 + n1 + n2);
+                prop_bwd(l, k % 2, true, f, sc, v, cur, cur + n2, cur + n2 + n1, nxt, nxt + n2, nxt + n2 + n1);
+                cur = nxt;
+            }
+            add(gin[3 * l], cur, n2);
+            add(gin[3 * l + 1], cur + n2, n1);
+            add(gin[3 * l + 2], cur + n2 + n1, n2);
+            model_bwd(l, ga0, ggr, gby, gbx, gimg[l]);
+        }
+        {
+            const int l = top;
+            const size_t n1 = g.n1(l), n2 = 2 * n1;
+            const T* a0 = out[3 * l + 1];
+            const T* grad = tp + tape.grad[l];
+            const int last = 2 * g.N[l] - 1;
+            const T* fh = tp + tape.prop[l][last];
+            const T* old = first ? a0 : in[3 * l + 1];
+            add(gfu, smooth_back(l, gout[3 * l]), n2);
+            zero(ga0, n1);
+            zero(ggr, n2);
+            zero(gold, n1);
+            zero(gh, n2);
+            ok(launch_k(update_bwd_k<T>, grid(l), kBlock, 0, s, a0, grad, old, fh, gamma + l, (const T*)gfu, ga0, ggr,
+                        gold, gh, ggamma + l, g.H[l], g.W[l], (T)g.maxflow[l]));
+            if (gout[3 * l + 1]) add(ga0, gout[3 * l + 1], n1);
+            if (first) add(ga0, gold, n1);
+            else add(gin[3 * l + 1], gold, n1);
+            if (gout[3 * l + 2]) add(gin[3 * l + 2], gout[3 * l + 2], n2);
+            T* cur = gh;
+            T* bufs[2] = {pa, pb};
+            for (int k = last; k >= 0; --k) {
+                const T* f = k == 0 ? in[3 * l] : tp + tape.prop[l][k - 1];
+                T* nxt = bufs[k % 2];
+                zero(nxt, n2);
+                prop_bwd(l, k % 2, false, f, nullptr, nullptr, cur, nullptr, nullptr, nxt, nullptr, nullptr);
+                cur = nxt;
+            }
+            add(gin[3 * l], cur, n2);
+            model_bwd(l, ga0, ggr, gby, gbx, gimg[l]);
+        }
+        for (int l = L - 1; l >= 1; --l)
+            ok(launch_k(pyr_bwd_k<T>, grid3(g.W[l - 1], g.H[l - 1], g.B), kBlock, 0, s, (const T*)gimg[l], gimg[l - 1],
+                        g.H[l - 1], g.W[l - 1]));
+        add(gframe, gimg[0], g.n1(0));
+    }
+};
+
+template <typename F>
+ff_status run_frame(F&& f) {
+    try {
+        f();
+        return FF_OK;
+    } catch (const std::invalid_argument& e) {
+        ffb_set_last_error(e.what());
+        return FF_ERR_INVALID_ARGUMENT;
+    } catch (const std::exception& e) {
+        ffb_set_last_error(std::string("CUDA: ") + e.what());
+        return FF_ERR_CUDA;
+    }
+}
+
+}  // namespace
+}  // namespace diff
+}  // namespace ffb
+
+extern "C" {
+
+size_t ff_diff_frame_tape_bytes(int dtype, const ff_diff_geom* geom) {
+    try {
+        return ffb::diff::Tape(ffb::diff::geo_of(geom)).total * (dtype ? 8 : 4);
+    } catch (...) {
+        return 0;
+    }
+}
+
+size_t ff_diff_frame_scratch_bytes(int dtype, const ff_diff_geom* geom) {
+    try {
+        return ffb::diff::Scratch(ffb::diff::geo_of(geom)).total * (dtype ? 8 : 4);
+    } catch (...) {
+        return 0;
+    }
+}
+
+ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                                const void* weights, const void* const* state_in, void* const* state_out,
+                                void* fu_out, void* tape, void* stream) {
+    return ffb::diff::run_frame([&] {
+        const ffb::diff::Geo g = ffb::diff::geo_of(geom);
+        if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
+        if (!frame || !gamma || !weights || !state_in || !state_out || !tape)
+            throw std::invalid_argument("null pointer argument");
+        if (dtype) {
+            ffb::diff::Driver<double>(g, (cudaStream_t)stream)
+                .forward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
+                         (const double* const*)state_in, (double* const*)state_out, (double*)fu_out, (double*)tape);
+        } else {
+            ffb::diff::Driver<float>(g, (cudaStream_t)stream)
+                .forward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
+                         (const float* const*)state_in, (float* const*)state_out, (float*)fu_out, (float*)tape);
+        }
+    });
+}
+
+ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                                 const void* weights, const void* const* state_in, const void* const* state_out,
+                                 const void* tape, const void* const* grad_state_out, const void* grad_fu,
+                                 void* grad_frame, void* grad_gamma, void* grad_weights, void* const* grad_state_in,
+                                 void* scratch, void* stream) {
+    return ffb::diff::run_frame([&] {
+        const ffb::diff::Geo g = ffb::diff::geo_of(geom);
+        if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
+        if (!frame || !gamma || !weights || !state_in || !state_out || !tape || !grad_state_out || !grad_frame ||
+            !grad_gamma || !grad_weights || !grad_state_in || !scratch)
+            throw std::invalid_argument("null pointer argument");
+        if (dtype) {
+            ffb::diff::Driver<double>(g, (cudaStream_t)stream)
+                .backward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
+                          (const double* const*)state_in, (const double* const*)state_out, (const double*)tape,
+                          (const double* const*)grad_state_out, (const double*)grad_fu, (double*)grad_frame,
+                          (double*)grad_gamma, (double*)grad_weights, (double* const*)grad_state_in, (double*)scratch);
+        } else {
+            ffb::diff::Driver<float>(g, (cudaStream_t)stream)
+                .backward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
+                          (const float* const*)state_in, (const float* const*)state_out, (const float*)tape,
+                          (const float* const*)grad_state_out, (const float*)grad_fu, (float*)grad_frame,
+                          (float*)grad_gamma, (float*)grad_weights, (float* const*)grad_state_in, (float*)scratch);
+        }
     });
 }
 

@@ -5,8 +5,9 @@ filter on float32 images in [0, 1] (the float path of ImagePyramid, FlowFilter(G
 and DeltaFlowFilter, src/gpu/flowfilter.cu:621-716; gamma used unscaled for float input,
 :279-284), run by the ff_diff_* kernels of libffb200.so in float32 or float64.  Every stage
 has an autograd Function whose backward is the matching adjoint kernel (``stages()``); the
-filter itself runs each frame as one autograd node (FrameStep) that calls the same forward
-kernels and, in its backward, the adjoint kernels in reverse order.  The time recurrence
+filter itself runs each frame as one autograd node (FrameStep) whose forward is one
+ff_diff_frame_forward call (the same forward kernels, launched by the library) and whose
+backward is one ff_diff_frame_backward call (the adjoint kernels in reverse order).  The time recurrence
 is chained by autograd and cut into checkpointed segments (recomputed in the backward pass)
 of ``checkpoint_every`` frames.
 
@@ -20,7 +21,7 @@ from __future__ import annotations
 import ctypes
 import math
 
-from ._lib import call
+from ._lib import call, lib
 
 
 def _torch():
@@ -375,284 +376,107 @@ def endpoint_error(flows, truth, first: int = 0):
     return (d[..., 0] ** 2 + d[..., 1] ** 2).sqrt().mean()
 
 
-class _Kernels:
-    """Direct calls of the ff_diff_* kernels for one dtype (no autograd bookkeeping)."""
-
-    def __init__(self, dtype):
-        torch = _torch()
-        self.torch = torch
-        self.d = 1 if dtype == torch.float64 else 0
-        self.item = 8 if self.d else 4
-
-    def at(self, t, i: int):
-        """Device pointer of element i of a contiguous 1-D or 2-D parameter tensor."""
-        return ctypes.c_void_p(t.data_ptr() + i * self.item)
-
-    def pyr(self, x):
-        B, H, W = x.shape
-        out = x.new_empty((B, H // 2, W // 2))
-        call("ff_diff_pyramid", self.d, B, H, W, _p(x), _p(out), _stream())
-        return out
-
-    def pyr_bwd(self, g, gin):
-        B, H, W = gin.shape
-        call("ff_diff_pyramid_bwd", self.d, B, H, W, _p(g), _p(gin), _stream())
-
-    def model(self, img):
-        B, H, W = img.shape
-        a0, grad = img.new_empty((B, H, W)), img.new_empty((B, H, W, 2))
-        call("ff_diff_model", self.d, B, H, W, _p(img), _p(a0), _p(grad), _stream())
-        return a0, grad
-
-    def model_bwd(self, ga0, ggrad, gimg):
-        B, H, W = gimg.shape
-        gby, gbx = gimg.new_empty((B, H, W)), gimg.new_empty((B, H, W))
-        call("ff_diff_model_bwd", self.d, B, H, W, _p(ga0), _p(ggrad), _p(gby), _p(gbx), _p(gimg), _stream())
-
-    def prop(self, f, s, v, axis, dt, border):
-        B, H, W, _ = f.shape
-        fo = self.torch.empty_like(f)
-        so = self.torch.empty_like(s) if s is not None else None
-        vo = self.torch.empty_like(v) if v is not None else None
-        call("ff_diff_propagate", self.d, B, H, W, axis, 1 if s is not None else 0, dt, border, _p(f), _p(s), _p(v),
-             _p(fo), _p(so), _p(vo), _stream())
-        return fo, so, vo
-
-    def prop_bwd(self, f, s, v, gfo, gso, gvo, gf, gs, gv, axis, dt, border):
-        B, H, W, _ = f.shape
-        call("ff_diff_propagate_bwd", self.d, B, H, W, axis, 1 if s is not None else 0, dt, border, _p(f), _p(s),
-             _p(v), _p(gfo), _p(gso), _p(gvo), _p(gf), _p(gs), _p(gv), _stream())
-
-    def update(self, a0, grad, old, fh, gamma, l, maxflow):
-        B, H, W = a0.shape
-        out = self.torch.empty_like(fh)
-        call("ff_diff_update", self.d, B, H, W, _p(a0), _p(grad), _p(old), _p(fh), self.at(gamma, l), maxflow,
-             _p(out), _stream())
-        return out
-
-    def update_bwd(self, a0, grad, old, fh, gamma, l, maxflow, gout, ga0, ggrad, gold, gfh, ggamma):
-        B, H, W = a0.shape
-        call("ff_diff_update_bwd", self.d, B, H, W, _p(a0), _p(grad), _p(old), _p(fh), self.at(gamma, l), maxflow,
-             _p(gout), _p(ga0), _p(ggrad), _p(gold), _p(gfh), self.at(ggamma, l), _stream())
-
-    def dupdate(self, a0, grad, old, dh, coarse, gamma, l, maxflow):
-        B, H, W = a0.shape
-        Hc, Wc = coarse.shape[1:3]
-        flow, delta = self.torch.empty_like(dh), self.torch.empty_like(dh)
-        call("ff_diff_delta_update", self.d, B, H, W, Hc, Wc, _p(a0), _p(grad), _p(old), _p(dh), _p(coarse),
-             self.at(gamma, l), maxflow, _p(flow), _p(delta), _stream())
-        return flow, delta
-
-    def dupdate_bwd(self, a0, grad, old, dh, coarse, gamma, l, maxflow, gflow, gdelta, ga0, ggrad, gold, gdh, gcoarse,
-                    ggamma):
-        B, H, W = a0.shape
-        Hc, Wc = coarse.shape[1:3]
-        call("ff_diff_delta_update_bwd", self.d, B, H, W, Hc, Wc, _p(a0), _p(grad), _p(old), _p(dh), _p(coarse),
-             self.at(gamma, l), maxflow, _p(gflow), _p(gdelta), _p(ga0), _p(ggrad), _p(gold), _p(gdh), _p(gcoarse),
-             self.at(ggamma, l), _stream())
-
-    def smooth(self, x, weights, l, axis):
-        B, H, W, _ = x.shape
-        out = self.torch.empty_like(x)
-        call("ff_diff_smooth", self.d, B, H, W, axis, self.at(weights, 5 * l), _p(x), _p(out), _stream())
-        return out
-
-    def smooth_bwd(self, x, weights, l, axis, gout, gin, gweights):
-        B, H, W, _ = x.shape
-        call("ff_diff_smooth_bwd", self.d, B, H, W, axis, self.at(weights, 5 * l), _p(x), _p(gout), _p(gin),
-             self.at(gweights, 5 * l), _stream())
+MAX_LEVELS = 8  # FF_DIFF_MAX_LEVELS
 
 
-def _frame_forward(k, flt, frame, gamma, weights, state, first: bool, keep: bool):
-    """One frame of the pyramidal filter by direct kernel calls.  Returns (new state, fu of
-    the top level, tape); the tape holds every intermediate the adjoint needs (if keep)."""
-    L = flt.L
-    tape = {"imgs": [frame]}
-    for _ in range(1, L):
-        tape["imgs"].append(k.pyr(tape["imgs"][-1]))
-    new = [None] * L
-    top = L - 1
-    a0, g = k.model(tape["imgs"][top])
-    dt, border = 1.0 / flt.iters[top], flt.border
-    fs = [state[top][0]]
-    for _ in range(flt.iters[top]):
-        fs.append(k.prop(fs[-1], None, None, 0, dt, border)[0])
-        fs.append(k.prop(fs[-1], None, None, 1, dt, border)[0])
-    old = a0 if first else state[top][1]
-    fu = k.update(a0, g, old, fs[-1], gamma, top, flt.maxflow[top])
-    sm = [fu]
-    for _ in range(flt.smooth[top]):
-        sm.append(k.smooth(sm[-1], weights, top, 0))
-        sm.append(k.smooth(sm[-1], weights, top, 1))
-    new[top] = (sm[-1], a0, state[top][2])
-    if keep:
-        tape[top] = dict(a0=a0, g=g, prop=fs[:-1], fh=fs[-1], old=old, sm=sm[:-1])
-    for l in range(L - 2, -1, -1):
-        a0, g = k.model(tape["imgs"][l])
-        dt = 1.0 / flt.iters[l]
-        fsv = [tuple(state[l])]
-        for _ in range(flt.iters[l]):
-            fsv.append(k.prop(*fsv[-1], 0, dt, border))
-            fsv.append(k.prop(*fsv[-1], 1, dt, border))
-        f_h, s_h, v_h = fsv[-1]
-        old = a0 if first else s_h
-        coarse = fu if l == L - 2 else state[l + 1][0]
-        flow, delta = k.dupdate(a0, g, old, v_h, coarse, gamma, l, flt.maxflow[l])
-        sm = [flow]
-        for _ in range(flt.smooth[l]):
-            sm.append(k.smooth(sm[-1], weights, l, 0))
-            sm.append(k.smooth(sm[-1], weights, l, 1))
-        new[l] = (sm[-1], a0, delta)
-        if keep:
-            tape[l] = dict(a0=a0, g=g, prop=fsv[:-1], vh=v_h, old=old, coarse=coarse, sm=sm[:-1])
-    return new, fu, tape
+class _Geom(ctypes.Structure):
+    """ff_diff_geom of include/ffb200.h."""
+
+    _fields_ = [("batch", ctypes.c_int), ("levels", ctypes.c_int), ("border", ctypes.c_int),
+                ("height", ctypes.c_int * MAX_LEVELS), ("width", ctypes.c_int * MAX_LEVELS),
+                ("iterations", ctypes.c_int * MAX_LEVELS), ("smooth", ctypes.c_int * MAX_LEVELS),
+                ("maxflow", ctypes.c_double * MAX_LEVELS)]
 
 
-def _smooth_backward(k, sm, weights, l, g, gweights):
-    """Adjoint of the 2S smoothing passes whose inputs are sm[0..2S-1]; g: output gradient."""
-    torch = k.torch
-    for j in range(len(sm) - 1, -1, -1):
-        gin = torch.zeros_like(sm[j])
-        k.smooth_bwd(sm[j], weights, l, j % 2, g, gin, gweights)
-        g = gin
+def _geom(flt, B: int) -> _Geom:
+    if flt.L > MAX_LEVELS:
+        raise ValueError(f"at most {MAX_LEVELS} levels")
+    g = _Geom()
+    g.batch, g.levels, g.border = int(B), flt.L, flt.border
+    for l, (h, w) in enumerate(flt.shapes):
+        g.height[l], g.width[l] = h, w
+        g.iterations[l], g.smooth[l] = flt.iters[l], flt.smooth[l]
+        g.maxflow[l] = flt.maxflow[l]
     return g
 
 
-def _frame_backward(k, flt, tape, gamma, weights, state, first: bool, g_new, g_fu_out):
-    """Reverse of _frame_forward.  g_new[l] = gradients of the new state (fs, io, d) (None =
-    zero); g_fu_out = gradient of the top level's fu as an output (single level).  Returns
-    (g_frame, g_gamma, g_weights, g_state)."""
-    torch = k.torch
-    L = flt.L
-    top = L - 1
-    z = lambda t: torch.zeros_like(t)  # noqa: E731
-    g_gamma, g_weights = torch.zeros_like(gamma), torch.zeros_like(weights)
-    g_state = [[z(state[l][0]), z(state[l][1]), z(state[l][2])] for l in range(L)]
-    g_img = [z(im) for im in tape["imgs"]]
-    g_fu = z(tape[top]["sm"][0])
-    if g_fu_out is not None:
-        g_fu += g_fu_out
-    border = flt.border
-
-    def gn(l, i, like):
-        t = g_new[l][i]
-        return t.contiguous() if t is not None else z(like)
-
-    for l in range(0, L - 1):
-        T = tape[l]
-        g_flow = _smooth_backward(k, T["sm"], weights, l, gn(l, 0, T["sm"][0]), g_weights)
-        ga0, gg, gold, gvh = z(T["a0"]), z(T["g"]), z(T["old"]), z(T["vh"])
-        gcoarse = z(T["coarse"])
-        k.dupdate_bwd(T["a0"], T["g"], T["old"], T["vh"], T["coarse"], gamma, l, flt.maxflow[l], g_flow,
-                      gn(l, 2, T["vh"]), ga0, gg, gold, gvh, gcoarse, g_gamma)
-        ga0 += gn(l, 1, T["a0"])
-        if l == L - 2:
-            g_fu += gcoarse
-        else:
-            g_state[l + 1][0] += gcoarse
-        if first:
-            ga0 += gold
-            gs = z(T["old"])
-        else:
-            gs = gold
-        gf, gv = z(T["prop"][0][0]), gvh
-        dt = 1.0 / flt.iters[l]
-        for j in range(len(T["prop"]) - 1, -1, -1):
-            f, s, v = T["prop"][j]
-            nf, ns, nv = z(f), z(s), z(v)
-            k.prop_bwd(f, s, v, gf, gs, gv, nf, ns, nv, j % 2, dt, border)
-            gf, gs, gv = nf, ns, nv
-        g_state[l][0] += gf
-        g_state[l][1] += gs
-        g_state[l][2] += gv
-        k.model_bwd(ga0, gg, g_img[l])
-
-    T = tape[top]
-    g_fu += _smooth_backward(k, T["sm"], weights, top, gn(top, 0, T["sm"][0]), g_weights)
-    ga0, gg, gold, gfh = z(T["a0"]), z(T["g"]), z(T["old"]), z(T["fh"])
-    k.update_bwd(T["a0"], T["g"], T["old"], T["fh"], gamma, top, flt.maxflow[top], g_fu, ga0, gg, gold, gfh, g_gamma)
-    ga0 += gn(top, 1, T["a0"])
-    if first:
-        ga0 += gold
-    else:
-        g_state[top][1] += gold
-    g_state[top][2] += gn(top, 2, state[top][2])
-    gf = gfh
-    dt = 1.0 / flt.iters[top]
-    for j in range(len(T["prop"]) - 1, -1, -1):
-        nf = z(T["prop"][j])
-        k.prop_bwd(T["prop"][j], None, None, gf, None, None, nf, None, None, j % 2, dt, border)
-        gf = nf
-    g_state[top][0] += gf
-    k.model_bwd(ga0, gg, g_img[top])
-    for l in range(L - 1, 0, -1):
-        k.pyr_bwd(g_img[l], g_img[l - 1])
-    return g_img[0], g_gamma, g_weights, g_state
+def _workspace(name: str, d: int, g: _Geom, like):
+    """A device buffer of the size ff_diff_frame_{tape,scratch}_bytes gives."""
+    n = getattr(lib(), name)(d, ctypes.byref(g))
+    if n == 0:
+        raise ValueError("bad differentiable-filter geometry")
+    return _torch().empty(n // (8 if d else 4), dtype=like.dtype, device=like.device)
 
 
-def _pack(obj, out: list):
-    """obj with every tensor replaced by its index in out (tensors appended to out)."""
+def _ptrs(ts):
+    return (ctypes.c_void_p * len(ts))(*[t.data_ptr() if t is not None else None for t in ts])
+
+
+def _frame_forward(flt, frame, gamma, weights, state_flat, first: bool):
+    """One frame through ff_diff_frame_forward (one host call launches the whole frame).
+    Returns (new state, flat; the top level's unsmoothed flow for one level, else None; the
+    tape the adjoint reads)."""
+    d = _dt(frame)
+    B = frame.shape[0]
+    g = _geom(flt, B)
+    tape = _workspace("ff_diff_frame_tape_bytes", d, g, frame)
+    new = []
+    for h, w in flt.shapes:
+        new += [frame.new_empty((B, h, w, 2)), frame.new_empty((B, h, w)), frame.new_empty((B, h, w, 2))]
+    fu = frame.new_empty((B,) + tuple(flt.shapes[0]) + (2,)) if flt.L == 1 else None
+    call("ff_diff_frame_forward", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
+         _ptrs(state_flat), _ptrs(new), _p(fu), _p(tape), _stream())
+    return new, fu, tape
+
+
+def _frame_backward(flt, first: bool, frame, gamma, weights, state_flat, new_flat, tape, g_new, g_fu):
+    """Adjoint of one frame through ff_diff_frame_backward: gradients of the new state (None
+    = zero) and of the top level's unsmoothed flow -> gradients of the frame, gamma, weights
+    and the input state."""
     torch = _torch()
-    if isinstance(obj, torch.Tensor):
-        out.append(obj)
-        return ("#", len(out) - 1)
-    if isinstance(obj, dict):
-        return {k: _pack(v, out) for k, v in obj.items()}
-    if isinstance(obj, (list, tuple)):
-        return type(obj)(_pack(v, out) for v in obj)
-    return obj
-
-
-def _unpack(obj, ts):
-    if isinstance(obj, tuple) and len(obj) == 2 and obj[0] == "#":
-        return ts[obj[1]]
-    if isinstance(obj, dict):
-        return {k: _unpack(v, ts) for k, v in obj.items()}
-    if isinstance(obj, (list, tuple)):
-        return type(obj)(_unpack(v, ts) for v in obj)
-    return obj
+    d = _dt(frame)
+    g = _geom(flt, frame.shape[0])
+    scratch = _workspace("ff_diff_frame_scratch_bytes", d, g, frame)
+    g_frame, g_gamma, g_weights = torch.zeros_like(frame), torch.zeros_like(gamma), torch.zeros_like(weights)
+    g_state = [torch.zeros_like(t) for t in state_flat]
+    g_new = [_c(t) for t in g_new]
+    call("ff_diff_frame_backward", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
+         _ptrs(state_flat), _ptrs(new_flat), _p(tape), _ptrs(g_new), _p(_c(g_fu)), _p(g_frame), _p(g_gamma),
+         _p(g_weights), _ptrs(g_state), _p(scratch), _stream())
+    return g_frame, g_gamma, g_weights, g_state
 
 
 def _frame_function():
     torch = _torch()
 
     class FrameStep(torch.autograd.Function):
-        """One frame of the pyramidal filter as a single autograd node: the forward runs the
-        stage kernels, the backward their adjoints in reverse order over the saved tape."""
+        """One frame of the pyramidal filter as a single autograd node: the forward is one
+        ff_diff_frame_forward call (every stage kernel, intermediates kept in a tape), the
+        backward one ff_diff_frame_backward call (the adjoint kernels in reverse order)."""
 
         @staticmethod
         def forward(ctx, flt, first, frame, gamma, weights, *state_flat):
-            k = _Kernels(frame.dtype)
-            L = flt.L
-            state = [tuple(t.contiguous() for t in state_flat[3 * l:3 * l + 3]) for l in range(L)]
+            state_flat = [t.contiguous() for t in state_flat]
             frame, gamma, weights = frame.contiguous(), gamma.contiguous(), weights.contiguous()
-            keep = torch.is_grad_enabled() or any(ctx.needs_input_grad)
-            new, fu, tape = _frame_forward(k, flt, frame, gamma, weights, state, first, keep)
+            new, fu, tape = _frame_forward(flt, frame, gamma, weights, state_flat, first)
             ctx.flt, ctx.first = flt, first
-            if keep:
-                # everything the adjoint reads goes through save_for_backward, so an enclosing
-                # checkpoint can drop it and recompute the frame in the backward pass
-                flat = []
-                ctx.skeleton = _pack({"tape": tape, "state": state, "params": (gamma, weights)}, flat)
-                ctx.save_for_backward(*flat)
-            outs = [t for lvl in new for t in lvl]
-            # the top level's delta slot passes its input through: return a copy so every
-            # output is a distinct tensor
-            outs[3 * (L - 1) + 2] = outs[3 * (L - 1) + 2].clone()
-            return (*outs, fu.clone() if L == 1 else fu.new_zeros(0))
+            if torch.is_grad_enabled() or any(ctx.needs_input_grad):
+                # the tape and the outputs the adjoint reads go through save_for_backward, so an
+                # enclosing checkpoint can drop them and recompute the frame in the backward pass
+                ctx.save_for_backward(frame, gamma, weights, tape, *state_flat, *new)
+            return (*new, fu if fu is not None else frame.new_zeros(0))
 
         @staticmethod
         def backward(ctx, *grads):
             flt = ctx.flt
-            saved = _unpack(ctx.skeleton, ctx.saved_tensors)
-            gamma, weights = saved["params"]
-            k = _Kernels(gamma.dtype)
             L = flt.L
-            g_new = [tuple(grads[3 * l:3 * l + 3]) for l in range(L)]
+            saved = ctx.saved_tensors
+            frame, gamma, weights, tape = saved[:4]
+            state_flat, new_flat = list(saved[4:4 + 3 * L]), list(saved[4 + 3 * L:])
             g_fu = grads[3 * L] if L == 1 and grads[3 * L] is not None and grads[3 * L].numel() else None
-            g_frame, g_gamma, g_weights, g_state = _frame_backward(k, flt, saved["tape"], gamma, weights,
-                                                                   saved["state"], ctx.first, g_new, g_fu)
-            return (None, None, g_frame, g_gamma, g_weights, *[t for lvl in g_state for t in lvl])
+            g_frame, g_gamma, g_weights, g_state = _frame_backward(flt, ctx.first, frame, gamma, weights, state_flat,
+                                                                   new_flat, tape, list(grads[:3 * L]), g_fu)
+            return (None, None, g_frame, g_gamma, g_weights, *g_state)
 
     return FrameStep
 

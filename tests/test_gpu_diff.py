@@ -234,15 +234,16 @@ def test_fitting_gamma_lowers_endpoint_error(dm, cuda):
     assert losses[-1] < losses[0]
 
 
-@pytest.mark.parametrize("levels", [1, 2, 3])
-def test_frame_node_matches_per_stage_nodes(dm, cuda, levels):
-    """The single autograd node per frame gives the per-stage nodes' flows and gradients."""
+@pytest.mark.parametrize("levels,smooth", [(1, [1]), (2, [1, 2]), (3, [1, 2, 1]), (2, [0, 1]), (3, [2, 0, 1])])
+def test_frame_node_matches_per_stage_nodes(dm, cuda, levels, smooth):
+    """The single autograd node per frame (ff_diff_frame_forward / _backward) gives the
+    per-stage nodes' flows and gradients, zero smoothing iterations included."""
     B, T, H, W = 2, 5, 26, 34
     frames = cuda.from_numpy(float_frames(B, T, H, W, 23).astype(np.float64)).cuda()
     proj = cuda.from_numpy(np.random.default_rng(5).normal(0, 1, (B, T, H, W, 2))).cuda()
     res = []
     for per_stage in (False, True):
-        f = dm.DiffPyramidalFlowFilter(H, W, levels, [3.0, 12.0, 40.0][:levels], [1, 2, 1][:levels], maxflow=4.0,
+        f = dm.DiffPyramidalFlowFilter(H, W, levels, [3.0, 12.0, 40.0][:levels], smooth, maxflow=4.0,
                                        dtype=cuda.float64, checkpoint_every=2)
         f.per_stage = per_stage
         x = frames.clone().requires_grad_(True)
@@ -253,3 +254,13 @@ def test_frame_node_matches_per_stage_nodes(dm, cuda, levels):
     np.testing.assert_array_equal(res[0][0], res[1][0])
     for a, b in zip(res[0][1:], res[1][1:]):
         np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-13)
+
+
+def test_frame_node_rejects_bad_geometry(dm, cuda):
+    """Level sizes that do not halve are refused by the library before any launch."""
+    f = dm.DiffPyramidalFlowFilter(20, 28, 2, dtype=cuda.float32)
+    g = dm._geom(f, 1)
+    g.height[1] = 11
+    assert dm.lib().ff_diff_frame_tape_bytes(0, dm.ctypes.byref(g)) == 0
+    with pytest.raises(ValueError):
+        dm._workspace("ff_diff_frame_tape_bytes", 0, g, cuda.zeros(1, device="cuda"))
