@@ -156,6 +156,39 @@ __device__ __forceinline__ void block_add(T v, T* dst) {
     }
 }
 
+// block-wide sums of NV values per thread in one pass; thread k < NV writes sum k to dst[k]
+// (added atomically if `atomic`, else stored: one slot set per block, reduced later)
+template <typename T, int NV>
+__device__ __forceinline__ void block_sum(const T (&v)[NV], T* dst, bool atomic) {
+    __shared__ T part[NV][32];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    for (int k = 0; k < NV; ++k) {
+        T x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) part[k][warp] = x;
+    }
+    __syncthreads();
+    if (t < NV) {
+        T acc = T(0);
+        for (int w = 0; w < nw; ++w) acc += part[t][w];
+        if (atomic) atomicAdd(&dst[t], acc);
+        else dst[t] = acc;
+    }
+}
+
+__device__ __forceinline__ size_t block_linear() {
+    return blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+}
+
+// write or add one gradient value
+template <bool ACC, typename T>
+__device__ __forceinline__ void put(T& dst, T v) {
+    if constexpr (ACC) dst += v;
+    else dst = v;
+}
+
 #define PIX_SETUP                                              \
     const int x = blockIdx.x * blockDim.x + threadIdx.x;       \
     const int y = blockIdx.y * blockDim.y + threadIdx.y;       \
@@ -246,6 +279,12 @@ __device__ __forceinline__ T tap_weight(const T* w, int i, int j, int n) {
     return acc;
 }
 
+// tap_weight where the stencil cannot reach a clamp (j - 2 .. j + 2 inside): the one tap j - i + 2
+template <typename T>
+__device__ __forceinline__ T tap_w(const T* w, int i, int j, int n, bool inner) {
+    return inner ? w[j - i + 2] : tap_weight(w, i, j, n);
+}
+
 // step 1 (gather): gradients of the Y blur by (used by a0 and ax along X) and of the X blur
 // bx (used by ay along Y) at this pixel
 template <typename T>
@@ -256,30 +295,32 @@ __global__ void model_bwd1_k(const T* __restrict__ ga0, const T* __restrict__ gg
     if (!live) return;
     const Masks<T> M;
     const size_t row = (b * H + y) * W;
+    const bool ix = x >= 2 && x + 2 <= W - 1, iy = y >= 2 && y + 2 <= H - 1;
     T aby = T(0), abx = T(0);
     for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) {
-        const T ws = tap_weight(M.s, i, x, W), wd = tap_weight(M.d, i, x, W);
+        const T ws = tap_w(M.s, i, x, W, ix), wd = tap_w(M.d, i, x, W, ix);
         aby += ws * ga0[row + i] + wd * ggrad[2 * (row + i)];
     }
     for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i)
-        abx += tap_weight(M.d, i, y, H) * ggrad[2 * ((b * H + i) * W + x) + 1];
+        abx += tap_w(M.d, i, y, H, iy) * ggrad[2 * ((b * H + i) * W + x) + 1];
     gby[row + x] = aby;
     gbx[row + x] = abx;
 }
 
 // step 2 (gather): by = Y blur of the image, bx = X blur of the image
-template <typename T>
+template <typename T, bool ACC = true>
 __global__ void model_bwd2_k(const T* __restrict__ gby, const T* __restrict__ gbx, T* gimg, int H, int W) {
     grid_dep_wait();
     grid_dep_launch();
     PIX_SETUP
     if (!live) return;
     const Masks<T> M;
+    const bool ix = x >= 2 && x + 2 <= W - 1, iy = y >= 2 && y + 2 <= H - 1;
     T acc = T(0);
-    for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i) acc += tap_weight(M.s, i, y, H) * gby[(b * H + i) * W + x];
+    for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i) acc += tap_w(M.s, i, y, H, iy) * gby[(b * H + i) * W + x];
     const size_t row = (b * H + y) * W;
-    for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) acc += tap_weight(M.s, i, x, W) * gbx[row + i];
-    gimg[row + x] += acc;
+    for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) acc += tap_w(M.s, i, x, W, ix) * gbx[row + i];
+    put<ACC>(gimg[row + x], acc);
 }
 
 // ------------------------------------------------------------------ propagation sub-step
@@ -309,7 +350,7 @@ __global__ void prop_fwd_k(const T* __restrict__ f, const T* __restrict__ s, con
 // Gather-form adjoint of one upwind sub-step: input pixel j (index along AXIS) collects
 // from the outputs i in {j-1, j, j+1} whose clamped stencil (i-1, i, i+1) reads it,
 // recomputing each output's dominant velocity, upwind branch and border freeze.
-template <typename T, int AXIS, bool PAYLOAD>
+template <typename T, int AXIS, bool PAYLOAD, bool ACC = true>
 __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v,
                            const T* __restrict__ gfo, const T* __restrict__ gso, const T* __restrict__ gvo, T* gf, T* gs,
                            T* gv, int H, int W, T dt, int border) {
@@ -331,6 +372,52 @@ __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, con
     };
     T acc[NC];
     for (int c = 0; c < NC; ++c) acc[c] = T(0);
+    if (j >= 2 && j + 2 <= n - 1) {
+        // away from the line ends no index clamps: the five positions j-2..j+2 in registers,
+        // the same operations in the same order as the general loop below
+        T ch[NC][5], go[NC][3];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+            const size_t k = at(j - 2 + p);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ch[c][p] = chan(k, c);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const size_t k = at(j - 1 + q);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) go[c][q] = gchan(k, c);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
+            const int i = j - 1 + q;
+            if (!(line_in && i >= border && i < n - border)) {
+                if (q == 1)
+                    for (int c = 0; c < NC; ++c) acc[c] += go[c][1];
+                continue;
+            }
+            const T vm_ = ch[AXIS][q], vp_ = ch[AXIS][q + 2];
+            const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
+            const T dv = take_p ? vp_ : vm_;
+            const T t = dt * dv;
+            T gdv = T(0);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const T g_o = go[c][q];
+                const T g0 = ch[c][q + 1];
+                if (dv >= T(0)) {
+                    if (q == 1) acc[c] += g_o * (T(1) - t);
+                    if (q == 2) acc[c] += g_o * t;
+                    gdv -= g_o * dt * (g0 - ch[c][q]);
+                } else {
+                    if (q == 1) acc[c] += g_o * (T(1) + t);
+                    if (q == 0) acc[c] -= g_o * t;
+                    gdv -= g_o * dt * (ch[c][q + 2] - g0);
+                }
+            }
+            if ((take_p ? q + 2 : q) == 2) acc[AXIS] += gdv;
+        }
+    } else
     for (int i = max(j - 1, 0); i <= min(j + 1, n - 1); ++i) {
         const size_t ki = at(i);
         const bool in = line_in && i >= border && i < n - border;
@@ -365,12 +452,12 @@ __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, con
         if ((take_p ? ip : im) == j) acc[AXIS] += gdv;
     }
     const size_t kj = at(j);
-    gf[2 * kj] += acc[0];
-    gf[2 * kj + 1] += acc[1];
+    put<ACC>(gf[2 * kj], acc[0]);
+    put<ACC>(gf[2 * kj + 1], acc[1]);
     if constexpr (PAYLOAD) {
-        gs[kj] += acc[2];
-        gv[2 * kj] += acc[3];
-        gv[2 * kj + 1] += acc[4];
+        put<ACC>(gs[kj], acc[2]);
+        put<ACC>(gv[2 * kj], acc[3]);
+        put<ACC>(gv[2 * kj + 1], acc[4]);
     }
 }
 
@@ -500,7 +587,8 @@ __global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in,
                                  in[2 * kk[4] + ch]);
 }
 
-template <typename T, int AXIS>
+// PART: gw5 is a partial-sum array, this block stores its 5 sums at gw5[5 * block]
+template <typename T, int AXIS, bool ACC = true, bool PART = false>
 __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in, const T* __restrict__ gout, T* gin,
                              T* gw5, int H, int W) {
     grid_dep_wait();
@@ -515,6 +603,18 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
         auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
         // input gradient at this pixel: outputs i in [j-2, j+2] whose clamped taps land on j
         T a0 = T(0), a1 = T(0);
+        if (j >= 2 && j + 2 <= n - 1) {
+            // no clamps: output i reads j through tap j - i + 2 only
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const T wt = w[4 - q];
+                const size_t ki = at(j - 2 + q);
+                if (wt != T(0)) {
+                    a0 += wt * gout[2 * ki];
+                    a1 += wt * gout[2 * ki + 1];
+                }
+            }
+        } else
         for (int i = max(j - 2, 0); i <= min(j + 2, n - 1); ++i) {
             const T wt = tap_weight(w, i, j, n);
             if (wt != T(0)) {
@@ -522,8 +622,8 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
                 a1 += wt * gout[2 * at(i) + 1];
             }
         }
-        gin[2 * at(j)] += a0;
-        gin[2 * at(j) + 1] += a1;
+        put<ACC>(gin[2 * at(j)], a0);
+        put<ACC>(gin[2 * at(j) + 1], a1);
         // weight gradient: this pixel as an output
         const T g0 = gout[2 * at(j)], g1 = gout[2 * at(j) + 1];
         for (int k = 0; k < 5; ++k) {
@@ -531,10 +631,124 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
             gw[k] = g0 * in[2 * kk] + g1 * in[2 * kk + 1];
         }
     }
-    for (int i = 0; i < 5; ++i) {
-        block_add(gw[i], &gw5[i]);
-        __syncthreads();
+    block_sum<T, 5>(gw, PART ? gw5 + 5 * block_linear() : gw5, !PART);
+}
+
+// Store-mode update adjoints of the frame driver: every per-pixel gradient is stored (the
+// destinations start undefined), the gradient of a0 as a state output (ga0_out, nullable)
+// is folded in, `first` (old image == a0) cancels the yt path, gold is added (a caller's
+// input-state gradient) or stored, and the gamma gradient goes to one partial per block.
+template <typename T>
+struct FrameAdj {
+    const T* ga0_out;
+    int first;
+    int gold_acc;
+    T* part;
+    __device__ void write(size_t k, const SolveGrad<T>& d, T* ga0, T* ggrad, T* gold, T* gfh) const {
+        const T gyt = first ? T(0) : d.gyt;
+        ga0[k] = (ga0_out ? ga0_out[k] : T(0)) - gyt;
+        ggrad[2 * k] = d.gax;
+        ggrad[2 * k + 1] = d.gay;
+        gfh[2 * k] = d.gfx;
+        gfh[2 * k + 1] = d.gfy;
+        if (gold_acc) {
+            if (!first) gold[k] += gyt;
+        } else {
+            gold[k] = gyt;
+        }
     }
+};
+
+template <typename T>
+__global__ void update_bwd_frame_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                                   const T* __restrict__ fh, const T* __restrict__ gamma, const T* __restrict__ gout,
+                                   T* ga0, T* ggrad, T* gold, T* gfh, FrameAdj<T> fa, int H, int W, T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    T gg[1] = {T(0)};
+    if (live) {
+        const size_t k = (b * H + y) * W + x;
+        const T g = *gamma, c = a0[k], ax = grad[2 * k], ay = grad[2 * k + 1], yt = Ar<T>::sub(old[k], c);
+        const T fx = fh[2 * k], fy = fh[2 * k + 1];
+        const Solve<T> s(g, ax, ay, yt, fx, fy);
+        const T gx = passes(s.ox, maxflow) ? gout[2 * k] : T(0);
+        const T gy = passes(s.oy, maxflow) ? gout[2 * k + 1] : T(0);
+        const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
+        fa.write(k, d, ga0, ggrad, gold, gfh);
+        gg[0] = d.gg;
+    }
+    block_sum<T, 1>(gg, fa.part + block_linear(), false);
+}
+
+template <typename T>
+__global__ void dupdate_bwd_frame_k(const T* __restrict__ a0, const T* __restrict__ grad, const T* __restrict__ old,
+                                    const T* __restrict__ dh, const T* __restrict__ coarse,
+                                    const T* __restrict__ gamma, const T* __restrict__ gflow,
+                                    const T* __restrict__ gdelta, T* ga0, T* ggrad, T* gold, T* gdh, T* gcoarse,
+                                    FrameAdj<T> fa, int H, int W, int Hc, int Wc, T maxflow) {
+    grid_dep_wait();
+    grid_dep_launch();
+    PIX_SETUP
+    T gg[1] = {T(0)};
+    // a warp is 32 consecutive pixels of one row and the coarse column is monotone in x, so
+    // lanes sharing a coarse pixel form runs: each run's sum is added by its first lane
+    unsigned long long key = ~0ull - threadIdx.x;  // distinct for pixels outside the image
+    T cx = T(0), cy = T(0);
+    size_t kc = 0;
+    if (live) {
+        const size_t k = (b * H + y) * W + x;
+        const T g = *gamma, c = a0[k], ax = grad[2 * k], ay = grad[2 * k + 1], yt = Ar<T>::sub(old[k], c);
+        const T fx = dh[2 * k], fy = dh[2 * k + 1];
+        const Solve<T> s(g, ax, ay, yt, fx, fy);
+        const T hm = Ar<T>::mul(T(0.5), maxflow);
+        const T dx = clampm(sanitize(s.ox), hm), dy = clampm(sanitize(s.oy), hm);
+        kc = (b * Hc + upmap_index(y, H, Hc)) * Wc + upmap_index(x, W, Wc);
+        key = kc;
+        const T ux = Ar<T>::add(dx, Ar<T>::mul(T(2), coarse[2 * kc]));
+        const T uy = Ar<T>::add(dy, Ar<T>::mul(T(2), coarse[2 * kc + 1]));
+        const T gux = passes(ux, maxflow) ? gflow[2 * k] : T(0);
+        const T guy = passes(uy, maxflow) ? gflow[2 * k + 1] : T(0);
+        cx = T(2) * gux;
+        cy = T(2) * guy;
+        const T gx = passes(s.ox, hm) ? gdelta[2 * k] + gux : T(0);
+        const T gy = passes(s.oy, hm) ? gdelta[2 * k + 1] + guy : T(0);
+        const SolveGrad<T> d(s, g, ax, ay, yt, fx, fy, gx, gy);
+        fa.write(k, d, ga0, ggrad, gold, gdh);
+        gg[0] = d.gg;
+    }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x;  // blocks are 32 wide
+    const unsigned run = __match_any_sync(full, key);
+    const unsigned longest = __reduce_max_sync(full, (unsigned)__popc(run));
+    T sx = cx, sy = cy;
+    for (unsigned d = 1; d < longest; ++d) {
+        const T ox = __shfl_down_sync(full, cx, d), oy = __shfl_down_sync(full, cy, d);
+        if (lane + d < 32 && ((run >> (lane + d)) & 1u)) {
+            sx += ox;
+            sy += oy;
+        }
+    }
+    if (live && lane == __ffs(run) - 1) {
+        atomic_add(&gcoarse[2 * kc], sx);
+        atomic_add(&gcoarse[2 * kc + 1], sy);
+    }
+    block_sum<T, 1>(gg, fa.part + block_linear(), false);
+}
+
+// dst[v] += sum over i < n of part[i * NV + v], one block (fixed order: deterministic)
+template <typename T, int NV>
+__global__ void reduce_parts_k(const T* __restrict__ part, int n, T* dst) {
+    grid_dep_wait();
+    grid_dep_launch();
+    T acc[NV];
+    for (int v = 0; v < NV; ++v) acc[v] = T(0);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int v = 0; v < NV; ++v) acc[v] += part[(size_t)i * NV + v];
+    __shared__ T tot[NV];
+    block_sum<T, NV>(acc, tot, false);
+    __syncthreads();
+    if (threadIdx.x < NV) dst[threadIdx.x] += tot[threadIdx.x];
 }
 
 // dst += src over n elements
@@ -875,10 +1089,15 @@ struct Tape {
     }
 };
 
+inline size_t blocks_of(const Geo& g, int l) {
+    const dim3 d = grid3(g.W[l], g.H[l], g.B);
+    return (size_t)d.x * d.y * d.z;
+}
+
 // backward scratch (elements of T)
 struct Scratch {
-    size_t gimg[FF_DIFF_MAX_LEVELS] = {};
-    size_t ga0, gg, gold, gh, gfu, gby, gbx, pa, pb, sa, sb, zero;
+    size_t gimg[FF_DIFF_MAX_LEVELS] = {};  // image gradients of levels >= 1
+    size_t ga0, gg, gfu, gby, gbx, pa, pb, sa, sb, zero, part;
     size_t total = 0;
     Scratch(const Geo& g) {
         auto take = [&](size_t n) {
@@ -886,16 +1105,15 @@ struct Scratch {
             total += (n + 31) / 32 * 32;
             return at;
         };
-        size_t n1m = 0;
+        size_t n1m = 0, nparts = 0;
         for (int l = 0; l < g.L; ++l) {
-            gimg[l] = take(g.n1(l));
+            if (l > 0) gimg[l] = take(g.n1(l));
             n1m = std::max(n1m, g.n1(l));
+            nparts = std::max(nparts, (size_t)std::max(2 * g.S[l], 1) * blocks_of(g, l) * 5);
         }
         const size_t n2m = 2 * n1m, st = n2m + n1m + n2m;
         ga0 = take(n1m);
         gg = take(n2m);
-        gold = take(n1m);
-        gh = take(n2m);
         gfu = take(2 * g.n1(g.L - 1));
         gby = take(n1m);
         gbx = take(n1m);
@@ -903,7 +1121,8 @@ struct Scratch {
         pb = take(st);
         sa = take(n2m);
         sb = take(n2m);
-        zero = take(st);  // zeros standing in for absent output gradients
+        zero = take(n2m);  // zeros standing in for absent output gradients
+        part = take(nparts);  // per-block partial sums of the gamma and weight gradients
     }
 };
 
@@ -917,8 +1136,15 @@ struct Driver {
     }
     dim3 grid(int l) const { return grid3(g.W[l], g.H[l], g.B); }
     void zero(T* p, size_t n) const { ok(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void copy(T* dst, const T* src, size_t n) const {
+        ok(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
     void add(T* dst, const T* src, size_t n) const {
         ok(launch_k(add_k<T>, dim3((unsigned)std::min<size_t>((n + 255) / 256, 4096)), dim3(256), 0, s, dst, src, n));
+    }
+    void reduce(const T* part, size_t n, int nv, T* dst) const {
+        ok(nv == 5 ? launch_k(reduce_parts_k<T, 5>, dim3(1), dim3(1024), 0, s, part, (int)n, dst)
+                   : launch_k(reduce_parts_k<T, 1>, dim3(1), dim3(1024), 0, s, part, (int)n, dst));
     }
     void prop(int l, int axis, bool payload, const T* f, const T* sc, const T* v, T* fo, T* so, T* vo) const {
         const T dt = (T)(1.0 / g.N[l]);
@@ -933,38 +1159,43 @@ struct Driver {
         }
         ok(e);
     }
-    void prop_bwd(int l, int axis, bool payload, const T* f, const T* sc, const T* v, const T* gfo, const T* gso,
-                  const T* gvo, T* gf, T* gs, T* gv) const {
+    template <bool PAYLOAD, bool ACC>
+    void prop_bwd(int l, int axis, const T* f, const T* sc, const T* v, const T* gfo, const T* gso, const T* gvo, T* gf,
+                  T* gs, T* gv) const {
         const T dt = (T)(1.0 / g.N[l]);
         const int H = g.H[l], W = g.W[l], b = g.border;
-        cudaError_t e;
-        if (payload) {
-            e = axis == 0 ? launch_k(prop_bwd_k<T, 0, true>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs, gv,
-                                     H, W, dt, b)
-                          : launch_k(prop_bwd_k<T, 1, true>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs, gv,
-                                     H, W, dt, b);
-        } else {
-            e = axis == 0 ? launch_k(prop_bwd_k<T, 0, false>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
-                                     gv, H, W, dt, b)
-                          : launch_k(prop_bwd_k<T, 1, false>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
-                                     gv, H, W, dt, b);
-        }
-        ok(e);
+        ok(axis == 0 ? launch_k(prop_bwd_k<T, 0, PAYLOAD, ACC>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
+                                gv, H, W, dt, b)
+                     : launch_k(prop_bwd_k<T, 1, PAYLOAD, ACC>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
+                                gv, H, W, dt, b));
     }
     void smooth(int l, int axis, const T* w5, const T* in, T* out) const {
         ok(axis == 0 ? launch_k(smooth_fwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l])
                      : launch_k(smooth_fwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l]));
     }
-    void smooth_bwd(int l, int axis, const T* w5, const T* in, const T* go, T* gi, T* gw5) const {
-        ok(axis == 0 ? launch_k(smooth_bwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, go, gi, gw5, g.H[l], g.W[l])
-                     : launch_k(smooth_bwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, go, gi, gw5, g.H[l], g.W[l]));
+    // one smoothing pass's adjoint: input gradient stored (or added), weight sums per block
+    void smooth_bwd(int l, int axis, bool acc, const T* w5, const T* in, const T* go, T* gi, T* part) const {
+        const dim3 gr = grid(l);
+        const int H = g.H[l], W = g.W[l];
+        cudaError_t e;
+        if (acc)
+            e = axis == 0 ? launch_k(smooth_bwd_k<T, 0, true, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W)
+                          : launch_k(smooth_bwd_k<T, 1, true, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W);
+        else
+            e = axis == 0 ? launch_k(smooth_bwd_k<T, 0, false, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W)
+                          : launch_k(smooth_bwd_k<T, 1, false, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W);
+        ok(e);
     }
     void model(int l, const T* img, T* a0, T* grad) const {
         ok(launch_k(model_fwd_k<T>, grid(l), kBlock, 0, s, img, a0, grad, g.H[l], g.W[l]));
     }
-    void model_bwd(int l, const T* ga0, const T* ggrad, T* gby, T* gbx, T* gimg) const {
+    // image gradient of the image model: stored into gimg, or added when acc
+    void model_bwd(int l, bool acc, const T* ga0, const T* ggrad, T* gby, T* gbx, T* gimg) const {
         ok(launch_k(model_bwd1_k<T>, grid(l), kBlock, 0, s, ga0, ggrad, gby, gbx, g.H[l], g.W[l]));
-        ok(launch_k(model_bwd2_k<T>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l], g.W[l]));
+        ok(acc ? launch_k(model_bwd2_k<T, true>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l],
+                          g.W[l])
+               : launch_k(model_bwd2_k<T, false>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l],
+                          g.W[l]));
     }
 
     // ---- forward
@@ -993,9 +1224,9 @@ struct Driver {
             T* fu = tp + tape.sm[l][0];
             ok(launch_k(update_fwd_k<T>, grid(l), kBlock, 0, s, (const T*)a0, (const T*)grad, old, f, gamma + l, fu,
                         g.H[l], g.W[l], (T)g.maxflow[l]));
-            if (fu_out) ok(cudaMemcpyAsync(fu_out, fu, n2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            if (fu_out) copy(fu_out, fu, n2);
             smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l]);
-            ok(cudaMemcpyAsync(out[3 * l + 2], in[3 * l + 2], n2 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            copy(out[3 * l + 2], in[3 * l + 2], n2);
         }
         // delta levels, L-2 down to 0
         for (int l = L - 2; l >= 0; --l) {
@@ -1022,47 +1253,57 @@ struct Driver {
     // 2S passes from tape.sm[l][0]; pass j writes tape.sm[l][j+1], the last writes `last`
     void smooth_chain(int l, const T* w5, const Tape& tape, T* tp, T* last) const {
         const int n = 2 * g.S[l];
-        if (n == 0) ok(cudaMemcpyAsync(last, tp + tape.sm[l][0], 2 * g.n1(l) * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        if (n == 0) copy(last, tp + tape.sm[l][0], 2 * g.n1(l));
         for (int j = 0; j < n; ++j) smooth(l, j % 2, w5, tp + tape.sm[l][j], j + 1 < n ? tp + tape.sm[l][j + 1] : last);
     }
 
-    // ---- backward: gradients of the outputs -> gradients of the inputs (all accumulated)
+    // ---- backward: gradients of the outputs -> gradients of the inputs, ADDED into the
+    // caller's buffers.  Inside, every intermediate gradient is stored by the kernel that
+    // produces it (no clearing), and only the kernels writing the caller's buffers add.
     void backward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in,
                   const T* const* out, const T* tp, const T* const* gout, const T* gfu_out, T* gframe, T* ggamma,
                   T* gweights, T* const* gin, T* sc_) const {
+        (void)frame;
         const Tape tape(g);
         const Scratch S_(g);
         const int L = g.L, top = L - 1;
+        // image gradients: level 0's is the caller's frame gradient itself
         T* gimg[FF_DIFF_MAX_LEVELS];
-        for (int l = 0; l < L; ++l) {
-            gimg[l] = sc_ + S_.gimg[l];
-            zero(gimg[l], g.n1(l));
-        }
+        gimg[0] = gframe;
+        for (int l = 1; l < L; ++l) gimg[l] = sc_ + S_.gimg[l];
         T* const zbuf = sc_ + S_.zero;
-        size_t n1m = 0;
-        for (int l = 0; l < L; ++l) n1m = std::max(n1m, g.n1(l));
-        zero(zbuf, 5 * n1m);
+        zero(zbuf, 2 * g.n1(0));
         auto gz = [&](const T* p) { return p ? p : (const T*)zbuf; };
+        // gradient of the top level's unsmoothed flow: the caller's, the coarse reads of level
+        // L-2 (scattered by its update adjoint) and the top's smoothing adjoint, in that order
         T* gfu = sc_ + S_.gfu;
-        zero(gfu, 2 * g.n1(top));
-        if (gfu_out) add(gfu, gfu_out, 2 * g.n1(top));
-        T *ga0 = sc_ + S_.ga0, *ggr = sc_ + S_.gg, *gold = sc_ + S_.gold, *gh = sc_ + S_.gh;
-        T *pa = sc_ + S_.pa, *pb = sc_ + S_.pb, *sa = sc_ + S_.sa, *sb = sc_ + S_.sb;
-        T *gby = sc_ + S_.gby, *gbx = sc_ + S_.gbx;
-        // smoothing chain adjoint: returns the gradient of tape.sm[l][0]
-        auto smooth_back = [&](int l, const T* g_last) -> const T* {
+        if (gfu_out) copy(gfu, gfu_out, 2 * g.n1(top));
+        else zero(gfu, 2 * g.n1(top));
+        T *ga0 = sc_ + S_.ga0, *ggr = sc_ + S_.gg, *gby = sc_ + S_.gby, *gbx = sc_ + S_.gbx;
+        T *pa = sc_ + S_.pa, *pb = sc_ + S_.pb, *sa = sc_ + S_.sa, *sb = sc_ + S_.sb, *part = sc_ + S_.part;
+
+        // adjoint of the 2S smoothing passes of level l, from the gradient of the smoothed
+        // flow; the gradient of the pass-0 input goes to dst (added if acc) and is returned.
+        // Pass j > 0 writes bufs[j % 2]; pass 1 writes sb, so dst may be sa.
+        auto smooth_back = [&](int l, const T* g_last, T* dst, bool acc) -> const T* {
             const int n = 2 * g.S[l];
-            const size_t n2 = 2 * g.n1(l);
             const T* gcur = gz(g_last);
+            if (n == 0) {
+                if (!acc) return gcur;
+                add(dst, gcur, 2 * g.n1(l));
+                return dst;
+            }
+            const size_t nb = blocks_of(g, l);
             T* bufs[2] = {sa, sb};
             for (int j = n - 1; j >= 0; --j) {
-                T* dst = bufs[j % 2];
-                zero(dst, n2);
-                smooth_bwd(l, j % 2, weights + 5 * l, tp + tape.sm[l][j], gcur, dst, gweights + 5 * l);
-                gcur = dst;
+                T* o = j == 0 ? dst : bufs[j % 2];
+                smooth_bwd(l, j % 2, j == 0 && acc, weights + 5 * l, tp + tape.sm[l][j], gcur, o, part + j * nb * 5);
+                gcur = o;
             }
+            reduce(part, n * nb, 5, gweights + 5 * l);
             return gcur;
         };
+
         for (int l = 0; l <= L - 2; ++l) {
             const size_t n1 = g.n1(l), n2 = 2 * n1;
             const T* a0 = out[3 * l + 1];
@@ -1073,79 +1314,74 @@ struct Driver {
             const T* vh = fh_base + n2 + n1;
             const T* old = first ? a0 : sh;
             const T* coarse = l == L - 2 ? tp + tape.sm[top][0] : in[3 * (l + 1)];
-            const T* gflow = smooth_back(l, gout[3 * l]);
-            zero(ga0, n1);
-            zero(ggr, n2);
-            zero(gold, n1);
-            zero(gh, n2);
+            const T* gflow = smooth_back(l, gout[3 * l], sa, false);
+            // gradients of the propagated (f, s, v): f is not read after propagation (zero),
+            // s is the old image unless first, v the delta input of the solve
+            T* gsh = pa + n2;
+            T* gvh = pa + n2 + n1;
             T* gco = l == L - 2 ? gfu : gin[3 * (l + 1)];
-            ok(launch_k(dupdate_bwd_k<T>, grid(l), kBlock, 0, s, a0, grad, old, vh, coarse, gamma + l, gflow,
-                        gz(gout[3 * l + 2]), ga0, ggr, gold, gh, gco, ggamma + l, g.H[l], g.W[l], g.H[l + 1],
-                        g.W[l + 1], (T)g.maxflow[l]));
-            if (gout[3 * l + 1]) add(ga0, gout[3 * l + 1], n1);
-            // gradient of the propagated (f, s, v): f none, s = old (unless first), v = gh
-            T* cur = pa;
-            zero(cur, n2 + n1 + n2);
-            if (first) add(ga0, gold, n1);
-            else add(cur + n2, gold, n1);
-            add(cur + n2 + n1, gh, n2);
+            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 0, part};
+            ok(launch_k(dupdate_bwd_frame_k<T>, grid(l), kBlock, 0, s, a0, grad, old, vh, coarse, gamma + l, gflow,
+                        gz(gout[3 * l + 2]), ga0, ggr, gsh, gvh, gco, fa, g.H[l], g.W[l], g.H[l + 1], g.W[l + 1],
+                        (T)g.maxflow[l]));
+            reduce(part, blocks_of(g, l), 1, ggamma + l);
+            const T *cf = zbuf, *cs = gsh, *cv = gvh;
+            T* bufs[2] = {pb, pa};
             for (int k = last; k >= 0; --k) {
                 const T *f, *sc, *v;
                 if (k == 0) {
                     f = in[3 * l];
                     sc = in[3 * l + 1];
                     v = in[3 * l + 2];
-                } else {
-                    const T* b = tp + tape.prop[l][k - 1];
-                    f = b;
-                    sc = b + n2;
-                    v = b + n2 + n1;
+                    prop_bwd<true, true>(l, 0, f, sc, v, cf, cs, cv, gin[3 * l], gin[3 * l + 1], gin[3 * l + 2]);
+                    break;
                 }
-                T* nxt = cur == pa ? pb : pa;
-                zero(nxt, n2 + n1 + n2);
-                prop_bwd(l, k % 2, true, f, sc, v, cur, cur + n2, cur + n2 + n1, nxt, nxt + n2, nxt + n2 + n1);
-                cur = nxt;
+                const T* b = tp + tape.prop[l][k - 1];
+                f = b;
+                sc = b + n2;
+                v = b + n2 + n1;
+                T* o = bufs[(last - k) % 2];
+                prop_bwd<true, false>(l, k % 2, f, sc, v, cf, cs, cv, o, o + n2, o + n2 + n1);
+                cf = o;
+                cs = o + n2;
+                cv = o + n2 + n1;
             }
-            add(gin[3 * l], cur, n2);
-            add(gin[3 * l + 1], cur + n2, n1);
-            add(gin[3 * l + 2], cur + n2 + n1, n2);
-            model_bwd(l, ga0, ggr, gby, gbx, gimg[l]);
+            model_bwd(l, l == 0, ga0, ggr, gby, gbx, gimg[l]);
         }
         {
             const int l = top;
-            const size_t n1 = g.n1(l), n2 = 2 * n1;
+            const size_t n2 = 2 * g.n1(l);
             const T* a0 = out[3 * l + 1];
             const T* grad = tp + tape.grad[l];
             const int last = 2 * g.N[l] - 1;
             const T* fh = tp + tape.prop[l][last];
             const T* old = first ? a0 : in[3 * l + 1];
-            add(gfu, smooth_back(l, gout[3 * l]), n2);
-            zero(ga0, n1);
-            zero(ggr, n2);
-            zero(gold, n1);
-            zero(gh, n2);
-            ok(launch_k(update_bwd_k<T>, grid(l), kBlock, 0, s, a0, grad, old, fh, gamma + l, (const T*)gfu, ga0, ggr,
-                        gold, gh, ggamma + l, g.H[l], g.W[l], (T)g.maxflow[l]));
-            if (gout[3 * l + 1]) add(ga0, gout[3 * l + 1], n1);
-            if (first) add(ga0, gold, n1);
-            else add(gin[3 * l + 1], gold, n1);
+            smooth_back(l, gout[3 * l], gfu, true);
+            T* gh = pa;
+            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 1, part};
+            ok(launch_k(update_bwd_frame_k<T>, grid(l), kBlock, 0, s, a0, grad, old, fh, gamma + l, (const T*)gfu, ga0,
+                        ggr, gin[3 * l + 1], gh, fa, g.H[l], g.W[l], (T)g.maxflow[l]));
+            reduce(part, blocks_of(g, l), 1, ggamma + l);
             if (gout[3 * l + 2]) add(gin[3 * l + 2], gout[3 * l + 2], n2);
-            T* cur = gh;
-            T* bufs[2] = {pa, pb};
+            const T* cur = gh;
+            T* bufs[2] = {pb, pa};
             for (int k = last; k >= 0; --k) {
-                const T* f = k == 0 ? in[3 * l] : tp + tape.prop[l][k - 1];
-                T* nxt = bufs[k % 2];
-                zero(nxt, n2);
-                prop_bwd(l, k % 2, false, f, nullptr, nullptr, cur, nullptr, nullptr, nxt, nullptr, nullptr);
-                cur = nxt;
+                if (k == 0) {
+                    prop_bwd<false, true>(l, 0, in[3 * l], nullptr, nullptr, cur, nullptr, nullptr, gin[3 * l],
+                                          nullptr, nullptr);
+                    break;
+                }
+                T* o = bufs[(last - k) % 2];
+                prop_bwd<false, false>(l, k % 2, tp + tape.prop[l][k - 1], nullptr, nullptr, cur, nullptr, nullptr, o,
+                                       nullptr, nullptr);
+                cur = o;
             }
-            add(gin[3 * l], cur, n2);
-            model_bwd(l, ga0, ggr, gby, gbx, gimg[l]);
+            model_bwd(l, l == 0, ga0, ggr, gby, gbx, gimg[l]);
         }
+        // pyramid adjoint, coarse to fine, added into the finer level's image gradient
         for (int l = L - 1; l >= 1; --l)
             ok(launch_k(pyr_bwd_k<T>, grid3(g.W[l - 1], g.H[l - 1], g.B), kBlock, 0, s, (const T*)gimg[l], gimg[l - 1],
                         g.H[l - 1], g.W[l - 1]));
-        add(gframe, gimg[0], g.n1(0));
     }
 };
 
