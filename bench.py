@@ -452,9 +452,10 @@ def bench_batched(steps, warmup):
 
 def bench_differentiable(steps):
     """The differentiable filter on 16 sequences of 256x256 float frames, 32 frames each,
-    2 levels (gamma [10, 50], smoothing [2, 4], maxflow 4, checkpoint every 8 frames):
-    device time of the forward pass alone and of forward + backward of the mean endpoint
-    error over frames 8-31 against the known flow."""
+    2 levels (gamma [10, 50], smoothing [2, 4], maxflow 4): device time of the forward pass
+    alone and of forward + backward of the mean endpoint error over frames 8-31 against the
+    known flow, with the whole tape resident in HBM (no recompute) and with checkpoints every
+    8 frames (each segment's forward recomputed in the backward pass)."""
     import torch
     from flowfilter_b200 import diff, synthetic
 
@@ -463,16 +464,19 @@ def bench_differentiable(steps):
                                       amp=2.0) for b in range(B)]
     frames = torch.from_numpy(np.stack([q[0] for q in seqs])).cuda()
     truth = torch.from_numpy(np.stack([np.stack([q[1], q[2]], -1) for q in seqs])).cuda()[:, None]
-    f = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=8)
+    f = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=T)
+    fc = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=8)
 
     def fwd():
         with torch.no_grad():
             return f(frames)
 
-    def fwd_bwd():
-        loss = diff.endpoint_error(f(frames), truth.expand(B, T, H, W, 2), first=8)
-        loss.backward()
-        return loss
+    def fwd_bwd(flt):
+        def run():
+            loss = diff.endpoint_error(flt(frames), truth.expand(B, T, H, W, 2), first=8)
+            loss.backward()
+            return loss
+        return run
 
     def timed(fn, n):
         for _ in range(2):
@@ -488,11 +492,15 @@ def bench_differentiable(steps):
 
     n = max(1, min(steps, 5))
     t_f = timed(fwd, n)
-    t_fb = timed(fwd_bwd, n)
+    t_fb = timed(fwd_bwd(f), n)
+    t_fbc = timed(fwd_bwd(fc), n)
+    tape = diff.lib().ff_diff_frame_tape_bytes(0, diff.ctypes.byref(diff._geom(f, B)))
     return {
         "workload": f"{B} sequences x {T} frames of {W}x{H} float32, 2 levels, gamma [10, 50], smoothing [2, 4], "
-                    "maxflow 4, loss = mean endpoint error over frames 8-31, checkpoint every 8 frames",
+                    "maxflow 4, loss = mean endpoint error over frames 8-31",
         "fwd_ms": t_f, "fwd_bwd_ms": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
+        "tape_bytes_per_frame": tape, "tape_note": "whole-sequence tape resident in HBM (no recompute)",
+        "fwd_bwd_ckpt8_ms": t_fbc, "fwd_bwd_ckpt8_over_fwd": t_fbc / t_f,
         "fwd_frames_per_s": B * T / (t_f / 1e3), "fwd_bwd_frames_per_s": B * T / (t_fb / 1e3),
         "dtype": "f32", "data": "synthetic: seeded bump flows (seed 200 + b), known flow",
     }
