@@ -450,6 +450,44 @@ def bench_batched(steps, warmup):
     }
 
 
+def bench_flow_to_color(filt, n):
+    """Mean device microseconds of ff_flow_to_color per launch on the filter's current
+    level-0 flow (a pitched device view): 20 launches captured in a CUDA graph, replayed
+    so that host launch overhead is not timed."""
+    import ctypes
+
+    import torch
+    from flowfilter_b200 import lib
+
+    flow = filt.getFlowDevice()
+    h, w = flow.shape[:2]
+    out = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    args = lambda st: (ctypes.c_void_p(flow.data_ptr()), flow.stride(0) * 4, h, w, 4.0, None,  # noqa: E731
+                       ctypes.c_void_p(out.data_ptr()), out.stride(0), ctypes.c_void_p(st.cuda_stream))
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            assert lib().ff_flow_to_color(*args(side)) == 0  # the first call uploads the default wheel
+    torch.cuda.synchronize()
+    per_graph = 20
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        for _ in range(per_graph):
+            lib().ff_flow_to_color(*args(side))
+    for _ in range(3):
+        g.replay()
+    reps = max(1, n // per_graph)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e3 / (reps * per_graph)
+
+
 def bench_differentiable(steps):
     """The differentiable filter on 16 sequences of 256x256 float frames, 32 frames each,
     2 levels (gamma [10, 50], smoothing [2, 4], maxflow 4): device time of the forward pass
@@ -537,6 +575,10 @@ def bench_b200(args):
         filt.compute()
         et.append(filt.elapsedTime())
     elapsed_ms = float(np.mean(et))
+
+    # ---- FlowToColor of the level-0 flow (the step after the filter in the reference's
+    # demos): device time per launch, back to back, the flow L2-resident as after a frame
+    ftc_us = bench_flow_to_color(filt, min(args.steps, 1000))
     l0_bytes = level0_kernel_bytes(w)
     achieved = l0_bytes / (l0_ms / 1000.0) / 1e9
     traffic = ncu_traffic(PRIMARY)
@@ -604,6 +646,10 @@ def bench_b200(args):
                          "algorithmic_bytes": l0_bytes, "launch_ms": l0_ms, "peak_kind": peak_kind,
                          "l2_resident": {"launch_ms": l0_ms_l2, "achieved": l0_bytes / (l0_ms_l2 / 1e3) / 1e9,
                                          "note": "same step without the L2 flush (state L2-resident)"}},
+            "flow_to_color": {"launch_us": ftc_us, "pixels": w["H"] * w["W"],
+                              "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
+                              "note": "ff_flow_to_color on the 640x480 level-0 flow, default wheel; "
+                                      "12 B/px (float2 in, RGBA out)"},
             "elapsed_time_ms": {"value": elapsed_ms, "frames": len(et),
                                 "path": "PyramidalFlowFilter.loadImage(host numpy) + compute(); mean elapsedTime(), "
                                         "as the reference notebook measures"},

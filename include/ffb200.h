@@ -297,6 +297,23 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
 ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
                              const void* gout, void* gin, void* gw5, void* stream);
 
+/* FlowToColor::compute (src/gpu/display.cu:95-110, kernel src/gpu/device/display_k.cu:14-43):
+ * colour-encodes a flow field [height][width] float2 (device, rows flow_pitch bytes apart,
+ * 8-byte aligned) into RGBA [height][width] uchar4 (device, color_pitch).  Each component is
+ * normalised to u = (f + maxflow) / (2 maxflow) and picks a column (x) and a row (y) of a
+ * 256x256 RGBA colour wheel exactly as the reference's clamped, point-sampled texture read
+ * does.  `wheel` is a dense device array of 256*256*4 bytes; NULL selects the library's
+ * default wheel (ff_color_wheel_default), which the first such call on a device uploads,
+ * synchronously (make it before any stream capture).  maxflow <= 0 is rejected as the
+ * reference's setMaxFlow does (display.cu:129-137). */
+ff_status ff_flow_to_color(const float* flow, size_t flow_pitch, int height, int width, float maxflow,
+                           const unsigned char* wheel, unsigned char* color, size_t color_pitch, void* stream);
+/* The library's default colour wheel into a host buffer of 256*256*4 bytes (rows of 256 RGBA
+ * texels, row = y, column = x): the Middlebury colour code at texel centres.  It stands in for
+ * the reference's embedded table (src/colorwheel.cpp, getColorWheelRGBA), which is a different
+ * image of the same code; pass that table as `wheel` for the reference's exact colours. */
+ff_status ff_color_wheel_default(unsigned char* rgba);
+
 /* One frame of the differentiable pyramidal filter, and its adjoint, as single calls that
  * launch every stage kernel (the schedule of PyramidalFlowFilter::compute on float input,
  * src/gpu/flowfilter.cu:685-716: pyramid, top level, then delta levels L-2 .. 0).  State per

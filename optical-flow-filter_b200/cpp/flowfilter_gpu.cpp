@@ -10,6 +10,8 @@
 #include <string>
 
 #include "ffb200.h"
+#include "flowfilter/colorwheel.h"
+#include "flowfilter/gpu/display.h"
 #include "flowfilter/gpu/flowfilter.h"
 #include "flowfilter/gpu/image.h"
 #include "flowfilter/gpu/imagemodel.h"
@@ -25,6 +27,24 @@ static_assert(offsetof(flowfilter::image_t, itemSize) == offsetof(ff_image, item
 static_assert(offsetof(flowfilter::image_t, data) == offsetof(ff_image, data), "image_t.data");
 
 namespace flowfilter {
+
+// the library's colour wheel, filled when the library loads
+unsigned char COLOR_WHEEL_D[COLOR_WHEEL_HEIGHT * COLOR_WHEEL_WIDTH * COLOR_WHEEL_DEPTH];
+namespace {
+const bool wheel_filled = ff_color_wheel_default(COLOR_WHEEL_D) == FF_OK;
+}  // namespace
+
+image_t getColorWheelRGBA() {
+    image_t img;
+    img.height = COLOR_WHEEL_HEIGHT;
+    img.width = COLOR_WHEEL_WIDTH;
+    img.depth = COLOR_WHEEL_DEPTH;
+    img.itemSize = 1;
+    img.pitch = (std::size_t)COLOR_WHEEL_WIDTH * COLOR_WHEEL_DEPTH;
+    img.data = wheel_filled ? COLOR_WHEEL_D : nullptr;
+    return img;
+}
+
 namespace gpu {
 
 namespace {
@@ -183,6 +203,65 @@ void ImageModel::compute() {
 
 GPUImage ImageModel::getImageConstant() { return constant_; }
 GPUImage ImageModel::getImageGradient() { return gradient_; }
+
+// ------------------------------------------------------------------ FlowToColor
+FlowToColor::FlowToColor() = default;
+
+FlowToColor::FlowToColor(GPUImage inputFlow, const float maxflow) {
+    setInputFlow(inputFlow);
+    setMaxFlow(maxflow);
+    configure();
+}
+
+FlowToColor::~FlowToColor() = default;
+
+void FlowToColor::configure() {
+    if (!inputFlowSet_) throw std::logic_error("FlowToColor::configure(): input flow not set");
+    colorFlow_ = GPUImage(inputFlow_.height(), inputFlow_.width(), 4, sizeof(unsigned char));
+    configured_ = true;
+}
+
+void FlowToColor::compute() {
+    if (!configured_) throw std::logic_error("FlowToColor::compute(): Stage not configured");
+    startTiming();
+    check(ff_flow_to_color((const float*)inputFlow_.data(), inputFlow_.pitch(), inputFlow_.height(),
+                           inputFlow_.width(), maxflow_, (const unsigned char*)wheel_.data(),
+                           (unsigned char*)colorFlow_.data(), colorFlow_.pitch(), stream_),
+          "FlowToColor::compute");
+    stopTiming();
+}
+
+void FlowToColor::downloadColorFlow(flowfilter::image_t& colorFlow) { colorFlow_.download(colorFlow); }
+
+void FlowToColor::setInputFlow(GPUImage inputFlow) {
+    if (inputFlow.depth() != 2 || inputFlow.itemSize() != sizeof(float))
+        throw std::invalid_argument("FlowToColor::setInputFlow(): input flow should have depth 2 of float");
+    inputFlow_ = inputFlow;
+    inputFlowSet_ = true;
+}
+
+GPUImage FlowToColor::getColorFlow() { return colorFlow_; }
+
+float FlowToColor::getMaxFlow() const { return maxflow_; }
+
+void FlowToColor::setMaxFlow(const float maxflow) {
+    if (!(maxflow > 0.0f))
+        throw std::invalid_argument("FlowToColor::setMaxFlow(): maxflow should be greater than 0.0: " +
+                                    std::to_string(maxflow));
+    maxflow_ = maxflow;
+}
+
+void FlowToColor::setColorWheel(flowfilter::image_t& wheel) {
+    if (wheel.height != COLOR_WHEEL_HEIGHT || wheel.width != COLOR_WHEEL_WIDTH || wheel.depth != COLOR_WHEEL_DEPTH ||
+        wheel.itemSize != 1)
+        throw std::invalid_argument("FlowToColor::setColorWheel(): the wheel should be 256x256 RGBA uint8");
+    // a dense device copy (ff_flow_to_color reads the wheel as 256 rows of 1 KB)
+    GPUImage w(COLOR_WHEEL_HEIGHT, COLOR_WHEEL_WIDTH, COLOR_WHEEL_DEPTH, 1);
+    if ((std::size_t)w.pitch() != (std::size_t)COLOR_WHEEL_WIDTH * COLOR_WHEEL_DEPTH)
+        throw std::runtime_error("FlowToColor::setColorWheel(): unexpected device row pitch");
+    w.upload(wheel);
+    wheel_ = w;
+}
 
 // ------------------------------------------------------------------ FilterHandle
 FilterHandle::~FilterHandle() { reset(nullptr); }

@@ -3,10 +3,12 @@
 Python face of libffb200.so (include/ffb200.h).  ``FlowFilter``,
 ``PyramidalFlowFilter`` and ``DeltaFlowFilter`` mirror the reference's classes;
 ``BatchFlowFilter`` advances many independent streams together; the
-``stages`` module exposes the individual stages on CUDA tensors.
+``stages`` module exposes the individual stages on CUDA tensors; ``FlowToColor`` colour-
+encodes a flow field.
 """
 
 from ._lib import FFError, FFIndexError, FFLogicError, FFValueError, lib  # noqa: F401
+from .display import FlowToColor, color_wheel  # noqa: F401
 from .filters import BatchFlowFilter, DeltaFlowFilter, FlowFilter, PyramidalFlowFilter, device_view  # noqa: F401
 
 __all__ = [
@@ -14,6 +16,8 @@ __all__ = [
     "PyramidalFlowFilter",
     "DeltaFlowFilter",
     "BatchFlowFilter",
+    "FlowToColor",
+    "color_wheel",
     "FFError",
     "FFValueError",
     "FFIndexError",

@@ -149,6 +149,8 @@ SIGNATURES = {
     "ff_diff_delta_update_bwd": (_st, [_i, _i, _i, _i, _i, _i] + [_vp] * 6 + [ctypes.c_double] + [_vp] * 9),
     "ff_diff_smooth": (_st, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "ff_diff_smooth_bwd": (_st, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ff_flow_to_color": (_st, [_vp, ctypes.c_size_t, _i, _i, ctypes.c_float, _vp, _vp, ctypes.c_size_t, _vp]),
+    "ff_color_wheel_default": (_st, [_vp]),
     "ff_diff_frame_tape_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_scratch_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_forward": (_st, [_i, _vp, _i] + [_vp] * 8),

@@ -2,10 +2,11 @@
 
 Two steps:
 
-  python oracle/make_reference_fixtures.py run  --out DIR   (on a machine with a GPU)
+  python oracle/make_reference_fixtures.py run  --out DIR [--only PART ...]   (with a GPU)
       builds nothing; needs oracle/_ref/ref_driver (``make -C oracle ref``).  Writes the
-      stage inputs, runs the reference driver on them and on the parity sequences,
-      and leaves raw outputs in DIR.
+      stage inputs, runs the reference driver on them, on the parity sequences and on the
+      colour-lookup probes, and leaves raw outputs in DIR.  PART: stages, norm, upmap,
+      cases, wheelidx (default: all).
 
   python oracle/make_reference_fixtures.py pack --raw DIR
       packs DIR into the small committed fixtures under tests/golden/.
@@ -30,6 +31,9 @@ ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "optical-flow-filter_b200"))
 
 from flowfilter_b200 import synthetic  # noqa: E402
+
+sys.path.insert(0, ROOT)
+from oracle import display_oracle  # noqa: E402
 
 DRIVER = os.path.join(HERE, "_ref", "ref_driver")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
@@ -57,6 +61,9 @@ CASES = {
                            kw=dict(height=64, width=96, sigma=1.0, seed=13, n_bumps=3,
                                    bump_sigma=20.0, amp=2.0, sensor_noise=2.0)),
 }
+
+# colour-lookup probes: (maxflow, seed) per case
+WHEEL_CASES = [(1.0, 31), (4.0, 32), (0.3, 33), (7.5, 34)]
 
 FULL_LIMIT = 64 * 128  # dumps up to this many pixels are stored whole
 
@@ -86,17 +93,28 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def run(out: str) -> None:
+def run(out: str, only=None) -> None:
+    parts = set(only or ["stages", "norm", "upmap", "cases", "wheelidx"])
     os.makedirs(out, exist_ok=True)
-    sin = os.path.join(out, "stage_in")
-    sout = os.path.join(out, "stage_out")
-    os.makedirs(sin, exist_ok=True)
-    os.makedirs(sout, exist_ok=True)
-    for k, v in stage_inputs().items():
-        np.save(os.path.join(sin, k + ".npy"), v)
-    subprocess.run([DRIVER, "stages", sin, sout], check=True)
-    subprocess.run([DRIVER, "norm", os.path.join(out, "norm.npy")], check=True)
-    subprocess.run([DRIVER, "upmap", os.path.join(out, "upmap.txt"), "4200"], check=True)
+    if "stages" in parts:
+        sin = os.path.join(out, "stage_in")
+        sout = os.path.join(out, "stage_out")
+        os.makedirs(sin, exist_ok=True)
+        os.makedirs(sout, exist_ok=True)
+        for k, v in stage_inputs().items():
+            np.save(os.path.join(sin, k + ".npy"), v)
+        subprocess.run([DRIVER, "stages", sin, sout], check=True)
+    if "norm" in parts:
+        subprocess.run([DRIVER, "norm", os.path.join(out, "norm.npy")], check=True)
+    if "upmap" in parts:
+        subprocess.run([DRIVER, "upmap", os.path.join(out, "upmap.txt"), "4200"], check=True)
+    if "wheelidx" in parts:
+        for k, (m, seed) in enumerate(WHEEL_CASES):
+            fpath = os.path.join(out, f"wheel_flows_{k}.npy")
+            np.save(fpath, display_oracle.probe_flows(m, seed))
+            subprocess.run([DRIVER, "wheelidx", fpath, repr(m), os.path.join(out, f"wheel_idx_{k}.npy")], check=True)
+    if "cases" not in parts:
+        return
     tmp = os.environ.get("TMPDIR", "/tmp")
     for name, case in CASES.items():
         frames = case_frames(case)
@@ -145,13 +163,26 @@ def pack(raw: str) -> None:
     os.makedirs(GOLDEN, exist_ok=True)
     # stage goldens: inputs are regenerated from the seed, outputs stored whole
     sout = os.path.join(raw, "stage_out")
-    outs = {f[:-4]: np.load(os.path.join(sout, f)) for f in sorted(os.listdir(sout)) if f.endswith(".npy")}
-    ins = stage_inputs()
-    np.savez_compressed(os.path.join(GOLDEN, "ref_stages.npz"),
-                        inputs_sha256=np.frombuffer(json.dumps({k: sha(v) for k, v in ins.items()}).encode(), np.uint8),
-                        **outs)
-    np.save(os.path.join(GOLDEN, "ref_norm_u8.npy"), np.load(os.path.join(raw, "norm.npy")))
-    np.save(os.path.join(GOLDEN, "ref_upmap_detail.npy"), np.load(os.path.join(raw, "upmap.txt.detail.npy")))
+    if os.path.isdir(sout):
+        outs = {f[:-4]: np.load(os.path.join(sout, f)) for f in sorted(os.listdir(sout)) if f.endswith(".npy")}
+        ins = stage_inputs()
+        np.savez_compressed(os.path.join(GOLDEN, "ref_stages.npz"),
+                            inputs_sha256=np.frombuffer(json.dumps({k: sha(v) for k, v in ins.items()}).encode(),
+                                                        np.uint8),
+                            **outs)
+    if os.path.exists(os.path.join(raw, "norm.npy")):
+        np.save(os.path.join(GOLDEN, "ref_norm_u8.npy"), np.load(os.path.join(raw, "norm.npy")))
+    if os.path.exists(os.path.join(raw, "upmap.txt.detail.npy")):
+        np.save(os.path.join(GOLDEN, "ref_upmap_detail.npy"), np.load(os.path.join(raw, "upmap.txt.detail.npy")))
+    if os.path.exists(os.path.join(raw, "wheel_idx_0.npy")):
+        # texel picked per pixel by the reference lookup: column (R), row (G)
+        idx = np.stack([np.load(os.path.join(raw, f"wheel_idx_{k}.npy")) for k in range(len(WHEEL_CASES))])
+        assert (idx[..., 2] == 0).all() and (idx[..., 3] == 255).all()
+        flows_sha = [sha(display_oracle.probe_flows(m, seed)) for m, seed in WHEEL_CASES]
+        np.savez_compressed(os.path.join(GOLDEN, "ref_flow_to_color.npz"), col=idx[..., 0], row=idx[..., 1],
+                            maxflow=np.array([m for m, _ in WHEEL_CASES], np.float32),
+                            seed=np.array([s for _, s in WHEEL_CASES], np.int64),
+                            flows_sha256=np.frombuffer(json.dumps(flows_sha).encode(), np.uint8))
     for name in CASES:
         src = os.path.join(raw, f"case_{name}.npz")
         if os.path.exists(src):
@@ -164,11 +195,12 @@ def main() -> None:
     sub = ap.add_subparsers(dest="cmd", required=True)
     r = sub.add_parser("run")
     r.add_argument("--out", required=True)
+    r.add_argument("--only", nargs="*", default=None)
     p = sub.add_parser("pack")
     p.add_argument("--raw", required=True)
     a = ap.parse_args()
     if a.cmd == "run":
-        run(a.out)
+        run(a.out, a.only)
     else:
         pack(a.raw)
 

@@ -12,6 +12,12 @@
 //                                      src/gpu/device/update_k.cu:151-155), listed
 //                                      where it differs from floor(u*Wc)
 //   stages IN_DIR OUT_DIR              every hot-path stage on the given inputs
+//   wheelidx FLOWS.npy MAXFLOW OUT.npy  the reference's flowToColor_k (display_k.cu, compiled
+//                                      into this driver from the reference sources) on the
+//                                      given (H, W, 2) flows with an index-encoding wheel
+//                                      (texel (i, j) = (j, i, 0, 255)) behind the texture
+//                                      FlowToColor::configure sets up: OUT names the texel
+//                                      each pixel read
 //   filter FRAMES.npy OUT.npy LEVELS MAXFLOW GAMMAS SMOOTHS DUMP [TIMING_CSV]
 //                                      LEVELS=0: FlowFilter(h, w, S, maxflow, gamma)
 //                                      LEVELS>=1: PyramidalFlowFilter(h, w, LEVELS)
@@ -39,6 +45,10 @@
 #include "flowfilter/gpu/update.h"
 #include "flowfilter/gpu/flowsmoothing.h"
 #include "flowfilter/gpu/flowfilter.h"
+
+// the reference's colour-lookup kernel, from its source tree (oracle/Makefile adds the
+// reference's src/ directory to the include path)
+#include "gpu/device/display_k.cu"
 
 using namespace flowfilter;
 using namespace flowfilter::gpu;
@@ -404,6 +414,35 @@ static int mode_filter(int argc, char** argv) {
     return e == cudaSuccess ? 0 : 1;
 }
 
+static int mode_wheelidx(const std::string& flows, float maxflow, const std::string& out) {
+    Npy a = npy_read(flows);
+    if (a.descr != "<f4" || a.shape.size() != 3 || a.shape[2] != 2)
+        throw std::runtime_error("wheelidx: flows should be (H, W, 2) float32");
+    const int h = (int)a.shape[0], w = (int)a.shape[1];
+    GPUImage flow = upload_npy(a, 2);
+    std::vector<unsigned char> wheel(256 * 256 * 4);
+    for (int i = 0; i < 256; ++i)
+        for (int j = 0; j < 256; ++j) {
+            unsigned char* px = &wheel[4 * (i * 256 + j)];
+            px[0] = (unsigned char)j;
+            px[1] = (unsigned char)i;
+            px[2] = 0;
+            px[3] = 255;
+        }
+    GPUImage wimg(256, 256, 4, 1);
+    image_t wi = wrap_host(wheel.data(), 256, 256, 4, 1);
+    wimg.upload(wi);
+    // the texture of FlowToColor::configure (display.cu:73-74)
+    GPUTexture tex(wimg, cudaChannelFormatKindUnsigned, cudaReadModeElementType, true);
+    GPUImage color(h, w, 4, 1);
+    dim3 block(32, 32, 1), grid((w + 31) / 32, (h + 31) / 32, 1);
+    flowToColor_k<<<grid, block>>>(flow.wrap<float2>(), tex.getTextureObject(), maxflow, color.wrap<uchar4>());
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) throw std::runtime_error(std::string("wheelidx: ") + cudaGetErrorString(e));
+    save_gpu(out, color);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) { fprintf(stderr, "usage: ref_driver MODE ...\n"); return 2; }
     std::string mode = argv[1];
@@ -412,6 +451,7 @@ int main(int argc, char** argv) {
         if (mode == "upmap" && argc >= 4) return mode_upmap(argv[2], atoi(argv[3]));
         if (mode == "stages" && argc >= 4) return mode_stages(argv[2], argv[3]);
         if (mode == "filter" && argc >= 9) return mode_filter(argc, argv);
+        if (mode == "wheelidx" && argc >= 5) return mode_wheelidx(argv[2], (float)atof(argv[3]), argv[4]);
     } catch (const std::exception& e) {
         fprintf(stderr, "ref_driver: %s\n", e.what());
         return 3;

@@ -1,19 +1,23 @@
 // Drives the C++ drop-in API (include/flowfilter/gpu/*.h) the way the reference's demos
 // do, for tests/test_gpu_cpp_dropin.py.
 //
-//   dropin_sequence <frames.u8> <H> <W> <T> <levels> <out.f32>
+//   dropin_sequence <frames.u8> <H> <W> <T> <levels> <out.f32> [<colour.u8>]
 //
 // levels 0: FlowFilter(H, W, 2, 4.0, 10.0); otherwise PyramidalFlowFilter(H, W, levels)
 // with gamma[l] = 5 * 2^l, smoothIterations[l] = 1 + l % 3, maxflow 4.  Per frame the
 // output holds downloadFlow (H*W*2), the getFlow() GPUImage taken once before the loop and
 // downloaded after every compute (H*W*2), and downloadImage (H*W); after the last frame,
-// an ImageModel of the last frame: constant (H*W) and gradient (H*W*2).
+// an ImageModel of the last frame: constant (H*W) and gradient (H*W*2).  With a colour path,
+// FlowToColor(filter.getFlow(), 4) after the last frame writes its RGBA image (H*W*4 bytes)
+// there, as the reference's webcam demo builds it (demos/flowWebCam/src/flowWebCam.cpp:100).
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
 #include <type_traits>
 #include <vector>
 
+#include "flowfilter/colorwheel.h"
+#include "flowfilter/gpu/display.h"
 #include "flowfilter/gpu/flowfilter.h"
 #include "flowfilter/gpu/imagemodel.h"
 
@@ -41,8 +45,8 @@ static bool throws(F&& f) {
 }
 
 int main(int argc, char** argv) {
-    if (argc != 7) {
-        std::fprintf(stderr, "usage: %s frames H W T levels out\n", argv[0]);
+    if (argc != 7 && argc != 8) {
+        std::fprintf(stderr, "usage: %s frames H W T levels out [colour]\n", argv[0]);
         return 2;
     }
     const int H = std::atoi(argv[2]), W = std::atoi(argv[3]), T = std::atoi(argv[4]), L = std::atoi(argv[5]);
@@ -56,6 +60,27 @@ int main(int argc, char** argv) {
     std::vector<float> flow((size_t)H * W * 2), alias((size_t)H * W * 2), img((size_t)H * W);
     image_t flow_t = host(flow.data(), H, W, 2, 4), alias_t = host(alias.data(), H, W, 2, 4),
             img_t = host(img.data(), H, W, 1, 4);
+    // FlowToColor of a filter's flow, and its error conventions
+    auto colour = [&](gpu::GPUImage flowImg) -> int {
+        if (argc != 8) return 0;
+        gpu::FlowToColor c(flowImg, 4.0f);
+        c.compute();
+        std::vector<unsigned char> rgba((size_t)H * W * 4);
+        image_t rgba_t = host(rgba.data(), H, W, 4, 1);
+        c.downloadColorFlow(rgba_t);
+        FILE* fc = std::fopen(argv[7], "wb");
+        if (!fc || std::fwrite(rgba.data(), 1, rgba.size(), fc) != rgba.size()) return 11;
+        std::fclose(fc);
+        if (c.getMaxFlow() != 4.0f || !(c.elapsedTime() > 0.0f)) return 12;
+        if (!throws([&] { c.setMaxFlow(0.0f); })) return 13;
+        gpu::FlowToColor unset;
+        if (!throws([&] { unset.compute(); }) || !throws([&] { unset.configure(); })) return 14;
+        gpu::GPUImage one(H, W, 1, 4);
+        if (!throws([&] { unset.setInputFlow(one); })) return 15;
+        image_t wheel = getColorWheelRGBA();
+        if (wheel.height != COLOR_WHEEL_HEIGHT || wheel.depth != 4 || wheel.data == nullptr) return 16;
+        return 0;
+    };
     auto dump = [&](gpu::GPUImage& a) {
         a.download(alias_t);
         std::fwrite(flow.data(), 4, flow.size(), fo);
@@ -75,6 +100,7 @@ int main(int argc, char** argv) {
                 dump(a);
             }
             if (f.getPropagationIterations() != 4 || f.getSmoothIterations() != 2 || f.height() != H) return 5;
+            if (int rc = colour(f.getFlow())) return rc;
             if (!(f.elapsedTime() > 0.0f)) return 6;
         } else {
             gpu::PyramidalFlowFilter f(H, W, L);
@@ -97,6 +123,7 @@ int main(int argc, char** argv) {
                 dump(a);
             }
             if (f.levels() != L || f.getSmoothIterations(L - 1) != s[L - 1]) return 5;
+            if (int rc = colour(f.getFlow())) return rc;
             if (!(f.elapsedTime() > 0.0f)) return 6;
             // reference error conventions: bad level index, wrong vector size
             if (!throws([&] { f.setGamma(L, 1.0f); })) return 7;

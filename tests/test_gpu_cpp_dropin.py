@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from oracle import display_oracle as D
 from conftest import ROOT
 from make_reference_fixtures import case_frames
 
@@ -33,10 +34,10 @@ def test_cpp_dropin_sequence_matches_oracle(program, tmp_path, h, w, levels):
     t = 6
     frames = case_frames(dict(seq="bumps", frames=t, kw=dict(height=h, width=w, sigma=1.0, seed=h + w, n_bumps=2,
                                                               bump_sigma=max(h, w) / 3, amp=2.0)))
-    fin, fout = tmp_path / "frames.u8", tmp_path / "out.f32"
+    fin, fout, fcol = tmp_path / "frames.u8", tmp_path / "out.f32", tmp_path / "colour.u8"
     frames.tofile(fin)
-    r = subprocess.run([program, str(fin), str(h), str(w), str(t), str(levels), str(fout)], capture_output=True,
-                       text=True)
+    r = subprocess.run([program, str(fin), str(h), str(w), str(t), str(levels), str(fout), str(fcol)],
+                       capture_output=True, text=True)
     assert r.returncode == 0, (r.returncode, r.stderr)
     got = np.fromfile(fout, np.float32)
     if levels == 0:
@@ -58,3 +59,6 @@ def test_cpp_dropin_sequence_matches_oracle(program, tmp_path, h, w, levels):
     np.testing.assert_array_equal(got[off:off + n1].reshape(h, w), a0); off += n1
     np.testing.assert_array_equal(got[off:off + n2].reshape(h, w, 2), grad); off += n2
     assert off == got.size
+    # FlowToColor(filter.getFlow(), 4) with the library's wheel
+    colour = np.fromfile(fcol, np.uint8).reshape(h, w, 4)
+    np.testing.assert_array_equal(colour, D.flow_to_color(of.get_flow(), 4.0, D.middlebury_wheel()))
