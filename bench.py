@@ -450,31 +450,24 @@ def bench_batched(steps, warmup):
     }
 
 
-def bench_flow_to_color(filt, n):
-    """Mean device microseconds of ff_flow_to_color per launch on the filter's current
-    level-0 flow (a pitched device view): 20 launches captured in a CUDA graph, replayed
-    so that host launch overhead is not timed."""
+def graph_us(launch, n, per_graph=20):
+    """Mean device microseconds of launch(stream) over replays of a CUDA graph holding
+    per_graph back-to-back launches (host launch overhead not timed)."""
     import ctypes
 
     import torch
-    from flowfilter_b200 import lib
 
-    flow = filt.getFlowDevice()
-    h, w = flow.shape[:2]
-    out = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda")
     side = torch.cuda.Stream()
-    args = lambda st: (ctypes.c_void_p(flow.data_ptr()), flow.stride(0) * 4, h, w, 4.0, None,  # noqa: E731
-                       ctypes.c_void_p(out.data_ptr()), out.stride(0), ctypes.c_void_p(st.cuda_stream))
     side.wait_stream(torch.cuda.current_stream())
+    st = ctypes.c_void_p(side.cuda_stream)
     with torch.cuda.stream(side):
         for _ in range(3):
-            assert lib().ff_flow_to_color(*args(side)) == 0  # the first call uploads the default wheel
+            launch(st)  # first calls do any one-time set-up outside the capture
     torch.cuda.synchronize()
-    per_graph = 20
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=side):
         for _ in range(per_graph):
-            lib().ff_flow_to_color(*args(side))
+            launch(st)
     for _ in range(3):
         g.replay()
     reps = max(1, n // per_graph)
@@ -486,6 +479,42 @@ def bench_flow_to_color(filt, n):
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) * 1e3 / (reps * per_graph)
+
+
+def bench_flow_to_color(filt, n):
+    """Mean device microseconds of ff_flow_to_color per launch on the filter's current
+    level-0 flow (a pitched device view), default wheel."""
+    import ctypes
+
+    import torch
+    from flowfilter_b200 import lib
+
+    flow = filt.getFlowDevice()
+    h, w = flow.shape[:2]
+    out = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda")
+    return graph_us(lambda st: lib().ff_flow_to_color(ctypes.c_void_p(flow.data_ptr()), flow.stride(0) * 4, h, w, 4.0,
+                                                      None, ctypes.c_void_p(out.data_ptr()), out.stride(0), st), n)
+
+
+def bench_rotational_predictor(n):
+    """RotationalFlowImagePredictor on a 640x480 float image, 4 iterations: device
+    microseconds per compute (one fused launch) and the bytes it must move."""
+    import ctypes
+
+    import torch
+    from flowfilter_b200 import createPerspectiveCamera, lib
+
+    h, w, it = 480, 640, 4
+    img = torch.rand((h, w), dtype=torch.float32, device="cuda")
+    flow = torch.empty((h, w, 2), dtype=torch.float32, device="cuda")
+    out = torch.empty_like(img)
+    cam = createPerspectiveCamera(0.004, h, w, 0.0036, 0.0048)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    us = graph_us(lambda st: lib().ff_rotational_predict(ctypes.byref(cam.cam), 0.01, -0.02, 0.03, vp(img), w * 4, 1,
+                                                         h, w, it, vp(flow), w * 8, vp(out), w * 4, None, 0, st), n)
+    return {"workload": f"{w}x{h} float32 image, {it} iterations, rotational flow written", "launch_us": us,
+            "launches": 1, "reference_launches": 1 + 2 * it,
+            "bytes": h * w * 16, "achieved_GBps": h * w * 16 / (us * 1e-6) / 1e9}
 
 
 def bench_differentiable(steps):
@@ -579,6 +608,7 @@ def bench_b200(args):
     # ---- FlowToColor of the level-0 flow (the step after the filter in the reference's
     # demos): device time per launch, back to back, the flow L2-resident as after a frame
     ftc_us = bench_flow_to_color(filt, min(args.steps, 1000))
+    rot = bench_rotational_predictor(min(args.steps, 1000))
     l0_bytes = level0_kernel_bytes(w)
     achieved = l0_bytes / (l0_ms / 1000.0) / 1e9
     traffic = ncu_traffic(PRIMARY)
@@ -650,6 +680,7 @@ def bench_b200(args):
                               "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
                               "note": "ff_flow_to_color on the 640x480 level-0 flow, default wheel; "
                                       "12 B/px (float2 in, RGBA out)"},
+            "rotational_predictor": rot,
             "elapsed_time_ms": {"value": elapsed_ms, "frames": len(et),
                                 "path": "PyramidalFlowFilter.loadImage(host numpy) + compute(); mean elapsedTime(), "
                                         "as the reference notebook measures"},

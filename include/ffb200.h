@@ -297,6 +297,36 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
 ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
                              const void* gout, void* gin, void* gw5, void* stream);
 
+/* Camera model and rotational image prediction (no scalar kernels of the filter use them).
+ * ff_camera is the reference's perspectiveCamera (include/flowfilter/gpu/camera.h:18-23);
+ * ff_camera_perspective is createPerspectiveCamera (src/gpu/camera.cu:15-31). */
+typedef struct ff_camera {
+    float alphaX, alphaY, centerX, centerY;
+} ff_camera;
+ff_status ff_camera_perspective(float focal, int height, int width, float sensor_height, float sensor_width,
+                                ff_camera* cam);
+/* rotationalOpticalFlow_k (src/gpu/device/rotation_k.cu:17-43): the image flow of a camera
+ * rotating at (wx, wy, wz) rad/frame, into [height][width] float2 (device, flow_pitch). */
+ff_status ff_rotational_flow(const ff_camera* cam, float wx, float wy, float wz, float* flow, size_t flow_pitch,
+                             int height, int width, void* stream);
+/* LaxWendroffPropagator::compute (src/gpu/propagation.cu:572-645): `iterations` times a Y
+ * then an X Lax-Wendroff pass of an image [height][width][depth] float (depth 1 or 4) by the
+ * flow [height][width] float2, dt = 1/iterations; iterations 0 (never set) runs one pass pair
+ * with dt = 0, as the reference does.  All device buffers; rows 4-byte (depth 1) or 16-byte
+ * (depth 4) aligned; `out` must not be `image`.  One launch covers up to
+ * ff_lax_wendroff_max_fused() iterations; more need `workspace` (an image like `out`). */
+int ff_lax_wendroff_max_fused(void);
+ff_status ff_lax_wendroff(const float* flow, size_t flow_pitch, const float* image, size_t image_pitch, int depth,
+                          int height, int width, int iterations, float* out, size_t out_pitch, float* workspace,
+                          size_t workspace_pitch, void* stream);
+/* RotationalFlowImagePredictor::compute (src/gpu/rotation.cu:72-88): the rotational flow
+ * (written to `flow`) and the image propagated by it (`out`), in one launch up to
+ * ff_lax_wendroff_max_fused() iterations.  Buffers as for ff_lax_wendroff. */
+ff_status ff_rotational_predict(const ff_camera* cam, float wx, float wy, float wz, const float* image,
+                                size_t image_pitch, int depth, int height, int width, int iterations, float* flow,
+                                size_t flow_pitch, float* out, size_t out_pitch, float* workspace,
+                                size_t workspace_pitch, void* stream);
+
 /* FlowToColor::compute (src/gpu/display.cu:95-110, kernel src/gpu/device/display_k.cu:14-43):
  * colour-encodes a flow field [height][width] float2 (device, rows flow_pitch bytes apart,
  * 8-byte aligned) into RGBA [height][width] uchar4 (device, color_pitch).  Each component is

@@ -11,11 +11,16 @@
 
 #include "ffb200.h"
 #include "flowfilter/colorwheel.h"
+#include "flowfilter/gpu/camera.h"
 #include "flowfilter/gpu/display.h"
 #include "flowfilter/gpu/flowfilter.h"
 #include "flowfilter/gpu/image.h"
 #include "flowfilter/gpu/imagemodel.h"
 #include "flowfilter/gpu/pipeline.h"
+#include "flowfilter/gpu/propagation.h"
+#include "flowfilter/gpu/rotation.h"
+
+static_assert(sizeof(flowfilter::gpu::perspectiveCamera) == sizeof(ff_camera), "perspectiveCamera / ff_camera");
 
 // flowfilter::image_t is passed to the C ABI as an ff_image: same fields, same layout
 static_assert(sizeof(flowfilter::image_t) == sizeof(ff_image), "image_t / ff_image size");
@@ -262,6 +267,148 @@ void FlowToColor::setColorWheel(flowfilter::image_t& wheel) {
     w.upload(wheel);
     wheel_ = w;
 }
+
+// ------------------------------------------------------------------ camera
+perspectiveCamera createPerspectiveCamera(const float focalLength, const int height, const int width,
+                                          const float sensorHeight, const float sensorWidth) {
+    perspectiveCamera cam;
+    check(ff_camera_perspective(focalLength, height, width, sensorHeight, sensorWidth,
+                                reinterpret_cast<ff_camera*>(&cam)),
+          "createPerspectiveCamera");
+    return cam;
+}
+
+namespace {
+// a second image like `like` when the run needs more than one launch, else an empty one
+GPUImage lw_workspace(GPUImage& ws, GPUImage& like, int iterations) {
+    if ((iterations > 0 ? iterations : 1) <= ff_lax_wendroff_max_fused()) return GPUImage();
+    if (!ws.data() || !ws.compareShapeGPU(like)) ws = GPUImage(like.height(), like.width(), like.depth(), 4);
+    return ws;
+}
+}  // namespace
+
+// ------------------------------------------------------------------ LaxWendroffPropagator
+LaxWendroffPropagator::LaxWendroffPropagator() = default;
+
+LaxWendroffPropagator::LaxWendroffPropagator(GPUImage inputFlow, GPUImage inputImage) {
+    setInputFlow(inputFlow);
+    setInputImage(inputImage);
+    configure();
+}
+
+LaxWendroffPropagator::~LaxWendroffPropagator() = default;
+
+void LaxWendroffPropagator::configure() {
+    if (!inputFlowSet_) throw std::logic_error("LaxWendroffPropagator::configure(): input flow has not been set");
+    if (!inputImageSet_) throw std::logic_error("LaxWendroffPropagator::configure(): input image has not been set");
+    propagated_ = GPUImage(inputFlow_.height(), inputFlow_.width(), inputImage_.depth(), sizeof(float));
+    configured_ = true;
+}
+
+void LaxWendroffPropagator::compute() {
+    if (!configured_) throw std::logic_error("LaxWendroffPropagator::compute(): stage not configured");
+    GPUImage ws = lw_workspace(workspace_, propagated_, iterations_);
+    startTiming();
+    check(ff_lax_wendroff((const float*)inputFlow_.data(), inputFlow_.pitch(), (const float*)inputImage_.data(),
+                          inputImage_.pitch(), inputImage_.depth(), inputImage_.height(), inputImage_.width(),
+                          iterations_, (float*)propagated_.data(), propagated_.pitch(), (float*)ws.data(),
+                          ws.data() ? ws.pitch() : 0, stream_),
+          "LaxWendroffPropagator::compute");
+    stopTiming();
+}
+
+void LaxWendroffPropagator::setIterations(const int N) {
+    if (N <= 0)
+        throw std::invalid_argument("LaxWendroffPropagator::setIterations(): iterations less than zero: " +
+                                    std::to_string(N));
+    iterations_ = N;
+    dt_ = 1.0f / float(N);
+}
+
+int LaxWendroffPropagator::getIterations() const { return iterations_; }
+float LaxWendroffPropagator::getDt() const { return dt_; }
+
+void LaxWendroffPropagator::setInputFlow(GPUImage inputFlow) {
+    if (inputFlow.depth() != 2 || inputFlow.itemSize() != 4)
+        throw std::invalid_argument("LaxWendroffPropagator::setInputFlow(): input flow should have depth 2 of float");
+    inputFlow_ = inputFlow;
+    inputFlowSet_ = true;
+}
+
+void LaxWendroffPropagator::setInputImage(GPUImage img) {
+    if ((img.depth() != 1 && img.depth() != 4) || img.itemSize() != 4)
+        throw std::invalid_argument("LaxWendroffPropagator::setInputImage(): input image should have depth 1 or 4 "
+                                    "of float");
+    if (img.height() != inputFlow_.height() || img.width() != inputFlow_.width())
+        throw std::invalid_argument("LaxWendroffPropagator::setInputImage(): image shape does not match with input "
+                                    "flow");
+    inputImage_ = img;
+    inputImageSet_ = true;
+}
+
+GPUImage LaxWendroffPropagator::getFlow() { return inputFlow_; }
+GPUImage LaxWendroffPropagator::getPropagatedImage() { return propagated_; }
+
+// ------------------------------------------------------------------ RotationalFlowImagePredictor
+RotationalFlowImagePredictor::RotationalFlowImagePredictor() = default;
+
+RotationalFlowImagePredictor::RotationalFlowImagePredictor(perspectiveCamera cam) { setCamera(cam); }
+
+RotationalFlowImagePredictor::RotationalFlowImagePredictor(perspectiveCamera cam, GPUImage inputImage) {
+    setCamera(cam);
+    setInputImage(inputImage);
+    configure();
+}
+
+RotationalFlowImagePredictor::~RotationalFlowImagePredictor() = default;
+
+void RotationalFlowImagePredictor::configure() {
+    if (!inputImageSet_) throw std::logic_error("RotationalFlowImagePredictor::configure(): input image not set");
+    opticalFlow_ = GPUImage(inputImage_.height(), inputImage_.width(), 2, sizeof(float));
+    predicted_ = GPUImage(inputImage_.height(), inputImage_.width(), inputImage_.depth(), sizeof(float));
+    iterations_ = 0;  // a new propagator, as the reference's configure() makes
+    configured_ = true;
+}
+
+void RotationalFlowImagePredictor::compute() {
+    if (!configured_) throw std::logic_error("RotationalFlowImagePredictor::compute(): stage not configured");
+    GPUImage ws = lw_workspace(workspace_, predicted_, iterations_);
+    startTiming();
+    check(ff_rotational_predict(reinterpret_cast<const ff_camera*>(&camera_), w_[0], w_[1], w_[2],
+                                (const float*)inputImage_.data(), inputImage_.pitch(), inputImage_.depth(),
+                                inputImage_.height(), inputImage_.width(), iterations_, (float*)opticalFlow_.data(),
+                                opticalFlow_.pitch(), (float*)predicted_.data(), predicted_.pitch(), (float*)ws.data(),
+                                ws.data() ? ws.pitch() : 0, stream_),
+          "RotationalFlowImagePredictor::compute");
+    stopTiming();
+}
+
+void RotationalFlowImagePredictor::setInputImage(GPUImage inputImage) {
+    if ((inputImage.depth() != 1 && inputImage.depth() != 4) || inputImage.itemSize() != 4)
+        throw std::invalid_argument("RotationalFlowImagePredictor::setInputImage(): input image should have depth 1 "
+                                    "or 4 of float");
+    inputImage_ = inputImage;
+    inputImageSet_ = true;
+}
+
+GPUImage RotationalFlowImagePredictor::getPredictedImage() { return predicted_; }
+GPUImage RotationalFlowImagePredictor::getOpticalFlow() { return opticalFlow_; }
+void RotationalFlowImagePredictor::setCamera(perspectiveCamera cam) { camera_ = cam; }
+
+void RotationalFlowImagePredictor::setAngularVelocity(const float wx, const float wy, const float wz) {
+    w_[0] = wx;
+    w_[1] = wy;
+    w_[2] = wz;
+}
+
+void RotationalFlowImagePredictor::setIterations(const int iterations) {
+    if (iterations <= 0)
+        throw std::invalid_argument("LaxWendroffPropagator::setIterations(): iterations less than zero: " +
+                                    std::to_string(iterations));
+    iterations_ = iterations;
+}
+
+int RotationalFlowImagePredictor::getIterations() const { return iterations_; }
 
 // ------------------------------------------------------------------ FilterHandle
 FilterHandle::~FilterHandle() { reset(nullptr); }

@@ -4,11 +4,14 @@ Python face of libffb200.so (include/ffb200.h).  ``FlowFilter``,
 ``PyramidalFlowFilter`` and ``DeltaFlowFilter`` mirror the reference's classes;
 ``BatchFlowFilter`` advances many independent streams together; the
 ``stages`` module exposes the individual stages on CUDA tensors; ``FlowToColor`` colour-
-encodes a flow field.
+encodes a flow field; ``RotationalFlowImagePredictor`` and ``LaxWendroffPropagator``
+predict an image under camera rotation.
 """
 
 from ._lib import FFError, FFIndexError, FFLogicError, FFValueError, lib  # noqa: F401
 from .display import FlowToColor, color_wheel  # noqa: F401
+from .rotation import (LaxWendroffPropagator, PerspectiveCamera, RotationalFlowImagePredictor,  # noqa: F401
+                       createPerspectiveCamera)
 from .filters import BatchFlowFilter, DeltaFlowFilter, FlowFilter, PyramidalFlowFilter, device_view  # noqa: F401
 
 __all__ = [
@@ -18,6 +21,10 @@ __all__ = [
     "BatchFlowFilter",
     "FlowToColor",
     "color_wheel",
+    "PerspectiveCamera",
+    "createPerspectiveCamera",
+    "LaxWendroffPropagator",
+    "RotationalFlowImagePredictor",
     "FFError",
     "FFValueError",
     "FFIndexError",

@@ -151,6 +151,14 @@ SIGNATURES = {
     "ff_diff_smooth_bwd": (_st, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ff_flow_to_color": (_st, [_vp, ctypes.c_size_t, _i, _i, ctypes.c_float, _vp, _vp, ctypes.c_size_t, _vp]),
     "ff_color_wheel_default": (_st, [_vp]),
+    "ff_camera_perspective": (_st, [ctypes.c_float, _i, _i, ctypes.c_float, ctypes.c_float, _vp]),
+    "ff_rotational_flow": (_st, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp, ctypes.c_size_t, _i, _i,
+                                 _vp]),
+    "ff_lax_wendroff_max_fused": (_i, []),
+    "ff_lax_wendroff": (_st, [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _i, _i, _i, _i, _vp, ctypes.c_size_t, _vp,
+                              ctypes.c_size_t, _vp]),
+    "ff_rotational_predict": (_st, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp, ctypes.c_size_t, _i, _i,
+                                    _i, _i, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]),
     "ff_diff_frame_tape_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_scratch_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_forward": (_st, [_i, _vp, _i] + [_vp] * 8),

@@ -52,6 +52,9 @@ def lib() -> ctypes.CDLL:
             "or_delta_update": (None, [_f32p, _f32p, _f32p, _f32p, _f32p, i, i, i, i, f, f, _f32p, _f32p, _f32p]),
             "or_smooth": (None, [_f32p, i, i, i, _f32p]),
             "or_upmap_index": (i, [i, i, i]),
+            "or_camera_perspective": (None, [f, i, i, f, f, _f32p]),
+            "or_rotational_flow": (None, [_f32p, f, f, f, i, i, _f32p]),
+            "or_lax_wendroff": (None, [_f32p, _f32p, i, i, i, i, _f32p]),
             "or_flowfilter_create": (vp, [i, i, i, f, f]),
             "or_flowfilter_create_on": (vp, [i, i, i]),
             "or_pyramidal_create": (vp, [i, i, i]),
@@ -177,6 +180,31 @@ def smooth(flow: np.ndarray, s: int) -> np.ndarray:
     flow = np.ascontiguousarray(flow, np.float32)
     out = np.empty_like(flow)
     lib().or_smooth(_p(flow), h, w, s, _p(out))
+    return out
+
+
+def camera_perspective(focal: float, h: int, w: int, sensor_h: float, sensor_w: float) -> np.ndarray:
+    """[alphaX, alphaY, centerX, centerY] (createPerspectiveCamera, camera.cu:15-31)."""
+    cam = np.zeros(4, np.float32)
+    lib().or_camera_perspective(focal, h, w, sensor_h, sensor_w, _p(cam))
+    return cam
+
+
+def rotational_flow(cam: np.ndarray, wx: float, wy: float, wz: float, h: int, w: int) -> np.ndarray:
+    cam = np.ascontiguousarray(cam, np.float32)
+    out = np.zeros((h, w, 2), np.float32)
+    lib().or_rotational_flow(_p(cam), wx, wy, wz, h, w, _p(out))
+    return out
+
+
+def lax_wendroff(flow: np.ndarray, image: np.ndarray, iterations: int) -> np.ndarray:
+    """image (H, W) or (H, W, 4) float32 propagated by flow (H, W, 2)."""
+    flow = np.ascontiguousarray(flow, np.float32)
+    image = np.ascontiguousarray(image, np.float32)
+    h, w = image.shape[:2]
+    d = 1 if image.ndim == 2 else image.shape[2]
+    out = np.zeros_like(image)
+    lib().or_lax_wendroff(_p(flow), _p(image), d, h, w, iterations, _p(out))
     return out
 
 

@@ -5,8 +5,8 @@ Two steps:
   python oracle/make_reference_fixtures.py run  --out DIR [--only PART ...]   (with a GPU)
       builds nothing; needs oracle/_ref/ref_driver (``make -C oracle ref``).  Writes the
       stage inputs, runs the reference driver on them, on the parity sequences and on the
-      colour-lookup probes, and leaves raw outputs in DIR.  PART: stages, norm, upmap,
-      cases, wheelidx (default: all).
+      colour-lookup probes and the rotational predictor / Lax-Wendroff cases, and leaves raw
+      outputs in DIR.  PART: stages, norm, upmap, cases, wheelidx, rotation (default: all).
 
   python oracle/make_reference_fixtures.py pack --raw DIR
       packs DIR into the small committed fixtures under tests/golden/.
@@ -65,6 +65,15 @@ CASES = {
 # colour-lookup probes: (maxflow, seed) per case
 WHEEL_CASES = [(1.0, 31), (4.0, 32), (0.3, 33), (7.5, 34)]
 
+# Lax-Wendroff propagation cases: (H, W, depth, iterations, seed); iterations 0 = never set
+LW_CASES = [(37, 53, 1, 1, 41), (37, 53, 1, 4, 42), (37, 53, 4, 3, 43), (64, 80, 1, 0, 44), (64, 80, 4, 1, 45),
+            (20, 33, 4, 8, 46), (96, 128, 1, 2, 47)]
+# rotational predictor cases: (H, W, depth, focal, sensorH, sensorW, wx, wy, wz, iterations, seed)
+ROT_CASES = [(48, 64, 1, 0.004, 0.0036, 0.0048, 0.02, -0.015, 0.04, 2, 51),
+             (45, 61, 4, 0.0035, 0.003, 0.004, -0.03, 0.01, -0.02, 3, 52),
+             (60, 90, 1, 0.006, 0.0045, 0.0068, 0.0, 0.0, 0.1, 0, 53),
+             (33, 40, 4, 0.002, 0.0024, 0.0032, 0.05, 0.05, 0.0, 1, 54)]
+
 FULL_LIMIT = 64 * 128  # dumps up to this many pixels are stored whole
 
 
@@ -89,12 +98,29 @@ def case_frames(case: dict) -> np.ndarray:
     return synthetic.sequence(case["seq"], frames=case["frames"], **case.get("kw", {}))
 
 
+def lw_inputs(h: int, w: int, depth: int, seed: int):
+    """(flow (H, W, 2), image (H, W) or (H, W, 4)) float32 for a Lax-Wendroff case: a smooth
+    flow of a few pixels with some large values, a noisy image."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    flow = np.stack([2.0 * np.sin(xx / 7.0 + yy / 11.0), 1.5 * np.cos(yy / 5.0 - xx / 13.0)], -1)
+    flow += rng.normal(0, 0.3, flow.shape)
+    flow.reshape(-1, 2)[rng.integers(0, h * w, 8)] = rng.uniform(-9, 9, (8, 2))
+    img = rng.random((h, w) if depth == 1 else (h, w, depth))
+    return flow.astype(np.float32), img.astype(np.float32)
+
+
+def rot_image(h: int, w: int, depth: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.random((h, w) if depth == 1 else (h, w, depth)).astype(np.float32)
+
+
 def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
 def run(out: str, only=None) -> None:
-    parts = set(only or ["stages", "norm", "upmap", "cases", "wheelidx"])
+    parts = set(only or ["stages", "norm", "upmap", "cases", "wheelidx", "rotation"])
     os.makedirs(out, exist_ok=True)
     if "stages" in parts:
         sin = os.path.join(out, "stage_in")
@@ -113,6 +139,19 @@ def run(out: str, only=None) -> None:
             fpath = os.path.join(out, f"wheel_flows_{k}.npy")
             np.save(fpath, display_oracle.probe_flows(m, seed))
             subprocess.run([DRIVER, "wheelidx", fpath, repr(m), os.path.join(out, f"wheel_idx_{k}.npy")], check=True)
+    if "rotation" in parts:
+        for k, (h, w, d, it, seed) in enumerate(LW_CASES):
+            flow, img = lw_inputs(h, w, d, seed)
+            fp, ip = os.path.join(out, f"lw_flow_{k}.npy"), os.path.join(out, f"lw_img_{k}.npy")
+            np.save(fp, flow)
+            np.save(ip, img)
+            subprocess.run([DRIVER, "lw", fp, ip, str(it), os.path.join(out, f"lw_out_{k}.npy")], check=True)
+        for k, (h, w, d, focal, sh, sw, wx, wy, wz, it, seed) in enumerate(ROT_CASES):
+            ip = os.path.join(out, f"rot_img_{k}.npy")
+            np.save(ip, rot_image(h, w, d, seed))
+            subprocess.run([DRIVER, "rotation", ip, repr(focal), repr(sh), repr(sw), repr(wx), repr(wy), repr(wz),
+                            str(it), os.path.join(out, f"rot_flow_{k}.npy"), os.path.join(out, f"rot_pred_{k}.npy")],
+                           check=True)
     if "cases" not in parts:
         return
     tmp = os.environ.get("TMPDIR", "/tmp")
@@ -183,6 +222,21 @@ def pack(raw: str) -> None:
                             maxflow=np.array([m for m, _ in WHEEL_CASES], np.float32),
                             seed=np.array([s for _, s in WHEEL_CASES], np.int64),
                             flows_sha256=np.frombuffer(json.dumps(flows_sha).encode(), np.uint8))
+    if os.path.exists(os.path.join(raw, "lw_out_0.npy")):
+        arrays = {}
+        shas = {}
+        for k, (h, w, d, it, seed) in enumerate(LW_CASES):
+            flow, img = lw_inputs(h, w, d, seed)
+            shas[f"lw_{k}"] = [sha(flow), sha(img)]
+            arrays[f"lw_out_{k}"] = np.load(os.path.join(raw, f"lw_out_{k}.npy"))
+        for k, case in enumerate(ROT_CASES):
+            h, w, d, seed = case[0], case[1], case[2], case[-1]
+            shas[f"rot_{k}"] = [sha(rot_image(h, w, d, seed))]
+            arrays[f"rot_flow_{k}"] = np.load(os.path.join(raw, f"rot_flow_{k}.npy"))
+            arrays[f"rot_pred_{k}"] = np.load(os.path.join(raw, f"rot_pred_{k}.npy"))
+            arrays[f"rot_cam_{k}"] = np.load(os.path.join(raw, f"rot_flow_{k}.npy.cam.npy"))
+        np.savez_compressed(os.path.join(GOLDEN, "ref_rotation.npz"),
+                            inputs_sha256=np.frombuffer(json.dumps(shas).encode(), np.uint8), **arrays)
     for name in CASES:
         src = os.path.join(raw, f"case_{name}.npz")
         if os.path.exists(src):

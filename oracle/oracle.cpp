@@ -38,6 +38,8 @@ int g_var[OR_V_COUNT] = {
     0,   // OR_V_UPD_OY
     1,   // OR_V_SMOOTH_FMA
     0,   // OR_V_UPMAP
+    3,   // OR_V_ROT: cx, cy fused; cz, flow x, flow y fuse their first product
+    0x3FFFF,  // OR_V_LW: every multiply-add fused
 };
 float g_norm[256];
 bool g_norm_init = false;
@@ -756,6 +758,96 @@ size_t or_filter_level_state(const or_filter* f, int level, int which, float* ou
 void or_filter_level_shape(const or_filter* f, int level, int* H, int* W) {
     *H = f->lv[level].H;
     *W = f->lv[level].W;
+}
+
+// ---- rotational flow (camera.cu:15-31, camera_k.h:15-20, rotation_k.cu:17-43).
+// p = ((x - cx) / ax, (y - cy) / ay, 1); c = w x p with the products by p.z = 1 folded;
+// flow = (ax c.x + (cx - x) c.z, ay c.y + (cy - y) c.z).  OR_V_ROT bits: 0 c.x fused,
+// 1 c.y fused, 2-3 c.z (0 fma(wx, py, -wy px), 1 fma(-wy, px, wx py), 2 none), 4-5 flow x
+// and 6-7 flow y (0 fuse the alpha product, 1 fuse the centre product, 2 none).
+void or_camera_perspective(float focal, int H, int W, float sensorH, float sensorW, float* cam4) {
+    const int imgX = W - 1, imgY = H - 1;
+    cam4[0] = focal * (float)imgX / sensorW;
+    cam4[1] = focal * (float)imgY / sensorH;
+    cam4[2] = 0.5f * (float)imgX;
+    cam4[3] = 0.5f * (float)imgY;
+}
+
+static float mad2(int v, float a, float b, float c, float d) {  // a*b + c*d
+    if (v == 0) return std::fma(a, b, c * d);
+    if (v == 1) return std::fma(c, d, a * b);
+    return a * b + c * d;
+}
+
+void or_rotational_flow(const float* cam, float wx, float wy, float wz, int H, int W, float* flow) {
+    const int v = g_var[OR_V_ROT];
+    const float ax = cam[0], ay = cam[1], cx = cam[2], cy = cam[3];
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const float px = ((float)x - cx) / ax, py = ((float)y - cy) / ay;
+            const float c_x = (v & 1) ? std::fma(-wz, py, wy) : wy - wz * py;
+            const float c_y = (v & 2) ? std::fma(wz, px, -wx) : wz * px - wx;
+            const float c_z = mad2((v >> 2) & 3, wx, py, -wy, px);
+            float* o = flow + 2 * ((size_t)y * W + x);
+            o[0] = mad2((v >> 4) & 3, ax, c_x, cx - (float)x, c_z);
+            o[1] = mad2((v >> 6) & 3, ay, c_y, cy - (float)y, c_z);
+        }
+}
+
+// ---- Lax-Wendroff propagation (propagation_k.h:49-132, propagation.cu:572-645): per
+// iteration a Y pass then an X pass, I' = I - R/2 (I+ - I-) + R^2/2 (I- - 2I + I+), R = dt f,
+// clamped neighbours.  Depth 1 evaluates the update in double (the source's 0.5 and, in the
+// Y pass, 2.0 are double literals) and rounds once to float; depth 4 works in float through
+// the float4 operators.  OR_V_LW bits: 0 / 1 the final double multiply-add fused in the X / Y
+// pass (depth 1); for depth 4 channel c: bit 2+4c X pass t1 = fma(-d0, R/2, I), 3+4c X final
+// fma(d2, R^2/2, t1), 4+4c / 5+4c the same in the Y pass.
+static void lw_pass(const float* flow, const float* in, float* out, int H, int W, int D, float dt, int axis) {
+    const int v = g_var[OR_V_LW];
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t k = (size_t)y * W + x;
+            const float R = dt * flow[2 * k + axis];
+            size_t km, kp;
+            if (axis == 0) {
+                km = (size_t)y * W + std::max(x - 1, 0);
+                kp = (size_t)y * W + std::min(x + 1, W - 1);
+            } else {
+                km = (size_t)std::max(y - 1, 0) * W + x;
+                kp = (size_t)std::min(y + 1, H - 1) * W + x;
+            }
+            for (int c = 0; c < D; ++c) {
+                const float m = in[D * km + c], i0 = in[D * k + c], p = in[D * kp + c];
+                const float d0 = p - m;
+                float r;
+                if (D == 1) {
+                    const float d2 = axis == 0 ? (m - 2.0f * i0) + p : (float)((double)m - 2.0 * (double)i0 + (double)p);
+                    const double h = 0.5 * (double)R;
+                    const double t1 = (double)i0 - h * (double)d0;
+                    const double g = h * (double)R;
+                    const bool fused = (v >> axis) & 1;
+                    r = (float)(fused ? std::fma(g, (double)d2, t1) : t1 + g * (double)d2);
+                } else {
+                    const float d2 = (m - 2.0f * i0) + p;
+                    const float b = (float)(0.5 * (double)R);
+                    const float b2 = (float)(0.5 * (double)R * (double)R);
+                    const int bit = 2 + 4 * c + 2 * axis;
+                    const float t1 = ((v >> bit) & 1) ? std::fma(-d0, b, i0) : i0 - d0 * b;
+                    r = ((v >> (bit + 1)) & 1) ? std::fma(d2, b2, t1) : t1 + d2 * b2;
+                }
+                out[D * k + c] = r;
+            }
+        }
+}
+
+void or_lax_wendroff(const float* flow, const float* image, int D, int H, int W, int iterations, float* out) {
+    const float dt = iterations > 0 ? 1.0f / (float)iterations : 0.0f;
+    const int n = std::max(iterations, 1);
+    std::vector<float> a(image, image + (size_t)H * W * D), b(a.size());
+    for (int it = 0; it < n; ++it) {
+        lw_pass(flow, a.data(), b.data(), H, W, D, dt, 1);
+        lw_pass(flow, b.data(), a.data(), H, W, D, dt, 0);
+    }
+    std::memcpy(out, a.data(), a.size() * sizeof(float));
 }
 
 }  // extern "C"

@@ -33,7 +33,9 @@ enum or_variant_key {
     OR_V_UPD_OY = 5,        /* N10*qx + N11*qy: 0 fma(N10,qx,.), 1 fma(N11,qy,.), 2 none */
     OR_V_SMOOTH_FMA = 6,    /* smoothing tap chain fused (1) or not (0) */
     OR_V_UPMAP = 7,         /* coarse index: 0 floor(u*Wc) in float */
-    OR_V_COUNT = 8
+    OR_V_ROT = 8,           /* rotational flow contraction bits, see or_rotational_flow */
+    OR_V_LW = 9,            /* Lax-Wendroff contraction bits, see or_lax_wendroff */
+    OR_V_COUNT = 10
 };
 
 void or_set_variant(int key, int value);
@@ -43,6 +45,15 @@ void or_set_norm_table(const float* table256);
 void or_get_norm_table(float* table256);
 /* 0 or 1 = single-threaded, otherwise the number of host threads for the stage loops */
 void or_set_threads(int n);
+
+/* ---- rotational flow and Lax-Wendroff propagation (src/gpu/camera.cu:15-31,
+ * src/gpu/device/rotation_k.cu:17-43, src/gpu/rotation.cu:72-88,
+ * include/flowfilter/gpu/device/propagation_k.h:49-132, src/gpu/propagation.cu:572-645) ---- */
+/* cam4 = {alphaX, alphaY, centerX, centerY} */
+void or_camera_perspective(float focal, int H, int W, float sensorH, float sensorW, float* cam4);
+void or_rotational_flow(const float* cam4, float wx, float wy, float wz, int H, int W, float* flow);
+/* image [H][W][depth] (depth 1 or 4); iterations <= 0 runs one pass pair with dt = 0 */
+void or_lax_wendroff(const float* flow, const float* image, int depth, int H, int W, int iterations, float* out);
 
 /* ---- stages (reference: src/gpu/device/*.cu) ---- */
 void or_pyramid_down_u8(const uint8_t* in, int H, int W, uint8_t* out);

@@ -18,6 +18,12 @@
 //                                      (texel (i, j) = (j, i, 0, 255)) behind the texture
 //                                      FlowToColor::configure sets up: OUT names the texel
 //                                      each pixel read
+//   lw FLOW.npy IMAGE.npy ITER OUT.npy  LaxWendroffPropagator(flow, image), setIterations(ITER)
+//                                      unless ITER is 0, compute(): the propagated image
+//   rotation IMAGE.npy FOCAL SH SW WX WY WZ ITER FLOW_OUT.npy PRED_OUT.npy
+//                                      RotationalFlowImagePredictor(createPerspectiveCamera(
+//                                      FOCAL, H, W, SH, SW), image), setAngularVelocity,
+//                                      setIterations(ITER) unless 0, compute()
 //   filter FRAMES.npy OUT.npy LEVELS MAXFLOW GAMMAS SMOOTHS DUMP [TIMING_CSV]
 //                                      LEVELS=0: FlowFilter(h, w, S, maxflow, gamma)
 //                                      LEVELS>=1: PyramidalFlowFilter(h, w, LEVELS)
@@ -45,6 +51,8 @@
 #include "flowfilter/gpu/update.h"
 #include "flowfilter/gpu/flowsmoothing.h"
 #include "flowfilter/gpu/flowfilter.h"
+#include "flowfilter/gpu/camera.h"
+#include "flowfilter/gpu/rotation.h"
 
 // the reference's colour-lookup kernel, from its source tree (oracle/Makefile adds the
 // reference's src/ directory to the include path)
@@ -443,6 +451,43 @@ static int mode_wheelidx(const std::string& flows, float maxflow, const std::str
     return 0;
 }
 
+static GPUImage upload_image(const Npy& a) {
+    if (a.descr != "<f4" || (a.shape.size() != 2 && !(a.shape.size() == 3 && a.shape[2] == 4)))
+        throw std::runtime_error("image should be (H, W) or (H, W, 4) float32");
+    return upload_npy(a, a.shape.size() == 2 ? 1 : 4);
+}
+
+static int mode_lw(const std::string& flowp, const std::string& imgp, int iters, const std::string& out) {
+    GPUImage flow = upload_npy(npy_read(flowp), 2);
+    GPUImage img = upload_image(npy_read(imgp));
+    LaxWendroffPropagator lw(flow, img);
+    if (iters > 0) lw.setIterations(iters);
+    lw.compute();
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) throw std::runtime_error(std::string("lw: ") + cudaGetErrorString(e));
+    save_gpu(out, lw.getPropagatedImage());
+    return 0;
+}
+
+static int mode_rotation(char** argv) {
+    GPUImage img = upload_image(npy_read(argv[2]));
+    perspectiveCamera cam = createPerspectiveCamera((float)atof(argv[3]), img.height(), img.width(),
+                                                    (float)atof(argv[4]), (float)atof(argv[5]));
+    RotationalFlowImagePredictor pred(cam, img);
+    pred.setAngularVelocity((float)atof(argv[6]), (float)atof(argv[7]), (float)atof(argv[8]));
+    const int iters = atoi(argv[9]);
+    if (iters > 0) pred.setIterations(iters);
+    pred.compute();
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) throw std::runtime_error(std::string("rotation: ") + cudaGetErrorString(e));
+    save_gpu(argv[10], pred.getOpticalFlow());
+    save_gpu(argv[11], pred.getPredictedImage());
+    const float cam4[4] = {cam.alphaX, cam.alphaY, cam.centerX, cam.centerY};
+    std::vector<size_t> shape = {4};
+    npy_write(std::string(argv[10]) + ".cam.npy", "<f4", shape, cam4, sizeof(cam4));
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) { fprintf(stderr, "usage: ref_driver MODE ...\n"); return 2; }
     std::string mode = argv[1];
@@ -451,6 +496,8 @@ int main(int argc, char** argv) {
         if (mode == "upmap" && argc >= 4) return mode_upmap(argv[2], atoi(argv[3]));
         if (mode == "stages" && argc >= 4) return mode_stages(argv[2], argv[3]);
         if (mode == "filter" && argc >= 9) return mode_filter(argc, argv);
+        if (mode == "lw" && argc >= 6) return mode_lw(argv[2], argv[3], atoi(argv[4]), argv[5]);
+        if (mode == "rotation" && argc >= 12) return mode_rotation(argv);
         if (mode == "wheelidx" && argc >= 5) return mode_wheelidx(argv[2], (float)atof(argv[3]), argv[4]);
     } catch (const std::exception& e) {
         fprintf(stderr, "ref_driver: %s\n", e.what());

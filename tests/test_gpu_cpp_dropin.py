@@ -62,3 +62,26 @@ def test_cpp_dropin_sequence_matches_oracle(program, tmp_path, h, w, levels):
     # FlowToColor(filter.getFlow(), 4) with the library's wheel
     colour = np.fromfile(fcol, np.uint8).reshape(h, w, 4)
     np.testing.assert_array_equal(colour, D.flow_to_color(of.get_flow(), 4.0, D.middlebury_wheel()))
+
+
+@pytest.mark.parametrize("h,w,d,n", [(45, 61, 1, 3), (50, 70, 4, 18)])
+def test_cpp_dropin_rotation_matches_oracle(cuda, tmp_path, h, w, d, n):
+    """The C++ camera, RotationalFlowImagePredictor and LaxWendroffPropagator classes."""
+    prog = str(tmp_path / "dropin_rotation")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "dropin_rotation.cpp"), "-o", prog, "-L", PKG,
+                    "-lflowfilter_gpu", "-Wl,-rpath," + PKG], check=True)
+    img = np.random.default_rng(h + w + d).random((h, w) if d == 1 else (h, w, d)).astype(np.float32)
+    fin, fout = tmp_path / "img.f32", tmp_path / "out.f32"
+    img.tofile(fin)
+    r = subprocess.run([prog, str(fin), str(h), str(w), str(d), str(n), str(fout)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    got = np.fromfile(fout, np.float32)
+    cam = O.camera_perspective(0.004, h, w, 0.003, 0.004)
+    np.testing.assert_array_equal(got[:4], cam)
+    flow = O.rotational_flow(cam, 0.01, -0.02, 0.03, h, w)
+    pred = O.lax_wendroff(flow, img, n)
+    n2, nd = h * w * 2, h * w * d
+    np.testing.assert_array_equal(got[4:4 + n2].reshape(flow.shape), flow)
+    np.testing.assert_array_equal(got[4 + n2:4 + n2 + nd].reshape(img.shape), pred)
+    np.testing.assert_array_equal(got[4 + n2 + nd:].reshape(img.shape), pred)
