@@ -119,14 +119,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(name):
+def ncu_traffic(name, key="dram_bytes_per_launch"):
+    """A per-launch figure of the level-0 kernel from one ncu capture (profiles/)."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
     v = d.get(name)
-    return None if v is None else float(v["dram_bytes_per_launch"])
+    return None if v is None or key not in v else float(v[key])
 
 
 class ClockSampler:
@@ -481,6 +482,21 @@ def graph_us(launch, n, per_graph=20):
     return e0.elapsed_time(e1) * 1e3 / (reps * per_graph)
 
 
+def issue_roofline(warp_instructions, launch_ms, clocks):
+    """The level-0 kernel against the instruction-issue ceiling that binds it: warp
+    instructions per launch (ncu) / live launch time, over SMs x 4 schedulers x one
+    instruction per clock at the median SM clock sampled during the timed region."""
+    import torch
+
+    if not warp_instructions or not clocks or not clocks.get("sm_mhz"):
+        return None
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = sms * 4 * clocks["sm_mhz"] * 1e6
+    achieved = warp_instructions / (launch_ms * 1e-3)
+    return {"warp_instructions": warp_instructions, "achieved": achieved, "peak": peak, "unit": "warp-inst/s",
+            "frac": achieved / peak}
+
+
 def bench_flow_to_color(filt, n):
     """Mean device microseconds of ff_flow_to_color per launch on the filter's current
     level-0 flow (a pitched device view), default wheel."""
@@ -675,7 +691,9 @@ def bench_b200(args):
                          "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
                          "algorithmic_bytes": l0_bytes, "launch_ms": l0_ms, "peak_kind": peak_kind,
                          "l2_resident": {"launch_ms": l0_ms_l2, "achieved": l0_bytes / (l0_ms_l2 / 1e3) / 1e9,
-                                         "note": "same step without the L2 flush (state L2-resident)"}},
+                                         "note": "same step without the L2 flush (state L2-resident)"},
+                         "issue": issue_roofline(ncu_traffic(PRIMARY, "warp_instructions_per_launch"), l0_ms,
+                                                 clk.summary())},
             "flow_to_color": {"launch_us": ftc_us, "pixels": w["H"] * w["W"],
                               "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
                               "note": "ff_flow_to_color on the 640x480 level-0 flow, default wheel; "

@@ -5,7 +5,7 @@
 // include/flowfilter/gpu/device/propagation_k.h:49-132).
 //
 // The reference runs 2N launches (a Y pass then an X pass per iteration, each a full-image
-// round trip through HBM or L2).  Here one CTA computes one T x T output tile: it loads the
+// round trip through HBM or L2).  Here one CTA computes one 32 x 32 output tile: it loads the
 // image over the tile plus a halo of P pixels (P = iterations in this launch) into shared
 // memory with the flow, then runs all 2P passes there, each over a region one pixel smaller
 // along its axis (clamped at the image edges as the reference's texture reads are), and
@@ -203,7 +203,13 @@ __global__ void rotational_flow_k(LWArgs a) {
     reinterpret_cast<float2*>(reinterpret_cast<char*>(a.flow_out) + y * a.flow_out_pitch)[x] = rotational_flow(a, x, y);
 }
 
-int tile_of(int D, int passes) { return D == 1 && passes <= 8 ? 64 : 32; }
+// 32 x 32 tiles: a VGA image gives 300 CTAs, several resident per SM (each a few to 164 KB
+// of shared memory), which hides the shared-memory and FP64 latency of the passes
+int tile_of(int D, int passes) {
+    (void)D;
+    (void)passes;
+    return 32;
+}
 
 size_t smem_of(int D, int tile, int passes) {
     const size_t r = (size_t)(tile + 2 * passes);
