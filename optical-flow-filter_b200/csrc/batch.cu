@@ -181,6 +181,10 @@ Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
     for (auto& t : tab_) t.reset(new Table);
     check_cuda(cudaFuncSetAttribute(tile_batch_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmemCap),
                "cudaFuncSetAttribute");
+    // full shared carve-out, so the L-2 launch's blocks can share SMs with the top launch's
+    check_cuda(cudaFuncSetAttribute(tile_batch_k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared),
+               "cudaFuncSetAttribute");
 }
 
 void Batch::release_table(Table& t) {

@@ -618,6 +618,10 @@ cudaError_t launch(const LevelArgs& a, cudaStream_t s) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // full shared carve-out, as for the tile kernels: SMs running this kernel can then
+        // also host the tile kernels of the levels that run beside it
+        cudaFuncSetAttribute(level_k<DELTA, N, S, P>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_k<DELTA, N, S, P>, kWarpsPerBlock * 32, smem);
         resident_warps = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarpsPerBlock;
     }

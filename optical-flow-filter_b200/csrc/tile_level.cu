@@ -112,6 +112,13 @@ cudaError_t launch_t(const LevelArgs& a, int N, int S, Cfg c, cudaStream_t s) {
         cudaError_t e = cudaFuncSetAttribute(tile_k<DELTA, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)device_info().smem_optin);
         if (e != cudaSuccess) return e;
+        // An SM's L1/shared split is fixed while blocks run on it.  A small tile (the top
+        // level's) would otherwise get a small shared carve-out, and the next level's large
+        // tiles, launched early to overlap it, could not share its SMs: ask for the full
+        // shared-memory carve-out for every tile kernel.
+        e = cudaFuncSetAttribute(tile_k<DELTA, P>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
         prepared.fetch_or(bit);
     }
     Geom g;
