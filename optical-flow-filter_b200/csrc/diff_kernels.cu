@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <initializer_list>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -180,6 +182,22 @@ __device__ __forceinline__ void block_sum(const T (&v)[NV], T* dst, bool atomic)
 
 __device__ __forceinline__ size_t block_linear() {
     return blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+}
+
+// a pair of T (the two channels of a flow pixel) as one vector access
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using V = float2;
+};
+template <>
+struct Pair<double> {
+    using V = double2;
+};
+template <typename T>
+__device__ __forceinline__ typename Pair<T>::V ld2(const T* p, size_t k) {
+    return reinterpret_cast<const typename Pair<T>::V*>(p)[k];
 }
 
 // write or add one gradient value
@@ -379,14 +397,28 @@ __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, con
 #pragma unroll
         for (int p = 0; p < 5; ++p) {
             const size_t k = at(j - 2 + p);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) ch[c][p] = chan(k, c);
+            const auto fv = ld2(f, k);
+            ch[0][p] = fv.x;
+            ch[1][p] = fv.y;
+            if constexpr (PAYLOAD) {
+                const auto vv = ld2(v, k);
+                ch[2 % NC][p] = s[k];
+                ch[3 % NC][p] = vv.x;
+                ch[4 % NC][p] = vv.y;
+            }
         }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const size_t k = at(j - 1 + q);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) go[c][q] = gchan(k, c);
+            const auto gf2 = ld2(gfo, k);
+            go[0][q] = gf2.x;
+            go[1][q] = gf2.y;
+            if constexpr (PAYLOAD) {
+                const auto gv2 = ld2(gvo, k);
+                go[2 % NC][q] = gso[k];
+                go[3 % NC][q] = gv2.x;
+                go[4 % NC][q] = gv2.y;
+            }
         }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
@@ -587,48 +619,57 @@ __global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in,
                                  in[2 * kk[4] + ch]);
 }
 
+// Blocks of 32 x 8 threads cover 32 x 32 pixels (kSmoothRows rows per thread), so the
+// weight gradient is reduced once per 1024 pixels.
 // PART: gw5 is a partial-sum array, this block stores its 5 sums at gw5[5 * block]
+constexpr int kSmoothRows = 4;
 template <typename T, int AXIS, bool ACC = true, bool PART = false>
 __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in, const T* __restrict__ gout, T* gin,
                              T* gw5, int H, int W) {
     grid_dep_wait();
     grid_dep_launch();
-    PIX_SETUP
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t b = blockIdx.z;
     T gw[5] = {T(0), T(0), T(0), T(0), T(0)};
-    if (live) {
-        T w[5];
-        for (int i = 0; i < 5; ++i) w[i] = w5[i];
-        const int n = AXIS == 0 ? W : H;
-        const int j = AXIS == 0 ? x : y;
-        auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
-        // input gradient at this pixel: outputs i in [j-2, j+2] whose clamped taps land on j
-        T a0 = T(0), a1 = T(0);
-        if (j >= 2 && j + 2 <= n - 1) {
-            // no clamps: output i reads j through tap j - i + 2 only
-#pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const T wt = w[4 - q];
-                const size_t ki = at(j - 2 + q);
+    for (int rr = 0; rr < kSmoothRows; ++rr) {
+        const int y = (blockIdx.y * kSmoothRows + rr) * blockDim.y + threadIdx.y;
+        if (x < W && y < H) {
+            T w[5];
+            for (int i = 0; i < 5; ++i) w[i] = w5[i];
+            const int n = AXIS == 0 ? W : H;
+            const int j = AXIS == 0 ? x : y;
+            auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
+            // input gradient at this pixel: outputs i in [j-2, j+2] whose clamped taps land on j
+            T a0 = T(0), a1 = T(0);
+            if (j >= 2 && j + 2 <= n - 1) {
+                // no clamps: output i reads j through tap j - i + 2 only
+    #pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const T wt = w[4 - q];
+                    if (wt != T(0)) {
+                        const auto gv = ld2(gout, at(j - 2 + q));
+                        a0 += wt * gv.x;
+                        a1 += wt * gv.y;
+                    }
+                }
+            } else
+            for (int i = max(j - 2, 0); i <= min(j + 2, n - 1); ++i) {
+                const T wt = tap_weight(w, i, j, n);
                 if (wt != T(0)) {
-                    a0 += wt * gout[2 * ki];
-                    a1 += wt * gout[2 * ki + 1];
+                    a0 += wt * gout[2 * at(i)];
+                    a1 += wt * gout[2 * at(i) + 1];
                 }
             }
-        } else
-        for (int i = max(j - 2, 0); i <= min(j + 2, n - 1); ++i) {
-            const T wt = tap_weight(w, i, j, n);
-            if (wt != T(0)) {
-                a0 += wt * gout[2 * at(i)];
-                a1 += wt * gout[2 * at(i) + 1];
+            put<ACC>(gin[2 * at(j)], a0);
+            put<ACC>(gin[2 * at(j) + 1], a1);
+            // weight gradient: this pixel as an output
+            const auto g01 = ld2(gout, at(j));
+            const T g0 = g01.x, g1 = g01.y;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const auto iv = ld2(in, at(clampi(j + k - 2, 0, n - 1)));
+                gw[k] += g0 * iv.x + g1 * iv.y;
             }
-        }
-        put<ACC>(gin[2 * at(j)], a0);
-        put<ACC>(gin[2 * at(j) + 1], a1);
-        // weight gradient: this pixel as an output
-        const T g0 = gout[2 * at(j)], g1 = gout[2 * at(j) + 1];
-        for (int k = 0; k < 5; ++k) {
-            const size_t kk = at(clampi(j + k - 2, 0, n - 1));
-            gw[k] = g0 * in[2 * kk] + g1 * in[2 * kk + 1];
         }
     }
     block_sum<T, 5>(gw, PART ? gw5 + 5 * block_linear() : gw5, !PART);
@@ -761,6 +802,8 @@ __global__ void add_k(T* __restrict__ dst, const T* __restrict__ src, size_t n) 
 }
 
 inline dim3 grid3(int w, int h, int B) { return dim3((w + 31) / 32, (h + 7) / 8, B); }
+// the smoothing adjoint's grid (32 x 8 threads over 32 x 32 pixels)
+inline dim3 grid_smooth(int w, int h, int B) { return dim3((w + 31) / 32, (h + 8 * kSmoothRows - 1) / (8 * kSmoothRows), B); }
 const dim3 kBlock(32, 8);
 
 template <typename T>
@@ -806,6 +849,22 @@ ff_status check_shape(int B, int H, int W) {
 }
 
 }  // namespace
+
+// two-channel fields are read as one vector per pixel: their base must be aligned to a pair
+bool pairs_aligned(int dtype, std::initializer_list<const void*> ps) {
+    const uintptr_t a = dtype ? 16 : 8;
+    for (const void* p : ps)
+        if (p && (uintptr_t)p % a) return false;
+    return true;
+}
+
+#define PAIRS_OR_RETURN(dtype, ...)                                                                   \
+    do {                                                                                              \
+        if (!pairs_aligned(dtype, {__VA_ARGS__})) {                                                   \
+            ffb_set_last_error("two-channel fields must be aligned to two elements (8 or 16 bytes)"); \
+            return FF_ERR_INVALID_ARGUMENT;                                                           \
+        }                                                                                             \
+    } while (0)
 
 #define SHAPE_OR_RETURN(B, H, W)                   \
     do {                                           \
@@ -893,6 +952,7 @@ ff_status ff_diff_propagate_bwd(int dtype, int B, int H, int W, int axis, int pa
                                 const void* f, const void* sc, const void* v, const void* gfo, const void* gso,
                                 const void* gvo, void* gf, void* gs, void* gv, void* stream) {
     SHAPE_OR_RETURN(B, H, W);
+    PAIRS_OR_RETURN(dtype, f, v, gfo, gvo, gf, gv);
     if ((axis != 0 && axis != 1) || border < 0) {
         ffb_set_last_error("axis must be 0 or 1 and border >= 0");
         return FF_ERR_INVALID_ARGUMENT;
@@ -1007,13 +1067,14 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
 ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const void* w5, const void* in,
                              const void* gout, void* gin, void* gw5, void* stream) {
     SHAPE_OR_RETURN(B, H, W);
+    PAIRS_OR_RETURN(dtype, in, gout, gin);
     if (axis != 0 && axis != 1) {
         ffb_set_last_error("axis must be 0 or 1");
         return FF_ERR_INVALID_ARGUMENT;
     }
     cudaStream_t s = (cudaStream_t)stream;
     return run(dtype, [&] {
-        const dim3 g = grid3(W, H, B);
+        const dim3 g = grid_smooth(W, H, B);
         if (dtype)
             return axis == 0 ? launch_k(smooth_bwd_k<double, 0>, g, kBlock, 0, s, (const double*)w5,
                                         (const double*)in, (const double*)gout, (double*)gin, (double*)gw5, H, W)
@@ -1175,7 +1236,7 @@ struct Driver {
     }
     // one smoothing pass's adjoint: input gradient stored (or added), weight sums per block
     void smooth_bwd(int l, int axis, bool acc, const T* w5, const T* in, const T* go, T* gi, T* part) const {
-        const dim3 gr = grid(l);
+        const dim3 gr = grid_smooth(g.W[l], g.H[l], g.B);
         const int H = g.H[l], W = g.W[l];
         cudaError_t e;
         if (acc)
@@ -1293,7 +1354,8 @@ struct Driver {
                 add(dst, gcur, 2 * g.n1(l));
                 return dst;
             }
-            const size_t nb = blocks_of(g, l);
+            const dim3 sg = grid_smooth(g.W[l], g.H[l], g.B);
+            const size_t nb = (size_t)sg.x * sg.y * sg.z;
             T* bufs[2] = {sa, sb};
             for (int j = n - 1; j >= 0; --j) {
                 T* o = j == 0 ? dst : bufs[j % 2];
@@ -1429,6 +1491,9 @@ ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, 
         if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
         if (!frame || !gamma || !weights || !state_in || !state_out || !tape)
             throw std::invalid_argument("null pointer argument");
+        for (int k = 0; k < 3 * g.L; ++k)
+            if (!::pairs_aligned(dtype, {state_in[k], state_out[k]}))
+                throw std::invalid_argument("state fields must be aligned to two elements (8 or 16 bytes)");
         if (dtype) {
             ffb::diff::Driver<double>(g, (cudaStream_t)stream)
                 .forward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
@@ -1452,6 +1517,9 @@ ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first,
         if (!frame || !gamma || !weights || !state_in || !state_out || !tape || !grad_state_out || !grad_frame ||
             !grad_gamma || !grad_weights || !grad_state_in || !scratch)
             throw std::invalid_argument("null pointer argument");
+        for (int k = 0; k < 3 * g.L; ++k)
+            if (!::pairs_aligned(dtype, {state_in[k], state_out[k], grad_state_out[k], grad_state_in[k]}))
+                throw std::invalid_argument("state fields must be aligned to two elements (8 or 16 bytes)");
         if (dtype) {
             ffb::diff::Driver<double>(g, (cudaStream_t)stream)
                 .backward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
