@@ -276,7 +276,10 @@ __device__ __forceinline__ void tile_body(const LevelArgs& a, const Geom& g, int
                     constexpr bool FREE = decltype(free_tag)::value;
                     auto xstep = [&](int row) {
                         const int k = (row - oy) * SW + kc;
-                        const PropIn p = prop_load<DELTA>(fs, ds, is, k, k - dxm, k + dxp);
+                        // a free tile lies inside the border, so its X neighbours are never clamped:
+                        // constant offsets let the loads share one address
+                        const PropIn p = FREE ? prop_load<DELTA>(fs, ds, is, k, k - 1, k + 1)
+                                              : prop_load<DELTA>(fs, ds, is, k, k - dxm, k + dxp);
                         return FREE ? prop_eval<0, DELTA>(p, dt, true) : prop_eval<0, DELTA>(p, dt, cin && row_in(row));
                     };
                     PropOut cur = xstep(by0);
