@@ -190,4 +190,34 @@ __device__ __forceinline__ float box5(float a, float b, float c, float d, float 
     return __fmaf_rn(kBox, e, s);
 }
 
+// 5-tap chains on two lanes at once with sm_100's packed two-lane FP32 instructions (two
+// channels of a pixel, or one channel of two pixels): each lane is the same IEEE fma.rn as
+// the scalar chain's, so the results are identical
+__device__ __forceinline__ float2 chain5_pair(float k0, float k1, float k2, float k3, float k4, float2 a, float2 b,
+                                              float2 c, float2 d, float2 e) {
+    float2 s = __ffma2_rn(make_float2(k0, k0), a, make_float2(0.0f, 0.0f));
+    s = __ffma2_rn(make_float2(k1, k1), b, s);
+    s = __ffma2_rn(make_float2(k2, k2), c, s);
+    s = __ffma2_rn(make_float2(k3, k3), d, s);
+    return __ffma2_rn(make_float2(k4, k4), e, s);
+}
+__device__ __forceinline__ float2 box5_pair(float2 a, float2 b, float2 c, float2 d, float2 e) {
+    return chain5_pair(kBox, kBox, kBox, kBox, kBox, a, b, c, d, e);
+}
+__device__ __forceinline__ float2 smooth5_pair(float2 a, float2 b, float2 c, float2 d, float2 e) {
+    return chain5_pair(kS0, kS1, kS2, kS1, kS0, a, b, c, d, e);
+}
+__device__ __forceinline__ float2 diff5_pair(float2 a, float2 b, float2 c, float2 d, float2 e) {
+    return chain5_pair(kD0, kD1, 0.0f, -kD1, -kD0, a, b, c, d, e);
+}
+
+// upwind() of both channels of a flow pixel (both fused, as for the payload kernels' flow),
+// with packed two-lane instructions; lane for lane the same operations as upwind()
+__device__ __forceinline__ float2 upwind_pair(float t, float dv, float2 fm, float2 f0, float2 fp) {
+    const float2 back = __fadd2_rn(f0, make_float2(-fm.x, -fm.y));
+    const float2 fwd = __fadd2_rn(fp, make_float2(-f0.x, -f0.y));
+    const float2 d = dv >= 0.0f ? back : fwd;
+    return __ffma2_rn(make_float2(-t, -t), d, f0);
+}
+
 }  // namespace ffb

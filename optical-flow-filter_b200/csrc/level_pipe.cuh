@@ -124,26 +124,23 @@ __device__ __forceinline__ void nb5_raw(float2 v, float2 (&t)[5]) {
     t[4] = make_float2(R.x, R.y);
 }
 
-__device__ __forceinline__ float2 smooth5p(const float2 (&t)[5]) {
-    return make_float2(smooth5(t[0].x, t[1].x, t[2].x, t[3].x, t[4].x), smooth5(t[0].y, t[1].y, t[2].y, t[3].y, t[4].y));
-}
-__device__ __forceinline__ float2 diff5p(const float2 (&t)[5]) {
-    return make_float2(diff5(t[0].x, t[1].x, t[2].x, t[3].x, t[4].x), diff5(t[0].y, t[1].y, t[2].y, t[3].y, t[4].y));
-}
-__device__ __forceinline__ float2 box5p(const float2 (&t)[5]) {
-    return make_float2(box5(t[0].x, t[1].x, t[2].x, t[3].x, t[4].x), box5(t[0].y, t[1].y, t[2].y, t[3].y, t[4].y));
-}
+// the pixel pair's 5-tap chains as packed two-lane instructions (lane = pixel)
+__device__ __forceinline__ float2 smooth5p(const float2 (&t)[5]) { return smooth5_pair(t[0], t[1], t[2], t[3], t[4]); }
+__device__ __forceinline__ float2 diff5p(const float2 (&t)[5]) { return diff5_pair(t[0], t[1], t[2], t[3], t[4]); }
+__device__ __forceinline__ float2 box5p(const float2 (&t)[5]) { return box5_pair(t[0], t[1], t[2], t[3], t[4]); }
 
 // upwind step of a pair: n = vel >= 0 ? m : p; d = v - n; v - |t|*d (fused or not).
 // Equals the reference's v - t*(vel >= 0 ? v - m : p - v) bit for bit: for vel < 0,
 // t = -|t| and p - v = -(v - p) exactly.
 // fw = (vel >= 0) per pixel, at = |t| per pixel
+// (packed two-lane instructions, lane = pixel; each lane the scalar operation)
 template <bool FUSED>
 __device__ __forceinline__ float2 upwind2(float2 v, float2 m, float2 p, bool fw0, bool fw1, float2 at) {
-    const float d0 = __fsub_rn(v.x, fw0 ? m.x : p.x);
-    const float d1 = __fsub_rn(v.y, fw1 ? m.y : p.y);
-    if (FUSED) return make_float2(__fmaf_rn(-at.x, d0, v.x), __fmaf_rn(-at.y, d1, v.y));
-    return make_float2(__fsub_rn(v.x, __fmul_rn(at.x, d0)), __fsub_rn(v.y, __fmul_rn(at.y, d1)));
+    const float2 n = make_float2(fw0 ? m.x : p.x, fw1 ? m.y : p.y);
+    const float2 d = __fadd2_rn(v, make_float2(-n.x, -n.y));
+    if (FUSED) return __ffma2_rn(make_float2(-at.x, -at.y), d, v);
+    const float2 q = __fmul2_rn(at, d);
+    return __fadd2_rn(v, make_float2(-q.x, -q.y));
 }
 
 __device__ __forceinline__ float2 abs_t(float dt, float2 vel) {

@@ -146,9 +146,12 @@ __device__ __forceinline__ PropOut prop_eval(const PropIn& p, float dt, bool in)
     const float dv = AXIS == 0 ? dominant(p.fm.x, p.fp.x) : dominant(p.fm.y, p.fp.y);
     const float t = __fmul_rn(dt, dv);
     PropOut o;
-    o.f.x = in ? upwind(t, dv, p.fm.x, p.f0.x, p.fp.x) : p.f0.x;
-    if constexpr (DELTA) o.f.y = in ? upwind(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
-    else o.f.y = in ? upwind_unfused(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
+    if constexpr (DELTA) {
+        o.f = in ? upwind_pair(t, dv, p.fm, p.f0, p.fp) : p.f0;
+    } else {
+        o.f.x = in ? upwind(t, dv, p.fm.x, p.f0.x, p.fp.x) : p.f0.x;
+        o.f.y = in ? upwind_unfused(t, dv, p.fm.y, p.f0.y, p.fp.y) : p.f0.y;
+    }
     if constexpr (DELTA) {
         o.s = in ? upwind(t, dv, p.sm, p.s0, p.sp) : p.s0;
         o.v.x = in ? upwind(t, dv, p.vm.x, p.v0.x, p.vp.x) : p.v0.x;
@@ -160,9 +163,7 @@ __device__ __forceinline__ PropOut prop_eval(const PropIn& p, float dt, bool in)
 struct Five {
     float2 v0, v1, v2, v3, v4;
 };
-__device__ __forceinline__ float2 box5_2(const Five& f) {
-    return make_float2(box5(f.v0.x, f.v1.x, f.v2.x, f.v3.x, f.v4.x), box5(f.v0.y, f.v1.y, f.v2.y, f.v3.y, f.v4.y));
-}
+__device__ __forceinline__ float2 box5_2(const Five& f) { return box5_pair(f.v0, f.v1, f.v2, f.v3, f.v4); }
 
 // One CTA's work: output tile `tile` (row-major over the tile grid) of the level step
 // described by (a, g), in the dynamic shared memory `sm`.
