@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -219,8 +220,18 @@ size_t smem_of(int D, int tile, int passes) {
 template <int D, bool ROT>
 cudaError_t launch_lw(LWArgs a, cudaStream_t s) {
     const size_t smem = smem_of(D, a.tile, a.passes);
-    cudaError_t e = cudaFuncSetAttribute(lw_tile_k<D, ROT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // once per device: room for the largest launch (kMaxFused iterations); no static smem
+    static std::atomic<unsigned long long> prepared{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(prepared.load() & bit)) {
+        e = cudaFuncSetAttribute(lw_tile_k<D, ROT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_of(D, tile_of(D, kMaxFused), kMaxFused));
+        if (e != cudaSuccess) return e;
+        prepared.fetch_or(bit);
+    }
     const dim3 grid((a.W + a.tile - 1) / a.tile, (a.H + a.tile - 1) / a.tile);
     return launch_k(lw_tile_k<D, ROT>, grid, dim3(32, 8), smem, s, a);
 }
