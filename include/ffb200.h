@@ -256,6 +256,10 @@ ff_status ff_batch_frame_layout(const ff_batch* batch, size_t* offsets, size_t* 
 ff_status ff_batch_launches(const ff_batch* batch, int* launches);
 /* frames: 16-byte aligned device buffer of total_bytes; stream: cudaStream_t (NULL = legacy) */
 ff_status ff_batch_step(ff_batch* batch, const void* frames, void* stream);
+/* Kernel selection (optional; results do not depend on it): levels of at least min_pixels
+ * pixels run the streaming level kernel in bands of band rows, the others the tile-fused
+ * kernel.  min_pixels < 0 selects the single filter's threshold, band <= 0 the default. */
+ff_status ff_batch_set_tuning(ff_batch* batch, long long min_pixels, int band);
 
 /* ------------------------------------------------------------ differentiable stages
  * No counterpart in the reference: the float-input filter's stages as forward and adjoint

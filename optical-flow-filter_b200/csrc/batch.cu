@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <string>
+#include <tuple>
 
 #include "tile_body.cuh"
 
@@ -147,11 +149,15 @@ T* to_device(const std::vector<T>& v) {
 struct Batch::Table {
     std::vector<int> parity;
     std::vector<unsigned long long> gen;
+    unsigned long long tune_gen = 0;
     PyrJob* d_pyr = nullptr;
     TileJob* d_tile = nullptr;
+    StreamJob* d_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int launches = 0;
 };
+
+// the streaming-kernel launches of a step: (phase, delta, N, S) -> its jobs
+using StreamGroups = std::map<std::tuple<int, int, int, int>, std::vector<StreamJob>>;
 
 Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
     if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: stream count must be positive");
@@ -191,6 +197,7 @@ void Batch::release_table(Table& t) {
     if (t.graph) cudaGraphExecDestroy(t.graph);
     if (t.d_pyr) cudaFree(t.d_pyr);
     if (t.d_tile) cudaFree(t.d_tile);
+    if (t.d_stream) cudaFree(t.d_stream);
     t = Table{};
 }
 
@@ -206,6 +213,8 @@ Batch::~Batch() {
         if (t) release_table(*t);
     if (d_ingest_) cudaFree(d_ingest_);
     if (cap_) cudaStreamDestroy(cap_);
+    for (cudaStream_t q : side_) cudaStreamDestroy(q);
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
 }
 
 Filter& Batch::stream(int i) {
@@ -219,10 +228,35 @@ size_t Batch::frame_offset(int i) const {
     return off_[i];
 }
 
-int Batch::launches_per_step() const { return 1 + (max_levels_ - 1) + 1 + (max_levels_ >= 2 ? 1 : 0); }
+bool Batch::streamed(const Filter& f, int l) const {
+    const Level& v = f.level(l);
+    const long min_px = min_px_ >= 0 ? min_px_ : Filter::kFusedMinPixels;
+    return v.item == 1 && (long)v.H * v.W >= min_px && f.streaming_ok(l);
+}
+
+void Batch::set_tuning(long min_pixels, int band) {
+    min_px_ = min_pixels < 0 ? -1 : min_pixels;
+    band_ = band > 0 ? band : 0;
+    ++tune_gen_;
+}
+
+int Batch::launches_per_step() const {
+    bool tile_a = false, tile_b = false;
+    std::map<std::tuple<int, int, int, int>, int> groups;
+    for (auto& f : f_) {
+        const int L = f->levels();
+        for (int l = 0; l < L; ++l) {
+            const Level& v = f->level(l);
+            const int late = L >= 2 && l == L - 2;
+            if (streamed(*f, l)) groups[{late, v.delta, v.iters, v.smooth}] = 1;
+            else (late ? tile_b : tile_a) = true;
+        }
+    }
+    return 1 + (max_levels_ - 1) + (int)tile_a + (int)tile_b + (int)groups.size();
+}
 
 bool Batch::matches(const Table& t) const {
-    if (!t.graph) return false;
+    if (!t.graph || t.tune_gen != tune_gen_) return false;
     for (size_t i = 0; i < f_.size(); ++i)
         if (t.parity[i] != f_[i]->parity() || t.gen[i] != f_[i]->config_generation()) return false;
     return true;
@@ -256,14 +290,60 @@ void Batch::build(Table& t) {
         pyr_count[d] = (int)pyr.size() - pyr_first[d];
         pyr_blocks[d] = blocks;
     }
-    // launch A: top levels and levels 0..L-3; launch B: levels L-2
+    // phase A: top levels and levels 0..L-3; phase B: levels L-2.  Large levels go to the
+    // streaming launches of their phase, the others to the phase's tile launch.
     std::vector<TileJob> ja, jb;
     int blocks_a = 0, blocks_b = 0;
     size_t smem_a = 0, smem_b = 0;
+    StreamGroups groups;
+    std::map<std::tuple<int, int, int, int>, int> group_blocks;
+    // Band rows: every band recomputes (2S + N)-row lead and tail windows, so long bands
+    // waste less, while the streaming branches need enough warps to balance over the SMs.
+    // One band for the step: the longest of 256..32 rows that gives phase A's streaming
+    // levels (phase B's when A has none) kWaves waves of resident warps (fitted to the
+    // 64-stream and single-size 640x480 .. 1920x1080 mixes on B200).
+    constexpr int kBands[] = {256, 128, 64, 32};
+    constexpr double kWaves = 3.5;
+    int band = band_;
+    if (band <= 0) {
+        const double resident = (double)fused_resident_warps();
+        auto warps_at = [&](int phase, int b) {
+            long warps = 0;
+            for (auto& f : f_) {
+                const int L = f->levels();
+                for (int l = 0; l < L; ++l) {
+                    if ((L >= 2 && l == L - 2) != (phase == 1) || !streamed(*f, l)) continue;
+                    const Level& v = f->level(l);
+                    int nwx = 0, nby = 0;
+                    fused_warp_grid(v.iters, v.smooth, v.W, v.H, b, &nwx, &nby);
+                    warps += (long)nwx * nby;
+                }
+            }
+            return warps;
+        };
+        const int phase = warps_at(0, 8) > 0 ? 0 : 1;
+        band = 32;
+        for (int b : kBands)
+            if (warps_at(phase, b) >= kWaves * resident) {
+                band = b;
+                break;
+            }
+    }
     for (auto& f : f_) {
         const int L = f->levels();
         for (int l = 0; l < L; ++l) {
             const Level& v = f->level(l);
+            if (streamed(*f, l)) {
+                const std::tuple<int, int, int, int> key{L >= 2 && l == L - 2, v.delta, v.iters, v.smooth};
+                StreamJob j{};
+                j.a = f->level_args(l);
+                j.band = std::min(std::max(band, 8), v.H);
+                int& blocks = group_blocks[key];
+                j.first_block = blocks;
+                blocks += fused_warp_grid(v.iters, v.smooth, v.W, v.H, j.band, &j.nwx, &j.nby);
+                groups[key].push_back(j);
+                continue;
+            }
             TileJob j{};
             j.a = f->level_args(l);
             j.delta = v.delta ? 1 : 0;
@@ -290,28 +370,74 @@ void Batch::build(Table& t) {
     }
     std::vector<TileJob> all(ja);
     all.insert(all.end(), jb.begin(), jb.end());
+    std::vector<StreamJob> sall;
+    std::vector<size_t> sfirst;
+    for (auto& kv : groups) {
+        sfirst.push_back(sall.size());
+        sall.insert(sall.end(), kv.second.begin(), kv.second.end());
+    }
     t.d_pyr = to_device(pyr);
     t.d_tile = to_device(all);
+    t.d_stream = to_device(sall);
     t.parity.clear();
     t.gen.clear();
     for (auto& f : f_) {
         t.parity.push_back(f->parity());
         t.gen.push_back(f->config_generation());
     }
-    // capture: pyramid depths, then launch A, then launch B
+    t.tune_gen = tune_gen_;
+    const int ngroups = (int)groups.size();
+    while ((int)side_.size() < ngroups) {
+        cudaStream_t q = nullptr;
+        check_cuda(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "cudaStreamCreate");
+        side_.push_back(q);
+    }
+    while ((int)ev_.size() < 2 + ngroups) {
+        cudaEvent_t ev = nullptr;
+        check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        ev_.push_back(ev);
+    }
+    // capture: pyramid depths; phase A (tile launch on the capture stream, each streaming
+    // group on a branch forked after the pyramid); join; phase B the same way; join
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t e = cudaSuccess;
-    for (int d = 1; d < max_levels_ && e == cudaSuccess; ++d)
+    auto ok = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
+    for (int d = 1; d < max_levels_; ++d)
         if (pyr_count[d] > 0)
-            e = launch_k(pyramid_batch_k, dim3(pyr_blocks[d]), dim3(256), 0, cap_, (const PyrJob*)(t.d_pyr + pyr_first[d]),
-                         pyr_count[d]);
-    if (e == cudaSuccess && !ja.empty())
-        e = launch_k(tile_batch_k, dim3(blocks_a), dim3(kTileThreads), smem_a, cap_, (const TileJob*)t.d_tile,
-                     (int)ja.size());
-    if (e == cudaSuccess && !jb.empty())
-        e = launch_k(tile_batch_k, dim3(blocks_b), dim3(kTileThreads), smem_b, cap_,
-                     (const TileJob*)(t.d_tile + ja.size()), (int)jb.size());
+            ok(launch_k(pyramid_batch_k, dim3(pyr_blocks[d]), dim3(256), 0, cap_,
+                        (const PyrJob*)(t.d_pyr + pyr_first[d]), pyr_count[d]));
+    std::vector<int> joins;
+    auto branches = [&](int phase, cudaEvent_t fork) {
+        int k = 0;
+        for (auto& kv : groups) {
+            const int i = k++;
+            if (std::get<0>(kv.first) != phase) continue;
+            ok(cudaStreamWaitEvent(side_[i], fork, 0));
+            ok(launch_fused_batch(std::get<1>(kv.first) != 0, std::get<2>(kv.first), std::get<3>(kv.first),
+                                  t.d_stream + sfirst[i], (int)kv.second.size(), group_blocks[kv.first], side_[i]));
+            ok(cudaEventRecord(ev_[2 + i], side_[i]));
+            joins.push_back(i);
+        }
+    };
+    auto join = [&] {
+        for (int i : joins) ok(cudaStreamWaitEvent(cap_, ev_[2 + i], 0));
+        joins.clear();
+    };
+    ok(cudaEventRecord(ev_[0], cap_));
+    branches(0, ev_[0]);
+    if (!ja.empty())
+        ok(launch_k(tile_batch_k, dim3(blocks_a), dim3(kTileThreads), smem_a, cap_, (const TileJob*)t.d_tile,
+                    (int)ja.size()));
+    join();
+    ok(cudaEventRecord(ev_[1], cap_));
+    if (!jb.empty())
+        ok(launch_k(tile_batch_k, dim3(blocks_b), dim3(kTileThreads), smem_b, cap_,
+                    (const TileJob*)(t.d_tile + ja.size()), (int)jb.size()));
+    branches(1, ev_[1]);
+    join();
     cudaError_t ec = cudaStreamEndCapture(cap_, &g);
     check_cuda(e, "batch capture");
     check_cuda(ec, "cudaStreamEndCapture");

@@ -6,14 +6,17 @@
 //
 //   ingest      one kernel copies every stream's frame out of one packed device buffer
 //   pyramid     one launch per pyramid depth, over all streams that have that level
-//   levels A    one tile-fused launch over every top level and every delta level that
-//               reads the previous frame's coarse flow (levels 0..L-3)
-//   levels B    one tile-fused launch over the levels L-2, which read this frame's
-//               unsmoothed top-level flow
+//   levels A    every top level and every delta level that reads the previous frame's
+//               coarse flow (levels 0..L-3)
+//   levels B    the levels L-2, which read this frame's unsmoothed top-level flow
 //
-// Each batched launch walks a device table of jobs (one per stream-level), each job a
-// contiguous range of CTAs.  The pyramid and level launches of a step are replayed from a
-// CUDA graph.  Every stream's results are those of the same stream filtered alone.
+// In each phase the small levels go to one tile-fused launch, and the large ones (as
+// large as the levels a single filter streams) to one streaming-kernel launch per
+// (delta, propagation iterations, smoothing iterations) group; the launches of a phase
+// are branches of the step graph that run side by side.  Each batched launch walks a
+// device table of jobs (one per stream-level), each job a contiguous range of CTAs.  The
+// pyramid and level launches of a step are replayed from a CUDA graph.  Every stream's
+// results are those of the same stream filtered alone.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,12 +48,17 @@ public:
     int launches_per_step() const;
     // advance every stream by one frame read from `frames` (frame_bytes() bytes on the device)
     void step(const void* frames, cudaStream_t s);
+    // levels of at least min_pixels pixels (< 0: the single filter's threshold) run the
+    // streaming kernel in bands of `band` rows (<= 0: chosen per phase); the others the
+    // tile kernel
+    void set_tuning(long min_pixels, int band);
 
 private:
     struct Table;
     void build(Table& t);
     bool matches(const Table& t) const;
     void release_table(Table& t);
+    bool streamed(const Filter& f, int l) const;
 
     std::vector<std::unique_ptr<Filter>> f_;
     std::vector<size_t> off_;
@@ -60,6 +68,11 @@ private:
     std::unique_ptr<Table> tab_[2];
     cudaStream_t cap_ = nullptr;
     int max_levels_ = 0;
+    long min_px_ = -1;
+    int band_ = 0;
+    unsigned long long tune_gen_ = 0;
+    std::vector<cudaStream_t> side_;  // capture branches of the streaming launches
+    std::vector<cudaEvent_t> ev_;     // fork and join events of those branches
 };
 
 }  // namespace ffb

@@ -657,6 +657,13 @@ ff_status ff_batch_launches(const ff_batch* b, int* launches) {
     });
 }
 
+ff_status ff_batch_set_tuning(ff_batch* b, long long min_pixels, int band) {
+    return guard([&] {
+        need(b, "batch");
+        b->impl->set_tuning((long)min_pixels, band);
+    });
+}
+
 ff_status ff_batch_step(ff_batch* b, const void* frames, void* stream) {
     return guard([&] {
         need(b, "batch");

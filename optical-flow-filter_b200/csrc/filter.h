@@ -168,6 +168,8 @@ public:
     LevelArgs level_args(int l) const;
     bool any_first() const;
     int parity() const { return cur_; }
+    // can level l run the streaming fused kernel (instantiated, aligned rows, coarse flow)?
+    bool streaming_ok(int l) const { return fused_ok(l); }
     // block until everything queued on the filter so far has finished
     void wait_done() const;
     // changes whenever a parameter that shapes the level steps changes

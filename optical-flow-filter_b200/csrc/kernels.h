@@ -63,6 +63,21 @@ struct LevelArgs {
 bool fused_available(bool delta, int item, int N, int S);
 cudaError_t launch_fused_level(bool delta, int N, int S, const LevelArgs& a, cudaStream_t s);
 
+// one level of a batched streaming launch (uint8 images): its arguments, its grid of
+// nwx window columns x nby bands of `band` rows, and the first of its blocks
+struct StreamJob {
+    LevelArgs a;
+    int nwx, nby, band;
+    int first_block;
+};
+// the warp grid of a level of W x H pixels cut into bands of `band` rows; returns the
+// blocks it takes
+int fused_warp_grid(int N, int S, int W, int H, int band, int* nwx, int* nby);
+// warps of the streaming kernel resident on the current device at once
+int fused_resident_warps();
+// one launch over jobs (blocks in total) that share (delta, N, S)
+cudaError_t launch_fused_batch(bool delta, int N, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
+
 // ---- tile-fused per-level kernels (tile_level.cu); cfg 0 = automatic tile shape
 int tile_config_count();
 bool tile_available(bool delta, int N, int S, int W, int H, int cfg);

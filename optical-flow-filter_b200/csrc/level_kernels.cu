@@ -1,5 +1,5 @@
 // Dispatch to the fused per-level kernels (level_pipe.cuh, instantiated in level_n*.cu).
-#include "kernels.h"
+#include "level_pipe.cuh"
 
 namespace ffb {
 
@@ -7,6 +7,10 @@ cudaError_t launch_level_n1(bool delta, int item, int S, const LevelArgs& a, cud
 cudaError_t launch_level_n2(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
 cudaError_t launch_level_n3(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
 cudaError_t launch_level_n4(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
+cudaError_t launch_level_batch_n1(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
+cudaError_t launch_level_batch_n2(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
+cudaError_t launch_level_batch_n3(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
+cudaError_t launch_level_batch_n4(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
 
 // instantiated: propagation iterations 1..4, smoothing iterations 1..4; delta levels on
 // uint8 images, top levels on uint8 or float images.  Other combinations run the
@@ -23,6 +27,32 @@ cudaError_t launch_fused_level(bool delta, int N, int S, const LevelArgs& a, cud
         case 2: return launch_level_n2(delta, a.item, S, a, s);
         case 3: return launch_level_n3(delta, a.item, S, a, s);
         case 4: return launch_level_n4(delta, a.item, S, a, s);
+    }
+    return cudaErrorNotSupported;
+}
+
+int fused_warp_grid(int N, int S, int W, int H, int band, int* nwx, int* nby) {
+    const int ox = 64 - 2 * lvl::halo_x(N, S);
+    band = band < 8 ? 8 : band;
+    band = band > H ? H : band;
+    *nwx = (W + ox - 1) / ox;
+    *nby = (H + band - 1) / band;
+    return (*nwx * *nby + lvl::kWarpsPerBlock - 1) / lvl::kWarpsPerBlock;
+}
+
+int fused_resident_warps() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (sms > 0 ? sms : 148) * lvl::kBlocksPerSM * lvl::kWarpsPerBlock;
+}
+
+cudaError_t launch_fused_batch(bool delta, int N, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
+    switch (N) {
+        case 1: return launch_level_batch_n1(delta, S, jobs, n, blocks, s);
+        case 2: return launch_level_batch_n2(delta, S, jobs, n, blocks, s);
+        case 3: return launch_level_batch_n3(delta, S, jobs, n, blocks, s);
+        case 4: return launch_level_batch_n4(delta, S, jobs, n, blocks, s);
     }
     return cudaErrorNotSupported;
 }

@@ -23,6 +23,8 @@
 // per-stage kernels (common.cuh), so results are bit-identical.
 #pragma once
 
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "launch.cuh"
@@ -539,14 +541,11 @@ __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int
 __host__ __device__ constexpr int halo_x(int N, int S) { return ((2 * S + (N > 2 ? N : 2)) + 1) & ~1; }
 __host__ __device__ constexpr int lead_rows(int N, int S) { return 2 * S + (N > 4 - N ? N : 4 - N); }
 
+// warp `warp` of a level's nwx x nby grid of (64-column window, band) warps
 template <bool DELTA, int N, int S, typename P>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int nby, int band) {
+__device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int nby, int band, int warp, char* smem_raw) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
-    extern __shared__ __align__(16) char smem_raw[];
-    grid_dep_wait();
-    grid_dep_launch();
-    const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (warp >= nwx * nby) return;  // whole warps exit together
     const int lane = threadIdx.x & 31;
     const int wx = warp % nwx, by = warp / nwx;
@@ -602,6 +601,50 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(Lev
     (void)rlo;
     (void)rhi;
     run_warp<DELTA, N, S, P, 3>(a, c, i0, iters);
+}
+
+template <bool DELTA, int N, int S, typename P>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int nby, int band) {
+    extern __shared__ __align__(16) char smem_raw[];
+    grid_dep_wait();
+    grid_dep_launch();
+    level_warp<DELTA, N, S, P>(a, nwx, nby, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
+}
+
+// many levels of one (DELTA, N, S) in one launch: each job a contiguous range of blocks
+// (jobs sorted by first_block, the first at 0; a block never spans two jobs)
+template <bool DELTA, int N, int S>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM)
+    level_batch_k(const StreamJob* __restrict__ jobs, int n) {
+    extern __shared__ __align__(16) char smem_raw[];
+    grid_dep_wait();
+    grid_dep_launch();
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].first_block <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const StreamJob& j = jobs[lo];
+    level_warp<DELTA, N, S, uint8_t>(j.a, j.nwx, j.nby, j.band,
+                                     ((int)blockIdx.x - j.first_block) * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
+}
+
+template <bool DELTA, int N, int S>
+cudaError_t launch_batch(const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
+    const int smem = kWarpsPerBlock * kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES);
+    static std::atomic<unsigned long long> prepared{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(prepared.load() & bit)) {
+        const cudaError_t e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>,
+                                                   cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                   (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        prepared.fetch_or(bit);
+    }
+    return launch_k(level_batch_k<DELTA, N, S>, dim3(blocks), dim3(kWarpsPerBlock * 32), smem, s, jobs, n);
 }
 
 template <bool DELTA, int N, int S, typename P>

@@ -590,6 +590,11 @@ class BatchFlowFilter:
         call("ff_batch_launches", self._h, ctypes.byref(n))
         return n.value
 
+    def setTuning(self, minPixels: int = -1, band: int = 0) -> None:
+        """Levels of at least ``minPixels`` pixels run the streaming level kernel in bands of
+        ``band`` rows, the others the tile kernel (-1 / 0: defaults).  Results are unchanged."""
+        call("ff_batch_set_tuning", self._h, int(minPixels), int(band))
+
     def pack(self, frames, out=None):
         """Pack one (H, W) uint8 CUDA tensor per stream into a step buffer (device copies)."""
         torch = _torch()

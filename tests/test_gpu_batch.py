@@ -37,21 +37,28 @@ def ffb(cuda):
     return flowfilter_b200
 
 
-def test_batch_matches_streams_alone(ffb, cuda):
-    t_frames = 8
+def run_against_alone(ffb, cuda, streams, t_frames=8, tuning=None, retune=None, launches=None):
+    """Steps a batch of `streams` and the same streams as single filters over seeded frames
+    and asserts identical flow and image every frame.  tuning / retune: setTuning arguments
+    before the first frame / from frame 3 on."""
     seqs = [case_frames(dict(seq="bumps", frames=t_frames, kw=dict(height=s[0], width=s[1], sigma=1.0, seed=11 + i,
                                                                     n_bumps=2, bump_sigma=max(s[0], s[1]) / 3,
                                                                     amp=2.0)))
-            for i, s in enumerate(STREAMS)]
-    alone = [ffb.PyramidalFlowFilter(s[0], s[1], s[2]) for s in STREAMS]
-    batch = ffb.BatchFlowFilter([s[:3] for s in STREAMS])
-    for f, b, s in zip(alone, [batch.stream(i) for i in range(len(STREAMS))], STREAMS):
+            for i, s in enumerate(streams)]
+    alone = [ffb.PyramidalFlowFilter(s[0], s[1], s[2]) for s in streams]
+    batch = ffb.BatchFlowFilter([s[:3] for s in streams])
+    for f, b, s in zip(alone, [batch.stream(i) for i in range(len(streams))], streams):
         configure(f, s)
         configure(b, s)
-    assert batch.launches() == 1 + (4 - 1) + 2
+    if tuning is not None:
+        batch.setTuning(*tuning)
+    if launches is not None:
+        launches(batch.launches())
     dev = [cuda.from_numpy(q).cuda() for q in seqs]
     buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
     for t in range(t_frames):
+        if t == 3 and retune is not None:
+            batch.setTuning(*retune)
         if t == 5:  # a parameter change rebuilds the batch's job tables
             for f in (alone[2], batch.stream(2)):
                 f.setGamma(1, 7.5)
@@ -65,6 +72,45 @@ def test_batch_matches_streams_alone(ffb, cuda):
             f.compute()
             np.testing.assert_array_equal(batch.stream(i).getFlow(), f.getFlow(), err_msg=f"stream {i} frame {t}")
             np.testing.assert_array_equal(batch.stream(i).getImage(), f.getImage(), err_msg=f"stream {i} frame {t}")
+    return batch
+
+
+def test_batch_matches_streams_alone(ffb, cuda):
+    def launches(n):
+        assert n == 1 + (4 - 1) + 2  # ingest, 3 pyramid depths, the two tile launches
+
+    run_against_alone(ffb, cuda, STREAMS, launches=launches)
+
+
+def test_batch_streaming_launches_match_streams_alone(ffb, cuda):
+    """Every level the streaming kernel can run goes to the batched streaming launches: bands
+    chosen by the batch (one per level at these sizes), then bands of 8 rows from frame 3 on
+    (band seams)."""
+    seen = []
+    run_against_alone(ffb, cuda, STREAMS, tuning=(0, 0), retune=(0, 8), launches=seen.append)
+    assert seen[0] > 1 + (4 - 1) + 2
+
+
+def test_batch_mixed_kernels_match_streams_alone(ffb, cuda):
+    """Levels of at least 3000 pixels stream and the rest tile: both kernels in both phases
+    (top levels and levels L-3.. in phase A, levels L-2 in phase B), 16-row bands; back to
+    the default selection from frame 3 on."""
+    run_against_alone(ffb, cuda, STREAMS, tuning=(3000, 16), retune=(-1, 0))
+
+
+def test_batch_default_selection_streams_large_levels(ffb, cuda):
+    """Levels as large as the ones a single filter streams take the streaming launches by
+    default, beside small streams in the tile launches."""
+    streams = [
+        (480, 640, 2, [10.0, 50.0], [2, 4], 4.0, 3),
+        (544, 960, 1, [20.0], [3], 4.0, 3),
+        (96, 128, 3, [5.0, 20.0, 50.0], [1, 2, 4], 4.0, 2),
+        (480, 640, 3, [5.0, 10.0, 30.0], [1, 1, 2], 4.0, 3),
+        (61, 77, 2, [4.0, 30.0], [1, 3], 2.0, 3),
+    ]
+    seen = []
+    run_against_alone(ffb, cuda, streams, t_frames=6, launches=seen.append)
+    assert seen[0] > 1 + (3 - 1) + 2
 
 
 def test_batch_frame_layout_and_errors(ffb, cuda):
