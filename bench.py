@@ -4,6 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
     python bench.py --profile WORKLOAD --steps K --warmup W     (profiler target only)
     python bench.py --profile-next --steps K --warmup W         (profiler target: FlowToColor, rotation)
+    python bench.py --profile-batched --steps K --warmup W      (profiler target: the 64-stream batched step)
 
 A step is one frame of the PyramidalFlowFilter: the frame (already resident in HBM) is
 loaded into the filter and one compute() runs (pyramid, then one fused kernel per
@@ -801,6 +802,30 @@ def profile_next(args):
     print(json.dumps({"profile": "next", "launches": 2 * args.steps}), flush=True)
 
 
+def profile_batched(args):
+    """A profiler target for the batched step: the 64-stream mix of the `batched` leg runs
+    --warmup untimed steps, then --steps steps inside the NVTX range "timed"."""
+    import torch
+    from flowfilter_b200 import BatchFlowFilter, synthetic
+
+    streams = batched_streams()
+    seqs = [torch.from_numpy(synthetic.seq_bumps(frames=BATCH_RING, height=h, width=w, seed=100 + k)).cuda()
+            for k, (h, w) in enumerate(BATCH_SIZES)]
+    batch = BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
+    for i, s in enumerate(streams):
+        configure_stream(batch.stream(i), s)
+    packed = [batch.pack([seqs[s["size"]][r] for s in streams]) for r in range(BATCH_RING)]
+    for t in range(args.warmup):
+        batch.step(packed[t % BATCH_RING])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    for t in range(args.steps):
+        batch.step(packed[t % BATCH_RING])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "batched", "steps": args.steps, "launches_per_step": batch.launches()}), flush=True)
+
+
 def profile_case(args):
     """A profiler target: the tuned filter of one workload runs --warmup untimed frames, then
     --steps frames inside the NVTX range "timed" (L2 flushed before each), and nothing else."""
@@ -836,6 +861,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--profile-next", action="store_true",
                     help="profiler target: the flow-to-colour and rotational-predictor kernels (no JSON line)")
+    ap.add_argument("--profile-batched", action="store_true",
+                    help="profiler target: steps of the 64-stream batched step (no JSON line)")
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="profiler target: run --steps frames of one workload in the NVTX range 'timed' (no JSON line)")
     args = ap.parse_args()
@@ -843,6 +870,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.profile_next:
         profile_next(args)
+    elif args.profile_batched:
+        profile_batched(args)
     elif args.profile:
         profile_case(args)
     elif args.impl == "reference":
