@@ -329,12 +329,25 @@ void Batch::build(Table& t) {
                 break;
             }
     }
-    for (auto& f : f_) {
+    // which launch of phase A holds each stream's top level (a group key, or the tile
+    // launch), and the streams of each phase-B launch: a phase-B launch waits only for the
+    // phase-A launches holding its streams' top levels
+    std::vector<std::tuple<int, int, int, int>> top_key(f_.size());
+    std::vector<char> top_tiled(f_.size(), 0);
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> group_streams;
+    std::vector<int> jb_streams;
+    for (size_t si = 0; si < f_.size(); ++si) {
+        Filter* f = f_[si].get();
         const int L = f->levels();
         for (int l = 0; l < L; ++l) {
             const Level& v = f->level(l);
+            const std::tuple<int, int, int, int> key{L >= 2 && l == L - 2, v.delta, v.iters, v.smooth};
+            if (l == L - 1) {
+                top_key[si] = key;
+                top_tiled[si] = !streamed(*f, l);
+            }
             if (streamed(*f, l)) {
-                const std::tuple<int, int, int, int> key{L >= 2 && l == L - 2, v.delta, v.iters, v.smooth};
+                group_streams[key].push_back((int)si);
                 StreamJob j{};
                 j.a = f->level_args(l);
                 j.band = std::min(std::max(band, 8), v.H);
@@ -351,11 +364,12 @@ void Batch::build(Table& t) {
             j.g = batch_geom(v.delta, v.iters, v.smooth, v.W, v.H, &smem);
             const int tiles = j.g.tiles_x * ((v.H + j.g.TH - 1) / j.g.TH);
             const bool late = L >= 2 && l == L - 2;
-            // launch B follows launch A (which holds every top level): its jobs wait for A only
-            // before their update, and A lets B's blocks start at once
+            // the tile launch of phase B follows that of phase A on one stream: its jobs wait
+            // for it only before their update, and A lets B's blocks start at once
             j.a.pdl_late_wait = late ? 1 : 0;
             j.a.pdl_early_trigger = late ? 0 : 1;
             if (late) {
+                jb_streams.push_back((int)si);
                 j.first_block = blocks_b;
                 blocks_b += tiles;
                 smem_b = std::max(smem_b, smem);
@@ -397,8 +411,24 @@ void Batch::build(Table& t) {
         check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
         ev_.push_back(ev);
     }
-    // capture: pyramid depths; phase A (tile launch on the capture stream, each streaming
-    // group on a branch forked after the pyramid); join; phase B the same way; join
+    // phase-A launches each phase-B launch waits for (-1: the tile launch)
+    std::map<std::tuple<int, int, int, int>, int> gindex;
+    for (auto& kv : groups) {
+        const int i = (int)gindex.size();
+        gindex[kv.first] = i;
+    }
+    auto deps_of = [&](const std::vector<int>& streams) {
+        std::vector<int> d;
+        for (int si : streams) {
+            const int k = top_tiled[si] ? -1 : gindex.at(top_key[si]);
+            if (std::find(d.begin(), d.end(), k) == d.end()) d.push_back(k);
+        }
+        return d;
+    };
+    // capture: pyramid depths; phase A: the tile launch on the capture stream and each
+    // streaming group on a branch forked after the pyramid; phase B: the tile launch on the
+    // capture stream after phase A's tile launch, and each streaming group on a branch; a
+    // phase-B launch waits for the phase-A launches holding its streams' top levels; join
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t e = cudaSuccess;
@@ -409,35 +439,37 @@ void Batch::build(Table& t) {
         if (pyr_count[d] > 0)
             ok(launch_k(pyramid_batch_k, dim3(pyr_blocks[d]), dim3(256), 0, cap_,
                         (const PyrJob*)(t.d_pyr + pyr_first[d]), pyr_count[d]));
-    std::vector<int> joins;
-    auto branches = [&](int phase, cudaEvent_t fork) {
-        int k = 0;
-        for (auto& kv : groups) {
-            const int i = k++;
-            if (std::get<0>(kv.first) != phase) continue;
-            ok(cudaStreamWaitEvent(side_[i], fork, 0));
-            ok(launch_fused_batch(std::get<1>(kv.first) != 0, std::get<2>(kv.first), std::get<3>(kv.first),
-                                  t.d_stream + sfirst[i], (int)kv.second.size(), group_blocks[kv.first], side_[i]));
-            ok(cudaEventRecord(ev_[2 + i], side_[i]));
-            joins.push_back(i);
-        }
-    };
-    auto join = [&] {
-        for (int i : joins) ok(cudaStreamWaitEvent(cap_, ev_[2 + i], 0));
-        joins.clear();
-    };
     ok(cudaEventRecord(ev_[0], cap_));
-    branches(0, ev_[0]);
+    auto branch = [&](int i, const std::tuple<int, int, int, int>& key, const std::vector<StreamJob>& jobs) {
+        ok(launch_fused_batch(std::get<1>(key) != 0, std::get<2>(key), std::get<3>(key), t.d_stream + sfirst[i],
+                              (int)jobs.size(), group_blocks.at(key), side_[i]));
+        ok(cudaEventRecord(ev_[2 + i], side_[i]));
+    };
+    for (auto& kv : groups) {
+        const int i = gindex[kv.first];
+        if (std::get<0>(kv.first) != 0) continue;
+        ok(cudaStreamWaitEvent(side_[i], ev_[0], 0));
+        branch(i, kv.first, kv.second);
+    }
     if (!ja.empty())
         ok(launch_k(tile_batch_k, dim3(blocks_a), dim3(kTileThreads), smem_a, cap_, (const TileJob*)t.d_tile,
                     (int)ja.size()));
-    join();
-    ok(cudaEventRecord(ev_[1], cap_));
-    if (!jb.empty())
+    ok(cudaEventRecord(ev_[1], cap_));  // phase A's tile launch (or the pyramid) done
+    for (auto& kv : groups) {
+        const int i = gindex[kv.first];
+        if (std::get<0>(kv.first) != 1) continue;
+        ok(cudaStreamWaitEvent(side_[i], ev_[1], 0));
+        for (int k : deps_of(group_streams.at(kv.first)))
+            if (k >= 0) ok(cudaStreamWaitEvent(side_[i], ev_[2 + k], 0));
+        branch(i, kv.first, kv.second);
+    }
+    if (!jb.empty()) {
+        for (int k : deps_of(jb_streams))
+            if (k >= 0) ok(cudaStreamWaitEvent(cap_, ev_[2 + k], 0));
         ok(launch_k(tile_batch_k, dim3(blocks_b), dim3(kTileThreads), smem_b, cap_,
                     (const TileJob*)(t.d_tile + ja.size()), (int)jb.size()));
-    branches(1, ev_[1]);
-    join();
+    }
+    for (int i = 0; i < ngroups; ++i) ok(cudaStreamWaitEvent(cap_, ev_[2 + i], 0));
     cudaError_t ec = cudaStreamEndCapture(cap_, &g);
     check_cuda(e, "batch capture");
     check_cuda(ec, "cudaStreamEndCapture");
