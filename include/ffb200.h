@@ -63,6 +63,12 @@ int ff_version(void);
 /* Select the CUDA device used by filters created afterwards on this thread (the
  * reference pins device 0 in every Stage constructor, src/gpu/pipeline.cu:26). */
 ff_status ff_set_device(int device);
+/* Testing aid (fault injection on the host; no reference counterpart): the library's
+ * device allocations succeed n more times, then the next one fails with
+ * FF_ERR_OUT_OF_MEMORY before CUDA is called, as a failed cudaMalloc would (the reference
+ * exits the process there, src/gpu/error.cu:22); the injection then switches itself off.
+ * n < 0 switches it off.  Process-wide. */
+ff_status ff_debug_fail_allocation_after(long long n);
 
 /* ------------------------------------------------------------ device buffers
  * Replaces GPUImage allocate/upload/download/copyFrom/clear (src/gpu/image.cu:81-197). */

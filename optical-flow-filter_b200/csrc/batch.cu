@@ -139,8 +139,10 @@ template <typename T>
 T* to_device(const std::vector<T>& v) {
     if (v.empty()) return nullptr;
     T* d = nullptr;
-    check_cuda(cudaMalloc(&d, v.size() * sizeof(T)), "batch tables");
-    check_cuda(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "batch tables");
+    check_cuda(device_malloc((void**)&d, v.size() * sizeof(T)), "batch tables");
+    const cudaError_t e = cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) cudaFree(d);
+    check_cuda(e, "batch tables");
     return d;
 }
 
@@ -162,6 +164,18 @@ using StreamGroups = std::map<std::tuple<int, int, int, int>, std::vector<Stream
 Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
     if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: stream count must be positive");
     if (!heights || !widths || !levels) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: null shape arrays");
+    try {
+        init(n, heights, widths, levels);
+    } catch (...) {
+        // a failed constructor runs no destructor: release what init made (the streams'
+        // filters go with f_)
+        if (d_ingest_) cudaFree(d_ingest_);
+        if (cap_) cudaStreamDestroy(cap_);
+        throw;
+    }
+}
+
+void Batch::init(int n, const int* heights, const int* widths, const int* levels) {
     check_cuda(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
     std::vector<IngestJob> ing;
     int blocks = 0;

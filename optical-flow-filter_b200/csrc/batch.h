@@ -55,6 +55,7 @@ public:
 
 private:
     struct Table;
+    void init(int n, const int* heights, const int* widths, const int* levels);
     void build(Table& t);
     bool matches(const Table& t) const;
     void release_table(Table& t);

@@ -118,8 +118,12 @@ ff_status ff_malloc_pitch(void** dptr, size_t* pitch, size_t width_bytes, size_t
     return guard([&] {
         need(dptr, "pointer");
         need(pitch, "pitch");
-        ffb::check_cuda(cudaMallocPitch(dptr, pitch, width_bytes, height), "cudaMallocPitch");
+        ffb::check_cuda(ffb::device_malloc_pitch(dptr, pitch, width_bytes, height), "cudaMallocPitch");
     });
+}
+
+ff_status ff_debug_fail_allocation_after(long long n) {
+    return guard([&] { ffb::inject_allocation_failure(n); });
 }
 
 ff_status ff_free(void* dptr) {

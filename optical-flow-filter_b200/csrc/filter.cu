@@ -8,6 +8,7 @@
 // is: coarse(h) = fs[cur] of level h+1, or fu of the top level for h = L-2.
 #include "filter.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -21,6 +22,30 @@ void check_cuda(cudaError_t e, const char* what) {
     throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+namespace {
+std::atomic<long long> g_alloc_fail_after{-1};
+
+// true for the allocation that the injection fails (one-shot)
+bool allocation_fails() {
+    long long n = g_alloc_fail_after.load();
+    while (n >= 0)
+        if (g_alloc_fail_after.compare_exchange_weak(n, n - 1)) return n == 0;
+    return false;
+}
+}  // namespace
+
+void inject_allocation_failure(long long n) { g_alloc_fail_after.store(n < 0 ? -1 : n); }
+
+cudaError_t device_malloc(void** p, size_t bytes) {
+    if (allocation_fails()) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t device_malloc_pitch(void** p, size_t* pitch, size_t width_bytes, size_t height) {
+    if (allocation_fails()) return cudaErrorMemoryAllocation;
+    return cudaMallocPitch(p, pitch, width_bytes, height);
+}
+
 // Rows are allocated with room for one extra pixel (and a 4-byte multiple), so the fused
 // kernels' aligned pair copies of columns (W-1, W) stay inside the allocation.
 void Buf::alloc(int h_, int w_, int bpp_) {
@@ -30,7 +55,7 @@ void Buf::alloc(int h_, int w_, int bpp_) {
     bpp = bpp_;
     if (h <= 0 || w <= 0) return;
     const size_t row = ((size_t)(w + 1) * bpp + 3) & ~(size_t)3;
-    check_cuda(cudaMallocPitch(&p, &pitch, row, (size_t)h), "cudaMallocPitch");
+    check_cuda(device_malloc_pitch(&p, &pitch, row, (size_t)h), "cudaMallocPitch");
     check_cuda(cudaMemset2D(p, pitch, 0, row, (size_t)h), "cudaMemset2D");
 }
 

@@ -30,6 +30,14 @@ struct Error : std::runtime_error {
 
 void check_cuda(cudaError_t e, const char* what);
 
+// Every device allocation of the library goes through these two.  For fault-injection
+// tests, inject_allocation_failure(n) lets n more allocations succeed and fails the next
+// one with cudaErrorMemoryAllocation before CUDA is called (then switches itself off);
+// n < 0 switches it off.
+cudaError_t device_malloc(void** p, size_t bytes);
+cudaError_t device_malloc_pitch(void** p, size_t* pitch, size_t width_bytes, size_t height);
+void inject_allocation_failure(long long n);
+
 // pitched device buffer (owning)
 struct Buf {
     void* p = nullptr;

@@ -137,6 +137,7 @@ SIGNATURES = {
     "ff_batch_frame_layout": (_st, [_vp, _szp, _szp]),
     "ff_batch_launches": (_st, [_vp, _ip]),
     "ff_batch_step": (_st, [_vp, _vp, _vp]),
+    "ff_debug_fail_allocation_after": (_st, [ctypes.c_longlong]),
     "ff_batch_set_tuning": (_st, [_vp, ctypes.c_longlong, _i]),
     "ff_diff_pyramid": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),
     "ff_diff_pyramid_bwd": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),

@@ -33,6 +33,13 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
 
 
+def test_allocation_failure_injection_switches_on_and_off():
+    L = _lib.lib()
+    assert L.ff_debug_fail_allocation_after(3) == _lib.FF_OK
+    assert L.ff_debug_fail_allocation_after(-1) == _lib.FF_OK
+    assert L.ff_debug_fail_allocation_after(-5) == _lib.FF_OK
+
+
 def test_version_and_status_strings():
     L = _lib.lib()
     assert L.ff_version() >= 10000

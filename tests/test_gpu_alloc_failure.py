@@ -1,0 +1,135 @@
+"""Device allocation failures, injected on the host (ff_debug_fail_allocation_after):
+every allocation a filter or a batch makes can fail; the call reports FF_ERR_OUT_OF_MEMORY,
+releases what it had made (no device memory leaks) and the library keeps working. The
+reference exits the process on any CUDA error (src/gpu/error.cu:15-24)."""
+
+from __future__ import annotations
+
+import ctypes
+import gc
+
+import numpy as np
+import pytest
+
+from make_reference_fixtures import case_frames
+
+pytestmark = pytest.mark.gpu
+
+# device memory the driver may keep or release late across create/destroy cycles; a leaked
+# level-0 buffer of the 1080x1920 filters below is 8 to 17 MB
+SLACK = 8 << 20
+
+
+@pytest.fixture
+def ffb(cuda):
+    import flowfilter_b200
+
+    return flowfilter_b200
+
+
+@pytest.fixture
+def inject(ffb):
+    from flowfilter_b200 import _lib
+
+    lib = _lib.lib()
+    yield lambda n: _lib.check(lib.ff_debug_fail_allocation_after(n))
+    lib.ff_debug_fail_allocation_after(-1)
+
+
+def free_bytes(cuda):
+    """Free device memory, after Python has dropped unreachable objects and torch has
+    returned its cached blocks."""
+    gc.collect()
+    cuda.cuda.synchronize()
+    cuda.cuda.empty_cache()
+    return cuda.cuda.mem_get_info()[0]
+
+
+def fail_until_created(ffb, cuda, inject, create, limit=400):
+    """Fails allocation 0, 1, 2, ... of create() until it succeeds; checks each failure's
+    status and that no device memory stays allocated. Returns (object, allocations)."""
+    from flowfilter_b200._lib import FF_ERR_OUT_OF_MEMORY, FFError
+
+    free0 = free_bytes(cuda)
+    n = 0
+    while True:
+        inject(n)
+        try:
+            obj = create()
+        except FFError as e:
+            assert e.status == FF_ERR_OUT_OF_MEMORY, str(e)
+            assert "out of memory" in str(e)
+            assert free_bytes(cuda) >= free0 - SLACK, f"device memory leaked after failing allocation {n}"
+            n += 1
+            assert n < limit
+            continue
+        inject(-1)
+        return obj, n
+
+
+def frames(h, w, t, seed):
+    return case_frames(dict(seq="bumps", frames=t, kw=dict(height=h, width=w, sigma=1.0, seed=seed, n_bumps=2,
+                                                          bump_sigma=max(h, w) / 3, amp=2.0)))
+
+
+def test_filter_creation_survives_every_allocation_failure(ffb, cuda, inject):
+    free0 = free_bytes(cuda)
+    f, n = fail_until_created(ffb, cuda, inject, lambda: ffb.PyramidalFlowFilter(1080, 1920, 2))
+    assert n >= 10  # input image, pyramid image, per-level state
+    ref = ffb.PyramidalFlowFilter(1080, 1920, 2)
+    for flt in (f, ref):
+        flt.gamma = [10.0, 50.0]
+        flt.smoothIterations = [2, 4]
+        flt.maxflow = 4.0
+    for img in frames(1080, 1920, 3, 5):
+        for flt in (f, ref):
+            flt.loadImage(img)
+            flt.compute()
+        np.testing.assert_array_equal(f.getFlow(), ref.getFlow())
+    del f, ref, flt
+    assert free_bytes(cuda) >= free0 - SLACK
+
+
+def test_batch_creation_and_rebuild_survive_allocation_failures(ffb, cuda, inject):
+    from flowfilter_b200._lib import FF_ERR_OUT_OF_MEMORY, FFError
+
+    shapes = [(1080, 1920, 2), (480, 640, 3), (240, 320, 1)]
+    free0 = free_bytes(cuda)
+    batch, n = fail_until_created(ffb, cuda, inject, lambda: ffb.BatchFlowFilter(shapes))
+    assert n >= 3 * 5
+    alone = [ffb.PyramidalFlowFilter(*s) for s in shapes]
+    for f in alone + [batch.stream(i) for i in range(len(shapes))]:
+        f.maxflow = 4.0
+    seqs = [frames(h, w, 4, 20 + i) for i, (h, w, _) in enumerate(shapes)]
+    dev = [cuda.from_numpy(q).cuda() for q in seqs]
+    buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
+    for t in range(4):
+        batch.pack([d[t] for d in dev], out=buf)
+        if t == 1:
+            # the first batched step builds the job tables: fail their first allocation
+            inject(0)
+            with pytest.raises(FFError) as err:
+                batch.step(buf)
+            assert err.value.status == FF_ERR_OUT_OF_MEMORY
+            del err  # its traceback holds the batch
+            inject(-1)
+        batch.step(buf)
+        cuda.cuda.synchronize()
+        for i, f in enumerate(alone):
+            f.loadImage(seqs[i][t])
+            f.compute()
+            np.testing.assert_array_equal(batch.stream(i).getFlow(), f.getFlow(), err_msg=f"stream {i} frame {t}")
+    del batch, alone, buf, dev, f
+    assert free_bytes(cuda) >= free0 - SLACK
+
+
+def test_malloc_pitch_failure(ffb, cuda, inject):
+    from flowfilter_b200 import _lib
+
+    lib = _lib.lib()
+    p, pitch = ctypes.c_void_p(), ctypes.c_size_t()
+    inject(0)
+    assert lib.ff_malloc_pitch(ctypes.byref(p), ctypes.byref(pitch), 640, 480) == _lib.FF_ERR_OUT_OF_MEMORY
+    assert lib.ff_malloc_pitch(ctypes.byref(p), ctypes.byref(pitch), 640, 480) == _lib.FF_OK  # one-shot
+    assert pitch.value >= 640
+    assert lib.ff_free(p) == _lib.FF_OK
