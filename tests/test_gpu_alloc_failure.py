@@ -18,6 +18,9 @@ pytestmark = pytest.mark.gpu
 # device memory the driver may keep or release late across create/destroy cycles; a leaked
 # level-0 buffer of the 1080x1920 filters below is 8 to 17 MB
 SLACK = 8 << 20
+# after a batch has stepped: kernels loaded on their first launch stay resident (about
+# 10 MB measured on B200), while the batch below holds over 100 MB
+STEPPED_SLACK = 64 << 20
 
 
 @pytest.fixture
@@ -120,7 +123,7 @@ def test_batch_creation_and_rebuild_survive_allocation_failures(ffb, cuda, injec
             f.compute()
             np.testing.assert_array_equal(batch.stream(i).getFlow(), f.getFlow(), err_msg=f"stream {i} frame {t}")
     del batch, alone, buf, dev, f
-    assert free_bytes(cuda) >= free0 - SLACK
+    assert free_bytes(cuda) >= free0 - STEPPED_SLACK
 
 
 def test_malloc_pitch_failure(ffb, cuda, inject):
