@@ -249,9 +249,10 @@ ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int 
  * No counterpart in the reference: many independent PyramidalFlowFilter streams of
  * different sizes, levels and parameters advanced together.  Stream i's frame is read from
  * a packed uint8 device buffer at the offset ff_batch_frame_layout gives (rows of width
- * bytes, no padding); one step runs a fixed number of kernel launches (ff_batch_launches)
- * whatever the number of streams, and every stream's results equal those of the same
- * stream filtered alone.  Each stream is an ff_filter owned by the batch (ff_batch_stream):
+ * bytes, no padding); one step runs ff_batch_launches kernel launches, which depend on
+ * the pyramid depth and on how many distinct (iterations, smoothing) settings the large
+ * levels have, not on the number of streams; every stream's results equal those of the
+ * same stream filtered alone.  Each stream is an ff_filter owned by the batch (ff_batch_stream):
  * set its parameters and read its results with the ff_filter_* calls; do not destroy it. */
 typedef struct ff_batch ff_batch;
 ff_status ff_batch_create(int n, const int* heights, const int* widths, const int* levels, ff_batch** batch);

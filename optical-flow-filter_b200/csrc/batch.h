@@ -1,8 +1,8 @@
 // Batched step over many independent flow-filter streams (no reference counterpart).
 //
 // A Batch owns one pyramidal Filter per stream; streams differ in size, levels and
-// parameters.  One step advances every stream by one frame with a fixed number of kernel
-// launches, whatever the number of streams:
+// parameters.  One step advances every stream by one frame with a number of kernel launches
+// that does not grow with the number of streams:
 //
 //   ingest      one kernel copies every stream's frame out of one packed device buffer
 //   pyramid     one launch per pyramid depth, over all streams that have that level

@@ -542,8 +542,8 @@ class BatchFlowFilter:
     getFlow() / getFlowDevice()); ``step(frames)`` advances every stream by one frame, where
     ``frames`` is one uint8 CUDA tensor of ``frameBytes()`` bytes holding stream i's frame
     at ``frameOffsets()[i]`` (``pack()`` builds it from a list of (H, W) tensors).  A step
-    runs ``launches()`` kernels whatever the number of streams; every stream's results
-    equal those of the same stream filtered alone.
+    runs ``launches()`` kernels, a number that does not grow with the number of streams;
+    every stream's results equal those of the same stream filtered alone.
     """
 
     def __init__(self, shapes):
