@@ -46,10 +46,10 @@ for _p in (ROOT, PKG):
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    # the reference's published notebook configuration
+    # the reference's published notebook configuration (notebooks/GPU_example.ipynb)
     "rotzoom_640x480_L2": dict(seq="rotzoom", H=480, W=640, levels=2, gamma=[10.0, 50.0], smooth=[2, 4],
                                maxflow=4.0, ring=96),
-    # BASELINE configuration 2: camera-sensor size, 3 levels (throughput / roofline run)
+    # camera-sensor size, 3 levels (throughput / roofline run)
     "bumps_2048x1088_L3": dict(seq="bumps", H=1088, W=2048, levels=3, gamma=[5.0, 20.0, 50.0], smooth=[1, 2, 4],
                                maxflow=4.0, ring=24),
 }
