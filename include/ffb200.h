@@ -188,6 +188,16 @@ ff_status ff_filter_compute_image_model(ff_filter* f);
 ff_status ff_filter_compute_propagation(ff_filter* f);
 ff_status ff_filter_compute_update(ff_filter* f);
 ff_status ff_filter_elapsed_ms(const ff_filter* f, float* ms);
+/* Checkpoint and resume (no counterpart in the reference, whose filter state lives only in
+ * device buffers): the state of the latest frame as a host byte image of
+ * ff_filter_state_bytes bytes.  It holds per level the smoothed flow, the old image, the
+ * delta flow (delta levels) or the unsmoothed flow (top level), and whether the level has
+ * seen a frame.  Importing it into a filter of the same kind and level sizes continues that
+ * stream exactly; parameters (gamma, maxflow, ...) are not part of it.  Both calls wait for
+ * the filter's queued work and must come between frames. */
+ff_status ff_filter_state_bytes(const ff_filter* f, size_t* bytes);
+ff_status ff_filter_export_state(ff_filter* f, void* host, size_t bytes);
+ff_status ff_filter_import_state(ff_filter* f, const void* host, size_t bytes);
 
 /* downloadFlow (flowfilter.cu:238-240, 734-741): level-0 smoothed flow, H x W x 2 floats. */
 ff_status ff_filter_download_flow_host(ff_filter* f, ff_image* flow);

@@ -416,6 +416,21 @@ ff_status ff_filter_elapsed_ms(const ff_filter* f, float* ms) {
     });
 }
 
+ff_status ff_filter_state_bytes(const ff_filter* f, size_t* bytes) {
+    return guard([&] {
+        need(bytes, "bytes");
+        *bytes = cget(f)->state_bytes();
+    });
+}
+
+ff_status ff_filter_export_state(ff_filter* f, void* host, size_t bytes) {
+    return guard([&] { get(f)->export_state(host, bytes); });
+}
+
+ff_status ff_filter_import_state(ff_filter* f, const void* host, size_t bytes) {
+    return guard([&] { get(f)->import_state(host, bytes); });
+}
+
 ff_status ff_filter_download_flow_host(ff_filter* f, ff_image* flow) {
     return guard([&] {
         need(flow, "flow");

@@ -11,6 +11,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "kernels.h"
 
@@ -1108,6 +1109,104 @@ void Filter::level_state(int l, int which, void* dst, size_t dst_pitch) {
                "level state");
     end_on(stream_);
     check_cuda(cudaStreamSynchronize(stream_), "level state");
+}
+
+// ------------------------------------------------------------------ state export / import
+// Layout: StateHeader, then per level a StateLevel, then per level the rows of its smoothed
+// flow (W float2), old image (W float) and delta flow (delta levels) or unsmoothed flow
+// (the top level, read by getFlow of a single-level filter) (W float2), each packed without
+// padding.
+namespace {
+constexpr char kStateMagic[8] = {'F', 'F', 'B', 'S', 'T', 'A', 'T', 'E'};
+constexpr uint32_t kStateVersion = 1;
+struct StateHeader {
+    char magic[8];
+    uint32_t version, kind, levels, reserved;
+};
+struct StateLevel {
+    uint32_t H, W, delta, first;
+};
+}  // namespace
+
+size_t Filter::state_bytes() const {
+    size_t n = sizeof(StateHeader) + (size_t)L_ * sizeof(StateLevel);
+    for (const Level& v : lv_) n += (size_t)v.H * v.W * (8 + 4 + 8);
+    return n;
+}
+
+void Filter::export_state(void* host, size_t bytes) const {
+    if (!host) throw Error(FF_ERR_INVALID_ARGUMENT, "null state buffer");
+    if (bytes < state_bytes())
+        throw Error(FF_ERR_INVALID_ARGUMENT, "state buffer too small: " + std::to_string(bytes) + " < " +
+                                                 std::to_string(state_bytes()));
+    if (phase_ != 0) throw Error(FF_ERR_LOGIC, "the state can be exported between frames only");
+    wait_done();
+    unsigned char* out = static_cast<unsigned char*>(host);
+    StateHeader h{};
+    std::memcpy(h.magic, kStateMagic, sizeof(h.magic));
+    h.version = kStateVersion;
+    h.kind = (uint32_t)kind_;
+    h.levels = (uint32_t)L_;
+    std::memcpy(out, &h, sizeof(h));
+    out += sizeof(h);
+    for (const Level& v : lv_) {
+        const StateLevel sl{(uint32_t)v.H, (uint32_t)v.W, v.delta ? 1u : 0u, v.first ? 1u : 0u};
+        std::memcpy(out, &sl, sizeof(sl));
+        out += sizeof(sl);
+    }
+    for (const Level& v : lv_) {
+        const Buf* bufs[3] = {&v.fs[cur_], &v.io[cur_], v.delta ? &v.d[cur_] : &v.fu};
+        for (const Buf* b : bufs) {
+            const size_t row = b->row_bytes();
+            check_cuda(cudaMemcpy2DAsync(out, row, b->p, b->pitch, row, (size_t)b->h, cudaMemcpyDeviceToHost,
+                                         stream_),
+                       "export state");
+            out += row * b->h;
+        }
+    }
+    check_cuda(cudaStreamSynchronize(stream_), "export state");
+}
+
+void Filter::import_state(const void* host, size_t bytes) {
+    if (!host) throw Error(FF_ERR_INVALID_ARGUMENT, "null state buffer");
+    if (phase_ != 0) throw Error(FF_ERR_LOGIC, "the state can be imported between frames only");
+    const unsigned char* in = static_cast<const unsigned char*>(host);
+    StateHeader h{};
+    if (bytes < sizeof(h)) throw Error(FF_ERR_SHAPE, "state image too short");
+    std::memcpy(&h, in, sizeof(h));
+    if (std::memcmp(h.magic, kStateMagic, sizeof(h.magic)) != 0 || h.version != kStateVersion)
+        throw Error(FF_ERR_INVALID_ARGUMENT, "not a filter state image (or another version)");
+    if (h.kind != (uint32_t)kind_ || h.levels != (uint32_t)L_)
+        throw Error(FF_ERR_SHAPE, "state image of another filter kind or level count");
+    if (bytes != state_bytes())
+        throw Error(FF_ERR_SHAPE, "state image size " + std::to_string(bytes) + ", this filter's is " +
+                                      std::to_string(state_bytes()));
+    in += sizeof(h);
+    std::vector<StateLevel> sl(L_);
+    for (int l = 0; l < L_; ++l) {
+        std::memcpy(&sl[l], in, sizeof(StateLevel));
+        in += sizeof(StateLevel);
+        const Level& v = lv_[l];
+        if (sl[l].H != (uint32_t)v.H || sl[l].W != (uint32_t)v.W || sl[l].delta != (v.delta ? 1u : 0u))
+            throw Error(FF_ERR_SHAPE, "state image level " + std::to_string(l) + " has another size");
+    }
+    wait_done();
+    for (int l = 0; l < L_; ++l) {
+        Level& v = lv_[l];
+        Buf* bufs[3] = {&v.fs[cur_], &v.io[cur_], v.delta ? &v.d[cur_] : &v.fu};
+        for (Buf* b : bufs) {
+            const size_t row = b->row_bytes();
+            check_cuda(cudaMemcpy2DAsync(b->p, b->pitch, in, row, row, (size_t)b->h, cudaMemcpyHostToDevice,
+                                         stream_),
+                       "import state");
+            in += row * b->h;
+        }
+        v.first = sl[l].first != 0;
+    }
+    // the copies are complete before any later work on any stream reads the state
+    check_cuda(cudaStreamSynchronize(stream_), "import state");
+    // the frame graphs hold the levels' first-frame flags; a batch rebuilds its tables
+    drop_graphs();
 }
 
 }  // namespace ffb

@@ -171,6 +171,15 @@ public:
         drop_graphs();
     }
 
+    // ---- checkpoint and resume: the state of the latest frame (per level the smoothed flow,
+    // the old image, the delta flow of delta levels or the unsmoothed flow of the top level,
+    // and whether the level has seen a frame) as a host byte image; importing it into a
+    // filter of the same kind and level sizes continues that stream exactly.  Parameters are
+    // not part of the state.
+    size_t state_bytes() const;
+    void export_state(void* host, size_t bytes) const;
+    void import_state(const void* host, size_t bytes);
+
     // ---- stepping by a Batch (batch.cu), which launches this filter's level steps itself
     // kernel arguments of level l for the next frame (state copy cur -> cur ^ 1)
     LevelArgs level_args(int l) const;

@@ -113,6 +113,9 @@ SIGNATURES = {
     "ff_filter_compute_propagation": (_st, [_vp]),
     "ff_filter_compute_update": (_st, [_vp]),
     "ff_filter_elapsed_ms": (_st, [_vp, _fp]),
+    "ff_filter_state_bytes": (_st, [_vp, _szp]),
+    "ff_filter_export_state": (_st, [_vp, _vp, _sz]),
+    "ff_filter_import_state": (_st, [_vp, _vp, _sz]),
     "ff_filter_download_flow_host": (_st, [_vp, ctypes.POINTER(FFImage)]),
     "ff_filter_download_image_host": (_st, [_vp, ctypes.POINTER(FFImage)]),
     "ff_filter_device_result": (_st, [_vp, _i, _vpp, _szp]),

@@ -163,6 +163,21 @@ class _FilterBase:
         call("ff_filter_elapsed_ms", self._h, ctypes.byref(ms))
         return ms.value
 
+    def exportState(self) -> np.ndarray:
+        """The filter's state after its latest frame as a uint8 array (checkpoint): per level
+        the smoothed flow, old image, delta or unsmoothed flow and the first-frame flag.
+        Parameters are not part of it."""
+        n = ctypes.c_size_t()
+        call("ff_filter_state_bytes", self._h, ctypes.byref(n))
+        out = np.empty(n.value, dtype=np.uint8)
+        call("ff_filter_export_state", self._h, out.ctypes.data_as(ctypes.c_void_p), n.value)
+        return out
+
+    def importState(self, state) -> None:
+        """Resume from exportState() of a filter of the same kind and level sizes."""
+        a = np.ascontiguousarray(np.asarray(state, dtype=np.uint8).reshape(-1))
+        call("ff_filter_import_state", self._h, a.ctypes.data_as(ctypes.c_void_p), a.size)
+
     def getFlow(self, flow: np.ndarray | None = None) -> np.ndarray:
         """Smoothed level-0 flow as (H, W, 2) float32 (downloadFlow, flowfilter.cu:238-240)."""
         if flow is None:

@@ -40,6 +40,15 @@ def test_allocation_failure_injection_switches_on_and_off():
     assert L.ff_debug_fail_allocation_after(-5) == _lib.FF_OK
 
 
+def test_state_calls_reject_null_handles():
+    L = _lib.lib()
+    n = ctypes.c_size_t()
+    buf = (ctypes.c_uint8 * 16)()
+    assert L.ff_filter_state_bytes(None, ctypes.byref(n)) == _lib.FF_ERR_INVALID_ARGUMENT
+    assert L.ff_filter_export_state(None, buf, 16) == _lib.FF_ERR_INVALID_ARGUMENT
+    assert L.ff_filter_import_state(None, buf, 16) == _lib.FF_ERR_INVALID_ARGUMENT
+
+
 def test_version_and_status_strings():
     L = _lib.lib()
     assert L.ff_version() >= 10000
