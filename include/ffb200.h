@@ -57,6 +57,14 @@ typedef struct ff_filter ff_filter; /* opaque: a single-level, delta-level or py
 
 /* ------------------------------------------------------------ library */
 const char* ff_last_error(void);
+/* Opt-in log.  The reference prints to stdout and stderr (a "first load" line on the first
+ * frame, flowfilter.cu:133; parameter errors); this library is silent unless a callback is
+ * set.  FF_LOG_ERROR: the message of every failing call (also kept for ff_last_error);
+ * FF_LOG_INFO: a batch (re)building its step graph.  The callback runs on the thread that
+ * made the call, under no lock of the library; NULL switches the log off. */
+typedef void (*ff_log_fn)(int level, const char* message, void* user);
+enum { FF_LOG_ERROR = 0, FF_LOG_INFO = 1 };
+ff_status ff_set_log_callback(ff_log_fn fn, void* user);
 const char* ff_status_string(ff_status s);
 /* Library version as an integer (major*10000 + minor*100 + patch). */
 int ff_version(void);

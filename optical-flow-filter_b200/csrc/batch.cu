@@ -490,6 +490,9 @@ void Batch::build(Table& t) {
     e = cudaGraphInstantiateWithFlags(&t.graph, g, 0);
     cudaGraphDestroy(g);
     check_cuda(e, "cudaGraphInstantiate");
+    log_message(FF_LOG_INFO, "batch: step graph built for " + std::to_string(f_.size()) + " streams, " +
+                                 std::to_string(launches_per_step()) + " launches, streaming band " +
+                                 std::to_string(band) + " rows");
 }
 
 void Batch::step(const void* frames, cudaStream_t s) {

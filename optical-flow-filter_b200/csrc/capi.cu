@@ -35,8 +35,14 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// the opt-in log callback (ff_set_log_callback)
+std::mutex g_log_mutex;
+ff_log_fn g_log_fn = nullptr;
+void* g_log_user = nullptr;
+
 ff_status fail(ff_status s, const std::string& msg) {
     g_last_error = msg;
+    ffb::log_message(FF_LOG_ERROR, std::string(ff_status_string(s)) + ": " + msg);
     return s;
 }
 
@@ -86,12 +92,32 @@ void check_stage_dims(int h, int w) {
 
 }  // namespace
 
+namespace ffb {
+void log_message(int level, const std::string& msg) {
+    ff_log_fn fn;
+    void* user;
+    {
+        std::lock_guard<std::mutex> lock(g_log_mutex);
+        fn = g_log_fn;
+        user = g_log_user;
+    }
+    if (fn) fn(level, msg.c_str(), user);
+}
+}  // namespace ffb
+
 // last-error setter for entry points defined in other files (diff_kernels.cu)
 void ffb_set_last_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" {
 
 const char* ff_last_error(void) { return g_last_error.c_str(); }
+
+ff_status ff_set_log_callback(ff_log_fn fn, void* user) {
+    std::lock_guard<std::mutex> lock(g_log_mutex);
+    g_log_fn = fn;
+    g_log_user = user;
+    return FF_OK;
+}
 
 const char* ff_status_string(ff_status s) {
     switch (s) {

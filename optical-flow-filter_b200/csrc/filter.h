@@ -30,6 +30,9 @@ struct Error : std::runtime_error {
 
 void check_cuda(cudaError_t e, const char* what);
 
+// sends a message to the caller's log callback, if one is set (ff_set_log_callback)
+void log_message(int level, const std::string& msg);
+
 // Every device allocation of the library goes through these two.  For fault-injection
 // tests, inject_allocation_failure(n) lets n more allocations succeed and fails the next
 // one with cudaErrorMemoryAllocation before CUDA is called (then switches itself off);

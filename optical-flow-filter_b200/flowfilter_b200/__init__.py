@@ -8,7 +8,7 @@ encodes a flow field; ``RotationalFlowImagePredictor`` and ``LaxWendroffPropagat
 predict an image under camera rotation.
 """
 
-from ._lib import FFError, FFIndexError, FFLogicError, FFValueError, lib  # noqa: F401
+from ._lib import FFError, FFIndexError, FFLogicError, FFValueError, lib, set_log_callback  # noqa: F401
 from .display import FlowToColor, color_wheel  # noqa: F401
 from .rotation import (LaxWendroffPropagator, PerspectiveCamera, RotationalFlowImagePredictor,  # noqa: F401
                        createPerspectiveCamera)
@@ -31,4 +31,5 @@ __all__ = [
     "FFLogicError",
     "device_view",
     "lib",
+    "set_log_callback",
 ]

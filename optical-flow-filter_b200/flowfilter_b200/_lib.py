@@ -64,9 +64,13 @@ _fp = ctypes.POINTER(ctypes.c_float)
 _szp = ctypes.POINTER(ctypes.c_size_t)
 _vpp = ctypes.POINTER(ctypes.c_void_p)
 _st = ctypes.c_int
+LOG_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p)
+FF_LOG_ERROR = 0
+FF_LOG_INFO = 1
 
 SIGNATURES = {
     "ff_last_error": (ctypes.c_char_p, []),
+    "ff_set_log_callback": (_st, [LOG_FN, _vp]),
     "ff_status_string": (ctypes.c_char_p, [_st]),
     "ff_version": (_i, []),
     "ff_set_device": (_st, [_i]),
@@ -209,3 +213,19 @@ def check(status: int) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(lib(), name)(*args))
+
+
+_log_callback = None  # the ctypes thunk the library holds, kept alive here
+
+
+def set_log_callback(fn) -> None:
+    """Send the library's log to ``fn(level, message)`` (level FF_LOG_ERROR or FF_LOG_INFO;
+    message a str); ``None`` switches it off.  The library is silent by default."""
+    global _log_callback
+    if fn is None:
+        call("ff_set_log_callback", LOG_FN(), None)
+        _log_callback = None
+        return
+    thunk = LOG_FN(lambda level, msg, user: fn(int(level), msg.decode(errors="replace")))
+    call("ff_set_log_callback", thunk, None)
+    _log_callback = thunk

@@ -49,6 +49,19 @@ def test_state_calls_reject_null_handles():
     assert L.ff_filter_import_state(None, buf, 16) == _lib.FF_ERR_INVALID_ARGUMENT
 
 
+def test_log_callback_receives_errors_until_switched_off():
+    seen = []
+    ffb.set_log_callback(lambda level, msg: seen.append((level, msg)))
+    try:
+        assert _lib.lib().ff_filter_compute(None) == _lib.FF_ERR_INVALID_ARGUMENT
+        assert seen == [(_lib.FF_LOG_ERROR, "invalid argument: null filter")]
+        assert _lib.lib().ff_last_error().decode() == "null filter"
+    finally:
+        ffb.set_log_callback(None)
+    assert _lib.lib().ff_filter_compute(None) == _lib.FF_ERR_INVALID_ARGUMENT
+    assert len(seen) == 1  # silent again
+
+
 def test_version_and_status_strings():
     L = _lib.lib()
     assert L.ff_version() >= 10000
