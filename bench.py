@@ -8,13 +8,15 @@
 
 A step is one frame of the PyramidalFlowFilter: the frame (already resident in HBM) is
 loaded into the filter and one compute() runs (pyramid, then one fused kernel per
-level; CUDA-graph replay).  The primary workload is the reference's published
-configuration: 640x480 uint8 frames, 2 levels, gamma [10, 50], smoothing [2, 4],
-maxflow 4, on a synthetic rotation+zoom sequence (seeded) standing in for the
-reference's Blender sequence.  The 2048x1088 3-level throughput workload is reported
-beside it under "extra", and the 64-stream mixed-size batched step (BatchFlowFilter,
-against the same 64 streams looped as single filters) under "batched", and the
-differentiable filter's forward and forward+backward time under "differentiable".
+level; CUDA-graph replay).  The primary workload is the throughput run: 2048x1088 uint8
+frames (the camera-sensor size), 3 levels, gamma [5, 20, 50], smoothing [1, 2, 4],
+maxflow 4, on a seeded synthetic sequence (blurred noise plus sensor noise, moved by a
+smooth field of Gaussian bumps).  The reference's published configuration (640x480,
+2 levels, gamma [10, 50], smoothing [2, 4], on a seeded rotation+zoom sequence standing in
+for the reference's Blender sequence) is reported beside it under "extra", the 64-stream
+mixed-size batched step (BatchFlowFilter, against the same 64 streams looped as single
+filters) under "batched", and the differentiable filter's forward and forward+backward
+time under "differentiable".
 
 Timing: every step is bracketed by CUDA events on the filter's stream and the L2 is
 flushed (a 256 MiB write) between steps outside those events, so every frame reads its
@@ -53,13 +55,29 @@ WORKLOADS = {
     "bumps_2048x1088_L3": dict(seq="bumps", H=1088, W=2048, levels=3, gamma=[5.0, 20.0, 50.0], smooth=[1, 2, 4],
                                maxflow=4.0, ring=24),
 }
-PRIMARY = "rotzoom_640x480_L2"
-EXTRA = "bumps_2048x1088_L3"
+# the throughput and roofline workload: camera-sensor size, 3 levels
+PRIMARY = "bumps_2048x1088_L3"
+# the reference's published configuration, reported beside it
+EXTRA = "rotzoom_640x480_L2"
 METRIC = "frames/s (PyramidalFlowFilter forward, flow err <= 1e-4 px vs reference)"
-# reference notebook: 1.172 ms/frame on its textured sequence for this configuration
-# (notebooks/GPU_example.ipynb:292); 0.996 ms/frame on all-zero frames (:400)
-PUBLISHED_FPS = 1000.0 / 1.172
+# reference notebook: 1.172 ms/frame on its textured sequence for the 640x480 2-level
+# configuration (notebooks/GPU_example.ipynb:292); 0.996 ms/frame on all-zero frames (:400).
+# Nothing is published for 2048x1088.
+PUBLISHED_FPS = {"rotzoom_640x480_L2": 1000.0 / 1.172}
 FLUSH_BYTES = 256 << 20
+L2_NOTE = "flushed between steps (256 MiB write outside the step events)"
+SEQUENCE = {
+    "rotzoom": "seeded blurred noise (sigma 1.5, seed 1), rotation 0.5 deg + zoom 1.004 per frame",
+    "bumps": "seeded blurred noise (sigma 1, seed 2) + N(0, 3 DN) sensor noise, flow = 8 Gaussian bumps "
+             "(sigma 150 px, amplitude U[-3, 3] px/frame)",
+}
+
+
+def bench_config(name):
+    """The workload as both arms print it (identical keys and values in both)."""
+    w = WORKLOADS[name]
+    return {"workload": name, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"], "gamma": w["gamma"],
+            "smoothIterations": w["smooth"], "maxflow": w["maxflow"], "l2": L2_NOTE}
 
 
 def level_shapes(w):
@@ -564,18 +582,21 @@ def bench_differentiable(steps):
         return run
 
     def timed(fn, n):
-        for _ in range(2):
+        """Median over n calls, each bracketed by its own events (3 untimed calls first)."""
+        for _ in range(3):
             fn()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        ms = []
         for _ in range(n):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
             fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / n
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
 
-    n = max(1, min(steps, 5))
+    n = max(3, min(steps, 7))
     t_f = timed(fwd, n)
     t_fb = timed(fwd_bwd(f), n)
     t_fbc = timed(fwd_bwd(fc), n)
@@ -591,28 +612,75 @@ def bench_differentiable(steps):
     }
 
 
+def workload_leg(world, name, steps, warmup, flush, hbm_peak):
+    """Device-timed frames of one workload plus its level-0 kernel timed alone (L2 flushed
+    before every frame and launch); returns (summary dict, tuned filter, frames on the host)."""
+    import torch
+
+    w = WORKLOADS[name]
+    frames = make_frames(w)
+    dev = torch.from_numpy(frames).cuda()
+    barrier(world)
+    ms, _, filt = device_run(w, dev, steps, warmup, flush, label="timed" if name == PRIMARY else "timed_" + name)
+    barrier(world)
+    ms = max_over_ranks(world, ms)
+    fps = aggregate_rate(world, steps, ms)
+    l0 = filt.timeLevel(0, min(steps, 1000), flush)
+    l0_l2 = filt.timeLevel(0, min(steps, 1000), None)
+    b0 = level0_kernel_bytes(w)
+    N0 = int(np.ceil(np.float32(w["maxflow"])))
+    kind = "delta level" if w["levels"] > 1 else "single level"
+    out = {
+        "workload": name, "value": fps, "unit": "frames/s", "steps": steps, "ms_per_step": ms / steps,
+        "mpix_per_s": fps * w["H"] * w["W"] / 1e6, "kernels": filt.tuning(),
+        "frame_bytes": frame_bytes(w), "frame_gbs": frame_bytes(w) * fps / world / 1e9,
+        "frame_roofline_frac": frame_bytes(w) * fps / world / 1e9 / hbm_peak,
+        "roofline": {"bound": "hbm", "kernel": f"level-0 step ({kind}, N={N0}, S={w['smooth'][0]}): "
+                                               + filt.tuning().split(";")[0],
+                     "achieved": b0 / (l0 / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": b0 / (l0 / 1e3) / 1e9 / hbm_peak, "traffic": ncu_traffic(name),
+                     "algorithmic_bytes": b0, "launch_ms": l0,
+                     "l2_resident": {"launch_ms": l0_l2, "achieved": b0 / (l0_l2 / 1e3) / 1e9,
+                                     "note": "same step without the L2 flush (state L2-resident)"}},
+        "launches_per_frame": kernels_per_frame(w, filt.tuning()),
+    }
+    return out, filt, frames
+
+
+def d2h_ceiling(nbytes, reps=20):
+    """Frames/s that the device-to-host copy of one frame's flow alone allows (pinned host
+    memory, one cudaMemcpyAsync per frame, back to back)."""
+    import torch
+
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    for _ in range(3):
+        dst.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        dst.copy_(src, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"fps": 1e3 / ms, "GBps": nbytes / (ms * 1e-3) / 1e9, "bytes": nbytes}
+
+
 def bench_b200(args):
     import torch
 
     world, rank, local = dist_setup()
     hbm_peak, peak_kind = peaks()
     w = WORKLOADS[PRIMARY]
-    frames = make_frames(w)
-    dev_frames = torch.from_numpy(frames).cuda()
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     # ---- timed region: device time of K frames, L2 flushed between frames
     barrier(world)
     with ClockSampler(gpu_uuid(local)) as clk:
-        step_ms, _, filt = device_run(w, dev_frames, args.steps, args.warmup, flush)
-        barrier(world)
-    step_ms = max_over_ranks(world, step_ms)
-    value = aggregate_rate(world, args.steps, step_ms)
-
-    # ---- dominant kernel step (level 0) timed live: its captured graph, L2 flushed before each
-    l0_ms = filt.timeLevel(0, min(args.steps, 1000), flush)
-    # ... and without the flush: the 640x480 state stays in the 126 MB L2 between frames
-    l0_ms_l2 = filt.timeLevel(0, min(args.steps, 1000), None)
+        prim, filt, frames = workload_leg(world, PRIMARY, args.steps, args.warmup, flush, hbm_peak)
+    step_ms = prim["ms_per_step"] * args.steps
+    value = prim["value"]
 
     # ---- elapsedTime() through the blocking drop-in calls (loadImage from host, compute),
     # the reference notebook's measure: mean over frames
@@ -627,38 +695,18 @@ def bench_b200(args):
     # demos): device time per launch, back to back, the flow L2-resident as after a frame
     ftc_us = bench_flow_to_color(filt, min(args.steps, 1000))
     rot = bench_rotational_predictor(min(args.steps, 1000))
-    l0_bytes = level0_kernel_bytes(w)
-    achieved = l0_bytes / (l0_ms / 1000.0) / 1e9
-    traffic = ncu_traffic(PRIMARY)
 
     # ---- end to end through the public API with host buffers
-    e2e_steps = min(args.steps, 2000)
+    e2e_steps = min(max(args.steps, 200), 2000)
     e2e_ms = max_over_ranks(world, e2e_run(w, frames, e2e_steps, args.warmup))
     e2e_fps = aggregate_rate(world, e2e_steps, e2e_ms)
+    ceiling = d2h_ceiling(w["H"] * w["W"] * 8)
 
-    # ---- the throughput workload beside it
-    we = WORKLOADS[EXTRA]
-    fe = make_frames(we)
-    dfe = torch.from_numpy(fe).cuda()
-    ksteps = min(args.steps, 4000)
-    barrier(world)
-    ems, _, efilt = device_run(we, dfe, ksteps, args.warmup, flush, label="timed_extra")
-    barrier(world)
-    ems = max_over_ranks(world, ems)
-    el0 = efilt.timeLevel(0, min(ksteps, 1000), flush)
-    eb = level0_kernel_bytes(we)
-    e_fps = aggregate_rate(world, ksteps, ems)
-    extra = {
-        "workload": EXTRA, "value": e_fps, "unit": "frames/s", "steps": ksteps,
-        "ms_per_step": ems / ksteps, "mpix_per_s": e_fps * we["H"] * we["W"] / 1e6,
-        "kernels": efilt.tuning(),
-        "frame_bytes": frame_bytes(we),
-        "frame_gbs": frame_bytes(we) * e_fps / world / 1e9,
-        "frame_roofline_frac": frame_bytes(we) * e_fps / world / 1e9 / hbm_peak,
-        "roofline": {"bound": "hbm", "kernel": "level-0 step (delta level, N=4, S=1): " + efilt.tuning().split(";")[0], "achieved": eb / (el0 / 1e3) / 1e9,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": eb / (el0 / 1e3) / 1e9 / hbm_peak,
-                     "traffic": ncu_traffic(EXTRA), "algorithmic_bytes": eb, "launch_ms": el0},
-    }
+    # ---- the reference's published configuration beside it
+    extra, efilt, _ = workload_leg(world, EXTRA, min(args.steps * 4, 4000), args.warmup, flush, hbm_peak)
+    extra["vs_published"] = extra["value"] / world / PUBLISHED_FPS[EXTRA]
+    extra["published_fps"] = PUBLISHED_FPS[EXTRA]
+    extra["sequence"] = SEQUENCE[WORKLOADS[EXTRA]["seq"]]
 
     # ---- the 64-stream batched step (each rank its own batch: replicas)
     barrier(world)
@@ -671,34 +719,30 @@ def bench_b200(args):
     if rank == 0 and world == 1:
         fps, cores, n = cpu_port_fps(w, frames)
         cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
-               "sample": f"{n} consecutive {w['W']}x{w['H']} frames, 2 levels, oracle/ C++ port, {cores} threads"}
+               "sample": f"{n} consecutive {w['W']}x{w['H']} frames, {w['levels']} levels, oracle/ C++ port, "
+                         f"{cores} threads"}
 
     if rank == 0:
-        launches_per_frame = kernels_per_frame(w, filt.tuning())
+        roof = dict(prim["roofline"])
+        roof["peak_kind"] = peak_kind
+        roof["issue"] = issue_roofline(ncu_traffic(PRIMARY, "warp_instructions_per_launch"), roof["launch_ms"],
+                                       clk.summary())
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": value / world / PUBLISHED_FPS if world == 1 else None,
+            "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": PRIMARY, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"],
-                       "gamma": w["gamma"], "smoothIterations": w["smooth"], "maxflow": w["maxflow"],
-                       "sequence": "seeded blurred noise, rotation 0.5 deg + zoom 1.004 per frame",
-                       "l2": "flushed between steps (256 MiB write outside the step events)",
-                       "step": "loadImage (device frame) + compute(), CUDA-graph replay",
-                       "kernels": filt.tuning(),
-                       "parallelism": f"replicas x{world}"},
-            "mpix_per_s": value * w["H"] * w["W"] / 1e6,
-            "frame_bytes": frame_bytes(w),
-            "roofline": {"bound": "hbm", "kernel": "level-0 step (delta level, N=4, S=2): " + filt.tuning().split(";")[0], "achieved": achieved,
-                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                         "algorithmic_bytes": l0_bytes, "launch_ms": l0_ms, "peak_kind": peak_kind,
-                         "l2_resident": {"launch_ms": l0_ms_l2, "achieved": l0_bytes / (l0_ms_l2 / 1e3) / 1e9,
-                                         "note": "same step without the L2 flush (state L2-resident)"},
-                         "issue": issue_roofline(ncu_traffic(PRIMARY, "warp_instructions_per_launch"), l0_ms,
-                                                 clk.summary())},
+            "config": bench_config(PRIMARY),
+            "notes": {"sequence": SEQUENCE[w["seq"]], "step": "loadImage (device frame) + compute(), CUDA-graph replay",
+                      "kernels": filt.tuning(), "parallelism": f"replicas x{world}",
+                      "vs_baseline": "null: the reference publishes no figure for this configuration"},
+            "mpix_per_s": prim["mpix_per_s"],
+            "frame_bytes": prim["frame_bytes"], "frame_gbs": prim["frame_gbs"],
+            "frame_roofline_frac": prim["frame_roofline_frac"],
+            "roofline": roof,
             "flow_to_color": {"launch_us": ftc_us, "pixels": w["H"] * w["W"],
                               "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
-                              "note": "ff_flow_to_color on the 640x480 level-0 flow, default wheel; "
+                              "note": f"ff_flow_to_color on the {w['W']}x{w['H']} level-0 flow, default wheel; "
                                       "12 B/px (float2 in, RGBA out)"},
             "rotational_predictor": rot,
             "elapsed_time_ms": {"value": elapsed_ms, "frames": len(et),
@@ -706,10 +750,11 @@ def bench_b200(args):
                                         "as the reference notebook measures"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": w["H"] * w["W"],
-                    "d2h_bytes_per_step": w["H"] * w["W"] * 8,
+                    "d2h_bytes_per_step": w["H"] * w["W"] * 8, "steps": e2e_steps,
+                    "d2h_ceiling": ceiling,
                     "path": "flowfilter_b200.PyramidalFlowFilter.processAsync(pinned host frame -> pinned host flow), "
                             "synchronize() at the end; wall clock"},
-            "gpu_launches": args.steps * launches_per_frame,
+            "gpu_launches": args.steps * prim["launches_per_frame"],
             "clocks": clk.summary(),
             "extra": extra,
             "batched": batched,
@@ -751,8 +796,9 @@ def bench_reference(args):
         "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1000.0 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": {"workload": PRIMARY, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"],
-                   "gamma": w["gamma"], "smoothIterations": w["smooth"], "maxflow": w["maxflow"]},
+        "config": bench_config(PRIMARY),
+        "notes": {"sequence": SEQUENCE[w["seq"]],
+                  "step": "one frame of the reference's CUDA path restated in C++ (oracle/), on the host cores"},
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} frames, reference CUDA path restated in C++ (oracle/), "
                                    f"{threads} host threads"},
@@ -770,7 +816,7 @@ def profile_next(args):
     import torch
     from flowfilter_b200 import createPerspectiveCamera, lib
 
-    w = dict(WORKLOADS[PRIMARY])
+    w = dict(WORKLOADS["rotzoom_640x480_L2"])
     w["ring"] = 4
     dev = torch.from_numpy(make_frames(w)).cuda()
     f = make_filter(w)

@@ -401,16 +401,19 @@ ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first,
                                  void* grad_frame, void* grad_gamma, void* grad_weights, void* const* grad_state_in,
                                  void* scratch, void* stream);
 
-/* ff_stage_smooth without a workspace and without any allocation (no counterpart in the
- * reference, whose FlowSmoother allocates its X-pass scratch image in configure(),
- * flowsmoothing.cu:59-62). The X-pass scratch is a 32 MiB static device array of the
- * library, so flows of up to 32 MiB of 512-byte-aligned float2 rows (2048x2048) are
- * accepted; larger ones fail with FF_ERR_INVALID_ARGUMENT. The scratch needs no initial
- * contents. It is one array per device: calls that overlap on one device (two streams, or
- * two threads) race on it; calls queued on one stream do not. Make each device's first
- * call outside stream capture (it looks the array's address up once per device). For
- * callers that may not allocate: code running under a frame deadline, where cudaMalloc
- * would synchronise the device, and hosts whose memory belongs to their own allocator. */
+/* ff_stage_smooth without a workspace and without any allocation. It has no counterpart
+ * in the reference. The X-pass scratch is a 32 MiB static device array of the library, so
+ * flows of up to 32 MiB of 512-byte-aligned float2 rows (2048x2048) are accepted; larger
+ * ones fail with FF_ERR_INVALID_ARGUMENT. The array is device memory that every device
+ * holds once the library's module is loaded there (at context creation under
+ * CUDA_MODULE_LOADING=EAGER, else at the library's first launch on it), whether or not this
+ * entry point is ever called, until the process exits or the device is reset. The scratch
+ * needs no initial contents. It is one array per device: calls that overlap on one device
+ * (two streams, or two threads) race on it; calls queued on one stream do not. Make each
+ * device's first call, and the first after a cudaDeviceReset, outside stream capture: it
+ * looks the array's address up once per device and context. For callers that may not
+ * allocate: code running under a frame deadline, where cudaMalloc would synchronise the
+ * device, and hosts whose memory belongs to their own allocator. */
 ff_status ff_stage_smooth_noalloc(const float* flow, size_t flow_pitch, int height, int width, int iterations,
                                   float* out, size_t out_pitch, void* stream);
 

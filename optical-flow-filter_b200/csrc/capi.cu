@@ -2,6 +2,8 @@
 //
 // Every entry point converts C++ exceptions into ff_status codes and stores the
 // message for ff_last_error(); nothing here exits the process.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -105,8 +107,9 @@ void log_message(int level, const std::string& msg) {
 }
 }  // namespace ffb
 
-// last-error setter for entry points defined in other files (diff_kernels.cu)
-void ffb_set_last_error(const std::string& msg) { g_last_error = msg; }
+// failure reporting for entry points defined in other files (diff_kernels.cu, display.cu,
+// rotation.cu): the last error and the FF_LOG_ERROR message, as for the entry points here
+ff_status ffb_fail(ff_status s, const std::string& msg) { return fail(s, msg); }
 
 extern "C" {
 
@@ -734,20 +737,49 @@ __device__ __align__(256) unsigned char g_smooth_scratch[kStaticScratchBytes];
 
 std::mutex g_scratch_mu;
 void* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of g_smooth_scratch on the current device, looked up once per device.
-// The first lookup may load this module onto the device, which is not allowed while a
-// stream is being captured, so each device's first call belongs before any capture.
+// Unique id of the current device's primary context (cuCtxGetId through the runtime's
+// driver entry points, so the library does not link libcuda). A cudaDeviceReset makes a
+// new context, in which the module and its array are loaded again, maybe elsewhere.
+unsigned long long current_context_id() {
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        ffb::check_cuda(cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa), "cuCtxGetCurrent");
+        ffb::check_cuda(cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb), "cuCtxGetId");
+        if (qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+            throw Error(FF_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId not found");
+        get_current = (PFN_cuCtxGetCurrent_v4000)a;
+        get_id = (PFN_cuCtxGetId_v12000)b;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        throw Error(FF_ERR_CUDA, "no current CUDA context");
+    return id;
+}
+
+// Device address of g_smooth_scratch on the current device, looked up once per device and
+// context (again after a cudaDeviceReset). The lookup may load this module onto the
+// device, which is not allowed while a stream is being captured, so each device's first
+// call belongs before any capture.
 void* static_scratch() {
     int dev = 0;
     ffb::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) throw Error(FF_ERR_UNSUPPORTED, "device ordinal above 63");
+    ffb::check_cuda(cudaSetDevice(dev), "cudaSetDevice");  // initialises and binds the device's context
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         ffb::check_cuda(cudaGetSymbolAddress(&p, g_smooth_scratch), "cudaGetSymbolAddress(static scratch)");
         if (!p) throw Error(FF_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
         g_scratch_ptr[dev] = p;
+        g_scratch_ctx[dev] = ctx;
     }
     return g_scratch_ptr[dev];
 }

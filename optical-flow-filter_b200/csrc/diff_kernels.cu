@@ -819,7 +819,7 @@ cudaError_t pyramid(bool bwd, int B, int H, int W, const void* a, void* o, cudaS
 }  // namespace ffb
 
 // ------------------------------------------------------------------ C ABI
-void ffb_set_last_error(const std::string& msg);  // capi.cu
+ff_status ffb_fail(ff_status s, const std::string& msg);  // capi.cu: last error + log
 
 using namespace ffb;
 using namespace ffb::diff;
@@ -829,21 +829,18 @@ namespace {
 template <typename F>
 ff_status run(int dtype, F&& f) {
     if (dtype != 0 && dtype != 1) {
-        ffb_set_last_error("dtype must be 0 (float32) or 1 (float64)");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "dtype must be 0 (float32) or 1 (float64)");
     }
     cudaError_t e = f();
     if (e != cudaSuccess) {
-        ffb_set_last_error(std::string("CUDA: ") + cudaGetErrorString(e));
-        return FF_ERR_CUDA;
+        return ffb_fail(FF_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
     }
     return FF_OK;
 }
 
 ff_status check_shape(int B, int H, int W) {
     if (B <= 0 || H <= 0 || W <= 0) {
-        ffb_set_last_error("batch, height and width must be positive");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "batch, height and width must be positive");
     }
     return FF_OK;
 }
@@ -861,8 +858,7 @@ bool pairs_aligned(int dtype, std::initializer_list<const void*> ps) {
 #define PAIRS_OR_RETURN(dtype, ...)                                                                   \
     do {                                                                                              \
         if (!pairs_aligned(dtype, {__VA_ARGS__})) {                                                   \
-            ffb_set_last_error("two-channel fields must be aligned to two elements (8 or 16 bytes)"); \
-            return FF_ERR_INVALID_ARGUMENT;                                                           \
+            return ffb_fail(FF_ERR_INVALID_ARGUMENT, "two-channel fields must be aligned to two elements (8 or 16 bytes)");                                                           \
         }                                                                                             \
     } while (0)
 
@@ -929,8 +925,7 @@ ff_status ff_diff_propagate(int dtype, int B, int H, int W, int axis, int payloa
                             void* stream) {
     SHAPE_OR_RETURN(B, H, W);
     if ((axis != 0 && axis != 1) || border < 0) {
-        ffb_set_last_error("axis must be 0 or 1 and border >= 0");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "axis must be 0 or 1 and border >= 0");
     }
     cudaStream_t s = (cudaStream_t)stream;
     return run(dtype, [&] {
@@ -954,8 +949,7 @@ ff_status ff_diff_propagate_bwd(int dtype, int B, int H, int W, int axis, int pa
     SHAPE_OR_RETURN(B, H, W);
     PAIRS_OR_RETURN(dtype, f, v, gfo, gvo, gf, gv);
     if ((axis != 0 && axis != 1) || border < 0) {
-        ffb_set_last_error("axis must be 0 or 1 and border >= 0");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "axis must be 0 or 1 and border >= 0");
     }
     cudaStream_t s = (cudaStream_t)stream;
     return run(dtype, [&] {
@@ -1046,8 +1040,7 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
                          void* stream) {
     SHAPE_OR_RETURN(B, H, W);
     if (axis != 0 && axis != 1) {
-        ffb_set_last_error("axis must be 0 or 1");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "axis must be 0 or 1");
     }
     cudaStream_t s = (cudaStream_t)stream;
     return run(dtype, [&] {
@@ -1069,8 +1062,7 @@ ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const voi
     SHAPE_OR_RETURN(B, H, W);
     PAIRS_OR_RETURN(dtype, in, gout, gin);
     if (axis != 0 && axis != 1) {
-        ffb_set_last_error("axis must be 0 or 1");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "axis must be 0 or 1");
     }
     cudaStream_t s = (cudaStream_t)stream;
     return run(dtype, [&] {
@@ -1453,11 +1445,9 @@ ff_status run_frame(F&& f) {
         f();
         return FF_OK;
     } catch (const std::invalid_argument& e) {
-        ffb_set_last_error(e.what());
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, e.what());
     } catch (const std::exception& e) {
-        ffb_set_last_error(std::string("CUDA: ") + e.what());
-        return FF_ERR_CUDA;
+        return ffb_fail(FF_ERR_CUDA, std::string("CUDA: ") + e.what());
     }
 }
 

@@ -21,7 +21,7 @@
 #include "ffb200.h"
 #include "launch.cuh"
 
-void ffb_set_last_error(const std::string& msg);  // capi.cu
+ff_status ffb_fail(ff_status s, const std::string& msg);  // capi.cu: last error + log
 
 namespace ffb {
 namespace {
@@ -130,8 +130,7 @@ extern "C" {
 
 ff_status ff_color_wheel_default(unsigned char* rgba) {
     if (!rgba) {
-        ffb_set_last_error("rgba must not be NULL");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "rgba must not be NULL");
     }
     const auto& w = ffb::default_wheel();
     std::copy(w.begin(), w.end(), rgba);
@@ -141,18 +140,15 @@ ff_status ff_color_wheel_default(unsigned char* rgba) {
 ff_status ff_flow_to_color(const float* flow, size_t flow_pitch, int height, int width, float maxflow,
                            const unsigned char* wheel, unsigned char* color, size_t color_pitch, void* stream) {
     if (height < 1 || width < 1 || height > 65535 * 8) {
-        ffb_set_last_error("flow_to_color: height must be in [1, 524280] and width positive");
-        return FF_ERR_SHAPE;
+        return ffb_fail(FF_ERR_SHAPE, "flow_to_color: height must be in [1, 524280] and width positive");
     }
     if (!(maxflow > 0.0f)) {
-        ffb_set_last_error("flow_to_color: maxflow should be greater than 0.0");
-        return FF_ERR_INVALID_ARGUMENT;
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "flow_to_color: maxflow should be greater than 0.0");
     }
     if (!flow || !color || flow_pitch < (size_t)width * 8 || color_pitch < (size_t)width * 4 ||
         ((uintptr_t)flow | flow_pitch) % 8 || ((uintptr_t)color | color_pitch) % 4 || (uintptr_t)wheel % 4) {
-        ffb_set_last_error("flow_to_color: flow needs 8-byte aligned rows of width float2, color 4-byte aligned "
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "flow_to_color: flow needs 8-byte aligned rows of width float2, color 4-byte aligned "
                            "rows of width RGBA, the wheel 4-byte alignment");
-        return FF_ERR_INVALID_ARGUMENT;
     }
     cudaError_t e = wheel ? cudaSuccess : ffb::ensure_default_wheel();
     if (e == cudaSuccess)
@@ -160,8 +156,7 @@ ff_status ff_flow_to_color(const float* flow, size_t flow_pitch, int height, int
                      (cudaStream_t)stream, flow, flow_pitch, height, width, maxflow,
                      reinterpret_cast<const uchar4*>(wheel), reinterpret_cast<uchar4*>(color), color_pitch);
     if (e != cudaSuccess) {
-        ffb_set_last_error(std::string("flow_to_color: ") + cudaGetErrorString(e));
-        return FF_ERR_CUDA;
+        return ffb_fail(FF_ERR_CUDA, std::string("flow_to_color: ") + cudaGetErrorString(e));
     }
     return FF_OK;
 }

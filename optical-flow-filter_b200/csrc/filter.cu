@@ -1140,7 +1140,12 @@ void Filter::export_state(void* host, size_t bytes) const {
         throw Error(FF_ERR_INVALID_ARGUMENT, "state buffer too small: " + std::to_string(bytes) + " < " +
                                                  std::to_string(state_bytes()));
     if (phase_ != 0) throw Error(FF_ERR_LOGIC, "the state can be exported between frames only");
+    // every frame computed so far, and the pipelined downloads of their flows, have finished
     wait_done();
+    if (pipe_) {
+        check_cuda(cudaStreamSynchronize(pipe_->out), "export state");
+        check_cuda(cudaStreamSynchronize(pipe_->in), "export state");
+    }
     unsigned char* out = static_cast<unsigned char*>(host);
     StateHeader h{};
     std::memcpy(h.magic, kStateMagic, sizeof(h.magic));
@@ -1190,7 +1195,8 @@ void Filter::import_state(const void* host, size_t bytes) {
         if (sl[l].H != (uint32_t)v.H || sl[l].W != (uint32_t)v.W || sl[l].delta != (v.delta ? 1u : 0u))
             throw Error(FF_ERR_SHAPE, "state image level " + std::to_string(l) + " has another size");
     }
-    wait_done();
+    // a pipelined download may still be reading the buffers the copies below overwrite
+    synchronize();
     for (int l = 0; l < L_; ++l) {
         Level& v = lv_[l];
         Buf* bufs[3] = {&v.fs[cur_], &v.io[cur_], v.delta ? &v.d[cur_] : &v.fu};

@@ -30,7 +30,7 @@
 #include "ffb200.h"
 #include "launch.cuh"
 
-void ffb_set_last_error(const std::string& msg);  // capi.cu
+ff_status ffb_fail(ff_status s, const std::string& msg);  // capi.cu: last error + log
 
 namespace ffb {
 namespace {
@@ -273,10 +273,7 @@ bool aligned(const void* p, size_t pitch, size_t row_bytes, size_t align) {
     return p && pitch >= row_bytes && (((uintptr_t)p | pitch) % align) == 0;
 }
 
-ff_status fail(ff_status st, const std::string& msg) {
-    ffb_set_last_error(msg);
-    return st;
-}
+ff_status fail(ff_status st, const std::string& msg) { return ffb_fail(st, msg); }
 
 ff_status check_common(int depth, int h, int w, int iterations, const float* image, size_t image_pitch, float* out,
                        size_t out_pitch, float* ws, size_t ws_pitch) {

@@ -21,6 +21,7 @@ same frames are produced on any machine with the same numpy version.
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -31,6 +32,7 @@ __all__ = [
     "seq_constant",
     "seq_rotzoom",
     "seq_bumps",
+    "iter_bumps",
     "seq_bumps_float",
     "sequence",
 ]
@@ -134,21 +136,46 @@ def seq_rotzoom(frames: int = 300, height: int = 480, width: int = 640,
     return out
 
 
+def iter_bumps(frames: int = 1000, height: int = 1088, width: int = 2048,
+               sigma: float = 1.0, seed: int = 2, n_bumps: int = 8,
+               bump_sigma: float = 150.0, amp: float = 3.0,
+               sensor_noise: float = 3.0, threads: int | None = None):
+    """The frames of ``seq_bumps`` one at a time (uint8 [H, W] each), for sequences too long to
+    hold.  The warps run on a thread pool a few frames ahead (numpy releases the GIL in them);
+    the sensor noise is drawn in frame order from the one generator, so the frames are
+    identical to ``seq_bumps``'s."""
+    from collections import deque
+    from concurrent.futures import ThreadPoolExecutor
+
+    rng = np.random.default_rng(seed)
+    tex = blurred_noise(height, width, sigma, rng)
+    u, v = bump_flow(height, width, n_bumps, bump_sigma, amp, rng)
+    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
+
+    def warp(t):
+        return warp_bilinear(tex, xx - t * u, yy - t * v)
+
+    threads = threads or min(16, os.cpu_count() or 1)
+    with ThreadPoolExecutor(threads) as pool:
+        ahead = deque(pool.submit(warp, t) for t in range(min(frames, 2 * threads)))
+        for t in range(frames):
+            noise = rng.normal(0.0, sensor_noise, size=(height, width)) if sensor_noise > 0 else None
+            img = ahead.popleft().result()
+            if t + len(ahead) + 1 < frames:
+                ahead.append(pool.submit(warp, t + len(ahead) + 1))
+            if noise is not None:
+                img = img + noise
+            yield _to_u8(img)
+
+
 def seq_bumps(frames: int = 1000, height: int = 1088, width: int = 2048,
               sigma: float = 1.0, seed: int = 2, n_bumps: int = 8,
               bump_sigma: float = 150.0, amp: float = 3.0,
               sensor_noise: float = 3.0) -> np.ndarray:
     """Bump-flow sequence with additive sensor noise, uint8 [T, H, W]."""
-    rng = np.random.default_rng(seed)
-    tex = blurred_noise(height, width, sigma, rng)
-    u, v = bump_flow(height, width, n_bumps, bump_sigma, amp, rng)
-    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
     out = np.empty((frames, height, width), np.uint8)
-    for t in range(frames):
-        img = warp_bilinear(tex, xx - t * u, yy - t * v)
-        if sensor_noise > 0:
-            img = img + rng.normal(0.0, sensor_noise, size=img.shape)
-        out[t] = _to_u8(img)
+    for t, f in enumerate(iter_bumps(frames, height, width, sigma, seed, n_bumps, bump_sigma, amp, sensor_noise)):
+        out[t] = f
     return out
 
 

@@ -6,7 +6,9 @@ Two steps:
       builds nothing; needs oracle/_ref/ref_driver (``make -C oracle ref``).  Writes the
       stage inputs, runs the reference driver on them, on the parity sequences and on the
       colour-lookup probes and the rotational predictor / Lax-Wendroff cases, and leaves raw
-      outputs in DIR.  PART: stages, norm, upmap, cases, wheelidx, rotation (default: all).
+      outputs in DIR.  PART: stages, norm, upmap, cases, wheelidx, rotation, long (default:
+      all).  "long" streams the long cases (1000 frames of 2048x1088) through the reference
+      one frame at a time and keeps a sha256 of every frame's flow.
 
   python oracle/make_reference_fixtures.py pack --raw DIR
       packs DIR into the small committed fixtures under tests/golden/.
@@ -76,6 +78,13 @@ ROT_CASES = [(48, 64, 1, 0.004, 0.0036, 0.0048, 0.02, -0.015, 0.04, 2, 51),
 
 FULL_LIMIT = 64 * 128  # dumps up to this many pixels are stored whole
 
+# long sequences: every frame's flow is hashed (sha256 of the float32 (H, W, 2) flow) and a few
+# frames are kept subsampled; frames are generated and streamed through the reference one at a time
+LONG_CASES = {
+    "bumps_2048x1088_L3_1000": dict(seq="bumps", frames=1000, levels=3, maxflow=4.0,
+                                    gamma=[5.0, 20.0, 50.0], smooth=[1, 2, 4], keep=[500, 999]),
+}
+
 
 def stage_inputs(seed: int = 5) -> dict[str, np.ndarray]:
     rng = np.random.default_rng(seed)
@@ -96,6 +105,59 @@ def stage_inputs(seed: int = 5) -> dict[str, np.ndarray]:
 
 def case_frames(case: dict) -> np.ndarray:
     return synthetic.sequence(case["seq"], frames=case["frames"], **case.get("kw", {}))
+
+
+def long_frames(case: dict):
+    """The frames of a long case one at a time (uint8 (H, W))."""
+    assert case["seq"] == "bumps"
+    return synthetic.iter_bumps(frames=case["frames"], **case.get("kw", {}))
+
+
+def run_long(out: str) -> None:
+    """Streams each long case through the reference (ref_driver filterpipe) and writes
+    long_NAME.npz: per-frame sha256 digests of the flow and the kept frames subsampled."""
+    import threading
+
+    for name, case in LONG_CASES.items():
+        frames = long_frames(case)
+        first = next(frames)
+        h, w = first.shape
+        cmd = [DRIVER, "filterpipe", str(h), str(w), str(case["levels"]), repr(case["maxflow"]),
+               ",".join(repr(g) for g in case["gamma"]), ",".join(str(s) for s in case["smooth"])]
+        proc = subprocess.Popen(cmd, stdin=subprocess.PIPE, stdout=subprocess.PIPE)
+        frame_sha = hashlib.sha256()
+
+        def feed():
+            try:
+                proc.stdin.write(first.tobytes())
+                frame_sha.update(first.tobytes())
+                for f in frames:
+                    proc.stdin.write(f.tobytes())
+                    frame_sha.update(f.tobytes())
+            finally:
+                proc.stdin.close()
+
+        th = threading.Thread(target=feed)
+        th.start()
+        fsz = h * w * 8
+        digests, kept = [], {}
+        rows, cols = subsample_rows_cols(h, w)
+        for t in range(case["frames"]):
+            buf = proc.stdout.read(fsz)
+            if len(buf) != fsz:
+                raise RuntimeError(f"{name}: reference stopped at frame {t}")
+            digests.append(hashlib.sha256(buf).digest())
+            if t in case["keep"]:
+                kept[t] = np.frombuffer(buf, np.float32).reshape(h, w, 2)[rows][:, cols].copy()
+        th.join()
+        if proc.wait() != 0:
+            raise RuntimeError(f"{name}: reference driver failed")
+        meta = dict(case, name=name, frames_sha256=frame_sha.hexdigest(), layout="subsampled")
+        np.savez_compressed(os.path.join(out, f"long_{name}.npz"),
+                            digests=np.frombuffer(b"".join(digests), np.uint8).reshape(-1, 32),
+                            keep=np.array(case["keep"], np.int64), rows=rows, cols=cols,
+                            flow=np.stack([kept[t] for t in case["keep"]]),
+                            meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8))
 
 
 def lw_inputs(h: int, w: int, depth: int, seed: int):
@@ -120,8 +182,10 @@ def sha(a: np.ndarray) -> str:
 
 
 def run(out: str, only=None) -> None:
-    parts = set(only or ["stages", "norm", "upmap", "cases", "wheelidx", "rotation"])
+    parts = set(only or ["stages", "norm", "upmap", "cases", "wheelidx", "rotation", "long"])
     os.makedirs(out, exist_ok=True)
+    if "long" in parts:
+        run_long(out)
     if "stages" in parts:
         sin = os.path.join(out, "stage_in")
         sout = os.path.join(out, "stage_out")
@@ -237,6 +301,11 @@ def pack(raw: str) -> None:
             arrays[f"rot_cam_{k}"] = np.load(os.path.join(raw, f"rot_flow_{k}.npy.cam.npy"))
         np.savez_compressed(os.path.join(GOLDEN, "ref_rotation.npz"),
                             inputs_sha256=np.frombuffer(json.dumps(shas).encode(), np.uint8), **arrays)
+    for name in LONG_CASES:
+        src = os.path.join(raw, f"long_{name}.npz")
+        if os.path.exists(src):
+            with open(src, "rb") as fi, open(os.path.join(GOLDEN, f"ref_long_{name}.npz"), "wb") as fo:
+                fo.write(fi.read())
     for name in CASES:
         src = os.path.join(raw, f"case_{name}.npz")
         if os.path.exists(src):

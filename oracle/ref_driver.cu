@@ -29,6 +29,10 @@
 //                                      LEVELS>=1: PyramidalFlowFilter(h, w, LEVELS)
 //                                      GAMMAS / SMOOTHS are comma lists (level 0 first),
 //                                      DUMP a comma list of frame indices to save.
+//   filterpipe H W LEVELS MAXFLOW GAMMAS SMOOTHS
+//                                      the same filters on frames read from stdin (H*W
+//                                      uint8 each, until EOF); each frame's smoothed flow
+//                                      (H*W*2 float32) is written to stdout
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -422,6 +426,43 @@ static int mode_filter(int argc, char** argv) {
     return e == cudaSuccess ? 0 : 1;
 }
 
+// Long sequences without files: frames (H*W uint8 each) arrive on stdin until EOF; after each
+// frame the smoothed flow (H*W*2 float32, downloadFlow) goes to stdout.
+static int mode_filterpipe(char** argv) {
+    const int H = atoi(argv[2]), W = atoi(argv[3]), levels = atoi(argv[4]);
+    const float maxflow = (float)atof(argv[5]);
+    std::vector<float> gammas = parse_floats(argv[6]);
+    std::vector<int> smooths = parse_ints(argv[7]);
+    const size_t fsz = (size_t)H * W;
+    std::vector<unsigned char> frame(fsz);
+    std::vector<float> host(fsz * 2);
+    image_t flowHost = wrap_host(host.data(), H, W, 2, 4);
+    FlowFilter* ff = nullptr;
+    PyramidalFlowFilter* pf = nullptr;
+    if (levels == 0) {
+        ff = new FlowFilter(H, W, smooths[0], maxflow, gammas[0]);
+    } else {
+        pf = new PyramidalFlowFilter(H, W, levels);
+        pf->setGamma(gammas);
+        pf->setSmoothIterations(smooths);
+        pf->setMaxFlow(maxflow);
+    }
+    int t = 0;
+    while (fread(frame.data(), 1, fsz, stdin) == fsz) {
+        image_t im = wrap_host(frame.data(), H, W, 1, 1);
+        if (ff) { ff->loadImage(im); ff->compute(); ff->downloadFlow(flowHost); }
+        else { pf->loadImage(im); pf->compute(); pf->downloadFlow(flowHost); }
+        if (fwrite(host.data(), sizeof(float), fsz * 2, stdout) != fsz * 2) break;
+        fflush(stdout);
+        ++t;
+    }
+    delete ff;
+    delete pf;
+    cudaError_t e = cudaDeviceSynchronize();
+    fprintf(stderr, "filterpipe: %d frames, %s\n", t, cudaGetErrorString(e));
+    return e == cudaSuccess ? 0 : 1;
+}
+
 static int mode_wheelidx(const std::string& flows, float maxflow, const std::string& out) {
     Npy a = npy_read(flows);
     if (a.descr != "<f4" || a.shape.size() != 3 || a.shape[2] != 2)
@@ -496,6 +537,7 @@ int main(int argc, char** argv) {
         if (mode == "upmap" && argc >= 4) return mode_upmap(argv[2], atoi(argv[3]));
         if (mode == "stages" && argc >= 4) return mode_stages(argv[2], argv[3]);
         if (mode == "filter" && argc >= 9) return mode_filter(argc, argv);
+        if (mode == "filterpipe" && argc >= 8) return mode_filterpipe(argv);
         if (mode == "lw" && argc >= 6) return mode_lw(argv[2], argv[3], atoi(argv[4]), argv[5]);
         if (mode == "rotation" && argc >= 12) return mode_rotation(argv);
         if (mode == "wheelidx" && argc >= 5) return mode_wheelidx(argv[2], (float)atof(argv[3]), argv[4]);

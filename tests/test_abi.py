@@ -151,3 +151,23 @@ def test_cpp_dropin_headers_compile(tmp_path):
     src.write_text('#include "flowfilter/gpu/flowfilter.h"\n#include "flowfilter/gpu/imagemodel.h"\n'
                    "int main() { flowfilter::image_t t{}; (void)t; return 0; }\n")
     subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)], check=True)
+
+
+def test_log_callback_receives_errors_of_every_module():
+    """Failing calls of the differentiable, colour and Lax-Wendroff entry points (rejected
+    before any GPU work) reach the log callback like the filter's."""
+    seen = []
+    ffb.set_log_callback(lambda level, msg: seen.append((level, msg)))
+    try:
+        L = _lib.lib()
+        assert L.ff_diff_smooth(0, 0, 4, 4, 0, None, None, None, None) == _lib.FF_ERR_INVALID_ARGUMENT
+        assert L.ff_diff_smooth(0, 1, 4, 4, 2, None, None, None, None) == _lib.FF_ERR_INVALID_ARGUMENT
+        assert L.ff_flow_to_color(None, 8, 1, 1, 0.0, None, None, 4, None) == _lib.FF_ERR_INVALID_ARGUMENT
+        assert L.ff_color_wheel_default(None) == _lib.FF_ERR_INVALID_ARGUMENT
+        assert seen == [(_lib.FF_LOG_ERROR, "invalid argument: batch, height and width must be positive"),
+                        (_lib.FF_LOG_ERROR, "invalid argument: axis must be 0 or 1"),
+                        (_lib.FF_LOG_ERROR, "invalid argument: flow_to_color: maxflow should be greater than 0.0"),
+                        (_lib.FF_LOG_ERROR, "invalid argument: rgba must not be NULL")]
+        assert L.ff_last_error().decode() == "rgba must not be NULL"
+    finally:
+        ffb.set_log_callback(None)

@@ -114,3 +114,44 @@ def test_state_moves_between_frames_only(ffb, cuda):
     f.computePropagation()
     f.computeUpdate()
     f.importState(f.exportState())
+
+
+@pytest.mark.parametrize("kind", ["single", "pyramidal"])
+def test_import_after_pipelined_frames_keeps_their_flows(ffb, cuda, kind):
+    """importState right after processAsync (no synchronize in between) waits for the pipelined
+    downloads: every output buffer holds the flow its frame computed, not the imported state."""
+    import torch
+
+    seq = frames(6, seed=5)
+    want = make(ffb, kind)
+    flows = []
+    for t in range(4):
+        want.loadImage(seq[t])
+        want.compute()
+        flows.append(want.getFlow())
+    other = make(ffb, kind)
+    for t in range(2):
+        other.loadImage(seq[5 - t])
+        other.compute()
+    state = other.exportState()
+    f = make(ffb, kind)
+    host = torch.from_numpy(seq[:4].copy()).pin_memory()
+    outs = [torch.full((H, W, 2), -7.0, dtype=torch.float32).pin_memory() for _ in range(4)]
+    for t in range(4):
+        f.processAsync(host[t], outs[t])
+    f.importState(state)
+    for t in range(4):
+        np.testing.assert_array_equal(outs[t].numpy(), flows[t], err_msg=f"frame {t}")
+    np.testing.assert_array_equal(f.exportState(), state)
+    exported = f.exportState()
+    g = make(ffb, kind)
+    for t in range(2):
+        g.processAsync(host[t], outs[t])
+    e = g.exportState()  # export after pipelined frames sees their state
+    np.testing.assert_array_equal(outs[1].numpy(), flows[1])
+    h = make(ffb, kind)
+    for t in range(2):
+        h.loadImage(seq[t])
+        h.compute()
+    np.testing.assert_array_equal(e, h.exportState())
+    assert exported.size == e.size
