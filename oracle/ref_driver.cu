@@ -45,6 +45,8 @@
 #include <chrono>
 #include <stdexcept>
 
+#include <unistd.h>
+
 #include <cuda_runtime.h>
 
 #include "flowfilter/image.h"
@@ -437,6 +439,13 @@ static int mode_filterpipe(char** argv) {
     std::vector<unsigned char> frame(fsz);
     std::vector<float> host(fsz * 2);
     image_t flowHost = wrap_host(host.data(), H, W, 2, 4);
+    // the flows go to the original stdout; the library's own messages on stdout (the
+    // filters print a line on their first frame) are sent to stderr instead
+    fflush(stdout);
+    const int data_fd = dup(1);
+    if (data_fd < 0 || dup2(2, 1) < 0) { fprintf(stderr, "filterpipe: cannot redirect stdout\n"); return 1; }
+    FILE* data = fdopen(data_fd, "wb");
+    if (!data) { fprintf(stderr, "filterpipe: fdopen failed\n"); return 1; }
     FlowFilter* ff = nullptr;
     PyramidalFlowFilter* pf = nullptr;
     if (levels == 0) {
@@ -452,10 +461,11 @@ static int mode_filterpipe(char** argv) {
         image_t im = wrap_host(frame.data(), H, W, 1, 1);
         if (ff) { ff->loadImage(im); ff->compute(); ff->downloadFlow(flowHost); }
         else { pf->loadImage(im); pf->compute(); pf->downloadFlow(flowHost); }
-        if (fwrite(host.data(), sizeof(float), fsz * 2, stdout) != fsz * 2) break;
-        fflush(stdout);
+        if (fwrite(host.data(), sizeof(float), fsz * 2, data) != fsz * 2) break;
+        fflush(data);
         ++t;
     }
+    fclose(data);
     delete ff;
     delete pf;
     cudaError_t e = cudaDeviceSynchronize();

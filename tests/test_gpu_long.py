@@ -48,6 +48,7 @@ def test_long_sequence_bit_exact_every_frame(cuda, name):
     rows, cols = arr["rows"], arr["cols"]
     keep = [int(k) for k in arr["keep"]]
     flow = np.empty((1088, 2048, 2), np.float32)
+    keep_err = {}
     n = 0
     for t, frame in enumerate(long_frames(case)):
         frames_sha.update(frame.tobytes())
@@ -58,10 +59,10 @@ def test_long_sequence_bit_exact_every_frame(cuda, name):
             if first_bad[mode] is None and hashlib.sha256(flow.tobytes()).digest() != arr["digests"][t].tobytes():
                 first_bad[mode] = t
             if t in keep:
-                got = flow[rows][:, cols]
-                want = arr["flow"][keep.index(t)]
-                assert np.max(np.abs(got - want)) <= 1e-4, f"mode {mode} frame {t}"  # the stated tolerance
+                err = float(np.max(np.abs(flow[rows][:, cols] - arr["flow"][keep.index(t)])))
+                keep_err[(mode, t)] = err
         n += 1
     assert n == case["frames"] == arr["digests"].shape[0]
     assert frames_sha.hexdigest() == meta["frames_sha256"], "the frame generator drifted"
+    assert all(e <= 1e-4 for e in keep_err.values()), keep_err  # the stated tolerance ...
     assert first_bad == {1: None, 3: None}, f"first frame whose flow differs, per kernel mode: {first_bad}"
