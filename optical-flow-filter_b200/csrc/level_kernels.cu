@@ -37,7 +37,7 @@ int fused_warp_grid(int N, int S, int W, int H, int band, int* nwx, int* nby) {
     band = band > H ? H : band;
     *nwx = (W + ox - 1) / ox;
     *nby = (H + band - 1) / band;
-    return (*nwx * *nby + lvl::kWarpsPerBlock - 1) / lvl::kWarpsPerBlock;
+    return (lvl::WarpGrid(*nwx, band, H).warps() + lvl::kWarpsPerBlock - 1) / lvl::kWarpsPerBlock;
 }
 
 int fused_resident_warps() {

@@ -35,12 +35,18 @@ namespace lvl {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerBlock = 4;
 #ifndef FFB_ROW_UNROLL
-#define FFB_ROW_UNROLL 1  // rows per loop body (2 saves the 2-row window moves, doubles code)
+#define FFB_ROW_UNROLL 1  // rows per loop body (2: the propagation windows rotate without moves, twice the code)
 #endif
 #ifndef FFB_BLOCKS_PER_SM
 #define FFB_BLOCKS_PER_SM 2
 #endif
 constexpr int kBlocksPerSM = FFB_BLOCKS_PER_SM;  // resident blocks per SM the register budget targets
+#ifndef FFB_PIPE_DELAY
+#define FFB_PIPE_DELAY 0
+#endif
+// rows the update and smoothing of a step run behind its propagation (1: the update chain of
+// the previous row runs beside the propagation chain of this one)
+constexpr int kDelay = FFB_PIPE_DELAY;
 
 // lane-constant geometry and arguments of one warp
 struct Ctx {
@@ -63,6 +69,7 @@ struct Ctx {
     bool any_split;        // some lane's two pixels are not the loaded pair (b0, b0+1)
     int b0;                // even base column of the lane's loaded pair
     char* smem;            // this warp's ring: kDepth slots
+    unsigned smem_s;       // the same as a shared-memory address
     int lane;
 };
 
@@ -136,26 +143,38 @@ __device__ __forceinline__ float2 box5p(const float2 (&t)[5]) { return box5_pair
 // t = -|t| and p - v = -(v - p) exactly.
 // fw = (vel >= 0) per pixel, at = |t| per pixel
 // (packed two-lane instructions, lane = pixel; each lane the scalar operation)
+#ifndef FFB_PACKED_UPWIND
+#define FFB_PACKED_UPWIND 1
+#endif
 template <bool FUSED>
 __device__ __forceinline__ float2 upwind2(float2 v, float2 m, float2 p, bool fw0, bool fw1, float2 at) {
     const float2 n = make_float2(fw0 ? m.x : p.x, fw1 ? m.y : p.y);
+#if FFB_PACKED_UPWIND
     const float2 d = __fadd2_rn(v, make_float2(-n.x, -n.y));
     if (FUSED) return __ffma2_rn(make_float2(-at.x, -at.y), d, v);
     const float2 q = __fmul2_rn(at, d);
     return __fadd2_rn(v, make_float2(-q.x, -q.y));
+#else
+    const float dx = __fsub_rn(v.x, n.x), dy = __fsub_rn(v.y, n.y);
+    if (FUSED) return make_float2(__fmaf_rn(-at.x, dx, v.x), __fmaf_rn(-at.y, dy, v.y));
+    return make_float2(__fsub_rn(v.x, __fmul_rn(at.x, dx)), __fsub_rn(v.y, __fmul_rn(at.y, dy)));
+#endif
 }
 
 __device__ __forceinline__ float2 abs_t(float dt, float2 vel) {
     return make_float2(fabsf(__fmul_rn(dt, vel.x)), fabsf(__fmul_rn(dt, vel.y)));
 }
 
+// row y >= 0 of a pitched image; pitches are below 2^32 bytes, so the offset is one
+// 32 x 32 -> 64-bit multiply
 template <typename T>
 __device__ __forceinline__ const T* rowp(const void* base, size_t pitch, int y) {
-    return reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + (size_t)y * pitch);
+    return reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) +
+                                      (unsigned long long)(unsigned)y * (unsigned)pitch);
 }
 template <typename T>
 __device__ __forceinline__ T* rowp_w(void* base, size_t pitch, int y) {
-    return reinterpret_cast<T*>(reinterpret_cast<char*>(base) + (size_t)y * pitch);
+    return reinterpret_cast<T*>(reinterpret_cast<char*>(base) + (unsigned long long)(unsigned)y * (unsigned)pitch);
 }
 
 // ---------------------------------------------------------------- cp.async staging
@@ -172,17 +191,15 @@ struct Slot {
     static constexpr int TOP_BYTES = 1024, DELTA_BYTES = 2048;
 };
 
-__device__ __forceinline__ void cp16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
+// dst: a shared-memory address (state space .shared, 32 bits)
+__device__ __forceinline__ void cp16(unsigned dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
+__device__ __forceinline__ void cp8(unsigned dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp4(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
+__device__ __forceinline__ void cp4(unsigned dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -190,33 +207,57 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// pair of interleaved float2 pixels (c0, c1) -> (x pair, y pair)
+// pair of interleaved float2 pixels (c0, c1) -> (x pair, y pair).  EX: a lane may store
+// c0 alone (odd right edge); otherwise both pixels of a lane are stored or neither
+template <bool EX>
 __device__ __forceinline__ void store_f2pair(const Ctx& c, float* base, size_t pitch, int y, float2 xs, float2 ysv) {
     float2* row = rowp_w<float2>(base, pitch, y);
     if (c.out1) {
         *reinterpret_cast<float4*>(row + c.c0) = make_float4(xs.x, ysv.x, xs.y, ysv.y);
-    } else if (c.out0) {
+    } else if (EX && c.out0) {
         row[c.c0] = make_float2(xs.x, ysv.x);
     }
 }
+template <bool EX>
 __device__ __forceinline__ void store_f1pair(const Ctx& c, float* base, size_t pitch, int y, float2 v) {
     float* row = rowp_w<float>(base, pitch, y);
     if (c.out1) {
         *reinterpret_cast<float2*>(row + c.c0) = v;
-    } else if (c.out0) {
+    } else if (EX && c.out0) {
         row[c.c0] = v.x;
     }
 }
 
+// ---------------------------------------------------------------- per-warp shared memory
+// [input ring: kDepth slots] [image-model window: 4 rows] [smoothing windows: S x 4 rows].
+// A window row is two planes of 32 lanes x 8 B (one float2 pixel pair per lane): the image
+// and its X blur for the model, the X-pass U and V for a smoothing iteration.  Row y of a
+// window lives in slot y & 3; every lane reads back only what it wrote itself.
+constexpr int kPlane = 32 * 8;
+constexpr int kWinRow = 2 * kPlane;
+template <bool DELTA, int S>
+struct WarpMem {
+    static constexpr int SLOT = DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES;
+    static constexpr int MODEL = kDepth * SLOT;
+    static constexpr int SMOOTH = MODEL + 4 * kWinRow;
+    static constexpr int BYTES = SMOOTH + S * 4 * kWinRow;
+};
+
+__device__ __forceinline__ float2 lds2(const char* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ void sts2(char* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+
 // The pipeline of one warp.  DELTA: delta level (flow, old image and delta flow are
 // propagated; the update refines the coarse flow).  Otherwise a top level (flow is
 // propagated; old image read in place).
-// EM: edge handling compiled in.  bit 0 (EX): the window reaches the left/right image
-// edge or border (column substitution, non-adjacent lanes); bit 1 (EY): the band's rows
-// reach the top/bottom (row clamping and substitution, border rows).
-template <bool DELTA, int N, int S, typename P, int EM>
+// EX: the warp's window reaches an image edge or the propagation border columns (column
+// substitution, per-lane freeze, lanes outside the image).  EY (per row, see run_warp):
+// the rows of this step reach the top/bottom edge or border rows (row clamping,
+// substitution and freeze).  Interior warps and rows compile without any of it.
+// The propagation windows (two rows per sub-step) stay in registers and swap roles with
+// the row parity PAR (the row loop is unrolled by two), so they rotate without moves;
+// the 4-row windows of the 5-tap vertical filters live in shared memory.
+template <bool DELTA, int N, int S, typename P, bool EX>
 struct Pipe {
-    static constexpr bool EX = (EM & 1) != 0, EY = (EM & 2) != 0;
     // propagated channels: U, V (flow) [, I old image, DX, DY delta flow]
     static constexpr int NC = DELTA ? 5 : 2;
     static constexpr int CU = 0, CV = 1, CI = 2, CDX = 3, CDY = 4;
@@ -224,13 +265,15 @@ struct Pipe {
     // last channel each reference kernel writes (flow .y of flowPropagate{X,Y}_k,
     // vector .y of flowPropagatePayload{X,Y}_k)
     static constexpr bool fused(int ch) { return DELTA ? ch != CDY : ch != CV; }
+    using M = WarpMem<DELTA, S>;
 
-    float2 pw[N][2][NC];  // Y sub-step windows: rows (q-1, q) of the X sub-step output
-    float2 imw[4];        // image rows j-4 .. j-1
-    float2 bxw[4];        // X-blurred image rows j-4 .. j-1
-    float2 sw[S][4][2];   // smoothing windows: rows q-2 .. q+1 of the X pass, (U, V)
+    float2 pw[N][2][NC];  // Y sub-step windows: the X sub-step output of the two rows before
+    // propagated channels the update reads (DELTA: old image and delta flow; top: flow),
+    // carried one row when the update runs a row behind the propagation (kDelay)
+    static constexpr int NU = DELTA ? 3 : 2;
+    float2 xu[NU];
 
-    __device__ __forceinline__ void init() {
+    __device__ __forceinline__ void init(const Ctx& c) {
 #pragma unroll
         for (int k = 0; k < N; ++k)
 #pragma unroll
@@ -238,16 +281,18 @@ struct Pipe {
 #pragma unroll
                 for (int ch = 0; ch < NC; ++ch) pw[k][r][ch] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) imw[r] = bxw[r] = make_float2(0.f, 0.f);
+        for (int u = 0; u < NU; ++u) xu[u] = make_float2(0.f, 0.f);
+        char* w = c.smem + M::MODEL + 8 * c.lane;
 #pragma unroll
-        for (int s = 0; s < S; ++s)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) sw[s][r][0] = sw[s][r][1] = make_float2(0.f, 0.f);
+        for (int r = 0; r < 4 * (1 + S); ++r) {
+            sts2(w + r * kWinRow, make_float2(0.f, 0.f));
+            sts2(w + r * kWinRow + kPlane, make_float2(0.f, 0.f));
+        }
     }
 
     // border freeze (propagation_k.cu:59-65): pixels within `border` of an edge keep v
+    template <bool EY>
     __device__ __forceinline__ static void freeze(const Ctx& c, int q, float2 (&out)[NC], const float2 (&v)[NC]) {
-        if (!EX && !EY) return;
         if (EY && (q < c.border || q >= c.H - c.border)) {  // warp-uniform
 #pragma unroll
             for (int ch = 0; ch < NC; ++ch) out[ch] = v[ch];
@@ -260,7 +305,10 @@ struct Pipe {
         }
     }
 
-    // X sub-step in place on row q (flowPropagateX_k / flowPropagatePayloadX_k)
+    // X sub-step in place on row q (flowPropagateX_k / flowPropagatePayloadX_k).  The minus
+    // and plus neighbours of the pair (c0, c1) are (lane-1's c1, c0) and (c1, lane+1's c0);
+    // the upwind neighbour is selected per pixel straight from them.
+    template <bool EY>
     __device__ __forceinline__ static void prop_x(const Ctx& c, int q, float2 (&v)[NC]) {
         float2 m[NC], p[NC];
 #pragma unroll
@@ -274,12 +322,13 @@ struct Pipe {
             if (fused(ch)) o[ch] = upwind2<true>(v[ch], m[ch], p[ch], fw0, fw1, at);
             else o[ch] = upwind2<false>(v[ch], m[ch], p[ch], fw0, fw1, at);
         }
-        freeze(c, q, o, v);
+        freeze<EY>(c, q, o, v);
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) v[ch] = o[ch];
     }
 
     // Y sub-step producing row q from rows q-1 (prev), q (cur), q+1 (next)
+    template <bool EY>
     __device__ __forceinline__ static void prop_y(const Ctx& c, int q, const float2 (&prev)[NC],
                                                   const float2 (&cur)[NC], const float2 (&next)[NC],
                                                   float2 (&o)[NC]) {
@@ -304,22 +353,22 @@ struct Pipe {
             if (fused(ch)) o[ch] = upwind2<true>(cur[ch], m[ch], p[ch], fw0, fw1, at);
             else o[ch] = upwind2<false>(cur[ch], m[ch], p[ch], fw0, fw1, at);
         }
-        freeze(c, q, o, cur);
+        freeze<EY>(c, q, o, cur);
     }
 
-    static constexpr int SLOT = DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES;
-
+    template <bool EY>
     __device__ __forceinline__ static int clampr(const Ctx& c, int r) { return EY ? min(max(r, 0), c.H - 1) : r; }
 
     // copy every input that iteration i consumes into slot `slot`.  Each lane copies the
     // aligned column pair (b0, b0+1) of every field; b0 = clamp(c0) rounded down to even,
     // so one 16/8/4-byte copy per field, and rows carry at least one column of padding.
+    template <bool EY>
     __device__ __forceinline__ static void issue(const Ctx& c, const LevelArgs& a, int slot, int i) {
-        char* sb = c.smem + slot * SLOT;
+        const unsigned sb = c.smem_s + slot * M::SLOT;
         const int l = c.lane;
-        const int r = clampr(c, i);
+        const int r = clampr<EY>(c, i);
         cp16(sb + Slot::FLOW + 16 * l, rowp<float2>(a.fs_in, a.fs_in_pitch, r) + c.b0);
-        const int ru = clampr(c, i - N);  // update row
+        const int ru = clampr<EY>(c, i - N - kDelay);  // update row
         cp8(sb + Slot::IO + 8 * l, rowp<float>(a.io_in, a.io_in_pitch, DELTA ? r : ru) + c.b0);
         if constexpr (DELTA) {
             cp16(sb + Slot::DELTA + 16 * l, rowp<float2>(a.d_in, a.d_in_pitch, r) + c.b0);
@@ -328,7 +377,7 @@ struct Pipe {
             cp8(sb + Slot::COARSE + 16 * l, crow + c.ix0);
             cp8(sb + Slot::COARSE + 16 * l + 8, crow + c.ix1);
         }
-        const int rj = clampr(c, i - N + 2);  // image row
+        const int rj = clampr<EY>(c, i - N + 2 - kDelay);  // image row
         if constexpr (sizeof(P) == 1) {
             // the aligned 32-bit word holding columns b0, b0+1 (image rows are 4-byte
             // aligned and padded to a multiple of 4 bytes; see fused_available)
@@ -349,11 +398,14 @@ struct Pipe {
         return v;
     }
 
-    // one streamed row; its inputs wait in slot `slot`
+    // one streamed row; its inputs wait in slot `slot`.  PAR: row parity (which register
+    // of each propagation window holds the older row), or -1 when the loop body holds one
+    // row and the windows shift; EA: the inputs this step stages need row clamping
+    template <bool EY, bool EA, int PAR>
     __device__ __forceinline__ void step(const Ctx& c, const LevelArgs& a, int i, int slot) {
         const int H = c.H;
         cp_wait<kDepth - 1>();
-        const char* sb = c.smem + slot * SLOT;
+        const char* sb = c.smem + slot * M::SLOT;
         const int l = c.lane;
         // ---- state row i
         float2 x[NC];
@@ -379,8 +431,15 @@ struct Pipe {
             }
             if constexpr (sizeof(P) == 1) {
                 const uint32_t w = *reinterpret_cast<const uint32_t*>(sb + Slot::IMG + 8 * l);
-                const uint32_t v0 = (w >> (8 * (c.cc0 & 3))) & 0xffu;
-                const uint32_t v1 = (w >> (8 * (c.cc1 & 3))) & 0xffu;
+                uint32_t v0, v1;
+                if (EX) {
+                    v0 = (w >> (8 * (c.cc0 & 3))) & 0xffu;
+                    v1 = (w >> (8 * (c.cc1 & 3))) & 0xffu;
+                } else {  // c0 even and inside: the pair is bytes sh, sh+1 of the word
+                    const uint32_t sh = 8 * (c.cc0 & 2);
+                    v0 = (w >> sh) & 0xffu;
+                    v1 = (w >> (sh + 8)) & 0xffu;
+                }
                 im = make_float2(u8_to_unit(v0), u8_to_unit(v1));
             } else {
                 const float2 ip = *reinterpret_cast<const float2*>(sb + Slot::IMG + 8 * l);
@@ -388,40 +447,51 @@ struct Pipe {
             }
         }
         // the slot is free again: stage the row needed kDepth iterations from now
-        issue(c, a, slot, i + kDepth);
+        issue<EA>(c, a, slot, i + kDepth);
         cp_commit();
         // ---- N propagation sub-steps
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             const int q = i - k;  // row of this X sub-step
-            prop_x(c, q, x);
+            prop_x<EY>(c, q, x);
             float2 y[NC];
-            prop_y(c, q - 1, pw[k][0], pw[k][1], x, y);
+            prop_y<EY>(c, q - 1, pw[k][PAR < 0 ? 0 : PAR], pw[k][PAR < 0 ? 1 : PAR ^ 1], x, y);
 #pragma unroll
             for (int ch = 0; ch < NC; ++ch) {
-                pw[k][0][ch] = pw[k][1][ch];
-                pw[k][1][ch] = x[ch];
+                if (PAR < 0) {  // one row per loop body: the window shifts
+                    pw[k][0][ch] = pw[k][1][ch];
+                    pw[k][1][ch] = x[ch];
+                } else {
+                    pw[k][PAR][ch] = x[ch];  // the newest row replaces the oldest
+                }
                 x[ch] = y[ch];
             }
         }
-        const int r = i - N;  // row of the update
+        const int r = i - N - kDelay;  // row of the update
+        // the propagated channels the update reads: this row's, or the previous row's
+        float2 pu[NU];
+#pragma unroll
+        for (int u = 0; u < NU; ++u) {
+            const float2 now = x[DELTA ? CI + u : CU + u];
+            pu[u] = kDelay ? xu[u] : now;
+            xu[u] = now;
+        }
+        // window rows: slot (i + k) & 3 holds the row k steps after the oldest
+        const int w0 = ((i + 0) & 3) * kWinRow, w1 = ((i + 1) & 3) * kWinRow;
+        const int w2 = ((i + 2) & 3) * kWinRow, w3 = ((i + 3) & 3) * kWinRow;
+        char* wl = c.smem + 8 * l;
         // ---- image model at row r (imagemodel_k.cu:31-133)
         float2 a0, ax, ay;
         {
+            char* mw = wl + M::MODEL;
             float2 t[5];
             nb5_raw(im, t);
             const float2 bx = smooth5p(t);
-            float2 by, rows[5] = {imw[0], imw[1], imw[2], imw[3], im};
-            by = smooth5p(rows);
-            float2 brows[5] = {bxw[0], bxw[1], bxw[2], bxw[3], bx};
-            ay = diff5p(brows);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                imw[k] = imw[k + 1];
-                bxw[k] = bxw[k + 1];
-            }
-            imw[3] = im;
-            bxw[3] = bx;
+            const float2 by = smooth5_pair(lds2(mw + w0), lds2(mw + w1), lds2(mw + w2), lds2(mw + w3), im);
+            ay = diff5_pair(lds2(mw + w0 + kPlane), lds2(mw + w1 + kPlane), lds2(mw + w2 + kPlane),
+                            lds2(mw + w3 + kPlane), bx);
+            sts2(mw + w0, im);
+            sts2(mw + w0 + kPlane, bx);
             float2 tb[5];
             nb5_raw(by, tb);
             a0 = smooth5p(tb);
@@ -429,19 +499,19 @@ struct Pipe {
         }
         // ---- update at row r
         float2 fu, fv;
-        const bool store_r = r >= c.ys && r < c.ye;
+        float2 dox, doy;  // the update's stored flow: delta flow (delta levels), unsmoothed flow (top)
         {
             float2 old;
-            if constexpr (DELTA) old = x[CI];
+            if constexpr (DELTA) old = pu[0];
             else old = io_u;
             if (c.first) old = a0;
             float2 fx, fy;
             if constexpr (DELTA) {
-                fx = x[CDX];
-                fy = x[CDY];
+                fx = pu[1];
+                fy = pu[2];
             } else {
-                fx = x[CU];
-                fy = x[CV];
+                fx = pu[0];
+                fy = pu[1];
             }
             float2 ox, oy;
             solve2(c.gamma, ax.x, ay.x, __fsub_rn(old.x, a0.x), fx.x, fy.x, ox.x, oy.x);
@@ -455,30 +525,30 @@ struct Pipe {
                                  clampm(__fadd_rn(ox.y, __fmul_rn(2.0f, u1.x)), c.maxflow));
                 fv = make_float2(clampm(__fadd_rn(oy.x, __fmul_rn(2.0f, u0.y)), c.maxflow),
                                  clampm(__fadd_rn(oy.y, __fmul_rn(2.0f, u1.y)), c.maxflow));
-                if (store_r) {
-                    store_f2pair(c, a.d_out, a.d_out_pitch, r, ox, oy);
-                    store_f1pair(c, a.io_out, a.io_out_pitch, r, a0);
-                }
+                dox = ox;
+                doy = oy;
             } else {
                 // flowUpdate_k (update_k.cu:65-78)
                 fu = make_float2(sanitize(clampm(ox.x, c.maxflow)), sanitize(clampm(ox.y, c.maxflow)));
                 fv = make_float2(sanitize(clampm(oy.x, c.maxflow)), sanitize(clampm(oy.y, c.maxflow)));
-                if (store_r) {
-                    store_f1pair(c, a.io_out, a.io_out_pitch, r, a0);
-                    if (a.fu_out) store_f2pair(c, a.fu_out, a.fu_out_pitch, r, fu, fv);
-                }
+                dox = fu;
+                doy = fv;
             }
         }
         // ---- S smoothing iterations (flowsmoothing_k.cu:21-87)
 #pragma unroll
         for (int s = 0; s < S; ++s) {
+            char* sw = wl + M::SMOOTH + s * 4 * kWinRow;
             float2 tu[5], tv[5];
             nb5<EX>(c, fu, tu);
             nb5<EX>(c, fv, tv);
             const float2 sxu = box5p(tu), sxv = box5p(tv);
             const int q = r - 2 * s - 2;  // row of this Y pass
-            float2 ru[5] = {sw[s][0][0], sw[s][1][0], sw[s][2][0], sw[s][3][0], sxu};
-            float2 rv[5] = {sw[s][0][1], sw[s][1][1], sw[s][2][1], sw[s][3][1], sxv};
+            float2 ru[5] = {lds2(sw + w0), lds2(sw + w1), lds2(sw + w2), lds2(sw + w3), sxu};
+            float2 rv[5] = {lds2(sw + w0 + kPlane), lds2(sw + w1 + kPlane), lds2(sw + w2 + kPlane),
+                            lds2(sw + w3 + kPlane), sxv};
+            sts2(sw + w0, sxu);
+            sts2(sw + w0 + kPlane, sxv);
             if (EY && (q < 2 || q > H - 3)) {
                 // clamp-to-edge rows: slot k holds row q-2+k
                 float2 cu[5], cv[5];
@@ -499,40 +569,77 @@ struct Pipe {
                 fu = box5p(ru);
                 fv = box5p(rv);
             }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                sw[s][k][0] = sw[s][k + 1][0];
-                sw[s][k][1] = sw[s][k + 1][1];
-            }
-            sw[s][3][0] = sxu;
-            sw[s][3][1] = sxv;
+        }
+        // ---- stores, after all arithmetic of the step
+        if (r >= c.ys && r < c.ye) {  // warp-uniform
+            store_f1pair<EX>(c, a.io_out, a.io_out_pitch, r, a0);
+            if (DELTA) store_f2pair<EX>(c, a.d_out, a.d_out_pitch, r, dox, doy);
+            else if (a.fu_out) store_f2pair<EX>(c, a.fu_out, a.fu_out_pitch, r, dox, doy);
         }
         const int rs = r - 2 * S;
-        if (rs >= c.ys && rs < c.ye) store_f2pair(c, a.fs_out, a.fs_out_pitch, rs, fu, fv);
+        if (rs >= c.ys && rs < c.ye) store_f2pair<EX>(c, a.fs_out, a.fs_out_pitch, rs, fu, fv);
     }
 };
 
-template <bool DELTA, int N, int S, typename P, int EM>
+// Rows [lo, hi] of a level are interior for the streaming pipeline when a step there and
+// the inputs it stages need no row clamping, substitution or freeze.  A step at row i
+// stages row i+kDepth, whose loads reach rows i+kDepth-N (update) up to i+kDepth (state)
+// and i+kDepth-N+2 (image, below the state row when N < 2); its propagation rows i-N .. i
+// stay inside the border, and its smoothing windows (down to row i-N-2S-2) inside the image.
+template <int N, int S>
+__device__ __forceinline__ void interior_rows(int H, int border, int& lo, int& hi) {
+    const int mb = border > 1 ? border : 1;
+    constexpr int ahead = kDepth + (N + kDelay < 2 ? 2 - N - kDelay : 0);  // rows below i the staged loads reach
+    lo = N + kDelay + (2 * S + 2 > mb ? 2 * S + 2 : mb);
+    hi = H - 1 - (ahead > mb ? ahead : mb);
+}
+
+template <bool DELTA, int N, int S, typename P, bool EX>
 __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int iters) {
-    using Pp = Pipe<DELTA, N, S, P, EM>;
+    using Pp = Pipe<DELTA, N, S, P, EX>;
     Pp pipe;
-    pipe.init();
+    pipe.init(c);
 #pragma unroll
     for (int u = 0; u < kDepth; ++u) {
-        Pp::issue(c, a, u, i0 + u);
+        Pp::template issue<true>(c, a, u, i0 + u);
         cp_commit();
     }
-    // one row per iteration, not unrolled: the loop body must stay small enough for the
-    // instruction cache; the windows rotate by register moves and the slot index cycles
+    // rows [lo, hi] are interior (no row clamping, substitution or freeze)
+    int lo, hi;
+    interior_rows<N, S>(c.H, c.border, lo, hi);
 #if FFB_ROW_UNROLL == 2
+    // two rows per loop body (the propagation windows swap roles instead of moving); a body
+    // is interior when both of its rows are.  kDepth is a multiple of 2, so the slot index
+    // of step it is it & (kDepth - 1)
 #pragma unroll 1
     for (int it = 0; it < iters; it += 2) {
-        pipe.step(c, a, i0 + it, it & (kDepth - 1));
-        pipe.step(c, a, i0 + it + 1, (it + 1) & (kDepth - 1));
+        const int i = i0 + it;
+        if (i >= lo && i + 1 <= hi) {  // warp-uniform
+            pipe.template step<false, false, 0>(c, a, i, it & (kDepth - 1));
+            pipe.template step<false, false, 1>(c, a, i + 1, (it + 1) & (kDepth - 1));
+        } else {
+            pipe.template step<true, true, 0>(c, a, i, it & (kDepth - 1));
+            pipe.template step<true, true, 1>(c, a, i + 1, (it + 1) & (kDepth - 1));
+        }
     }
 #else
+    // one row per loop body, kept small for the instruction cache: the edge rows before and
+    // after the interior ones run one loop, the interior rows another
+    int it_a = lo - i0, it_b = hi - i0 + 1;
+    it_a = it_a < 0 ? 0 : (it_a > iters ? iters : it_a);
+    it_b = it_b < it_a ? it_a : (it_b > iters ? iters : it_b);
+    int it = 0;
 #pragma unroll 1
-    for (int it = 0; it < iters; ++it) pipe.step(c, a, i0 + it, it & (kDepth - 1));
+    for (int ph = 0; ph < 3; ++ph) {
+        const int end = ph == 0 ? it_a : (ph == 1 ? it_b : iters);
+        if (ph == 1) {
+#pragma unroll 1
+            for (; it < end; ++it) pipe.template step<false, false, -1>(c, a, i0 + it, it & (kDepth - 1));
+        } else {
+#pragma unroll 1
+            for (; it < end; ++it) pipe.template step<true, true, -1>(c, a, i0 + it, it & (kDepth - 1));
+        }
+    }
 #endif
     cp_wait<0>();
 }
@@ -541,21 +648,52 @@ __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int
 __host__ __device__ constexpr int halo_x(int N, int S) { return ((2 * S + (N > 2 ? N : 2)) + 1) & ~1; }
 __host__ __device__ constexpr int lead_rows(int N, int S) { return 2 * S + (N > 4 - N ? N : 4 - N); }
 
-// warp `warp` of a level's nwx x nby grid of (64-column window, band) warps
+// The warps of a level: nwx windows of 64 columns, each cut into bands of `band` rows.
+// The first and last windows (where the image edges are, and the column handling makes a
+// row dearer) are cut into bands of half the height, so their warps finish with the rest.
+struct WarpGrid {
+    int nwx, band, nby;   // interior windows: nby bands of `band` rows
+    int ne, band_e, nby_e;  // edge windows (ne of them): nby_e bands of band_e rows
+    __host__ __device__ WarpGrid(int nwx_, int band_, int H) : nwx(nwx_), band(band_) {
+        nby = (H + band - 1) / band;
+        ne = nwx < 2 ? nwx : 2;
+        band_e = (band + 1) / 2 < 8 ? (band < 8 ? band : 8) : (band + 1) / 2;
+        nby_e = (H + band_e - 1) / band_e;
+    }
+    __host__ __device__ int warps() const { return ne * nby_e + (nwx - ne) * nby; }
+    // window column, first row and row count of warp w
+    __host__ __device__ void at(int w, int& wx, int& ys, int& rows) const {
+        if (w < ne * nby_e) {
+            wx = w < nby_e ? 0 : nwx - 1;
+            ys = (w % nby_e) * band_e;
+            rows = band_e;
+        } else {
+            w -= ne * nby_e;
+            wx = 1 + w % (nwx - ne);
+            ys = (w / (nwx - ne)) * band;
+            rows = band;
+        }
+    }
+};
+
+// warp `warp` of a level's WarpGrid of (64-column window, band) warps
 template <bool DELTA, int N, int S, typename P>
-__device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int nby, int band, int warp, char* smem_raw) {
+__device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band, int warp, char* smem_raw) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
-    if (warp >= nwx * nby) return;  // whole warps exit together
+    const WarpGrid g(nwx, band, a.H);
+    if (warp >= g.warps()) return;  // whole warps exit together
     const int lane = threadIdx.x & 31;
-    const int wx = warp % nwx, by = warp / nwx;
+    int wx, ys0, rows;
+    g.at(warp, wx, ys0, rows);
     const int W = a.W, H = a.H;
 
     Ctx c;
     c.W = W;
     c.H = H;
     c.lane = lane;
-    c.smem = smem_raw + (threadIdx.x >> 5) * (kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES));
+    c.smem = smem_raw + (threadIdx.x >> 5) * WarpMem<DELTA, S>::BYTES;
+    c.smem_s = (unsigned)__cvta_generic_to_shared(c.smem);
     const int xo = wx * OX, x0 = xo - HX;
     c.c0 = x0 + 2 * lane;
     c.c1 = c.c0 + 1;
@@ -568,8 +706,8 @@ __device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int nby,
     c.border = a.border;
     c.col0 = c.c0 >= a.border && c.c0 < W - a.border;
     c.col1 = c.c1 >= a.border && c.c1 < W - a.border;
-    c.ys = by * band;
-    c.ye = min(c.ys + band, H);
+    c.ys = ys0;
+    c.ye = min(ys0 + rows, H);
     c.first = a.first;
     c.dt = 1.0f / (float)N;  // FlowPropagator::setIterations (propagation.cu:146-147)
     c.gamma = a.gamma;
@@ -590,25 +728,22 @@ __device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int nby,
     c.any_edge = __any_sync(kFull, c.e_l || c.e_r0 || c.e_r1 || c.e_r2);
     c.any_split = __any_sync(kFull, c.cc0 != c.b0 || c.cc1 != c.b0 + 1);
     const int i0 = c.ys - lead_rows(N, S);
-    const int last = c.ye - 1 + N + 2 * S;
+    const int last = c.ye - 1 + N + kDelay + 2 * S;
     const int iters = (last - i0 + 1 + 1) & ~1;  // even: the loop body holds two rows
-    // interior warps: no clamping, substitution or border freeze can reach them
-    const int m = (a.border > 2 ? a.border : 2) + 1;
-    const int rlo = i0 - N - 2 * S - 2, rhi = i0 + iters + 2;
-    // One code path for every warp: the edge handling costs a few selects per row, while
-    // several variants of this large loop body in one kernel thrash the instruction cache.
-    (void)m;
-    (void)rlo;
-    (void)rhi;
-    run_warp<DELTA, N, S, P, 3>(a, c, i0, iters);
+    // Warps whose 64 columns lie inside the image and outside the border columns (all but
+    // the first and last window of each band) run the pipeline without column handling.
+    if (c.any_edge || c.freeze_cols || c.any_split)  // warp-uniform
+        run_warp<DELTA, N, S, P, true>(a, c, i0, iters);
+    else
+        run_warp<DELTA, N, S, P, false>(a, c, i0, iters);
 }
 
 template <bool DELTA, int N, int S, typename P>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int nby, int band) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int band) {
     extern __shared__ __align__(16) char smem_raw[];
     grid_dep_wait();
     grid_dep_launch();
-    level_warp<DELTA, N, S, P>(a, nwx, nby, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
+    level_warp<DELTA, N, S, P>(a, nwx, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
 }
 
 // many levels of one (DELTA, N, S) in one launch: each job a contiguous range of blocks
@@ -626,21 +761,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM)
         else hi = mid - 1;
     }
     const StreamJob& j = jobs[lo];
-    level_warp<DELTA, N, S, uint8_t>(j.a, j.nwx, j.nby, j.band,
+    level_warp<DELTA, N, S, uint8_t>(j.a, j.nwx, j.band,
                                      ((int)blockIdx.x - j.first_block) * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
 }
 
 template <bool DELTA, int N, int S>
 cudaError_t launch_batch(const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
-    const int smem = kWarpsPerBlock * kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES);
+    const int smem = kWarpsPerBlock * WarpMem<DELTA, S>::BYTES;
     static std::atomic<unsigned long long> prepared{0};
     int dev = 0;
     cudaGetDevice(&dev);
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(prepared.load() & bit)) {
-        const cudaError_t e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>,
-                                                   cudaFuncAttributePreferredSharedMemoryCarveout,
-                                                   (int)cudaSharedmemCarveoutMaxShared);
+        cudaError_t e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>,
+                                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         prepared.fetch_or(bit);
     }
@@ -651,33 +788,45 @@ template <bool DELTA, int N, int S, typename P>
 cudaError_t launch(const LevelArgs& a, cudaStream_t s) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
-    const int smem = kWarpsPerBlock * kDepth * (DELTA ? Slot::DELTA_BYTES : Slot::TOP_BYTES);
-    // resident warps on this device, queried once per instantiation
-    static int resident_warps = 0;
+    const int smem = kWarpsPerBlock * WarpMem<DELTA, S>::BYTES;
+    // row offsets are computed as 32 x 32-bit products (rowp)
+    for (size_t p : {a.img_pitch, a.fs_in_pitch, a.io_in_pitch, a.d_in_pitch, a.fs_out_pitch, a.io_out_pitch,
+                     a.d_out_pitch, a.fu_out_pitch, a.coarse_pitch})
+        if (p >> 32) return cudaErrorInvalidPitchValue;
+    // resident warps on this device, queried once per instantiation and device (the
+    // function attributes are set per device as well)
+    static int resident[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& resident_warps = resident[dev & 63];
     if (resident_warps == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         // full shared carve-out, as for the tile kernels: SMs running this kernel can then
         // also host the tile kernels of the levels that run beside it
         cudaFuncSetAttribute(level_k<DELTA, N, S, P>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
+        const cudaError_t e =
+            cudaFuncSetAttribute(level_k<DELTA, N, S, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_k<DELTA, N, S, P>, kWarpsPerBlock * 32, smem);
         resident_warps = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1) * kWarpsPerBlock;
     }
     const int nwx = (a.W + OX - 1) / OX;
-    // bands: as few as fill the resident warps once (every extra band restarts a pipeline)
+    // bands: as few as fill the resident warps once (every extra band restarts a pipeline);
+    // the edge windows' half-height bands count twice
     int band = a.band;
     if (band <= 0) {
-        const int bands = resident_warps / nwx > 0 ? resident_warps / nwx : 1;
+        const int cols = nwx + (nwx < 2 ? nwx : 2);
+        const int bands = resident_warps / cols > 0 ? resident_warps / cols : 1;
         band = (a.H + bands - 1) / bands;
+        while (band < a.H && WarpGrid(nwx, band, a.H).warps() > resident_warps) ++band;
     }
     band = band < 8 ? 8 : band;
     band = band > a.H ? a.H : band;
-    const int nby = (a.H + band - 1) / band;
-    const int warps = nwx * nby;
+    const int warps = WarpGrid(nwx, band, a.H).warps();
     const int blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    return launch_k(level_k<DELTA, N, S, P>, dim3(blocks), dim3(kWarpsPerBlock * 32), smem, s, a, nwx, nby, band);
+    return launch_k(level_k<DELTA, N, S, P>, dim3(blocks), dim3(kWarpsPerBlock * 32), smem, s, a, nwx, band);
 }
 
 }  // namespace lvl

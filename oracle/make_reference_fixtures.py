@@ -152,6 +152,13 @@ def run_long(out: str) -> None:
         th.join()
         if proc.wait() != 0:
             raise RuntimeError(f"{name}: reference driver failed")
+        # the frames this run shares with a short parity case must give that case's flows
+        short = os.path.join(GOLDEN, "ref_case_bumps_2048x1088_L3.npz")
+        if name.startswith("bumps_2048x1088_L3") and os.path.exists(short):
+            m = json.loads(bytes(np.load(short)["meta"]).decode())
+            for t, want in zip(m["dump"], m["flow_sha256"]):
+                if digests[t].hex() != want:
+                    raise RuntimeError(f"{name}: frame {t} differs from the short reference run")
         meta = dict(case, name=name, frames_sha256=frame_sha.hexdigest(), layout="subsampled")
         np.savez_compressed(os.path.join(out, f"long_{name}.npz"),
                             digests=np.frombuffer(b"".join(digests), np.uint8).reshape(-1, 32),
