@@ -68,8 +68,8 @@ struct Ctx {
     bool any_edge;         // some lane of this warp needs horizontal edge substitution
     bool any_split;        // some lane's two pixels are not the loaded pair (b0, b0+1)
     int b0;                // even base column of the lane's loaded pair
-    char* smem;            // this warp's ring: kDepth slots
-    unsigned smem_s;       // the same as a shared-memory address
+    unsigned o8, o16;      // this warp's shared memory (lvl_smem offset) + 8 / 16 bytes per lane
+    unsigned smem_s;       // this warp's shared memory as a shared-state-space address
     int lane;
 };
 
@@ -243,8 +243,12 @@ struct WarpMem {
     static constexpr int BYTES = SMOOTH + S * 4 * kWinRow;
 };
 
-__device__ __forceinline__ float2 lds2(const char* p) { return *reinterpret_cast<const float2*>(p); }
-__device__ __forceinline__ void sts2(char* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+// The block's dynamic shared memory, addressed by 32-bit byte offsets (the kernels below
+// declare the same array)
+extern __shared__ __align__(16) char lvl_smem[];
+__device__ __forceinline__ float2 lds2(unsigned off) { return *reinterpret_cast<const float2*>(lvl_smem + off); }
+__device__ __forceinline__ void sts2(unsigned off, float2 v) { *reinterpret_cast<float2*>(lvl_smem + off) = v; }
+__device__ __forceinline__ float4 lds4(unsigned off) { return *reinterpret_cast<const float4*>(lvl_smem + off); }
 
 // The pipeline of one warp.  DELTA: delta level (flow, old image and delta flow are
 // propagated; the update refines the coarse flow).  Otherwise a top level (flow is
@@ -272,6 +276,13 @@ struct Pipe {
     // carried one row when the update runs a row behind the propagation (kDelay)
     static constexpr int NU = DELTA ? 3 : 2;
     float2 xu[NU];
+    int cr_next;  // delta levels: coarse row of the update row the next step stages
+
+    // coarse row (upmap_index of the row, from the level's table) read by the update of the
+    // row that step i stages
+    __device__ __forceinline__ static int coarse_row(const Ctx& c, const LevelArgs& a, int i) {
+        return __ldg(a.coarse_rows + min(max(i - N - kDelay, 0), c.H - 1));
+    }
 
     __device__ __forceinline__ void init(const Ctx& c) {
 #pragma unroll
@@ -282,7 +293,7 @@ struct Pipe {
                 for (int ch = 0; ch < NC; ++ch) pw[k][r][ch] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int u = 0; u < NU; ++u) xu[u] = make_float2(0.f, 0.f);
-        char* w = c.smem + M::MODEL + 8 * c.lane;
+        const unsigned w = c.o8 + M::MODEL;
 #pragma unroll
         for (int r = 0; r < 4 * (1 + S); ++r) {
             sts2(w + r * kWinRow, make_float2(0.f, 0.f));
@@ -363,27 +374,28 @@ struct Pipe {
     // aligned column pair (b0, b0+1) of every field; b0 = clamp(c0) rounded down to even,
     // so one 16/8/4-byte copy per field, and rows carry at least one column of padding.
     template <bool EY>
-    __device__ __forceinline__ static void issue(const Ctx& c, const LevelArgs& a, int slot, int i) {
-        const unsigned sb = c.smem_s + slot * M::SLOT;
-        const int l = c.lane;
+    // crow: the coarse row of the update row i - N - kDelay (delta levels)
+    __device__ __forceinline__ static void issue(const Ctx& c, const LevelArgs& a, int slot, int i, int crow_y) {
+        const unsigned sb8 = c.smem_s + 8 * c.lane + slot * M::SLOT;
+        const unsigned sb16 = c.smem_s + 16 * c.lane + slot * M::SLOT;
         const int r = clampr<EY>(c, i);
-        cp16(sb + Slot::FLOW + 16 * l, rowp<float2>(a.fs_in, a.fs_in_pitch, r) + c.b0);
+        cp16(sb16 + Slot::FLOW, rowp<float2>(a.fs_in, a.fs_in_pitch, r) + c.b0);
         const int ru = clampr<EY>(c, i - N - kDelay);  // update row
-        cp8(sb + Slot::IO + 8 * l, rowp<float>(a.io_in, a.io_in_pitch, DELTA ? r : ru) + c.b0);
+        cp8(sb8 + Slot::IO, rowp<float>(a.io_in, a.io_in_pitch, DELTA ? r : ru) + c.b0);
         if constexpr (DELTA) {
-            cp16(sb + Slot::DELTA + 16 * l, rowp<float2>(a.d_in, a.d_in_pitch, r) + c.b0);
+            cp16(sb16 + Slot::DELTA, rowp<float2>(a.d_in, a.d_in_pitch, r) + c.b0);
             // coarse row of the update row from the level's row table (upmap_index of each row)
-            const float2* crow = rowp<float2>(a.coarse, a.coarse_pitch, __ldg(a.coarse_rows + ru));
-            cp8(sb + Slot::COARSE + 16 * l, crow + c.ix0);
-            cp8(sb + Slot::COARSE + 16 * l + 8, crow + c.ix1);
+            const float2* crow = rowp<float2>(a.coarse, a.coarse_pitch, crow_y);
+            cp8(sb16 + Slot::COARSE, crow + c.ix0);
+            cp8(sb16 + Slot::COARSE + 8, crow + c.ix1);
         }
         const int rj = clampr<EY>(c, i - N + 2 - kDelay);  // image row
         if constexpr (sizeof(P) == 1) {
             // the aligned 32-bit word holding columns b0, b0+1 (image rows are 4-byte
             // aligned and padded to a multiple of 4 bytes; see fused_available)
-            cp4(sb + Slot::IMG + 8 * l, reinterpret_cast<const uint8_t*>(rowp<P>(a.img, a.img_pitch, rj)) + (c.b0 & ~3));
+            cp4(sb8 + Slot::IMG, reinterpret_cast<const uint8_t*>(rowp<P>(a.img, a.img_pitch, rj)) + (c.b0 & ~3));
         } else {
-            cp8(sb + Slot::IMG + 8 * l, rowp<P>(a.img, a.img_pitch, rj) + c.b0);
+            cp8(sb8 + Slot::IMG, rowp<P>(a.img, a.img_pitch, rj) + c.b0);
         }
     }
 
@@ -405,32 +417,31 @@ struct Pipe {
     __device__ __forceinline__ void step(const Ctx& c, const LevelArgs& a, int i, int slot) {
         const int H = c.H;
         cp_wait<kDepth - 1>();
-        const char* sb = c.smem + slot * M::SLOT;
-        const int l = c.lane;
+        const unsigned sb8 = c.o8 + slot * M::SLOT, sb16 = c.o16 + slot * M::SLOT;
         // ---- state row i
         float2 x[NC];
         float2 io_u;  // top levels: old image at the update row
         float2 im;    // image row i-N+2
         float4 cf;    // delta levels: coarse flow (u0, v0, u1, v1) at the update row
         {
-            const float4 q = *reinterpret_cast<const float4*>(sb + Slot::FLOW + 16 * l);
+            const float4 q = lds4(sb16 + Slot::FLOW);
             x[CU] = unpair(c, q.x, q.z);
             x[CV] = unpair(c, q.y, q.w);
-            const float2 iop = *reinterpret_cast<const float2*>(sb + Slot::IO + 8 * l);
+            const float2 iop = lds2(sb8 + Slot::IO);
             const float2 io = unpair(c, iop.x, iop.y);
             if constexpr (DELTA) {
                 x[CI] = io;
-                const float4 d = *reinterpret_cast<const float4*>(sb + Slot::DELTA + 16 * l);
+                const float4 d = lds4(sb16 + Slot::DELTA);
                 x[CDX] = unpair(c, d.x, d.z);
                 x[CDY] = unpair(c, d.y, d.w);
-                cf = *reinterpret_cast<const float4*>(sb + Slot::COARSE + 16 * l);
+                cf = lds4(sb16 + Slot::COARSE);
                 io_u = make_float2(0.f, 0.f);
             } else {
                 io_u = io;
                 cf = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             if constexpr (sizeof(P) == 1) {
-                const uint32_t w = *reinterpret_cast<const uint32_t*>(sb + Slot::IMG + 8 * l);
+                const uint32_t w = *reinterpret_cast<const uint32_t*>(lvl_smem + sb8 + Slot::IMG);
                 uint32_t v0, v1;
                 if (EX) {
                     v0 = (w >> (8 * (c.cc0 & 3))) & 0xffu;
@@ -442,12 +453,15 @@ struct Pipe {
                 }
                 im = make_float2(u8_to_unit(v0), u8_to_unit(v1));
             } else {
-                const float2 ip = *reinterpret_cast<const float2*>(sb + Slot::IMG + 8 * l);
+                const float2 ip = lds2(sb8 + Slot::IMG);
                 im = unpair(c, ip.x, ip.y);
             }
         }
         // the slot is free again: stage the row needed kDepth iterations from now
-        issue<EA>(c, a, slot, i + kDepth);
+        // the coarse row of the row staged next step is loaded a step ahead
+        const int crow_y = cr_next;
+        if constexpr (DELTA) cr_next = coarse_row(c, a, i + 1 + kDepth);
+        issue<EA>(c, a, slot, i + kDepth, crow_y);
         cp_commit();
         // ---- N propagation sub-steps
 #pragma unroll
@@ -479,11 +493,11 @@ struct Pipe {
         // window rows: slot (i + k) & 3 holds the row k steps after the oldest
         const int w0 = ((i + 0) & 3) * kWinRow, w1 = ((i + 1) & 3) * kWinRow;
         const int w2 = ((i + 2) & 3) * kWinRow, w3 = ((i + 3) & 3) * kWinRow;
-        char* wl = c.smem + 8 * l;
+        const unsigned wl = c.o8;
         // ---- image model at row r (imagemodel_k.cu:31-133)
         float2 a0, ax, ay;
         {
-            char* mw = wl + M::MODEL;
+            const unsigned mw = wl + M::MODEL;
             float2 t[5];
             nb5_raw(im, t);
             const float2 bx = smooth5p(t);
@@ -538,7 +552,7 @@ struct Pipe {
         // ---- S smoothing iterations (flowsmoothing_k.cu:21-87)
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            char* sw = wl + M::SMOOTH + s * 4 * kWinRow;
+            const unsigned sw = wl + M::SMOOTH + s * 4 * kWinRow;
             float2 tu[5], tv[5];
             nb5<EX>(c, fu, tu);
             nb5<EX>(c, fv, tv);
@@ -599,9 +613,10 @@ __device__ __forceinline__ void run_warp(const LevelArgs& a, Ctx& c, int i0, int
     using Pp = Pipe<DELTA, N, S, P, EX>;
     Pp pipe;
     pipe.init(c);
+    pipe.cr_next = DELTA ? Pp::coarse_row(c, a, i0 + kDepth) : 0;
 #pragma unroll
     for (int u = 0; u < kDepth; ++u) {
-        Pp::template issue<true>(c, a, u, i0 + u);
+        Pp::template issue<true>(c, a, u, i0 + u, DELTA ? Pp::coarse_row(c, a, i0 + u) : 0);
         cp_commit();
     }
     // rows [lo, hi] are interior (no row clamping, substitution or freeze)
@@ -678,7 +693,7 @@ struct WarpGrid {
 
 // warp `warp` of a level's WarpGrid of (64-column window, band) warps
 template <bool DELTA, int N, int S, typename P>
-__device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band, int warp, char* smem_raw) {
+__device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band, int warp) {
     constexpr int HX = halo_x(N, S);
     constexpr int OX = 64 - 2 * HX;
     const WarpGrid g(nwx, band, a.H);
@@ -692,8 +707,10 @@ __device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band
     c.W = W;
     c.H = H;
     c.lane = lane;
-    c.smem = smem_raw + (threadIdx.x >> 5) * WarpMem<DELTA, S>::BYTES;
-    c.smem_s = (unsigned)__cvta_generic_to_shared(c.smem);
+    const unsigned so = (threadIdx.x >> 5) * WarpMem<DELTA, S>::BYTES;
+    c.o8 = so + 8 * lane;
+    c.o16 = so + 16 * lane;
+    c.smem_s = (unsigned)__cvta_generic_to_shared(lvl_smem) + so;
     const int xo = wx * OX, x0 = xo - HX;
     c.c0 = x0 + 2 * lane;
     c.c1 = c.c0 + 1;
@@ -740,10 +757,9 @@ __device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band
 
 template <bool DELTA, int N, int S, typename P>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(LevelArgs a, int nwx, int band) {
-    extern __shared__ __align__(16) char smem_raw[];
     grid_dep_wait();
     grid_dep_launch();
-    level_warp<DELTA, N, S, P>(a, nwx, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
+    level_warp<DELTA, N, S, P>(a, nwx, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5));
 }
 
 // many levels of one (DELTA, N, S) in one launch: each job a contiguous range of blocks
@@ -751,7 +767,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(Lev
 template <bool DELTA, int N, int S>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM)
     level_batch_k(const StreamJob* __restrict__ jobs, int n) {
-    extern __shared__ __align__(16) char smem_raw[];
     grid_dep_wait();
     grid_dep_launch();
     int lo = 0, hi = n - 1;
@@ -762,7 +777,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM)
     }
     const StreamJob& j = jobs[lo];
     level_warp<DELTA, N, S, uint8_t>(j.a, j.nwx, j.band,
-                                     ((int)blockIdx.x - j.first_block) * kWarpsPerBlock + (threadIdx.x >> 5), smem_raw);
+                                     ((int)blockIdx.x - j.first_block) * kWarpsPerBlock + (threadIdx.x >> 5));
 }
 
 template <bool DELTA, int N, int S>
