@@ -409,6 +409,21 @@ def batched_streams(seed=100):
     return out
 
 
+def batched_sequences(streams, frames):
+    """Stream i's frames: the bump-flow sequence of its size from seed 100 + i (uint8
+    [frames, H, W] each), generated on a thread pool (numpy releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from flowfilter_b200 import synthetic
+
+    def one(i):
+        s = streams[i]
+        return synthetic.seq_bumps(frames=frames, height=s["H"], width=s["W"], seed=100 + i)
+
+    with ThreadPoolExecutor(min(8, os.cpu_count() or 1)) as ex:
+        return list(ex.map(one, range(len(streams))))
+
+
 def configure_stream(f, s):
     f.gamma = s["gamma"] if s["levels"] > 1 else s["gamma"][0]
     f.smoothIterations = s["smooth"] if s["levels"] > 1 else s["smooth"][0]
@@ -423,12 +438,11 @@ def bench_batched(steps, warmup):
     from flowfilter_b200 import BatchFlowFilter, PyramidalFlowFilter, synthetic
 
     streams = batched_streams()
-    seqs = [torch.from_numpy(synthetic.seq_bumps(frames=BATCH_RING, height=h, width=w, seed=100 + k)).cuda()
-            for k, (h, w) in enumerate(BATCH_SIZES)]
+    seqs = [torch.from_numpy(q).cuda() for q in batched_sequences(streams, BATCH_RING)]
     batch = BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
     for i, s in enumerate(streams):
         configure_stream(batch.stream(i), s)
-    packed = [batch.pack([seqs[s["size"]][r] for s in streams]) for r in range(BATCH_RING)]
+    packed = [batch.pack([seqs[i][r] for i in range(len(streams))]) for r in range(BATCH_RING)]
 
     def timed(run):
         for t in range(warmup):
@@ -450,8 +464,8 @@ def bench_batched(steps, warmup):
         loop.append(f)
 
     def loop_step(t):
-        for s, f in zip(streams, loop):
-            f.loadImage(seqs[s["size"]][t % BATCH_RING])
+        for i, f in enumerate(loop):
+            f.loadImage(seqs[i][t % BATCH_RING])
             f.computeAsync()
             if t == 0:
                 f.setGraphs(True)
@@ -467,7 +481,7 @@ def bench_batched(steps, warmup):
         "launches_per_step": batch.launches(),
         "loop_value": n * steps / (l_ms / 1e3), "loop_ms_per_step": l_ms / steps,
         "speedup_vs_loop": l_ms / b_ms,
-        "data": "synthetic: one seeded bump-flow sequence per size (seed 100 + size index), shared by that size's streams",
+        "data": "synthetic: stream i is a seeded bump-flow sequence of its size from seed 100 + i",
     }
 
 
@@ -855,12 +869,11 @@ def profile_batched(args):
     from flowfilter_b200 import BatchFlowFilter, synthetic
 
     streams = batched_streams()
-    seqs = [torch.from_numpy(synthetic.seq_bumps(frames=BATCH_RING, height=h, width=w, seed=100 + k)).cuda()
-            for k, (h, w) in enumerate(BATCH_SIZES)]
+    seqs = [torch.from_numpy(q).cuda() for q in batched_sequences(streams, BATCH_RING)]
     batch = BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
     for i, s in enumerate(streams):
         configure_stream(batch.stream(i), s)
-    packed = [batch.pack([seqs[s["size"]][r] for s in streams]) for r in range(BATCH_RING)]
+    packed = [batch.pack([seqs[i][r] for i in range(len(streams))]) for r in range(BATCH_RING)]
     for t in range(args.warmup):
         batch.step(packed[t % BATCH_RING])
     torch.cuda.synchronize()

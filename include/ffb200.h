@@ -368,9 +368,9 @@ ff_status ff_rotational_predict(const ff_camera* cam, float wx, float wy, float 
 ff_status ff_flow_to_color(const float* flow, size_t flow_pitch, int height, int width, float maxflow,
                            const unsigned char* wheel, unsigned char* color, size_t color_pitch, void* stream);
 /* The library's default colour wheel into a host buffer of 256*256*4 bytes (rows of 256 RGBA
- * texels, row = y, column = x): the Middlebury colour code at texel centres.  It stands in for
- * the reference's embedded table (src/colorwheel.cpp, getColorWheelRGBA), which is a different
- * image of the same code; pass that table as `wheel` for the reference's exact colours. */
+ * texels, row = y, column = x): the reference's embedded table (src/colorwheel.cpp,
+ * COLOR_WHEEL_D, returned by getColorWheelRGBA, include/flowfilter/colorwheel.h:20-27), byte
+ * for byte, so default colours are the reference's. */
 ff_status ff_color_wheel_default(unsigned char* rgba);
 
 /* One frame of the differentiable pyramidal filter, and its adjoint, as single calls that

@@ -2,9 +2,7 @@
  * Colour wheel for the B200 drop-in C++ API (reference: include/flowfilter/colorwheel.h:14-27).
  *
  * The same names and sizes as the reference: a 256x256 RGBA table COLOR_WHEEL_D and
- * getColorWheelRGBA() viewing it.  The values are this library's wheel (the Middlebury
- * colour code computed at texel centres, ff_color_wheel_default), a different image of the
- * same code than the reference's embedded table.
+ * getColorWheelRGBA() viewing it, with the reference's values (ff_color_wheel_default).
  */
 #ifndef FLOWFILTER_B200_COLORWHEEL_H_
 #define FLOWFILTER_B200_COLORWHEEL_H_

@@ -4,8 +4,8 @@
  *
  * Colour-encodes a float2 flow image into an RGBA uint8 image through a 256x256 colour
  * wheel read at (flow + maxflow) / (2 maxflow), as the reference's texture lookup does.
- * The wheel is the library's default (getColorWheelRGBA(), the Middlebury colour code)
- * unless setColorWheel() gives another table.  The reference throws bare std::exception;
+ * The wheel is the library's default (getColorWheelRGBA(), the reference's table) unless
+ * setColorWheel() gives another table.  The reference throws bare std::exception;
  * here the same conditions throw std::invalid_argument (bad input flow, maxflow <= 0) or
  * std::logic_error (configure without an input, compute before configure), both of which
  * derive from std::exception.

@@ -5,10 +5,9 @@
 // component, row from the y component.  The texel index is computed here in integer
 // arithmetic (one thread per pixel, plain loads; the 256 KB wheel stays in L1/L2).
 //
-// The wheel is an input.  With none given, the library's own wheel is used: the Middlebury
-// colour code (Baker et al., "A Database and Evaluation Methodology for Optical Flow",
-// IJCV 2011: hue from the flow direction over a 55-colour cycle, saturation from the
-// magnitude up to |flow| = maxflow, 0.75 brightness beyond), computed at texel centres.
+// The wheel is an input.  With none given, the library's own wheel is used: the reference's
+// 256x256 RGBA table (src/colorwheel.cpp, include/flowfilter/colorwheel.h:20-27), byte for
+// byte, so default colours are the reference's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +21,7 @@
 #include "launch.cuh"
 
 ff_status ffb_fail(ff_status s, const std::string& msg);  // capi.cu: last error + log
+extern const unsigned char ffb_colorwheel_rgba[256 * 256 * 4];  // colorwheel_data.cpp (generated)
 
 namespace ffb {
 namespace {
@@ -55,56 +55,9 @@ __global__ void flow_to_color_k(const float* __restrict__ flow, size_t flow_pitc
     reinterpret_cast<uchar4*>(reinterpret_cast<char*>(color) + y * color_pitch)[x] = c;
 }
 
-// ---- the default wheel (host)
-// The 55-colour hue cycle of the Middlebury colour code: red-yellow 15, yellow-green 6,
-// green-cyan 4, cyan-blue 11, blue-magenta 13, magenta-red 6 steps, integer RGB.
-std::vector<int> hue_cycle() {
-    const int seg[6] = {15, 6, 4, 11, 13, 6};
-    std::vector<int> c;
-    auto put = [&](int r, int g, int b) {
-        c.push_back(r);
-        c.push_back(g);
-        c.push_back(b);
-    };
-    for (int i = 0; i < seg[0]; ++i) put(255, 255 * i / seg[0], 0);
-    for (int i = 0; i < seg[1]; ++i) put(255 - 255 * i / seg[1], 255, 0);
-    for (int i = 0; i < seg[2]; ++i) put(0, 255, 255 * i / seg[2]);
-    for (int i = 0; i < seg[3]; ++i) put(0, 255 - 255 * i / seg[3], 255);
-    for (int i = 0; i < seg[4]; ++i) put(255 * i / seg[4], 0, 255);
-    for (int i = 0; i < seg[5]; ++i) put(255, 0, 255 - 255 * i / seg[5]);
-    return c;
-}
-
-void make_default_wheel(unsigned char* rgba) {
-    const std::vector<int> cyc = hue_cycle();
-    const int n = (int)cyc.size() / 3;
-    for (int i = 0; i < kWheel; ++i) {
-        for (int j = 0; j < kWheel; ++j) {
-            // flow / maxflow at the texel centre
-            const double u = (j + 0.5) / (kWheel / 2) - 1.0, v = (i + 0.5) / (kWheel / 2) - 1.0;
-            const double rad = std::sqrt(u * u + v * v);
-            const double a = std::atan2(-v, -u) / M_PI;
-            const double fk = (a + 1.0) / 2.0 * (n - 1);
-            const int k0 = (int)std::floor(fk);
-            const int k1 = k0 + 1 == n ? 0 : k0 + 1;
-            const double f = fk - k0;
-            unsigned char* px = rgba + 4 * ((size_t)i * kWheel + j);
-            for (int ch = 0; ch < 3; ++ch) {
-                double col = (1.0 - f) * cyc[3 * k0 + ch] / 255.0 + f * cyc[3 * k1 + ch] / 255.0;
-                col = rad <= 1.0 ? 1.0 - rad * (1.0 - col) : col * 0.75;
-                px[ch] = (unsigned char)(int)std::floor(255.0 * col);
-            }
-            px[3] = 255;
-        }
-    }
-}
-
+// ---- the default wheel (host): the reference's table (colorwheel_asset.py, colorwheel.z)
 const std::vector<unsigned char>& default_wheel() {
-    static const std::vector<unsigned char> w = [] {
-        std::vector<unsigned char> v((size_t)kWheel * kWheel * 4);
-        make_default_wheel(v.data());
-        return v;
-    }();
+    static const std::vector<unsigned char> w(ffb_colorwheel_rgba, ffb_colorwheel_rgba + kWheel * kWheel * 4);
     return w;
 }
 

@@ -5,8 +5,8 @@
 ``FlowToColor(inputFlow, maxflow)`` takes a (H, W, 2) float32 CUDA tensor (for example a
 filter's ``getFlowDevice()``), and ``compute()`` writes a (H, W, 4) uint8 RGBA image that
 ``getColorFlow()`` returns as a CUDA tensor and ``download()`` as a numpy array.  The
-colour wheel is the library's default (the Middlebury colour code) unless
-``setColorWheel`` gives another 256x256 RGBA table, such as the reference's own.
+colour wheel is the library's default (the reference's own 256x256 RGBA table, byte for
+byte) unless ``setColorWheel`` gives another one.
 """
 
 from __future__ import annotations

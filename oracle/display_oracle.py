@@ -2,8 +2,8 @@
 
 A numpy restatement of the reference's FlowToColor lookup (src/gpu/device/display_k.cu:14-43;
 texture set up in src/gpu/display.cu:64-75 as normalised-coordinate, point-sampled,
-clamp-addressed, element-type reads, src/gpu/image.cu:241-247) and of the Middlebury
-colour code that the library uses as its default wheel (Baker et al., IJCV 2011).  tests/
+clamp-addressed, element-type reads, src/gpu/image.cu:241-247) and the
+reference's colour wheel table that the library uses as its default wheel.  tests/
 use it to check ff_flow_to_color and ff_color_wheel_default; the product never imports it.
 The texel choice is pinned against the reference kernel run on a B200 with an
 index-encoding wheel (tests/golden/ref_flow_to_color.npz).
@@ -12,6 +12,7 @@ index-encoding wheel (tests/golden/ref_flow_to_color.npz).
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -39,35 +40,16 @@ def flow_to_color(flow: np.ndarray, maxflow: float, wheel: np.ndarray) -> np.nda
     return wheel[iy, ix]
 
 
-def middlebury_wheel() -> np.ndarray:
-    """The Middlebury colour code at texel centres: 55-colour hue cycle (RY 15, YG 6, GC 4,
-    CB 11, BM 13, MR 6, integer RGB), saturation from the radius, 0.75 outside |flow| = 1."""
-    seg = [15, 6, 4, 11, 13, 6]
-    cyc = []
-    cyc += [(255, 255 * i // seg[0], 0) for i in range(seg[0])]
-    cyc += [(255 - 255 * i // seg[1], 255, 0) for i in range(seg[1])]
-    cyc += [(0, 255, 255 * i // seg[2]) for i in range(seg[2])]
-    cyc += [(0, 255 - 255 * i // seg[3], 255) for i in range(seg[3])]
-    cyc += [(255 * i // seg[4], 0, 255) for i in range(seg[4])]
-    cyc += [(255, 0, 255 - 255 * i // seg[5]) for i in range(seg[5])]
-    cyc = np.array(cyc, np.float64)
-    n = len(cyc)
-    c = (np.arange(WHEEL) + 0.5) / (WHEEL // 2) - 1.0
-    u, v = np.meshgrid(c, c)
-    rad = np.sqrt(u * u + v * v)
-    # the C library's atan2 (as the library computes it), not numpy's vectorised one
-    a = np.vectorize(math.atan2, otypes=[np.float64])(-v, -u) / np.pi
-    fk = (a + 1.0) / 2.0 * (n - 1)
-    k0 = np.floor(fk).astype(np.int64)
-    k1 = np.where(k0 + 1 == n, 0, k0 + 1)
-    f = fk - k0
-    out = np.empty((WHEEL, WHEEL, 4), np.uint8)
-    for ch in range(3):
-        col = (1.0 - f) * cyc[k0, ch] / 255.0 + f * cyc[k1, ch] / 255.0
-        col = np.where(rad <= 1.0, 1.0 - rad * (1.0 - col), col * 0.75)
-        out[..., ch] = np.floor(255.0 * col).astype(np.int64)
-    out[..., 3] = 255
-    return out
+def reference_wheel() -> np.ndarray:
+    """The reference's colour wheel table (src/colorwheel.cpp), as the package keeps it
+    (optical-flow-filter_b200/csrc/colorwheel.z, decoded by colorwheel_asset.py)."""
+    import importlib.util
+
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "optical-flow-filter_b200", "csrc")
+    spec = importlib.util.spec_from_file_location("colorwheel_asset", os.path.join(csrc, "colorwheel_asset.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.load(os.path.join(csrc, "colorwheel.z"))
 
 
 def index_wheel() -> np.ndarray:

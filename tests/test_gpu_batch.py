@@ -127,3 +127,34 @@ def test_batch_frame_layout_and_errors(ffb, cuda):
     assert _lib.lib().ff_batch_stream(batch._h, 2, ctypes.byref(h)) == _lib.FF_ERR_OUT_OF_RANGE
     with pytest.raises(ValueError):
         ffb.BatchFlowFilter([])
+
+
+def test_sixty_four_stream_mix_matches_streams_alone(ffb, cuda):
+    """The benchmark's 64-stream mix (16 each at 320x240, 640x480, 1280x720, 1920x1080; levels,
+    gamma and smoothing seeded per stream; stream i's frames from seed 100 + i) at the default
+    kernel selection: every stream bit for bit equal to the same stream filtered alone, over
+    four frames.  Its large levels run the batched streaming kernel at the batch's own bands."""
+    import bench
+
+    streams = bench.batched_streams()
+    assert len(streams) == 64
+    seqs = bench.batched_sequences(streams, 4)
+    alone = []
+    batch = ffb.BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
+    for i, s in enumerate(streams):
+        f = ffb.PyramidalFlowFilter(s["H"], s["W"], s["levels"])
+        bench.configure_stream(f, s)
+        bench.configure_stream(batch.stream(i), s)
+        alone.append(f)
+    assert batch.launches() > 1 + 2 + 2  # streaming launches are in the step
+    dev = [cuda.from_numpy(q).cuda() for q in seqs]
+    buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
+    for t in range(4):
+        batch.pack([d[t] for d in dev], out=buf)
+        batch.step(buf)
+        for f, d in zip(alone, dev):
+            f.loadImage(d[t])
+            f.computeAsync()
+        cuda.cuda.synchronize()
+        for i, f in enumerate(alone):
+            np.testing.assert_array_equal(batch.stream(i).getFlow(), f.getFlow(), err_msg=f"stream {i} frame {t}")

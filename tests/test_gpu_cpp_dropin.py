@@ -61,7 +61,7 @@ def test_cpp_dropin_sequence_matches_oracle(program, tmp_path, h, w, levels):
     assert off == got.size
     # FlowToColor(filter.getFlow(), 4) with the library's wheel
     colour = np.fromfile(fcol, np.uint8).reshape(h, w, 4)
-    np.testing.assert_array_equal(colour, D.flow_to_color(of.get_flow(), 4.0, D.middlebury_wheel()))
+    np.testing.assert_array_equal(colour, D.flow_to_color(of.get_flow(), 4.0, D.reference_wheel()))
 
 
 @pytest.mark.parametrize("h,w,d,n", [(45, 61, 1, 3), (50, 70, 4, 18)])

@@ -74,6 +74,25 @@ def test_fp32_forward_equals_the_reference_float_path(dm, cuda, levels):
     np.testing.assert_array_equal(got, want)
 
 
+def test_fp32_forward_at_the_benchmark_size(dm, cuda):
+    """The differentiable filter's float32 forward on the full benchmark batch (16 sequences of
+    32 frames of 256x256, seeded bump flows from seed 200 + b, 2 levels, gamma [10, 50],
+    smoothing [2, 4], maxflow 4) equals the reference float path composed from the oracle's
+    stages, bit for bit."""
+    from flowfilter_b200 import synthetic
+
+    B, T, H, W = 16, 32, 256, 256
+    frames = np.stack([synthetic.seq_bumps_float(frames=T, height=H, width=W, seed=200 + b, n_bumps=8,
+                                                 bump_sigma=40.0, amp=2.0)[0] for b in range(B)])
+    gamma, smooth = [10.0, 50.0], [2, 4]
+    f = dm.DiffPyramidalFlowFilter(H, W, 2, gamma, smooth, maxflow=4.0, checkpoint_every=8)
+    with cuda.no_grad():
+        got = f(cuda.from_numpy(frames).cuda()).cpu().numpy()
+    want = oracle_fp32_sequence(frames, gamma, smooth, 4.0, 2)
+    assert np.max(np.abs(got - want)) <= 1e-4  # the stated tolerance ...
+    np.testing.assert_array_equal(got, want)  # ... and in fact bit-exact
+
+
 def test_fp64_forward_matches_fp64_oracle(dm, cuda):
     B, T, H, W = 2, 6, 24, 32
     frames = float_frames(B, T, H, W, 7).astype(np.float64)

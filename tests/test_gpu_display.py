@@ -49,12 +49,22 @@ def test_texels_equal_the_reference_lookup(cuda):
         assert (got[..., 2] == 0).all() and (got[..., 3] == 255).all()
 
 
+def test_default_colours_equal_the_reference_lookup(cuda):
+    """With its default wheel, ff_flow_to_color gives the reference FlowToColor's bytes: the
+    reference's table at the texel the reference kernel read for every probe pixel."""
+    g = np.load(FIXTURE)
+    w = D.reference_wheel()
+    for k, (m, seed) in enumerate(zip(g["maxflow"], g["seed"])):
+        flow = D.probe_flows(float(m), int(seed))
+        np.testing.assert_array_equal(run_c_abi(cuda, flow, float(m)), w[g["row"][k], g["col"][k]])
+
+
 @pytest.mark.parametrize("h,w,maxflow", [(1, 1, 1.0), (7, 5, 2.0), (53, 70, 4.0), (480, 640, 4.0)])
 def test_default_wheel_matches_oracle(cuda, h, w, maxflow):
     rng = np.random.default_rng(h * w)
     flow = rng.normal(0, maxflow * 0.7, (h, w, 2)).astype(np.float32)
     got = run_c_abi(cuda, flow, maxflow)
-    np.testing.assert_array_equal(got, D.flow_to_color(flow, maxflow, D.middlebury_wheel()))
+    np.testing.assert_array_equal(got, D.flow_to_color(flow, maxflow, D.reference_wheel()))
 
 
 def test_flow_to_color_class_on_filter_flow(cuda):
@@ -72,7 +82,7 @@ def test_flow_to_color_class_on_filter_flow(cuda):
     c.compute()
     assert c.elapsedTime() > 0.0
     got = c.download()
-    np.testing.assert_array_equal(got, D.flow_to_color(f.getFlow(), 3.0, D.middlebury_wheel()))
+    np.testing.assert_array_equal(got, D.flow_to_color(f.getFlow(), 3.0, D.reference_wheel()))
     # another wheel, given as a host table
     wheel = np.random.default_rng(9).integers(0, 256, (256, 256, 4), dtype=np.uint8)
     c.setColorWheel(wheel)
@@ -81,7 +91,7 @@ def test_flow_to_color_class_on_filter_flow(cuda):
     np.testing.assert_array_equal(c.download(), D.flow_to_color(f.getFlow(), 2.5, wheel))
     c.setColorWheel(None)
     c.compute()
-    np.testing.assert_array_equal(c.download(), D.flow_to_color(f.getFlow(), 2.5, D.middlebury_wheel()))
+    np.testing.assert_array_equal(c.download(), D.flow_to_color(f.getFlow(), 2.5, D.reference_wheel()))
 
 
 def test_flow_to_color_errors(cuda):
