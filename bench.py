@@ -5,6 +5,7 @@
     python bench.py --profile WORKLOAD --steps K --warmup W     (profiler target only)
     python bench.py --profile-next --steps K --warmup W         (profiler target: FlowToColor, rotation)
     python bench.py --profile-batched --steps K --warmup W      (profiler target: the 64-stream batched step)
+    python bench.py --profile-diff --steps K --warmup W         (profiler target: the differentiable filter)
 
 A step is one frame of the PyramidalFlowFilter: the frame (already resident in HBM) is
 loaded into the filter and one compute() runs (pyramid, then one fused kernel per
@@ -615,13 +616,29 @@ def bench_differentiable(steps):
     t_fb = timed(fwd_bwd(f), n)
     t_fbc = timed(fwd_bwd(fc), n)
     tape = diff.lib().ff_diff_frame_tape_bytes(0, diff.ctypes.byref(diff._geom(f, B)))
+
+    # the fit: Adam on per-level log gamma and smoothing weights, checkpoints every 8 frames
+    ft = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=8)
+    fit_steps = 200
+    res = ft.fit(frames, truth.expand(B, T, H, W, 2), steps=fit_steps, lr=0.05, first=8, fit_weights=True)
+    fit = {
+        "steps": fit_steps,
+        "optimizer": "Adam lr 0.05 on log gamma and on softmax logits of the 5-tap weights, checkpoint every 8",
+        "epe_before": res["losses"][0], "epe_after": res["final"],
+        "gamma": [float(x) for x in ft.gamma.detach().cpu()],
+        "weights": [[float(x) for x in row] for row in ft.weights.detach().cpu()],
+        "ms_per_step": res["ms"] / fit_steps,
+        "loss_every_20": res["losses"][::20],
+    }
     return {
         "workload": f"{B} sequences x {T} frames of {W}x{H} float32, 2 levels, gamma [10, 50], smoothing [2, 4], "
                     "maxflow 4, loss = mean endpoint error over frames 8-31",
-        "fwd_ms": t_f, "fwd_bwd_ms": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
+        "fwd_ms": t_f, "fwd_note": "forward under torch.no_grad: no tape (ff_diff_frame_infer)",
+        "fwd_bwd_ms": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
         "tape_bytes_per_frame": tape, "tape_note": "whole-sequence tape resident in HBM (no recompute)",
         "fwd_bwd_ckpt8_ms": t_fbc, "fwd_bwd_ckpt8_over_fwd": t_fbc / t_f,
         "fwd_frames_per_s": B * T / (t_f / 1e3), "fwd_bwd_frames_per_s": B * T / (t_fb / 1e3),
+        "fit": fit,
         "dtype": "f32", "data": "synthetic: seeded bump flows (seed 200 + b), known flow",
     }
 
@@ -885,6 +902,36 @@ def profile_batched(args):
     print(json.dumps({"profile": "batched", "steps": args.steps, "launches_per_step": batch.launches()}), flush=True)
 
 
+def profile_diff(args):
+    """A profiler target for the differentiable filter: --warmup untimed passes, then --steps
+    times one forward without a tape and one forward + backward with the whole tape, on the
+    differentiable leg's batch (16 sequences x 32 frames of 256x256), in the NVTX range "timed"."""
+    import torch
+    from flowfilter_b200 import diff, synthetic
+
+    B, T, H, W = 16, 32, 256, 256
+    seqs = [synthetic.seq_bumps_float(frames=T, height=H, width=W, seed=200 + b, n_bumps=8, bump_sigma=40.0,
+                                      amp=2.0) for b in range(B)]
+    frames = torch.from_numpy(np.stack([q[0] for q in seqs])).cuda()
+    truth = torch.from_numpy(np.stack([np.stack([q[1], q[2]], -1) for q in seqs])).cuda()[:, None]
+    f = diff.DiffPyramidalFlowFilter(H, W, 2, [10.0, 50.0], [2, 4], maxflow=4.0, checkpoint_every=T)
+
+    def once():
+        with torch.no_grad():
+            f(frames)
+        diff.endpoint_error(f(frames), truth.expand(B, T, H, W, 2), first=8).backward()
+
+    for _ in range(args.warmup):
+        once()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    for _ in range(args.steps):
+        once()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "diff", "steps": args.steps}), flush=True)
+
+
 def profile_case(args):
     """A profiler target: the tuned filter of one workload runs --warmup untimed frames, then
     --steps frames inside the NVTX range "timed" (L2 flushed before each), and nothing else."""
@@ -922,6 +969,8 @@ def main():
                     help="profiler target: the flow-to-colour and rotational-predictor kernels (no JSON line)")
     ap.add_argument("--profile-batched", action="store_true",
                     help="profiler target: steps of the 64-stream batched step (no JSON line)")
+    ap.add_argument("--profile-diff", action="store_true",
+                    help="profiler target: the differentiable filter's forward and forward+backward (no JSON line)")
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="profiler target: run --steps frames of one workload in the NVTX range 'timed' (no JSON line)")
     args = ap.parse_args()
@@ -929,6 +978,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.profile_next:
         profile_next(args)
+    elif args.profile_diff:
+        profile_diff(args)
     elif args.profile_batched:
         profile_batched(args)
     elif args.profile:

@@ -395,6 +395,13 @@ size_t ff_diff_frame_scratch_bytes(int dtype, const ff_diff_geom* geom);
 ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                 const void* weights, const void* const* state_in, void* const* state_out,
                                 void* fu_out, void* tape, void* stream);
+/* The same frame forward without a tape, for inference: identical outputs, with the
+ * intermediates in a reused `scratch` of ff_diff_frame_infer_bytes (a few fields per level
+ * instead of every sub-step's).  No counterpart in the reference (no adjoint there). */
+size_t ff_diff_frame_infer_bytes(int dtype, const ff_diff_geom* geom);
+ff_status ff_diff_frame_infer(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                              const void* weights, const void* const* state_in, void* const* state_out, void* fu_out,
+                              void* scratch, void* stream);
 ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                  const void* weights, const void* const* state_in, const void* const* state_out,
                                  const void* tape, const void* const* grad_state_out, const void* grad_fu,

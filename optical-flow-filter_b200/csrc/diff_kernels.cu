@@ -1117,19 +1117,41 @@ Geo geo_of(const ff_diff_geom* g) {
     return o;
 }
 
-// offsets (in elements of T) of everything the adjoint reads, laid out in one tape
+// offsets (in elements of T) of the forward's intermediates.  As a tape, everything the
+// adjoint reads gets its own place.  Compact (a forward without adjoint): the buffers are
+// reused as soon as the forward is done with them, and only the level images and the top
+// level's unsmoothed flow (the coarse flow of level L-2) stay apart.
 struct Tape {
     size_t img[FF_DIFF_MAX_LEVELS] = {};                // level images, l >= 1
     size_t grad[FF_DIFF_MAX_LEVELS] = {};               // image gradients
     std::vector<size_t> prop[FF_DIFF_MAX_LEVELS];       // outputs of sub-steps 0..2N-1
     std::vector<size_t> sm[FF_DIFF_MAX_LEVELS];         // inputs of smoothing passes (sm[0] = update output)
     size_t total = 0;
-    Tape(const Geo& g) {
+    Tape(const Geo& g, bool compact = false) {
         auto take = [&](size_t n) {
             size_t at = total;
             total += (n + 31) / 32 * 32;
             return at;
         };
+        if (compact) {
+            size_t n1m = 0, stm = 0;
+            for (int l = 0; l < g.L; ++l) {
+                n1m = std::max(n1m, g.n1(l));
+                stm = std::max(stm, (l < g.L - 1 ? 5 : 2) * g.n1(l));
+                if (l > 0) img[l] = take(g.n1(l));
+            }
+            const size_t gr = take(2 * n1m), pa = take(stm), pb = take(stm), sa = take(2 * n1m), sb = take(2 * n1m);
+            const size_t fu_top = take(2 * g.n1(g.L - 1));
+            for (int l = 0; l < g.L; ++l) {
+                grad[l] = gr;
+                for (int k = 1; k <= 2 * g.N[l]; ++k) prop[l].push_back(k % 2 ? pa : pb);
+                // pass j reads sm[j] and writes sm[j+1]: two buffers alternate after sm[0]
+                const int ns = std::max(2 * g.S[l], 1);
+                for (int k = 0; k < ns; ++k)
+                    sm[l].push_back(k == 0 ? (l == g.L - 1 ? fu_top : sa) : (k % 2 ? sb : sa));
+            }
+            return;
+        }
         for (int l = 0; l < g.L; ++l) {
             const size_t n1 = g.n1(l), n2 = 2 * n1;
             const bool delta = l < g.L - 1;
@@ -1253,8 +1275,8 @@ struct Driver {
 
     // ---- forward
     void forward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in, T* const* out,
-                 T* fu_out, T* tp) const {
-        const Tape tape(g);
+                 T* fu_out, T* tp, bool compact = false) const {
+        const Tape tape(g, compact);
         const int L = g.L, top = L - 1;
         auto img = [&](int l) -> const T* { return l == 0 ? frame : tp + tape.img[l]; };
         for (int l = 1; l < L; ++l)
@@ -1492,6 +1514,39 @@ ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, 
             ffb::diff::Driver<float>(g, (cudaStream_t)stream)
                 .forward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
                          (const float* const*)state_in, (float* const*)state_out, (float*)fu_out, (float*)tape);
+        }
+    });
+}
+
+size_t ff_diff_frame_infer_bytes(int dtype, const ff_diff_geom* geom) {
+    try {
+        return ffb::diff::Tape(ffb::diff::geo_of(geom), true).total * (dtype ? 8 : 4);
+    } catch (...) {
+        return 0;
+    }
+}
+
+ff_status ff_diff_frame_infer(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
+                              const void* weights, const void* const* state_in, void* const* state_out, void* fu_out,
+                              void* scratch, void* stream) {
+    return ffb::diff::run_frame([&] {
+        const ffb::diff::Geo g = ffb::diff::geo_of(geom);
+        if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
+        if (!frame || !gamma || !weights || !state_in || !state_out || !scratch)
+            throw std::invalid_argument("null pointer argument");
+        for (int k = 0; k < 3 * g.L; ++k)
+            if (!::pairs_aligned(dtype, {state_in[k], state_out[k]}))
+                throw std::invalid_argument("state fields must be aligned to two elements (8 or 16 bytes)");
+        if (dtype) {
+            ffb::diff::Driver<double>(g, (cudaStream_t)stream)
+                .forward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
+                         (const double* const*)state_in, (double* const*)state_out, (double*)fu_out,
+                         (double*)scratch, true);
+        } else {
+            ffb::diff::Driver<float>(g, (cudaStream_t)stream)
+                .forward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
+                         (const float* const*)state_in, (float* const*)state_out, (float*)fu_out, (float*)scratch,
+                         true);
         }
     });
 }

@@ -171,6 +171,8 @@ SIGNATURES = {
     "ff_diff_frame_tape_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_scratch_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_forward": (_st, [_i, _vp, _i] + [_vp] * 8),
+    "ff_diff_frame_infer_bytes": (ctypes.c_size_t, [_i, _vp]),
+    "ff_diff_frame_infer": (_st, [_i, _vp, _i] + [_vp] * 8),
     "ff_diff_frame_backward": (_st, [_i, _vp, _i] + [_vp] * 14),
 }
 

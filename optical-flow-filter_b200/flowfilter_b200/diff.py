@@ -278,6 +278,39 @@ class DiffPyramidalFlowFilter:
     def parameters(self):
         return [self.gamma, self.weights]
 
+    def fit(self, frames, truth, steps: int = 200, lr: float = 0.05, first: int = 8, fit_weights: bool = True):
+        """Fits the per-level gamma and, with fit_weights, the per-level 5-tap smoothing
+        weights by Adam on the mean endpoint error of the flows against ``truth``
+        (B, T, H, W, 2) over frames first.. .  gamma is fitted through its logarithm (it stays
+        positive), the weights through a softmax of five logits per level (they stay positive
+        and sum to 1, as the reference's 0.2 box does, which is the softmax of equal logits).
+        Checkpointing follows ``checkpoint_every``.  Returns the loss of every step, the final
+        loss and the device milliseconds of the steps; the fitted values are left in gamma /
+        weights."""
+        torch = _torch()
+        log_g = torch.log(self.gamma.detach().clone()).requires_grad_(True)
+        w0 = self.weights.detach().clone()
+        logits = torch.log(w0 / w0.sum(1, keepdim=True)).requires_grad_(fit_weights)
+        opt = torch.optim.Adam([log_g, logits] if fit_weights else [log_g], lr=lr)
+        losses = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(int(steps)):
+            self.gamma = log_g.exp()
+            self.weights = torch.softmax(logits, 1) if fit_weights else w0
+            loss = endpoint_error(self(frames), truth, first=first, eps=1e-12)
+            opt.zero_grad()
+            loss.backward()
+            opt.step()
+            losses.append(loss.detach())
+        e1.record()
+        torch.cuda.synchronize()
+        self.gamma = log_g.detach().exp().requires_grad_(True)
+        self.weights = (torch.softmax(logits.detach(), 1) if fit_weights else w0).clone().requires_grad_(True)
+        with torch.no_grad():
+            final = float(endpoint_error(self(frames), truth, first=first))
+        return {"losses": [float(x) for x in losses], "final": final, "ms": e0.elapsed_time(e1)}
+
     def _smooth(self, x, l):
         F = stages()
         w = self.weights[l]
@@ -369,11 +402,12 @@ class DiffPyramidalFlowFilter:
         return torch.cat(outs, 1)
 
 
-def endpoint_error(flows, truth, first: int = 0):
+def endpoint_error(flows, truth, first: int = 0, eps: float = 0.0):
     """Mean endpoint error over frames first.. of flows (B, T, H, W, 2) against truth of the
-    same shape (or broadcastable)."""
+    same shape (or broadcastable).  eps > 0 is added under the square root, which keeps the
+    gradient finite where a flow equals the truth exactly (used by fit())."""
     d = flows[:, first:] - truth[:, first:]
-    return (d[..., 0] ** 2 + d[..., 1] ** 2).sqrt().mean()
+    return (d[..., 0] ** 2 + d[..., 1] ** 2 + eps).sqrt().mean()
 
 
 MAX_LEVELS = 8  # FF_DIFF_MAX_LEVELS
@@ -484,12 +518,42 @@ def _frame_function():
 _FrameStep = None
 
 
+def _frame_infer(flt, frame, gamma, weights, state_flat, first: bool):
+    """One frame without a tape (ff_diff_frame_infer): the same outputs as _frame_forward, the
+    intermediates in a scratch buffer kept on the filter and reused every frame."""
+    d = _dt(frame)
+    B = frame.shape[0]
+    g = _geom(flt, B)
+    key = (d, B, frame.device)
+    cache = flt.__dict__.setdefault("_infer_scratch", {})
+    if key not in cache:
+        cache.clear()
+        cache[key] = _workspace("ff_diff_frame_infer_bytes", d, g, frame)
+    scratch = cache[key]
+    new = []
+    for h, w in flt.shapes:
+        new += [frame.new_empty((B, h, w, 2)), frame.new_empty((B, h, w)), frame.new_empty((B, h, w, 2))]
+    fu = frame.new_empty((B,) + tuple(flt.shapes[0]) + (2,)) if flt.L == 1 else None
+    call("ff_diff_frame_infer", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
+         _ptrs(state_flat), _ptrs(new), _p(fu), _p(scratch), _stream())
+    return new, fu
+
+
 def frame_step(flt, frame, state, first: bool):
-    """One frame through the single-node FrameStep; returns (level-0 flow, new state)."""
+    """One frame through the single-node FrameStep; returns (level-0 flow, new state).  With
+    gradients off (torch.no_grad or inference mode) the frame runs without a tape."""
     global _FrameStep
     if _FrameStep is None:
         _FrameStep = _frame_function()
     L = flt.L
+    torch = _torch()
+    if not torch.is_grad_enabled():
+        state_flat = [t.contiguous() for lvl in state for t in lvl]
+        new, fu = _frame_infer(flt, frame.contiguous(), flt.gamma.detach().contiguous(),
+                               flt.weights.detach().contiguous(), state_flat, first)
+        out = (*new, fu if fu is not None else frame.new_zeros(0))
+        newst = [tuple(out[3 * l:3 * l + 3]) for l in range(L)]
+        return (out[3 * L] if L == 1 else newst[0][0]), newst
     out = _FrameStep.apply(flt, first, frame, flt.gamma, flt.weights, *[t for lvl in state for t in lvl])
     new = [tuple(out[3 * l:3 * l + 3]) for l in range(L)]
     y = out[3 * L] if L == 1 else new[0][0]

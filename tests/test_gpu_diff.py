@@ -227,7 +227,8 @@ def test_checkpointing_leaves_gradients_unchanged(dm, cuda):
 
 
 def test_fitting_gamma_lowers_endpoint_error(dm, cuda):
-    """A few Adam steps on log-gamma against the known flow of a synthetic sequence."""
+    """A few Adam steps (DiffPyramidalFlowFilter.fit) on log-gamma, then on log-gamma and the
+    smoothing weights, against the known flow of a synthetic sequence."""
     from flowfilter_b200 import synthetic
 
     B, T, H, W = 2, 10, 48, 64
@@ -240,17 +241,15 @@ def test_fitting_gamma_lowers_endpoint_error(dm, cuda):
     frames = cuda.from_numpy(np.stack(seqs)).cuda()
     truth = cuda.from_numpy(np.ascontiguousarray(np.stack(truth)).astype(np.float32)).cuda()
     f = dm.DiffPyramidalFlowFilter(H, W, 2, [200.0, 200.0], [1, 1], maxflow=4.0, checkpoint_every=5)
-    log_g = cuda.log(f.gamma.detach().clone()).requires_grad_(True)
-    opt = cuda.optim.Adam([log_g], lr=0.3)
-    losses = []
-    for _ in range(12):
-        f.gamma = log_g.exp()
-        loss = dm.endpoint_error(f(frames), truth, first=4)
-        opt.zero_grad()
-        loss.backward()
-        opt.step()
-        losses.append(float(loss.detach()))
-    assert losses[-1] < losses[0]
+    res = f.fit(frames, truth, steps=12, lr=0.3, first=4, fit_weights=False)
+    assert res["final"] < res["losses"][0]
+    # gamma and the smoothing weights together: finite throughout, weights positive summing to 1
+    g = dm.DiffPyramidalFlowFilter(H, W, 2, [200.0, 200.0], [1, 1], maxflow=4.0, checkpoint_every=5)
+    res = g.fit(frames, truth, steps=12, lr=0.1, first=4, fit_weights=True)
+    assert np.all(np.isfinite(res["losses"])) and res["final"] < res["losses"][0]
+    w = g.weights.detach().cpu().numpy()
+    assert (w > 0).all() and np.allclose(w.sum(1), 1.0, atol=1e-5)
+    assert (g.gamma.detach().cpu().numpy() > 0).all()
 
 
 @pytest.mark.parametrize("levels,smooth", [(1, [1]), (2, [1, 2]), (3, [1, 2, 1]), (2, [0, 1]), (3, [2, 0, 1])])
@@ -283,3 +282,19 @@ def test_frame_node_rejects_bad_geometry(dm, cuda):
     assert dm.lib().ff_diff_frame_tape_bytes(0, dm.ctypes.byref(g)) == 0
     with pytest.raises(ValueError):
         dm._workspace("ff_diff_frame_tape_bytes", 0, g, cuda.zeros(1, device="cuda"))
+
+
+@pytest.mark.parametrize("levels,dtype", [(1, "float32"), (2, "float32"), (3, "float64")])
+def test_forward_without_tape_equals_forward_with_tape(dm, cuda, levels, dtype):
+    """Under no_grad the frames run without a tape (ff_diff_frame_infer): the flows are the
+    ones the taped forward gives, bit for bit."""
+    B, T, H, W = 2, 6, 40, 56
+    frames = cuda.from_numpy(float_frames(B, T, H, W, 11).astype(dtype)).cuda()
+    gamma, smooth = [4.0, 15.0, 40.0][:levels], [1, 3, 0][:levels]
+    f = dm.DiffPyramidalFlowFilter(H, W, levels, gamma, smooth, maxflow=3.0, checkpoint_every=T,
+                                   dtype=getattr(cuda, dtype))
+    with cuda.no_grad():
+        free = f(frames)
+    taped = f(frames.clone().requires_grad_(True)).detach()
+    assert free.dtype == taped.dtype
+    np.testing.assert_array_equal(free.cpu().numpy(), taped.cpu().numpy())
