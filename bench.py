@@ -285,7 +285,7 @@ def make_filter(w):
 TUNING_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "flowfilter_b200", "tuning.json")
 
 
-def tuned(f, w, key=None):
+def tuned(f, w, key=None, flush=None):
     """Apply the cached autotuning result for this workload and GPU, or autotune now (after
     the filter computed a frame) and cache it, so repeated runs make the same choice."""
     import torch
@@ -301,7 +301,7 @@ def tuned(f, w, key=None):
     if key in cache:
         f.setTuningState(cache[key])
         return
-    f.autotune(5)
+    f.autotune(5, flush)
     cache[key] = f.tuningState()
     os.makedirs(os.path.dirname(TUNING_CACHE), exist_ok=True)
     with open(TUNING_CACHE, "w") as fh:
@@ -320,7 +320,7 @@ def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, 
         f.loadImage(dev_frames[t % ring])
         f.computeAsync()
         if tune and t == 1:
-            tuned(f, w)  # per-level kernel choice on live data (results unchanged)
+            tuned(f, w, flush=flush)  # kernel choice per level on live data (results unchanged)
     f.setGraphs(graphs)
     torch.cuda.synchronize()
     if profile:
@@ -947,7 +947,7 @@ def profile_case(args):
         f.loadImage(dev[t % 4])
         f.computeAsync()
         if t == 1:
-            tuned(f, w)
+            tuned(f, w, flush=flush)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("timed")
     for t in range(args.steps):

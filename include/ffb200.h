@@ -139,9 +139,16 @@ ff_status ff_filter_set_fused(ff_filter* f, int mode);
 ff_status ff_filter_set_graphs(ff_filter* f, int enabled);
 /* Autotuner: on the current inputs, time each level's per-stage kernels, its streaming
  * fused kernel at several band heights and its tile-fused kernel at several tile shapes
- * (`repetitions` runs each) and keep the fastest per level, used while the mode is 2.  Needs one computed frame; results are unchanged
- * because every candidate writes bit-identical outputs.  Parameter changes reset it. */
+ * (`repetitions` runs each); then, for pyramids, time whole frames over combinations of each
+ * level's best choices (the levels share the GPU within a frame) from a snapshot of the state
+ * that is restored afterwards, and keep the fastest combination, used while the mode is 2.
+ * Needs one computed frame; results are unchanged because every candidate writes
+ * bit-identical outputs.  Parameter changes reset it. */
 ff_status ff_filter_autotune(ff_filter* f, int repetitions);
+/* ff_filter_autotune with the device buffer `flush` overwritten before every timed frame of
+ * the whole-frame stage (outside the timing), so that frames read their state from HBM as
+ * in a measurement that flushes L2 between frames. */
+ff_status ff_filter_autotune_flush(ff_filter* f, int repetitions, void* flush, size_t flush_bytes);
 /* Read or set one level's kernel choice (path: -1 untuned, 0 per-stage, 1 streaming fused,
  * 2 tile-fused; band: rows of a streaming band or the tile-shape index, 0 automatic), e.g.
  * to reuse a saved autotuning result. */

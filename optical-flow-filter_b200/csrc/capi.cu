@@ -337,6 +337,10 @@ ff_status ff_filter_autotune(ff_filter* f, int repetitions) {
     return guard([&] { get(f)->autotune(repetitions); });
 }
 
+ff_status ff_filter_autotune_flush(ff_filter* f, int repetitions, void* flush, size_t flush_bytes) {
+    return guard([&] { get(f)->autotune(repetitions, flush, flush_bytes); });
+}
+
 ff_status ff_filter_get_level_tuning(const ff_filter* f, int level, int* path, int* band) {
     return guard([&] {
         need(path, "path");

@@ -8,6 +8,7 @@
 // is: coarse(h) = fs[cur] of level h+1, or fu of the top level for h = L-2.
 #include "filter.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -714,7 +715,7 @@ int Filter::path_of(int l, int* param) const {
     return kPerStage;
 }
 
-void Filter::autotune(int reps) {
+void Filter::autotune(int reps, void* flush, size_t flush_bytes) {
     if (reps < 1) throw Error(FF_ERR_INVALID_ARGUMENT, "autotune repetitions must be >= 1");
     for (const Level& v : lv_)
         if (v.first) throw Error(FF_ERR_LOGIC, "autotune needs at least one computed frame");
@@ -759,40 +760,115 @@ void Filter::autotune(int reps) {
         check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
         return ms;
     };
+    // Stage 1, every level alone: each choice timed as a graph of `reps` level steps.
     // top level first: level L-2 reads its unsmoothed flow
+    struct Choice {
+        float ms;
+        int path, band;
+    };
+    std::vector<std::vector<Choice>> timed(L_);
     for (int l = L_ - 1; l >= 0; --l) {
         Level& v = lv_[l];
         v.alloc_scratch();  // allocations cannot happen inside a capture
-        float best = time_it([&](cudaStream_t st) { step_level_unfused(l, st); });
-        int path = kPerStage, band = 0;
+        std::vector<Choice>& c = timed[l];
+        c.push_back({time_it([&](cudaStream_t st) { step_level_unfused(l, st); }), kPerStage, 0});
         if (fused_ok(l)) {
-            const int auto_rows = 0;
-            const int rows[] = {auto_rows, 8, 16, 24, 32, 48, 64, 96, 128};
+            const int rows[] = {0, 8, 10, 12, 16, 24, 32, 48, 64, 96, 128};
             for (int b : rows) {
                 if (b > v.H) continue;
-                const float t = time_it([&](cudaStream_t st) { launch_fused(l, b, st); });
-                if (t < best) {
-                    best = t;
-                    path = kStream;
-                    band = b;
-                }
+                c.push_back({time_it([&](cudaStream_t st) { launch_fused(l, b, st); }), kStream, b});
             }
         }
-        for (int c = 0; c < tile_config_count(); ++c) {
-            if (!tile_ok(l, c)) continue;
-            const float t = time_it([&](cudaStream_t st) { launch_tile(l, c, st); });
-            if (t < best) {
-                best = t;
-                path = kTile;
-                band = c;
-            }
+        for (int k = 0; k < tile_config_count(); ++k) {
+            if (!tile_ok(l, k)) continue;
+            c.push_back({time_it([&](cudaStream_t st) { launch_tile(l, k, st); }), kTile, k});
         }
-        v.tuned_path = path;
-        v.tuned_band = band;
+        std::stable_sort(c.begin(), c.end(), [](const Choice& a, const Choice& b) { return a.ms < b.ms; });
+        v.tuned_path = c[0].path;
+        v.tuned_band = c[0].band;
     }
     if (keep.p) {
         check_cuda(cudaMemcpy2DAsync(top.fu.p, top.fu.pitch, keep.p, keep.pitch, top.fu.row_bytes(), top.fu.h,
                                      cudaMemcpyDeviceToDevice, stream_), "autotune");
+    }
+    // Stage 2, whole frames: the levels of a frame share the GPU (level 0 runs beside the
+    // chain pyramid -> top level -> level L-2 on a side stream), so the fastest level alone is
+    // not always the fastest beside the others: a streaming level 0 in long bands leaves
+    // room on every SM for the latency-bound small levels.  Combinations of each level's
+    // three best choices (and, for a streaming level 0, longer bands) are timed as replayed
+    // frames from a snapshot of the state, which is restored afterwards.
+    if (L_ > 1) {
+        check_cuda(cudaStreamSynchronize(stream_), "autotune");
+        // per level: the three best choices, and the two best of each fused kernel
+        std::vector<std::vector<Choice>> cand(L_);
+        for (int l = 0; l < L_; ++l) {
+            auto have = [&](const Choice& c) {
+                for (const Choice& d : cand[l])
+                    if (d.path == c.path && d.band == c.band) return true;
+                return false;
+            };
+            for (const Choice& c : timed[l])
+                if (cand[l].size() < 3) cand[l].push_back(c);
+            for (int path : {(int)kStream, (int)kTile}) {
+                int n = 0;
+                for (const Choice& c : timed[l])
+                    if (c.path == path && n < 2) {
+                        ++n;
+                        if (!have(c)) cand[l].push_back(c);
+                    }
+            }
+        }
+        if (fused_ok(0)) {
+            for (int b : {48, 64, 80, 96}) {
+                if (b > lv_[0].H) continue;
+                bool have = false;
+                for (const Choice& c : cand[0]) have |= c.path == kStream && c.band == b;
+                if (!have) cand[0].push_back({0.f, kStream, b});
+            }
+        }
+        std::vector<unsigned char> snap(state_bytes());
+        export_state(snap.data(), snap.size());
+        const bool graphs_was = graphs_;
+        graphs_ = true;
+        std::vector<size_t> idx(L_, 0), best_idx(L_, 0);
+        float best_ms = -1.f;
+        const int frames = std::max(reps, 4);
+        for (;;) {
+            for (int l = 0; l < L_; ++l) {
+                lv_[l].tuned_path = cand[l][idx[l]].path;
+                lv_[l].tuned_band = cand[l][idx[l]].band;
+            }
+            drop_graphs();
+            // two frames capture both parities' graphs, then `frames` replays are timed one
+            // by one (with `flush` overwritten before each, outside the timing, if given)
+            compute_async(stream_);
+            compute_async(stream_);
+            float ms = 0.f;
+            for (int k = 0; k < frames; ++k) {
+                if (flush && flush_bytes)
+                    check_cuda(cudaMemsetAsync(flush, k & 0xff, flush_bytes, stream_), "flush");
+                check_cuda(cudaEventRecord(e0, stream_), "cudaEventRecord");
+                compute_async(stream_);
+                check_cuda(cudaEventRecord(e1, stream_), "cudaEventRecord");
+                check_cuda(cudaEventSynchronize(e1), "autotune");
+                float t = 0.f;
+                check_cuda(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+                ms += t;
+            }
+            if (best_ms < 0.f || ms < best_ms) {
+                best_ms = ms;
+                best_idx = idx;
+            }
+            int l = 0;
+            while (l < L_ && ++idx[l] == cand[l].size()) idx[l++] = 0;
+            if (l == L_) break;
+        }
+        for (int l = 0; l < L_; ++l) {
+            lv_[l].tuned_path = cand[l][best_idx[l]].path;
+            lv_[l].tuned_band = cand[l][best_idx[l]].band;
+        }
+        graphs_ = graphs_was;
+        import_state(snap.data(), snap.size());
     }
     check_cuda(cudaStreamSynchronize(stream_), "autotune");
     keep.release();

@@ -155,7 +155,7 @@ public:
     static constexpr long kFusedMinPixels = 200000;
     // time every candidate kernel configuration of each level on the current inputs and
     // keep the fastest (re-running a level step rewrites bit-identical outputs)
-    void autotune(int reps);
+    void autotune(int reps, void* flush = nullptr, size_t flush_bytes = 0);
     float time_level(int l, int reps, void* flush, size_t flush_bytes);
     std::string tuning() const;
     void set_level_tuning(int l, int path, int band) {

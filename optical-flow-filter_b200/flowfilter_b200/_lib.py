@@ -99,6 +99,7 @@ SIGNATURES = {
     "ff_filter_set_graphs": (_st, [_vp, _i]),
     "ff_filter_set_band": (_st, [_vp, _i]),
     "ff_filter_autotune": (_st, [_vp, _i]),
+    "ff_filter_autotune_flush": (_st, [_vp, _i, _vp, _sz]),
     "ff_filter_tuning": (_st, [_vp, ctypes.c_char_p, _sz]),
     "ff_filter_get_level_tuning": (_st, [_vp, _i, _ip, _ip]),
     "ff_filter_set_level_tuning": (_st, [_vp, _i, _i, _i]),

@@ -237,10 +237,16 @@ class _FilterBase:
         """Replay the frame step from captured CUDA graphs (one per state parity)."""
         call("ff_filter_set_graphs", self._h, 1 if enabled else 0)
 
-    def autotune(self, repetitions: int = 5) -> str:
-        """Time each level's kernel choices on the current inputs and keep the fastest;
-        returns the choice per level.  Needs one computed frame; results are unchanged."""
-        call("ff_filter_autotune", self._h, int(repetitions))
+    def autotune(self, repetitions: int = 5, flush=None) -> str:
+        """Time each level's kernel choices on the current inputs, then (pyramids) whole frames
+        over combinations of the best ones, and keep the fastest; returns the choice per level.
+        ``flush`` (a CUDA tensor) is overwritten before every timed whole frame.  Needs one
+        computed frame; results are unchanged."""
+        if flush is None:
+            call("ff_filter_autotune", self._h, int(repetitions))
+        else:
+            call("ff_filter_autotune_flush", self._h, int(repetitions), ctypes.c_void_p(flush.data_ptr()),
+                 flush.numel() * flush.element_size())
         return self.tuning()
 
     def tuningState(self) -> list:
