@@ -830,20 +830,18 @@ void Filter::autotune(int reps, void* flush, size_t flush_bytes) {
         export_state(snap.data(), snap.size());
         const bool graphs_was = graphs_;
         graphs_ = true;
-        std::vector<size_t> idx(L_, 0), best_idx(L_, 0);
-        float best_ms = -1.f;
-        const int frames = std::max(reps, 4);
-        for (;;) {
+        // a combination's score: the median of its timed frames
+        auto score = [&](const std::vector<size_t>& pick, int frames) {
             for (int l = 0; l < L_; ++l) {
-                lv_[l].tuned_path = cand[l][idx[l]].path;
-                lv_[l].tuned_band = cand[l][idx[l]].band;
+                lv_[l].tuned_path = cand[l][pick[l]].path;
+                lv_[l].tuned_band = cand[l][pick[l]].band;
             }
             drop_graphs();
             // two frames capture both parities' graphs, then `frames` replays are timed one
             // by one (with `flush` overwritten before each, outside the timing, if given)
             compute_async(stream_);
             compute_async(stream_);
-            float ms = 0.f;
+            std::vector<float> t(frames);
             for (int k = 0; k < frames; ++k) {
                 if (flush && flush_bytes)
                     check_cuda(cudaMemsetAsync(flush, k & 0xff, flush_bytes, stream_), "flush");
@@ -851,17 +849,31 @@ void Filter::autotune(int reps, void* flush, size_t flush_bytes) {
                 compute_async(stream_);
                 check_cuda(cudaEventRecord(e1, stream_), "cudaEventRecord");
                 check_cuda(cudaEventSynchronize(e1), "autotune");
-                float t = 0.f;
-                check_cuda(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
-                ms += t;
+                check_cuda(cudaEventElapsedTime(&t[k], e0, e1), "cudaEventElapsedTime");
             }
-            if (best_ms < 0.f || ms < best_ms) {
-                best_ms = ms;
-                best_idx = idx;
-            }
+            std::nth_element(t.begin(), t.begin() + frames / 2, t.end());
+            return t[frames / 2];
+        };
+        const int frames = std::max(reps, 7);
+        std::vector<std::pair<float, std::vector<size_t>>> scored;
+        std::vector<size_t> idx(L_, 0);
+        for (;;) {
+            const float ms = score(idx, frames);
+            scored.push_back({ms, idx});
             int l = 0;
             while (l < L_ && ++idx[l] == cand[l].size()) idx[l++] = 0;
             if (l == L_) break;
+        }
+        // the four best again, over three times the frames
+        std::sort(scored.begin(), scored.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        std::vector<size_t> best_idx = scored[0].second;
+        float best_ms = -1.f;
+        for (size_t k = 0; k < scored.size() && k < 4; ++k) {
+            const float ms = score(scored[k].second, 3 * frames);
+            if (best_ms < 0.f || ms < best_ms) {
+                best_ms = ms;
+                best_idx = scored[k].second;
+            }
         }
         for (int l = 0; l < L_; ++l) {
             lv_[l].tuned_path = cand[l][best_idx[l]].path;
@@ -975,7 +987,15 @@ void Filter::enqueue_frame(cudaStream_t s) {
     int p_top = 0;
     fuse_pyramid_ = kind_ == Kind::Pyramidal && L_ == 2 && path_of(1, &p_top) == kTile;
     if (kind_ == Kind::Pyramidal && !fuse_pyramid_) {
-        for (int l = 1; l < L_; ++l) {
+        int l = 1;
+        if (L_ >= 3 && lv_[2].H >= 1 && lv_[2].W >= 1) {  // levels 1 and 2 in one launch
+            const Level& fine = lv_[0];
+            check_cuda(launch_pyramid_down2(fine.img, fine.img_pitch, item_, fine.H, fine.W, pyr_[0].p, pyr_[0].pitch,
+                                            pyr_[1].p, pyr_[1].pitch, s),
+                       "pyramid");
+            l = 3;
+        }
+        for (; l < L_; ++l) {
             const Level& fine = lv_[l - 1];
             check_cuda(launch_pyramid_down(fine.img, fine.img_pitch, item_, fine.H, fine.W, pyr_[l - 1].p,
                                            pyr_[l - 1].pitch, s),

@@ -29,6 +29,46 @@ __global__ void pyramid_down_k(CView<P> in, View<P> out) {
     pyramid_px(in, out, x, y);
 }
 
+// Two pyramid steps in one launch: a block computes a 64 x 16 tile of level 1 (plus the
+// one-pixel ring that level 2 reads, at clamped coordinates) into shared memory, stores the
+// tile, and computes the 32 x 8 level-2 pixels under it from shared memory: the same values
+// as two pyramid_down_k launches.  Level 1 is H1 x W1 = (H/2) x (W/2), level 2 (H1/2) x (W1/2).
+constexpr int P2X = 2 * BX, P2Y = 2 * BY;  // level-1 tile
+template <typename P>
+__global__ void pyramid_down2_k(CView<P> in, View<P> out1, View<P> out2) {
+    __shared__ P ring[P2Y + 2][P2X + 2];
+    grid_dep_wait();
+    grid_dep_launch();
+    const int x1 = blockIdx.x * P2X, y1 = blockIdx.y * P2Y;  // level-1 tile origin
+    const int H1 = out1.h, W1 = out1.w;
+    const CView<P> lv1{out1.ptr, out1.pitch, H1, W1};
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += blockDim.x * blockDim.y) {
+        const int i = k % (P2X + 2), j = k / (P2X + 2);
+        const int ux = x1 - 1 + i, uy = y1 - 1 + j;  // unclamped level-1 position
+        const int cx = min(max(ux, 0), W1 - 1), cy = min(max(uy, 0), H1 - 1);
+        const P v = pyramid_val(in, cx, cy);
+        ring[j][i] = v;
+        if (ux == cx && uy == cy && ux >= x1 && ux < x1 + P2X && uy >= y1 && uy < y1 + P2Y) out1.at(ux, uy) = v;
+    }
+    __syncthreads();
+    const int x2 = x1 / 2 + threadIdx.x, y2 = y1 / 2 + threadIdx.y;
+    if (x2 >= out2.w || y2 >= out2.h) return;
+    // pyramid_val over level 1, whose clamped reads the ring already holds
+    float xs[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int r = 2 * y2 - 1 + j - (y1 - 1);
+        const int c = 2 * x2 - 1 - (x1 - 1);
+        const float s = down3(Pix<P>::get(ring[r][c]), Pix<P>::get(ring[r][c + 1]), Pix<P>::get(ring[r][c + 2]));
+        if constexpr (sizeof(P) == 1) xs[j] = u8_to_unit(quantize_u8(s));
+        else xs[j] = s;
+    }
+    const float s = down3(xs[0], xs[1], xs[2]);
+    if constexpr (sizeof(P) == 1) out2.at(x2, y2) = quantize_u8(s);
+    else out2.at(x2, y2) = s;
+}
+
 // imagePrefilter_k + imageModel_k fused per pixel (imagemodel_k.cu:31-133):
 // bY = Y-blur, bX = X-blur of the input; a0 = X-blur(bY), ax = X-diff(bY), ay = Y-diff(bX).
 template <typename P>
@@ -170,6 +210,19 @@ bool pdl_enabled() {
         return !(v && v[0] == '0');
     }();
     return on;
+}
+
+cudaError_t launch_pyramid_down2(const void* in, size_t in_pitch, int item, int H, int W, void* out1,
+                                 size_t out1_pitch, void* out2, size_t out2_pitch, cudaStream_t s) {
+    const int h1 = H / 2, w1 = W / 2, h2 = h1 / 2, w2 = w1 / 2;
+    if (h2 <= 0 || w2 <= 0) return cudaErrorInvalidValue;
+    const dim3 grid((w1 + P2X - 1) / P2X, (h1 + P2Y - 1) / P2Y);
+    if (item == 1)
+        return launch_k(pyramid_down2_k<uint8_t>, grid, dim3(BX, BY), 0, s,
+                        CView<uint8_t>{(const uint8_t*)in, in_pitch, H, W},
+                        View<uint8_t>{(uint8_t*)out1, out1_pitch, h1, w1}, View<uint8_t>{(uint8_t*)out2, out2_pitch, h2, w2});
+    return launch_k(pyramid_down2_k<float>, grid, dim3(BX, BY), 0, s, CView<float>{(const float*)in, in_pitch, H, W},
+                    View<float>{(float*)out1, out1_pitch, h1, w1}, View<float>{(float*)out2, out2_pitch, h2, w2});
 }
 
 cudaError_t launch_pyramid_down(const void* in, size_t in_pitch, int item, int H, int W, void* out,
