@@ -270,6 +270,10 @@ ff_status ff_stage_delta_update(const float* a0, size_t a0_pitch, const float* g
 size_t ff_stage_smooth_workspace_size(int height, int width);
 ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int width, int iterations,
                           float* out, size_t out_pitch, void* ws, void* stream);
+/* scalarProductF2_k (src/gpu/device/misc_k.cu:18-38): every float2 of a flow field times
+ * `scalar` (FlowPropagator::setInvertInputFlow uses -1, propagation.cu:92-96). */
+ff_status ff_stage_scale_flow(const float* flow, size_t flow_pitch, int height, int width, float scalar, float* out,
+                              size_t out_pitch, void* stream);
 /* ------------------------------------------------------------ batched streams
  * No counterpart in the reference: many independent PyramidalFlowFilter streams of
  * different sizes, levels and parameters advanced together.  Stream i's frame is read from

@@ -5,6 +5,7 @@
 // reference's callers link against.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <stdexcept>
 #include <string>
@@ -14,11 +15,14 @@
 #include "flowfilter/gpu/camera.h"
 #include "flowfilter/gpu/display.h"
 #include "flowfilter/gpu/flowfilter.h"
+#include "flowfilter/gpu/flowsmoothing.h"
 #include "flowfilter/gpu/image.h"
 #include "flowfilter/gpu/imagemodel.h"
 #include "flowfilter/gpu/pipeline.h"
 #include "flowfilter/gpu/propagation.h"
+#include "flowfilter/gpu/pyramid.h"
 #include "flowfilter/gpu/rotation.h"
+#include "flowfilter/gpu/update.h"
 
 static_assert(sizeof(flowfilter::gpu::perspectiveCamera) == sizeof(ff_camera), "perspectiveCamera / ff_camera");
 
@@ -208,6 +212,374 @@ void ImageModel::compute() {
 
 GPUImage ImageModel::getImageConstant() { return constant_; }
 GPUImage ImageModel::getImageGradient() { return gradient_; }
+
+// ------------------------------------------------------------------ stage classes
+namespace {
+
+// a device scratch buffer of at least `bytes` (reused while large enough)
+GPUImage scratch(GPUImage& ws, std::size_t bytes) {
+    const int w = (int)std::max<std::size_t>(bytes, 1);
+    if (!ws.data() || (std::size_t)ws.pitch() < (std::size_t)w) ws = GPUImage(1, w, 1, 1);
+    return ws;
+}
+
+void need_flow(GPUImage& img, const char* where) {
+    if (img.depth() != 2 || img.itemSize() != 4)
+        throw std::invalid_argument(std::string(where) + ": a flow field should have depth 2 of float");
+}
+void need_scalar(GPUImage& img, const char* where) {
+    if (img.depth() != 1 || img.itemSize() != 4)
+        throw std::invalid_argument(std::string(where) + ": the field should have depth 1 of float");
+}
+void same_shape(GPUImage& a, GPUImage& b, const char* where) {
+    if (a.height() != b.height() || a.width() != b.width())
+        throw std::invalid_argument(std::string(where) + ": input buffers do not match height and width");
+}
+
+}  // namespace
+
+// FlowSmoother (flowsmoothing.cu:20-127)
+FlowSmoother::FlowSmoother() = default;
+FlowSmoother::FlowSmoother(GPUImage inputFlow, const int iterations) {
+    setIterations(iterations);
+    setInputFlow(inputFlow);
+    configure();
+}
+FlowSmoother::~FlowSmoother() = default;
+void FlowSmoother::configure() {
+    if (!input_.data()) throw std::logic_error("FlowSmoother::configure(): input flow not set");
+    smoothed_ = GPUImage(input_.height(), input_.width(), 2, sizeof(float));
+    smoothed_.clear();
+    configured_ = true;
+}
+void FlowSmoother::compute() {
+    if (!configured_) throw std::logic_error("FlowSmoother::compute(): stage not configured");
+    GPUImage ws = scratch(workspace_, ff_stage_smooth_workspace_size(input_.height(), input_.width()));
+    startTiming();
+    check(ff_stage_smooth((const float*)input_.data(), input_.pitch(), input_.height(), input_.width(), iterations_,
+                          (float*)smoothed_.data(), smoothed_.pitch(), ws.data(), stream_),
+          "FlowSmoother::compute");
+    stopTiming();
+}
+int FlowSmoother::getIterations() const { return iterations_; }
+void FlowSmoother::setIterations(const int N) {
+    if (N <= 0)
+        throw std::invalid_argument("FlowSmoother::setIterations(): iterations should be greater than zero: " +
+                                    std::to_string(N));
+    iterations_ = N;
+}
+void FlowSmoother::setInputFlow(GPUImage inputFlow) {
+    need_flow(inputFlow, "FlowSmoother::setInputFlow()");
+    input_ = inputFlow;
+}
+GPUImage FlowSmoother::getSmoothedFlow() { return smoothed_; }
+
+// ImagePyramid (pyramid.cu:20-219)
+ImagePyramid::ImagePyramid() = default;
+ImagePyramid::ImagePyramid(GPUImage image, const int levels) {
+    setInputImage(image);
+    setLevels(levels);
+    configure();
+}
+ImagePyramid::~ImagePyramid() = default;
+void ImagePyramid::configure() {
+    if (!input_.data()) throw std::logic_error("ImagePyramid::configure(): input image not set");
+    images_.clear();
+    int h = input_.height(), w = input_.width();
+    for (int l = 1; l < levels_; ++l) {
+        h /= 2;
+        w /= 2;
+        if (h < 1 || w < 1) throw std::invalid_argument("ImagePyramid::configure(): too many levels for the image");
+        images_.emplace_back(h, w, 1, input_.itemSize());
+        images_.back().clear();
+    }
+    configured_ = true;
+}
+void ImagePyramid::compute() {
+    if (!configured_) throw std::logic_error("ImagePyramid::compute(): stage not configured");
+    startTiming();
+    GPUImage prev = input_;
+    for (GPUImage& img : images_) {
+        check(ff_stage_pyramid_down(prev.data(), prev.pitch(), prev.itemSize(), prev.height(), prev.width(),
+                                    img.data(), img.pitch(), stream_),
+              "ImagePyramid::compute");
+        prev = img;
+    }
+    stopTiming();
+}
+void ImagePyramid::setInputImage(GPUImage img) {
+    if (img.depth() != 1 || (img.itemSize() != 1 && img.itemSize() != 4))
+        throw std::invalid_argument("ImagePyramid::setInputImage(): image should have depth 1 of uint8 or float");
+    input_ = img;
+    configured_ = false;
+}
+void ImagePyramid::setLevels(const int levels) {
+    if (levels <= 0)
+        throw std::invalid_argument("ImagePyramid::setLevels(): levels should be greater than zero: " +
+                                    std::to_string(levels));
+    levels_ = levels;
+    configured_ = false;
+}
+GPUImage ImagePyramid::getImage(int level) {
+    if (level < 0 || level >= levels_)
+        throw std::out_of_range("ImagePyramid::getImage(): level index out of bounds: " + std::to_string(level));
+    if (level == 0) return input_;
+    if (!configured_) throw std::logic_error("ImagePyramid::getImage(): stage not configured");
+    return images_[level - 1];
+}
+int ImagePyramid::getLevels() const { return levels_; }
+
+// FlowPropagator (propagation.cu:20-210)
+FlowPropagator::FlowPropagator() = default;
+FlowPropagator::FlowPropagator(GPUImage inputFlow, const int iterations) {
+    setIterations(iterations);
+    setInputFlow(inputFlow);
+    configure();
+}
+FlowPropagator::~FlowPropagator() = default;
+void FlowPropagator::configure() {
+    if (!input_.data()) throw std::logic_error("FlowPropagator::configure(): input flow not set");
+    propagated_ = GPUImage(input_.height(), input_.width(), 2, sizeof(float));
+    propagated_.clear();
+    configured_ = true;
+}
+void FlowPropagator::compute() {
+    if (!configured_) throw std::logic_error("FlowPropagator::compute(): stage not configured");
+    GPUImage ws = scratch(workspace_, ff_stage_propagate_workspace_size(input_.height(), input_.width()));
+    GPUImage src = input_;
+    startTiming();
+    if (invert_) {  // scalarProductF2_k with -1 (propagation.cu:92-96)
+        if (!negated_.data() || negated_.height() != input_.height() || negated_.width() != input_.width())
+            negated_ = GPUImage(input_.height(), input_.width(), 2, sizeof(float));
+        check(ff_stage_scale_flow((const float*)input_.data(), input_.pitch(), input_.height(), input_.width(), -1.0f,
+                                  (float*)negated_.data(), negated_.pitch(), stream_),
+              "FlowPropagator::compute");
+        src = negated_;
+    }
+    check(ff_stage_propagate((const float*)src.data(), src.pitch(), src.height(), src.width(), iterations_, border_,
+                             (float*)propagated_.data(), propagated_.pitch(), ws.data(), stream_),
+          "FlowPropagator::compute");
+    stopTiming();
+}
+void FlowPropagator::setIterations(const int N) {
+    if (N <= 0)
+        throw std::invalid_argument("FlowPropagator::setIterations(): iterations should be greater than zero: " +
+                                    std::to_string(N));
+    iterations_ = N;
+}
+int FlowPropagator::getIterations() const { return iterations_; }
+float FlowPropagator::getDt() const { return 1.0f / float(iterations_); }
+void FlowPropagator::setBorder(const int border) {
+    if (border < 0) throw std::invalid_argument("FlowPropagator::setBorder(): border should be >= 0");
+    border_ = border;
+}
+int FlowPropagator::getBorder() const { return border_; }
+void FlowPropagator::setInvertInputFlow(const bool invert) { invert_ = invert; }
+bool FlowPropagator::getInvertInputFlow() const { return invert_; }
+void FlowPropagator::setInputFlow(GPUImage inputFlow) {
+    need_flow(inputFlow, "FlowPropagator::setInputFlow()");
+    input_ = inputFlow;
+}
+GPUImage FlowPropagator::getPropagatedFlow() { return propagated_; }
+
+// FlowPropagatorPayload (propagation.cu:212-412)
+FlowPropagatorPayload::FlowPropagatorPayload() = default;
+FlowPropagatorPayload::FlowPropagatorPayload(GPUImage inputFlow, GPUImage scalarPayload, GPUImage vectorPayload,
+                                             const int iterations) {
+    setIterations(iterations);
+    setInputFlow(inputFlow);
+    setScalarPayload(scalarPayload);
+    setVectorPayload(vectorPayload);
+    configure();
+}
+FlowPropagatorPayload::~FlowPropagatorPayload() = default;
+void FlowPropagatorPayload::configure() {
+    if (!flow_.data() || !scalar_.data() || !vector_.data())
+        throw std::logic_error("FlowPropagatorPayload::configure(): inputs not set");
+    same_shape(flow_, scalar_, "FlowPropagatorPayload::configure()");
+    same_shape(flow_, vector_, "FlowPropagatorPayload::configure()");
+    flowOut_ = GPUImage(flow_.height(), flow_.width(), 2, sizeof(float));
+    scalarOut_ = GPUImage(flow_.height(), flow_.width(), 1, sizeof(float));
+    vectorOut_ = GPUImage(flow_.height(), flow_.width(), 2, sizeof(float));
+    flowOut_.clear();
+    scalarOut_.clear();
+    vectorOut_.clear();
+    configured_ = true;
+}
+void FlowPropagatorPayload::compute() {
+    if (!configured_) throw std::logic_error("FlowPropagatorPayload::compute(): stage not configured");
+    GPUImage ws = scratch(workspace_, ff_stage_propagate_payload_workspace_size(flow_.height(), flow_.width()));
+    startTiming();
+    check(ff_stage_propagate_payload((const float*)flow_.data(), flow_.pitch(), (const float*)scalar_.data(),
+                                     scalar_.pitch(), (const float*)vector_.data(), vector_.pitch(), flow_.height(),
+                                     flow_.width(), iterations_, border_, (float*)flowOut_.data(), flowOut_.pitch(),
+                                     (float*)scalarOut_.data(), scalarOut_.pitch(), (float*)vectorOut_.data(),
+                                     vectorOut_.pitch(), ws.data(), stream_),
+          "FlowPropagatorPayload::compute");
+    stopTiming();
+}
+void FlowPropagatorPayload::setIterations(const int N) {
+    if (N <= 0)
+        throw std::invalid_argument("FlowPropagatorPayload::setIterations(): iterations should be greater than zero: " +
+                                    std::to_string(N));
+    iterations_ = N;
+}
+int FlowPropagatorPayload::getIterations() const { return iterations_; }
+float FlowPropagatorPayload::getDt() const { return 1.0f / float(iterations_); }
+void FlowPropagatorPayload::setBorder(const int border) {
+    if (border < 0) throw std::invalid_argument("FlowPropagatorPayload::setBorder(): border should be >= 0");
+    border_ = border;
+}
+int FlowPropagatorPayload::getBorder() const { return border_; }
+void FlowPropagatorPayload::setInputFlow(GPUImage img) {
+    need_flow(img, "FlowPropagatorPayload::setInputFlow()");
+    flow_ = img;
+}
+void FlowPropagatorPayload::setScalarPayload(GPUImage img) {
+    need_scalar(img, "FlowPropagatorPayload::setScalarPayload()");
+    scalar_ = img;
+}
+void FlowPropagatorPayload::setVectorPayload(GPUImage img) {
+    need_flow(img, "FlowPropagatorPayload::setVectorPayload()");
+    vector_ = img;
+}
+GPUImage FlowPropagatorPayload::getPropagatedFlow() { return flowOut_; }
+GPUImage FlowPropagatorPayload::getPropagatedScalar() { return scalarOut_; }
+GPUImage FlowPropagatorPayload::getPropagatedVector() { return vectorOut_; }
+
+// FlowUpdate (update.cu:20-210)
+FlowUpdate::FlowUpdate() = default;
+FlowUpdate::FlowUpdate(GPUImage inputFlow, GPUImage inputImage, GPUImage inputImageGradient, const float gamma,
+                       const float maxflow) {
+    setGamma(gamma);
+    setMaxFlow(maxflow);
+    setInputFlow(inputFlow);
+    setInputImage(inputImage);
+    setInputImageGradient(inputImageGradient);
+    configure();
+}
+FlowUpdate::~FlowUpdate() = default;
+void FlowUpdate::configure() {
+    if (!flow_.data() || !image_.data() || !gradient_.data())
+        throw std::logic_error("FlowUpdate::configure(): inputs not set");
+    same_shape(flow_, image_, "FlowUpdate::configure()");
+    same_shape(flow_, gradient_, "FlowUpdate::configure()");
+    flowUpdated_ = GPUImage(flow_.height(), flow_.width(), 2, sizeof(float));
+    imageUpdated_ = GPUImage(flow_.height(), flow_.width(), 1, sizeof(float));
+    flowUpdated_.clear();
+    imageUpdated_.clear();
+    configured_ = true;
+}
+void FlowUpdate::compute() {
+    if (!configured_) throw std::logic_error("FlowUpdate::compute(): stage not configured");
+    startTiming();
+    // the old image is read from, and the new image constant written to, the updated image
+    check(ff_stage_update((const float*)image_.data(), image_.pitch(), (const float*)gradient_.data(),
+                          gradient_.pitch(), (const float*)imageUpdated_.data(), imageUpdated_.pitch(),
+                          (const float*)flow_.data(), flow_.pitch(), flow_.height(), flow_.width(), gamma_, maxflow_,
+                          (float*)flowUpdated_.data(), flowUpdated_.pitch(), (float*)imageUpdated_.data(),
+                          imageUpdated_.pitch(), stream_),
+          "FlowUpdate::compute");
+    stopTiming();
+}
+float FlowUpdate::getGamma() const { return gamma_; }
+void FlowUpdate::setGamma(const float gamma) {
+    if (!(gamma > 0))
+        throw std::invalid_argument("FlowUpdate::setGamma(): gamma should be greater than zero: " +
+                                    std::to_string(gamma));
+    gamma_ = gamma;
+}
+float FlowUpdate::getMaxFlow() const { return maxflow_; }
+void FlowUpdate::setMaxFlow(const float maxflow) { maxflow_ = maxflow; }
+void FlowUpdate::setInputFlow(GPUImage inputFlow) {
+    need_flow(inputFlow, "FlowUpdate::setInputFlow()");
+    flow_ = inputFlow;
+}
+void FlowUpdate::setInputImage(GPUImage image) {
+    need_scalar(image, "FlowUpdate::setInputImage()");
+    image_ = image;
+}
+void FlowUpdate::setInputImageGradient(GPUImage imageGradient) {
+    need_flow(imageGradient, "FlowUpdate::setInputImageGradient()");
+    gradient_ = imageGradient;
+}
+GPUImage FlowUpdate::getUpdatedFlow() { return flowUpdated_; }
+GPUImage FlowUpdate::getUpdatedImage() { return imageUpdated_; }
+
+// DeltaFlowUpdate (update.cu:212-420)
+DeltaFlowUpdate::DeltaFlowUpdate() = default;
+DeltaFlowUpdate::DeltaFlowUpdate(GPUImage inputFlow, GPUImage inputDeltaFlow, GPUImage inputOldImage,
+                                 GPUImage inputImage, GPUImage inputImageGradient, const float gamma,
+                                 const float maxflow) {
+    setGamma(gamma);
+    setMaxFlow(maxflow);
+    setInputDeltaFlow(inputDeltaFlow);
+    setInputFlow(inputFlow);
+    setInputImageOld(inputOldImage);
+    setInputImage(inputImage);
+    setInputImageGradient(inputImageGradient);
+    configure();
+}
+DeltaFlowUpdate::~DeltaFlowUpdate() = default;
+void DeltaFlowUpdate::configure() {
+    if (!coarse_.data() || !delta_.data() || !oldImage_.data() || !image_.data() || !gradient_.data())
+        throw std::logic_error("DeltaFlowUpdate::configure(): inputs not set");
+    same_shape(delta_, oldImage_, "DeltaFlowUpdate::configure()");
+    same_shape(delta_, image_, "DeltaFlowUpdate::configure()");
+    same_shape(delta_, gradient_, "DeltaFlowUpdate::configure()");
+    flowUpdated_ = GPUImage(delta_.height(), delta_.width(), 2, sizeof(float));
+    deltaUpdated_ = GPUImage(delta_.height(), delta_.width(), 2, sizeof(float));
+    imageUpdated_ = GPUImage(delta_.height(), delta_.width(), 1, sizeof(float));
+    flowUpdated_.clear();
+    deltaUpdated_.clear();
+    imageUpdated_.clear();
+    configured_ = true;
+}
+void DeltaFlowUpdate::compute() {
+    if (!configured_) throw std::logic_error("DeltaFlowUpdate::compute(): stage not configured");
+    startTiming();
+    check(ff_stage_delta_update((const float*)image_.data(), image_.pitch(), (const float*)gradient_.data(),
+                                gradient_.pitch(), (const float*)oldImage_.data(), oldImage_.pitch(),
+                                (const float*)delta_.data(), delta_.pitch(), (const float*)coarse_.data(),
+                                coarse_.pitch(), coarse_.height(), coarse_.width(), delta_.height(), delta_.width(),
+                                gamma_, maxflow_, (float*)flowUpdated_.data(), flowUpdated_.pitch(),
+                                (float*)deltaUpdated_.data(), deltaUpdated_.pitch(), (float*)imageUpdated_.data(),
+                                imageUpdated_.pitch(), stream_),
+          "DeltaFlowUpdate::compute");
+    stopTiming();
+}
+float DeltaFlowUpdate::getGamma() const { return gamma_; }
+void DeltaFlowUpdate::setGamma(const float gamma) {
+    if (!(gamma > 0))
+        throw std::invalid_argument("DeltaFlowUpdate::setGamma(): gamma should be greater than zero: " +
+                                    std::to_string(gamma));
+    gamma_ = gamma;
+}
+float DeltaFlowUpdate::getMaxFlow() const { return maxflow_; }
+void DeltaFlowUpdate::setMaxFlow(const float maxflow) { maxflow_ = maxflow; }
+void DeltaFlowUpdate::setInputFlow(GPUImage inputFlow) {
+    need_flow(inputFlow, "DeltaFlowUpdate::setInputFlow()");
+    coarse_ = inputFlow;
+}
+void DeltaFlowUpdate::setInputDeltaFlow(GPUImage inputDeltaFlow) {
+    need_flow(inputDeltaFlow, "DeltaFlowUpdate::setInputDeltaFlow()");
+    delta_ = inputDeltaFlow;
+}
+void DeltaFlowUpdate::setInputImageOld(GPUImage image) {
+    need_scalar(image, "DeltaFlowUpdate::setInputImageOld()");
+    oldImage_ = image;
+}
+void DeltaFlowUpdate::setInputImage(GPUImage image) {
+    need_scalar(image, "DeltaFlowUpdate::setInputImage()");
+    image_ = image;
+}
+void DeltaFlowUpdate::setInputImageGradient(GPUImage imageGradient) {
+    need_flow(imageGradient, "DeltaFlowUpdate::setInputImageGradient()");
+    gradient_ = imageGradient;
+}
+GPUImage DeltaFlowUpdate::getUpdatedFlow() { return flowUpdated_; }
+GPUImage DeltaFlowUpdate::getUpdatedDeltaFlow() { return deltaUpdated_; }
+GPUImage DeltaFlowUpdate::getUpdatedImage() { return imageUpdated_; }
 
 // ------------------------------------------------------------------ FlowToColor
 FlowToColor::FlowToColor() = default;

@@ -636,6 +636,21 @@ ff_status ff_stage_smooth(const float* flow, size_t flow_pitch, int height, int 
     });
 }
 
+ff_status ff_stage_scale_flow(const float* flow, size_t flow_pitch, int height, int width, float scalar, float* out,
+                              size_t out_pitch, void* stream) {
+    return guard([&] {
+        need(flow, "flow");
+        need(out, "output");
+        check_stage_dims(height, width);
+        if ((uintptr_t)flow % 8 || (uintptr_t)out % 8 || flow_pitch % 8 || out_pitch % 8 ||
+            flow_pitch < (size_t)width * 8 || out_pitch < (size_t)width * 8)
+            throw Error(FF_ERR_INVALID_ARGUMENT, "flow fields need 8-byte aligned rows of width float2");
+        ffb::check_cuda(ffb::launch_scale_flow(flow, flow_pitch, height, width, scalar, out, out_pitch,
+                                               (cudaStream_t)stream),
+                        "scale flow");
+    });
+}
+
 }  // extern "C"
 
 // ---- batched step over many streams (batch.h)

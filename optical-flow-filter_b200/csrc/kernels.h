@@ -9,6 +9,9 @@ namespace ffb {
 // ---- per-stage kernels (stage_kernels.cu)
 cudaError_t launch_pyramid_down(const void* in, size_t in_pitch, int item, int H, int W, void* out,
                                 size_t out_pitch, cudaStream_t s);
+// every float2 of an H x W field times k
+cudaError_t launch_scale_flow(const float* in, size_t in_pitch, int H, int W, float k, float* out, size_t out_pitch,
+                              cudaStream_t s);
 // two pyramid steps (levels 1 and 2 of an H x W level 0) in one launch; needs a level 2
 cudaError_t launch_pyramid_down2(const void* in, size_t in_pitch, int item, int H, int W, void* out1,
                                  size_t out1_pitch, void* out2, size_t out2_pitch, cudaStream_t s);

@@ -137,6 +137,7 @@ SIGNATURES = {
                                     _vp, _sz, _vp, _sz, _vp]),
     "ff_stage_smooth_workspace_size": (_sz, [_i, _i]),
     "ff_stage_smooth": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp, _vp]),
+    "ff_stage_scale_flow": (_st, [_vp, _sz, _i, _i, ctypes.c_float, _vp, _sz, _vp]),
     "ff_stage_smooth_noalloc": (_st, [_vp, _sz, _i, _i, _i, _vp, _sz, _vp]),
     "ff_batch_create": (_st, [_i, _ip, _ip, _ip, _vpp]),
     "ff_batch_destroy": (_st, [_vp]),

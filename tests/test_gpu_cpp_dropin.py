@@ -85,3 +85,35 @@ def test_cpp_dropin_rotation_matches_oracle(cuda, tmp_path, h, w, d, n):
     np.testing.assert_array_equal(got[4:4 + n2].reshape(flow.shape), flow)
     np.testing.assert_array_equal(got[4 + n2:4 + n2 + nd].reshape(img.shape), pred)
     np.testing.assert_array_equal(got[4 + n2 + nd:].reshape(img.shape), pred)
+
+
+@pytest.fixture(scope="module")
+def stages_program(cuda, tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("dropin") / "dropin_stages")
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "dropin_stages.cpp"), "-o", out,
+           "-L", PKG, "-lflowfilter_gpu", "-Wl,-rpath," + PKG]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+@pytest.mark.parametrize("name", ["constant_320x240_L1", "small_96x64_L2", "odd_150x98_L3"])
+def test_cpp_stage_classes_rebuild_the_reference_filters(stages_program, tmp_path, name):
+    """FlowSmoother, ImagePyramid, FlowPropagator[Payload], [Delta]FlowUpdate and ImageModel
+    wired into the reference's filters by a C++ program: the flows of the reference library,
+    bit for bit (sha256 per dumped frame)."""
+    from conftest import golden_case
+    from make_reference_fixtures import CASES, sha
+
+    case = CASES[name]
+    meta, _ = golden_case(name)
+    frames = case_frames(case)
+    t, h, w = frames.shape
+    fin, fout = tmp_path / "frames.u8", tmp_path / "flows.f32"
+    frames.tofile(fin)
+    r = subprocess.run([stages_program, str(fin), str(h), str(w), str(t), str(case["levels"]), repr(case["maxflow"]),
+                        ",".join(repr(g) for g in case["gamma"]), ",".join(str(s) for s in case["smooth"]), str(fout)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    flows = np.fromfile(fout, np.float32).reshape(t, h, w, 2)
+    assert [sha(flows[k]) for k in case["dump"]] == meta["flow_sha256"]
