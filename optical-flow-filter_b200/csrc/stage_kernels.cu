@@ -29,57 +29,27 @@ __global__ void pyramid_down_k(CView<P> in, View<P> out) {
     pyramid_px(in, out, x, y);
 }
 
-// Two pyramid steps in one launch.  A block owns a 64 x 16 tile of level 1 and the 32 x 8
-// level-2 pixels under it.  It stages the level-0 rows and columns the tile reads (at
-// clamped coordinates) in shared memory, runs the X pass (imageDownX) there for the tile
-// plus the one-pixel ring level 2 reads, then the Y pass (imageDownY), stores the tile, and
-// finishes level 2 from the ring: every value as two pyramid_down_k launches compute it.
-// Level 1 is H1 x W1 = (H/2) x (W/2), level 2 (H1/2) x (W1/2).
-constexpr int P2X = 2 * BX, P2Y = 2 * BY;        // level-1 tile
-constexpr int R1X = P2X + 2, R1Y = P2Y + 2;      // with its ring: level-1 columns / rows
-constexpr int S0X = 2 * R1X + 1, S0Y = 2 * R1Y + 1;  // level-0 columns / rows they read
+// Two pyramid steps in one launch: a block computes a 64 x 16 tile of level 1 (plus the
+// one-pixel ring that level 2 reads, at clamped coordinates) into shared memory, stores the
+// tile, and computes the 32 x 8 level-2 pixels under it from shared memory: the same values
+// as two pyramid_down_k launches.  Level 1 is H1 x W1 = (H/2) x (W/2), level 2 (H1/2) x (W1/2).
+constexpr int P2X = 2 * BX, P2Y = 2 * BY;  // level-1 tile
 template <typename P>
 __global__ void pyramid_down2_k(CView<P> in, View<P> out1, View<P> out2) {
-    __shared__ float img0[S0Y][S0X];   // level 0, normalised, at clamped coordinates
-    __shared__ float xpass[S0Y][R1X];  // imageDownX of those rows at the ring's columns
-    __shared__ P ring[R1Y][R1X];       // level 1 at the ring's (clamped) coordinates
+    __shared__ P ring[P2Y + 2][P2X + 2];
     grid_dep_wait();
     grid_dep_launch();
     const int x1 = blockIdx.x * P2X, y1 = blockIdx.y * P2Y;  // level-1 tile origin
     const int H1 = out1.h, W1 = out1.w;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-    // level-1 ring position (i, j) is the clamped level-1 pixel (cx(i), cy(j)); it reads level-0
-    // columns 2 cx - 1 .. 2 cx + 1 and rows 2 cy - 1 .. 2 cy + 1 (clamped to level 0)
-    auto cx = [&](int i) { return min(max(x1 - 1 + i, 0), W1 - 1); };
-    auto cy = [&](int j) { return min(max(y1 - 1 + j, 0), H1 - 1); };
-    const int gx0 = 2 * (x1 - 1) - 1, gy0 = 2 * (y1 - 1) - 1;  // level-0 origin of img0
-    for (int k = tid; k < S0X * S0Y; k += nt) {
-        const int i = k % S0X, j = k / S0X;
-        img0[j][i] = Pix<P>::get(in.clamped(gx0 + i, gy0 + j));
-    }
-    __syncthreads();
-    // X pass at level-1 column cx(i), level-0 row gy0 + j (its clamped column reads map into
-    // img0 because clamping level-1 first keeps 2 cx - 1 .. 2 cx + 1 inside img0's span)
-    for (int k = tid; k < R1X * S0Y; k += nt) {
-        const int i = k % R1X, j = k / R1X;
-        const int c = 2 * cx(i) - gx0;  // img0 column of level-0 column 2 cx
-        const int cm = max(2 * cx(i) - 1, 0) - gx0, cp = min(2 * cx(i) + 1, in.w - 1) - gx0;
-        const float s = down3(img0[j][cm], img0[j][c], img0[j][cp]);
-        if constexpr (sizeof(P) == 1) xpass[j][i] = u8_to_unit(quantize_u8(s));
-        else xpass[j][i] = s;
-    }
-    __syncthreads();
-    for (int k = tid; k < R1X * R1Y; k += nt) {
-        const int i = k % R1X, j = k / R1X;
-        const int r = 2 * cy(j) - gy0;
-        const int rm = max(2 * cy(j) - 1, 0) - gy0, rp = min(2 * cy(j) + 1, in.h - 1) - gy0;
-        const float s = down3(xpass[rm][i], xpass[r][i], xpass[rp][i]);
-        P v;
-        if constexpr (sizeof(P) == 1) v = quantize_u8(s);
-        else v = s;
+    const CView<P> lv1{out1.ptr, out1.pitch, H1, W1};
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += blockDim.x * blockDim.y) {
+        const int i = k % (P2X + 2), j = k / (P2X + 2);
+        const int ux = x1 - 1 + i, uy = y1 - 1 + j;  // unclamped level-1 position
+        const int cx = min(max(ux, 0), W1 - 1), cy = min(max(uy, 0), H1 - 1);
+        const P v = pyramid_val(in, cx, cy);
         ring[j][i] = v;
-        const int ux = x1 - 1 + i, uy = y1 - 1 + j;
-        if (ux >= x1 && ux < x1 + P2X && uy >= y1 && uy < y1 + P2Y && ux < W1 && uy < H1) out1.at(ux, uy) = v;
+        if (ux == cx && uy == cy && ux >= x1 && ux < x1 + P2X && uy >= y1 && uy < y1 + P2Y) out1.at(ux, uy) = v;
     }
     __syncthreads();
     const int x2 = x1 / 2 + threadIdx.x, y2 = y1 / 2 + threadIdx.y;
