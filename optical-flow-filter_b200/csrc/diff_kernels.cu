@@ -365,9 +365,110 @@ __global__ void prop_fwd_k(const T* __restrict__ f, const T* __restrict__ s, con
     }
 }
 
-// Gather-form adjoint of one upwind sub-step: input pixel j (index along AXIS) collects
-// from the outputs i in {j-1, j, j+1} whose clamped stencil (i-1, i, i+1) reads it,
-// recomputing each output's dominant velocity, upwind branch and border freeze.
+// Gather-form adjoint of one upwind sub-step at position j of a line of n positions along
+// the sub-step's axis: the gradients of the input channels at j, collected from the outputs
+// i in {j-1, j, j+1} whose clamped stencil (i-1, i, i+1) reads j, recomputing each output's
+// dominant velocity, upwind branch and border freeze.  chan(p, o): every input channel at
+// position p into o; gchan(p, o): every output-gradient channel at p (p always inside the
+// line).  Channels: flow x, flow y [, scalar, vector x, vector y]; line_in: the line lies
+// inside the border across the axis.
+template <typename T, int AXIS, bool PAYLOAD, typename CH, typename GO>
+__device__ __forceinline__ void prop_adj_at(int j, int n, bool line_in, int border, T dt, const CH& chan,
+                                            const GO& gchan, T (&acc)[PAYLOAD ? 5 : 2]) {
+    constexpr int NC = PAYLOAD ? 5 : 2;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = T(0);
+    if (j >= 2 && j + 2 <= n - 1) {
+        // away from the line ends no index clamps: the five positions j-2..j+2 in registers,
+        // the same operations in the same order as the general loop below
+        T px[5][NC], gx[3][NC];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) chan(j - 2 + p, px[p]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) gchan(j - 1 + q, gx[q]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
+            const int i = j - 1 + q;
+            if (!(line_in && i >= border && i < n - border)) {
+                if (q == 1)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) acc[c] += gx[1][c];
+                continue;
+            }
+            const T vm_ = px[q][AXIS], vp_ = px[q + 2][AXIS];
+            const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
+            const T dv = take_p ? vp_ : vm_;
+            const T t = dt * dv;
+            T gdv = T(0);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const T g_o = gx[q][c];
+                const T g0 = px[q + 1][c];
+                if (dv >= T(0)) {
+                    if (q == 1) acc[c] += g_o * (T(1) - t);
+                    if (q == 2) acc[c] += g_o * t;
+                    gdv -= g_o * dt * (g0 - px[q][c]);
+                } else {
+                    if (q == 1) acc[c] += g_o * (T(1) + t);
+                    if (q == 0) acc[c] -= g_o * t;
+                    gdv -= g_o * dt * (px[q + 2][c] - g0);
+                }
+            }
+            if ((take_p ? q + 2 : q) == 2) acc[AXIS] += gdv;
+        }
+        return;
+    }
+    for (int i = max(j - 1, 0); i <= min(j + 1, n - 1); ++i) {
+        const bool in = line_in && i >= border && i < n - border;
+        T go[NC];
+        gchan(i, go);
+        if (!in) {
+            if (i == j)
+                for (int c = 0; c < NC; ++c) acc[c] += go[c];
+            continue;
+        }
+        const int im = max(i - 1, 0), ip = min(i + 1, n - 1);
+        T pm[NC], p0[NC], pp[NC];
+        chan(im, pm);
+        chan(i, p0);
+        chan(ip, pp);
+        const T vm_ = pm[AXIS], vp_ = pp[AXIS];
+        const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
+        const T dv = take_p ? vp_ : vm_;
+        const T t = dt * dv;
+        T gdv = T(0);
+        for (int c = 0; c < NC; ++c) {
+            if (dv >= T(0)) {
+                if (i == j) acc[c] += go[c] * (T(1) - t);
+                if (im == j) acc[c] += go[c] * t;
+                gdv -= go[c] * dt * (p0[c] - pm[c]);
+            } else {
+                if (i == j) acc[c] += go[c] * (T(1) + t);
+                if (ip == j) acc[c] -= go[c] * t;
+                gdv -= go[c] * dt * (pp[c] - p0[c]);
+            }
+        }
+        // the dominant velocity is the chosen neighbour's AXIS component
+        if ((take_p ? ip : im) == j) acc[AXIS] += gdv;
+    }
+}
+
+// every channel of one pixel of a propagated field (f pairs, s scalars, v pairs) at index k
+template <typename T, bool PAYLOAD>
+__device__ __forceinline__ void field_px(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v,
+                                         size_t k, T (&o)[PAYLOAD ? 5 : 2]) {
+    const auto a = ld2(f, k);
+    o[0] = a.x;
+    o[1] = a.y;
+    if constexpr (PAYLOAD) {
+        const auto b = ld2(v, k);
+        o[2] = s[k];
+        o[3] = b.x;
+        o[4] = b.y;
+    }
+}
+
+// Adjoint of one upwind sub-step, one thread per input pixel (prop_adj_at over global memory)
 template <typename T, int AXIS, bool PAYLOAD, bool ACC = true>
 __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, const T* __restrict__ v,
                            const T* __restrict__ gfo, const T* __restrict__ gso, const T* __restrict__ gvo, T* gf, T* gs,
@@ -376,114 +477,16 @@ __global__ void prop_bwd_k(const T* __restrict__ f, const T* __restrict__ s, con
     grid_dep_launch();
     PIX_SETUP
     if (!live) return;
-    const int n = AXIS == 0 ? W : H;
-    const int j = AXIS == 0 ? x : y;
+    constexpr int NC = PAYLOAD ? 5 : 2;
     // linear index of position p along the axis, on this pixel's line
     auto at = [&](int p) -> size_t { return AXIS == 0 ? (b * H + y) * W + p : (b * H + p) * W + x; };
     const bool line_in = AXIS == 0 ? (y >= border && y < H - border) : (x >= border && x < W - border);
-    constexpr int NC = PAYLOAD ? 5 : 2;  // channels: flow x, flow y [, scalar, vector x, vector y]
-    auto chan = [&](size_t k, int c) -> T {
-        return c < 2 ? f[2 * k + c] : (c == 2 ? s[k] : v[2 * k + (c - 3)]);
-    };
-    auto gchan = [&](size_t k, int c) -> T {
-        return c < 2 ? gfo[2 * k + c] : (c == 2 ? gso[k] : gvo[2 * k + (c - 3)]);
-    };
     T acc[NC];
-    for (int c = 0; c < NC; ++c) acc[c] = T(0);
-    if (j >= 2 && j + 2 <= n - 1) {
-        // away from the line ends no index clamps: the five positions j-2..j+2 in registers,
-        // the same operations in the same order as the general loop below
-        T ch[NC][5], go[NC][3];
-#pragma unroll
-        for (int p = 0; p < 5; ++p) {
-            const size_t k = at(j - 2 + p);
-            const auto fv = ld2(f, k);
-            ch[0][p] = fv.x;
-            ch[1][p] = fv.y;
-            if constexpr (PAYLOAD) {
-                const auto vv = ld2(v, k);
-                ch[2 % NC][p] = s[k];
-                ch[3 % NC][p] = vv.x;
-                ch[4 % NC][p] = vv.y;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const size_t k = at(j - 1 + q);
-            const auto gf2 = ld2(gfo, k);
-            go[0][q] = gf2.x;
-            go[1][q] = gf2.y;
-            if constexpr (PAYLOAD) {
-                const auto gv2 = ld2(gvo, k);
-                go[2 % NC][q] = gso[k];
-                go[3 % NC][q] = gv2.x;
-                go[4 % NC][q] = gv2.y;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
-            const int i = j - 1 + q;
-            if (!(line_in && i >= border && i < n - border)) {
-                if (q == 1)
-                    for (int c = 0; c < NC; ++c) acc[c] += go[c][1];
-                continue;
-            }
-            const T vm_ = ch[AXIS][q], vp_ = ch[AXIS][q + 2];
-            const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
-            const T dv = take_p ? vp_ : vm_;
-            const T t = dt * dv;
-            T gdv = T(0);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const T g_o = go[c][q];
-                const T g0 = ch[c][q + 1];
-                if (dv >= T(0)) {
-                    if (q == 1) acc[c] += g_o * (T(1) - t);
-                    if (q == 2) acc[c] += g_o * t;
-                    gdv -= g_o * dt * (g0 - ch[c][q]);
-                } else {
-                    if (q == 1) acc[c] += g_o * (T(1) + t);
-                    if (q == 0) acc[c] -= g_o * t;
-                    gdv -= g_o * dt * (ch[c][q + 2] - g0);
-                }
-            }
-            if ((take_p ? q + 2 : q) == 2) acc[AXIS] += gdv;
-        }
-    } else
-    for (int i = max(j - 1, 0); i <= min(j + 1, n - 1); ++i) {
-        const size_t ki = at(i);
-        const bool in = line_in && i >= border && i < n - border;
-        if (!in) {
-            if (i == j)
-                for (int c = 0; c < NC; ++c) acc[c] += gchan(ki, c);
-            continue;
-        }
-        const int im = max(i - 1, 0), ip = min(i + 1, n - 1);
-        const size_t km = at(im), kp = at(ip);
-        const T vm_ = f[2 * km + AXIS], vp_ = f[2 * kp + AXIS];
-        const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
-        const T dv = take_p ? vp_ : vm_;
-        const T t = dt * dv;
-        T gdv = T(0);
-        for (int c = 0; c < NC; ++c) {
-            const T go = gchan(ki, c);
-            const T g0 = chan(ki, c);
-            if (dv >= T(0)) {
-                const T gm = chan(km, c);
-                if (i == j) acc[c] += go * (T(1) - t);
-                if (im == j) acc[c] += go * t;
-                gdv -= go * dt * (g0 - gm);
-            } else {
-                const T gp = chan(kp, c);
-                if (i == j) acc[c] += go * (T(1) + t);
-                if (ip == j) acc[c] -= go * t;
-                gdv -= go * dt * (gp - g0);
-            }
-        }
-        // the dominant velocity is the chosen neighbour's AXIS component
-        if ((take_p ? ip : im) == j) acc[AXIS] += gdv;
-    }
-    const size_t kj = at(j);
+    prop_adj_at<T, AXIS, PAYLOAD>(
+        AXIS == 0 ? x : y, AXIS == 0 ? W : H, line_in, border, dt,
+        [&](int p, T(&o)[NC]) { field_px<T, PAYLOAD>(f, s, v, at(p), o); },
+        [&](int p, T(&o)[NC]) { field_px<T, PAYLOAD>(gfo, gso, gvo, at(p), o); }, acc);
+    const size_t kj = at(AXIS == 0 ? x : y);
     put<ACC>(gf[2 * kj], acc[0]);
     put<ACC>(gf[2 * kj + 1], acc[1]);
     if constexpr (PAYLOAD) {
@@ -675,6 +678,397 @@ __global__ void smooth_bwd_k(const T* __restrict__ w5, const T* __restrict__ in,
     block_sum<T, 5>(gw, PART ? gw5 + 5 * block_linear() : gw5, !PART);
 }
 
+// Adjoint of one smoothing iteration (X pass, then Y pass) of a 32 x 32 tile in one block of
+// the frame driver.  Every input the tile needs is staged in shared memory first, in one
+// batch of independent loads: the output gradient on the tile and two halo rows and columns,
+// the Y pass's input (the tape) on the tile's columns and the halo rows, the X pass's input
+// on the tile's rows and the halo columns (both at clamped coordinates).  Then the Y adjoint
+// on the tile's rows and the halo columns (shared), and the X adjoint from it into gin
+// (stored, or added when ACC).  The weight gradients of both passes are summed over the
+// tile's own pixels (each pass's output gradient times its clamped input taps) and stored as
+// 5 sums at part[5 * block].  Gradient halo entries outside the image are never read: the
+// gathers visit only the outputs inside the image.
+constexpr int kST = 32;
+constexpr int kSW = kST + 4;
+inline dim3 grid_tile32(int w, int h, int B) { return dim3((w + kST - 1) / kST, (h + kST - 1) / kST, B); }
+template <typename T>
+constexpr size_t smooth_iter_smem() {
+    return sizeof(typename Pair<T>::V) * (size_t)(kSW * kSW + 3 * kST * kSW);
+}
+template <typename T, bool ACC>
+__global__ void __launch_bounds__(256) smooth_iter_bwd_k(const T* __restrict__ w5, const T* __restrict__ xin,
+                                                         const T* __restrict__ xmid, const T* __restrict__ gout,
+                                                         T* __restrict__ gin, T* __restrict__ part, int H, int W) {
+    grid_dep_wait();
+    using V = typename Pair<T>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V(*sg)[kSW] = reinterpret_cast<V(*)[kSW]>(smem_raw);          // gout: rows y0-2.., cols x0-2..
+    V(*sym)[kST] = reinterpret_cast<V(*)[kST]>(sg + kSW);        // xmid: rows y0-2.., cols x0..
+    V(*sxi)[kSW] = reinterpret_cast<V(*)[kSW]>(sym + kSW);       // xin: rows y0.., cols x0-2..
+    V(*sm)[kSW] = sxi + kST;                                      // gradient of the X pass output
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int x0 = blockIdx.x * kST, y0 = blockIdx.y * kST;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    const V* go = reinterpret_cast<const V*>(gout) + base;
+    const V* xi = reinterpret_cast<const V*>(xin) + base;
+    const V* xm = reinterpret_cast<const V*>(xmid) + base;
+    V* gi = reinterpret_cast<V*>(gin) + base;
+    T w[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) w[k] = w5[k];
+    {
+        constexpr int NG = (kSW * kSW + 255) / 256, NT = (kST * kSW + 255) / 256;
+        V a[NG], bm[NT], bi[NT];
+#pragma unroll
+        for (int u = 0; u < NG; ++u) {
+            const int e = tid + 256 * u, r = e / kSW, c = e - r * kSW;
+            const int y = y0 - 2 + r, x = x0 - 2 + c;
+            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) a[u] = go[(size_t)y * W + x];
+        }
+#pragma unroll
+        for (int u = 0; u < NT; ++u) {
+            const int e = tid + 256 * u;
+            const int rm = e / kST, cm = e - rm * kST;   // xmid: kSW rows x kST columns
+            const int rx = e / kSW, cx = e - rx * kSW;   // xin: kST rows x kSW columns
+            if (e < kST * kSW) {
+                const int ym = clampi(y0 - 2 + rm, 0, H - 1), xm_ = x0 + cm;
+                if (xm_ < W) bm[u] = xm[(size_t)ym * W + xm_];
+                const int yx = y0 + rx, xx = clampi(x0 - 2 + cx, 0, W - 1);
+                if (yx < H) bi[u] = xi[(size_t)yx * W + xx];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NG; ++u) {
+            const int e = tid + 256 * u, r = e / kSW, c = e - r * kSW;
+            const int y = y0 - 2 + r, x = x0 - 2 + c;
+            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) sg[r][c] = a[u];
+        }
+#pragma unroll
+        for (int u = 0; u < NT; ++u) {
+            const int e = tid + 256 * u;
+            const int rm = e / kST, cm = e - rm * kST, rx = e / kSW, cx = e - rx * kSW;
+            if (e < kST * kSW) {
+                if (x0 + cm < W) sym[rm][cm] = bm[u];
+                if (y0 + rx < H) sxi[rx][cx] = bi[u];
+            }
+        }
+    }
+    __syncthreads();
+    T gw[5] = {T(0), T(0), T(0), T(0), T(0)};
+    for (int e = tid; e < kST * kSW; e += 256) {
+        const int r = e / kSW, c = e - r * kSW;
+        const int y = y0 + r, x = x0 - 2 + c;
+        if (y >= H || x < 0 || x >= W) continue;
+        T ax = T(0), ay = T(0);
+        if (y >= 2 && y + 2 <= H - 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const V v = sg[r + q][c];
+                ax += w[4 - q] * v.x;
+                ay += w[4 - q] * v.y;
+            }
+        } else {
+            for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i) {
+                const T wt = tap_weight(w, i, y, H);
+                const V v = sg[i - y0 + 2][c];
+                ax += wt * v.x;
+                ay += wt * v.y;
+            }
+        }
+        V m;
+        m.x = ax;
+        m.y = ay;
+        sm[r][c] = m;
+        if (c >= 2 && c < kST + 2) {  // the Y pass's output (y, x) is this tile's pixel
+            const V g = sg[r + 2][c];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const V iv = sym[r + k][c - 2];  // row clamp(y + k - 2)
+                gw[k] += g.x * iv.x + g.y * iv.y;
+            }
+        }
+    }
+    __syncthreads();
+    grid_dep_launch();  // the next kernel's blocks may now take this block's place
+    for (int e = tid; e < kST * kST; e += 256) {
+        const int r = e / kST, c = e - r * kST;
+        const int y = y0 + r, x = x0 + c;
+        if (y >= H || x >= W) continue;
+        T ax = T(0), ay = T(0);
+        if (x >= 2 && x + 2 <= W - 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const V v = sm[r][c + q];
+                ax += w[4 - q] * v.x;
+                ay += w[4 - q] * v.y;
+            }
+        } else {
+            for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) {
+                const T wt = tap_weight(w, i, x, W);
+                const V v = sm[r][i - x0 + 2];
+                ax += wt * v.x;
+                ay += wt * v.y;
+            }
+        }
+        const size_t k = (size_t)y * W + x;
+        V o;
+        if constexpr (ACC) {
+            o = gi[k];
+            o.x += ax;
+            o.y += ay;
+        } else {
+            o.x = ax;
+            o.y = ay;
+        }
+        gi[k] = o;
+        const V g = sm[r][c + 2];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const V iv = sxi[r][c + q];  // column clamp(x + q - 2)
+            gw[q] += g.x * iv.x + g.y * iv.y;
+        }
+    }
+    block_sum<T, 5>(gw, part + 5 * block_linear(), false);
+}
+
+// asynchronous global -> shared copy of N bytes (4, 8 or 16; both addresses N-aligned)
+template <int N>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Adjoint of one propagation iteration (X sub-step, then Y sub-step) of a 32 x 32 tile in one
+// block of the frame driver.  Staged in shared memory in one batch of asynchronous copies:
+// the gradient of the Y sub-step's output on the tile and one halo row and column, the Y
+// sub-step's input on the tile's columns plus one and the rows plus two each side, the X
+// sub-step's input on the tile's rows and the columns plus two each side (the tape, or the
+// state before the first sub-step).  Then the Y adjoint on the tile's rows and the halo
+// columns (shared), and the X adjoint from it into the X sub-step's input gradient (stored,
+// or added when ACC).  Entries outside the image are never read.
+constexpr int kPG = kST + 2;
+constexpr int kPropThreads = 512;  // 32 x 16
+template <typename T, bool PAYLOAD>
+struct PropTile {
+    using V = typename Pair<T>::V;
+    static constexpr int NC = PAYLOAD ? 5 : 2;
+    // pixel fields of a staged region: f pairs [, s, v pairs]
+    template <int R, int C>
+    struct Field {
+        V f[R][C];
+        T s[PAYLOAD ? R : 1][PAYLOAD ? C : 1];
+        V v[PAYLOAD ? R : 1][PAYLOAD ? C : 1];
+    };
+    Field<kPG, kPG> go;      // output gradient: rows y0-1.., cols x0-1..
+    Field<kST + 4, kPG> ty;  // Y sub-step input: rows y0-2.., cols x0-1..
+    Field<kST, kST + 4> tx;  // X sub-step input: rows y0.., cols x0-2..
+    T mid[NC][kST][kPG];     // gradient of the X sub-step's output: rows y0.., cols x0-1..
+};
+
+// copy pixel k of a field into slot (r, c) of a staged region
+template <typename T, bool PAYLOAD, typename F>
+__device__ __forceinline__ void stage_px(F& dst, int r, int c, const T* f, const T* s, const T* v, size_t k) {
+    constexpr int P = 2 * sizeof(T);
+    cp_async<P>(&dst.f[r][c], f + 2 * k);
+    if constexpr (PAYLOAD) {
+        cp_async<sizeof(T)>(&dst.s[r][c], s + k);
+        cp_async<P>(&dst.v[r][c], v + 2 * k);
+    }
+}
+template <typename T, bool PAYLOAD, typename F>
+__device__ __forceinline__ void read_px(const F& src, int r, int c, T (&o)[PAYLOAD ? 5 : 2]) {
+    o[0] = src.f[r][c].x;
+    o[1] = src.f[r][c].y;
+    if constexpr (PAYLOAD) {
+        o[2] = src.s[r][c];
+        o[3] = src.v[r][c].x;
+        o[4] = src.v[r][c].y;
+    }
+}
+
+template <typename T, bool PAYLOAD, bool ACC>
+__global__ void __launch_bounds__(kPropThreads) prop_iter_bwd_k(const T* __restrict__ xf, const T* __restrict__ xs,
+                                                                const T* __restrict__ xv, const T* __restrict__ yf,
+                                                                const T* __restrict__ ys, const T* __restrict__ yv,
+                                                                const T* __restrict__ gfo, const T* __restrict__ gso,
+                                                                const T* __restrict__ gvo, T* __restrict__ gf,
+                                                                T* __restrict__ gs, T* __restrict__ gv, int H, int W,
+                                                                T dt, int border) {
+    grid_dep_wait();
+    using Tile = PropTile<T, PAYLOAD>;
+    constexpr int NC = Tile::NC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Tile& S = *reinterpret_cast<Tile*>(smem_raw);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int x0 = blockIdx.x * kST, y0 = blockIdx.y * kST;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    for (int e = tid; e < kPG * kPG; e += kPropThreads) {
+        const int r = e / kPG, c = e - r * kPG, y = y0 - 1 + r, x = x0 - 1 + c;
+        if (y >= 0 && y < H && x >= 0 && x < W)
+            stage_px<T, PAYLOAD>(S.go, r, c, gfo, gso, gvo, base + (size_t)y * W + x);
+    }
+    for (int e = tid; e < (kST + 4) * kPG; e += kPropThreads) {
+        const int r = e / kPG, c = e - r * kPG, y = y0 - 2 + r, x = x0 - 1 + c;
+        if (y >= 0 && y < H && x >= 0 && x < W) stage_px<T, PAYLOAD>(S.ty, r, c, yf, ys, yv, base + (size_t)y * W + x);
+    }
+    for (int e = tid; e < kST * (kST + 4); e += kPropThreads) {
+        const int r = e / (kST + 4), c = e - r * (kST + 4), y = y0 + r, x = x0 - 2 + c;
+        if (y < H && x >= 0 && x < W) stage_px<T, PAYLOAD>(S.tx, r, c, xf, xs, xv, base + (size_t)y * W + x);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // Y adjoint at rows y0.., columns x0-1..
+    for (int e = tid; e < kST * kPG; e += kPropThreads) {
+        const int r = e / kPG, c = e - r * kPG;
+        const int y = y0 + r, x = x0 - 1 + c;
+        if (y >= H || x < 0 || x >= W) continue;
+        T acc[NC];
+        prop_adj_at<T, 1, PAYLOAD>(
+            y, H, x >= border && x < W - border, border, dt,
+            [&](int p, T(&o)[NC]) { read_px<T, PAYLOAD>(S.ty, p - y0 + 2, c, o); },
+            [&](int p, T(&o)[NC]) { read_px<T, PAYLOAD>(S.go, p - y0 + 1, c, o); }, acc);
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) S.mid[ch][r][c] = acc[ch];
+    }
+    __syncthreads();
+    grid_dep_launch();  // the next kernel's blocks may now take this block's place
+    // X adjoint at the tile's pixels
+    for (int e = tid; e < kST * kST; e += kPropThreads) {
+        const int r = e / kST, c = e - r * kST;
+        const int y = y0 + r, x = x0 + c;
+        if (y >= H || x >= W) continue;
+        T acc[NC];
+        prop_adj_at<T, 0, PAYLOAD>(
+            x, W, y >= border && y < H - border, border, dt,
+            [&](int p, T(&o)[NC]) { read_px<T, PAYLOAD>(S.tx, r, p - x0 + 2, o); },
+            [&](int p, T(&o)[NC]) {
+#pragma unroll
+                for (int ch = 0; ch < NC; ++ch) o[ch] = S.mid[ch][r][p - x0 + 1];
+            },
+            acc);
+        const size_t k = base + (size_t)y * W + x;
+        put<ACC>(gf[2 * k], acc[0]);
+        put<ACC>(gf[2 * k + 1], acc[1]);
+        if constexpr (PAYLOAD) {
+            put<ACC>(gs[k], acc[2]);
+            put<ACC>(gv[2 * k], acc[3]);
+            put<ACC>(gv[2 * k + 1], acc[4]);
+        }
+    }
+}
+
+// The image model's adjoint (model_bwd1_k then model_bwd2_k) of a 32 x 32 tile in one block
+// of the frame driver: the gradients of a0 and of the image gradient on the tile and two halo
+// rows and columns staged in shared memory in one batch of loads; the gradients of the Y
+// blur (rows y0-2.., the tile's columns) and of the X blur (the tile's rows, columns x0-2..)
+// in shared memory; the image gradient from them, stored (or added when ACC).
+template <typename T>
+constexpr size_t model_tile_smem() {
+    return sizeof(T) * (size_t)(kSW * kSW + 2 * kSW * kSW + 2 * kST * kSW);
+}
+template <typename T, bool ACC>
+__global__ void __launch_bounds__(256) model_tile_bwd_k(const T* __restrict__ ga0, const T* __restrict__ ggrad,
+                                                        T* __restrict__ gimg, int H, int W) {
+    grid_dep_wait();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*sa)[kSW] = reinterpret_cast<T(*)[kSW]>(smem_raw);         // ga0: rows y0-2.., cols x0-2..
+    T(*sgx)[kSW] = sa + kSW;                                      // ggrad x: same
+    T(*sgy)[kSW] = sgx + kSW;                                     // ggrad y: same
+    T(*sby)[kST] = reinterpret_cast<T(*)[kST]>(sgy + kSW);       // gby: rows y0-2.., cols x0..
+    T(*sbx)[kSW] = reinterpret_cast<T(*)[kSW]>(sby + kSW);       // gbx: rows y0.., cols x0-2..
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int x0 = blockIdx.x * kST, y0 = blockIdx.y * kST;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    const T* a0g = ga0 + base;
+    const typename Pair<T>::V* gg = reinterpret_cast<const typename Pair<T>::V*>(ggrad) + base;
+    const Masks<T> M;
+    {
+        constexpr int NG = (kSW * kSW + 255) / 256;
+        T va[NG];
+        typename Pair<T>::V vg[NG];
+#pragma unroll
+        for (int u = 0; u < NG; ++u) {
+            const int e = tid + 256 * u, r = e / kSW, c = e - r * kSW;
+            const int y = y0 - 2 + r, x = x0 - 2 + c;
+            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) {
+                const size_t k = (size_t)y * W + x;
+                va[u] = a0g[k];
+                vg[u] = gg[k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NG; ++u) {
+            const int e = tid + 256 * u, r = e / kSW, c = e - r * kSW;
+            const int y = y0 - 2 + r, x = x0 - 2 + c;
+            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) {
+                sa[r][c] = va[u];
+                sgx[r][c] = vg[u].x;
+                sgy[r][c] = vg[u].y;
+            }
+        }
+    }
+    __syncthreads();
+    // gby at rows y0-2.. (X gathers of a0 and the x gradient), gbx at columns x0-2.. (Y gather
+    // of the y gradient)
+    for (int e = tid; e < kSW * kST; e += 256) {
+        {
+            const int r = e / kST, c = e - r * kST;
+            const int y = y0 - 2 + r, x = x0 + c;
+            if (y >= 0 && y < H && x < W) {
+                T acc = T(0);
+                if (x >= 2 && x + 2 <= W - 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) acc += M.s[4 - q] * sa[r][c + q] + M.d[4 - q] * sgx[r][c + q];
+                } else {
+                    for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i)
+                        acc += tap_weight(M.s, i, x, W) * sa[r][i - x0 + 2] + tap_weight(M.d, i, x, W) * sgx[r][i - x0 + 2];
+                }
+                sby[r][c] = acc;
+            }
+        }
+        {
+            const int r = e / kSW, c = e - r * kSW;
+            const int y = y0 + r, x = x0 - 2 + c;
+            if (y < H && x >= 0 && x < W) {
+                T acc = T(0);
+                if (y >= 2 && y + 2 <= H - 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) acc += M.d[4 - q] * sgy[r + q][c];
+                } else {
+                    for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i)
+                        acc += tap_weight(M.d, i, y, H) * sgy[i - y0 + 2][c];
+                }
+                sbx[r][c] = acc;
+            }
+        }
+    }
+    __syncthreads();
+    grid_dep_launch();  // the next kernel's blocks may now take this block's place
+    T* gi = gimg + base;
+    for (int e = tid; e < kST * kST; e += 256) {
+        const int r = e / kST, c = e - r * kST;
+        const int y = y0 + r, x = x0 + c;
+        if (y >= H || x >= W) continue;
+        T acc = T(0);
+        if (y >= 2 && y + 2 <= H - 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) acc += M.s[4 - q] * sby[r + q][c];
+        } else {
+            for (int i = max(y - 2, 0); i <= min(y + 2, H - 1); ++i) acc += tap_weight(M.s, i, y, H) * sby[i - y0 + 2][c];
+        }
+        if (x >= 2 && x + 2 <= W - 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) acc += M.s[4 - q] * sbx[r][c + q];
+        } else {
+            for (int i = max(x - 2, 0); i <= min(x + 2, W - 1); ++i) acc += tap_weight(M.s, i, x, W) * sbx[r][i - x0 + 2];
+        }
+        put<ACC>(gi[(size_t)y * W + x], acc);
+    }
+}
+
 // Store-mode update adjoints of the frame driver: every per-pixel gradient is stored (the
 // destinations start undefined), the gradient of a0 as a state output (ga0_out, nullable)
 // is folded in, `first` (old image == a0) cancels the yt path, gold is added (a caller's
@@ -790,6 +1184,37 @@ __global__ void reduce_parts_k(const T* __restrict__ part, int n, T* dst) {
     block_sum<T, NV>(acc, tot, false);
     __syncthreads();
     if (threadIdx.x < NV) dst[threadIdx.x] += tot[threadIdx.x];
+}
+
+// The per-block partial sums of one frame's backward, reduced in one launch: block j adds
+// the sum of its segment (n[j] rows of nv[j] values) to dst[j] (fixed order: deterministic)
+template <typename T>
+struct ReduceJobs {
+    static constexpr int kMax = 2 * FF_DIFF_MAX_LEVELS;
+    const T* part[kMax];
+    T* dst[kMax];
+    int n[kMax], nv[kMax];
+    int count = 0;
+};
+template <typename T>
+__global__ void __launch_bounds__(1024) reduce_jobs_k(ReduceJobs<T> J) {
+    grid_dep_wait();
+    grid_dep_launch();
+    const int j = blockIdx.x;
+    const T* part = J.part[j];
+    const int n = J.n[j], nv = J.nv[j];
+    T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
+    if (nv == 5) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) acc[v] += part[(size_t)i * 5 + v];
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] += part[i];
+    }
+    __shared__ T tot[5];
+    block_sum<T, 5>(acc, tot, false);
+    __syncthreads();
+    if ((int)threadIdx.x < nv) J.dst[j][threadIdx.x] += tot[threadIdx.x];
 }
 
 // dst += src over n elements
@@ -1169,10 +1594,19 @@ inline size_t blocks_of(const Geo& g, int l) {
     return (size_t)d.x * d.y * d.z;
 }
 
+// blocks of the fused smoothing adjoint at level l
+inline size_t tiles32_of(const Geo& g, int l) {
+    const dim3 d = grid_tile32(g.W[l], g.H[l], g.B);
+    return (size_t)d.x * d.y * d.z;
+}
+
 // backward scratch (elements of T)
 struct Scratch {
     size_t gimg[FF_DIFF_MAX_LEVELS] = {};  // image gradients of levels >= 1
-    size_t ga0, gg, gfu, gby, gbx, pa, pb, sa, sb, zero, part;
+    // per-block partial sums: weight gradients (S iterations x tiles x 5) and gamma gradient
+    // (update blocks x 1) of each level, reduced together at the end of the frame
+    size_t part_w[FF_DIFF_MAX_LEVELS] = {}, part_g[FF_DIFF_MAX_LEVELS] = {};
+    size_t ga0, gg, gfu, pa, pb, sa, sb, zero;
     size_t total = 0;
     Scratch(const Geo& g) {
         auto take = [&](size_t n) {
@@ -1180,24 +1614,22 @@ struct Scratch {
             total += (n + 31) / 32 * 32;
             return at;
         };
-        size_t n1m = 0, nparts = 0;
+        size_t n1m = 0;
         for (int l = 0; l < g.L; ++l) {
             if (l > 0) gimg[l] = take(g.n1(l));
             n1m = std::max(n1m, g.n1(l));
-            nparts = std::max(nparts, (size_t)std::max(2 * g.S[l], 1) * blocks_of(g, l) * 5);
+            part_w[l] = take((size_t)std::max(g.S[l], 1) * tiles32_of(g, l) * 5);
+            part_g[l] = take(blocks_of(g, l));
         }
         const size_t n2m = 2 * n1m, st = n2m + n1m + n2m;
         ga0 = take(n1m);
         gg = take(n2m);
         gfu = take(2 * g.n1(g.L - 1));
-        gby = take(n1m);
-        gbx = take(n1m);
         pa = take(st);
         pb = take(st);
         sa = take(n2m);
         sb = take(n2m);
         zero = take(n2m);  // zeros standing in for absent output gradients
-        part = take(nparts);  // per-block partial sums of the gamma and weight gradients
     }
 };
 
@@ -1217,9 +1649,8 @@ struct Driver {
     void add(T* dst, const T* src, size_t n) const {
         ok(launch_k(add_k<T>, dim3((unsigned)std::min<size_t>((n + 255) / 256, 4096)), dim3(256), 0, s, dst, src, n));
     }
-    void reduce(const T* part, size_t n, int nv, T* dst) const {
-        ok(nv == 5 ? launch_k(reduce_parts_k<T, 5>, dim3(1), dim3(1024), 0, s, part, (int)n, dst)
-                   : launch_k(reduce_parts_k<T, 1>, dim3(1), dim3(1024), 0, s, part, (int)n, dst));
+    void reduce(const ReduceJobs<T>& jobs) const {
+        if (jobs.count > 0) ok(launch_k(reduce_jobs_k<T>, dim3(jobs.count), dim3(1024), 0, s, jobs));
     }
     void prop(int l, int axis, bool payload, const T* f, const T* sc, const T* v, T* fo, T* so, T* vo) const {
         const T dt = (T)(1.0 / g.N[l]);
@@ -1234,43 +1665,68 @@ struct Driver {
         }
         ok(e);
     }
-    template <bool PAYLOAD, bool ACC>
-    void prop_bwd(int l, int axis, const T* f, const T* sc, const T* v, const T* gfo, const T* gso, const T* gvo, T* gf,
-                  T* gs, T* gv) const {
-        const T dt = (T)(1.0 / g.N[l]);
-        const int H = g.H[l], W = g.W[l], b = g.border;
-        ok(axis == 0 ? launch_k(prop_bwd_k<T, 0, PAYLOAD, ACC>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
-                                gv, H, W, dt, b)
-                     : launch_k(prop_bwd_k<T, 1, PAYLOAD, ACC>, grid(l), kBlock, 0, s, f, sc, v, gfo, gso, gvo, gf, gs,
-                                gv, H, W, dt, b));
-    }
     void smooth(int l, int axis, const T* w5, const T* in, T* out) const {
         ok(axis == 0 ? launch_k(smooth_fwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l])
                      : launch_k(smooth_fwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l]));
     }
-    // one smoothing pass's adjoint: input gradient stored (or added), weight sums per block
-    void smooth_bwd(int l, int axis, bool acc, const T* w5, const T* in, const T* go, T* gi, T* part) const {
-        const dim3 gr = grid_smooth(g.W[l], g.H[l], g.B);
+    // one propagation iteration's adjoint (X and Y sub-step): X input x*, Y input y*, output
+    // gradient g*o, X input gradient g* (stored, or added when ACC)
+    template <bool PAYLOAD, bool ACC>
+    void prop_iter_bwd(int l, const T* xf, const T* xs, const T* xv, const T* yf, const T* ys, const T* yv,
+                       const T* gfo, const T* gso, const T* gvo, T* gf, T* gs, T* gv) const {
+        constexpr size_t smem = sizeof(PropTile<T, PAYLOAD>);
+        static bool prepared[64] = {};  // the dynamic shared-memory limit, set once per device
+        int dev = 0;
+        ok(cudaGetDevice(&dev));
+        if (!prepared[dev & 63]) {
+            ok(cudaFuncSetAttribute(prop_iter_bwd_k<T, PAYLOAD, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+            prepared[dev & 63] = true;
+        }
+        const T dt = (T)(1.0 / g.N[l]);
+        ok(launch_k(prop_iter_bwd_k<T, PAYLOAD, ACC>, grid_tile32(g.W[l], g.H[l], g.B), dim3(32, kPropThreads / 32),
+                    smem, s, xf, xs, xv,
+                    yf, ys, yv, gfo, gso, gvo, gf, gs, gv, g.H[l], g.W[l], dt, g.border));
+    }
+    // one smoothing iteration's adjoint (X and Y pass): input gradient stored (or added),
+    // weight sums per block
+    void smooth_iter_bwd(int l, bool acc, const T* w5, const T* xin, const T* xmid, const T* go, T* gi,
+                         T* part) const {
+        const dim3 gr = grid_tile32(g.W[l], g.H[l], g.B);
         const int H = g.H[l], W = g.W[l];
-        cudaError_t e;
-        if (acc)
-            e = axis == 0 ? launch_k(smooth_bwd_k<T, 0, true, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W)
-                          : launch_k(smooth_bwd_k<T, 1, true, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W);
-        else
-            e = axis == 0 ? launch_k(smooth_bwd_k<T, 0, false, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W)
-                          : launch_k(smooth_bwd_k<T, 1, false, true>, gr, kBlock, 0, s, w5, in, go, gi, part, H, W);
-        ok(e);
+        constexpr size_t smem = smooth_iter_smem<T>();
+        static bool prepared[64][2] = {};  // the dynamic shared-memory limit, set once per device
+        int dev = 0;
+        ok(cudaGetDevice(&dev));
+        if (!prepared[dev & 63][acc]) {
+            ok(acc ? cudaFuncSetAttribute(smooth_iter_bwd_k<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem)
+                   : cudaFuncSetAttribute(smooth_iter_bwd_k<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            prepared[dev & 63][acc] = true;
+        }
+        ok(acc ? launch_k(smooth_iter_bwd_k<T, true>, gr, kBlock, smem, s, w5, xin, xmid, go, gi, part, H, W)
+               : launch_k(smooth_iter_bwd_k<T, false>, gr, kBlock, smem, s, w5, xin, xmid, go, gi, part, H, W));
     }
     void model(int l, const T* img, T* a0, T* grad) const {
         ok(launch_k(model_fwd_k<T>, grid(l), kBlock, 0, s, img, a0, grad, g.H[l], g.W[l]));
     }
     // image gradient of the image model: stored into gimg, or added when acc
-    void model_bwd(int l, bool acc, const T* ga0, const T* ggrad, T* gby, T* gbx, T* gimg) const {
-        ok(launch_k(model_bwd1_k<T>, grid(l), kBlock, 0, s, ga0, ggrad, gby, gbx, g.H[l], g.W[l]));
-        ok(acc ? launch_k(model_bwd2_k<T, true>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l],
-                          g.W[l])
-               : launch_k(model_bwd2_k<T, false>, grid(l), kBlock, 0, s, (const T*)gby, (const T*)gbx, gimg, g.H[l],
-                          g.W[l]));
+    void model_bwd(int l, bool acc, const T* ga0, const T* ggrad, T* gimg) const {
+        constexpr size_t smem = model_tile_smem<T>();
+        static bool prepared[64][2] = {};  // the dynamic shared-memory limit, set once per device
+        int dev = 0;
+        ok(cudaGetDevice(&dev));
+        if (!prepared[dev & 63][acc]) {
+            ok(acc ? cudaFuncSetAttribute(model_tile_bwd_k<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem)
+                   : cudaFuncSetAttribute(model_tile_bwd_k<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            prepared[dev & 63][acc] = true;
+        }
+        const dim3 gr = grid_tile32(g.W[l], g.H[l], g.B);
+        ok(acc ? launch_k(model_tile_bwd_k<T, true>, gr, kBlock, smem, s, ga0, ggrad, gimg, g.H[l], g.W[l])
+               : launch_k(model_tile_bwd_k<T, false>, gr, kBlock, smem, s, ga0, ggrad, gimg, g.H[l], g.W[l]));
     }
 
     // ---- forward
@@ -1354,8 +1810,17 @@ struct Driver {
         T* gfu = sc_ + S_.gfu;
         if (gfu_out) copy(gfu, gfu_out, 2 * g.n1(top));
         else zero(gfu, 2 * g.n1(top));
-        T *ga0 = sc_ + S_.ga0, *ggr = sc_ + S_.gg, *gby = sc_ + S_.gby, *gbx = sc_ + S_.gbx;
-        T *pa = sc_ + S_.pa, *pb = sc_ + S_.pb, *sa = sc_ + S_.sa, *sb = sc_ + S_.sb, *part = sc_ + S_.part;
+        T *ga0 = sc_ + S_.ga0, *ggr = sc_ + S_.gg;
+        T *pa = sc_ + S_.pa, *pb = sc_ + S_.pb, *sa = sc_ + S_.sa, *sb = sc_ + S_.sb;
+        // the partial sums of the weight and gamma gradients, reduced in one launch at the end
+        ReduceJobs<T> jobs;
+        auto jobs_add = [&](const T* part, int n, int nv, T* dst) {
+            jobs.part[jobs.count] = part;
+            jobs.n[jobs.count] = n;
+            jobs.nv[jobs.count] = nv;
+            jobs.dst[jobs.count] = dst;
+            ++jobs.count;
+        };
 
         // adjoint of the 2S smoothing passes of level l, from the gradient of the smoothed
         // flow; the gradient of the pass-0 input goes to dst (added if acc) and is returned.
@@ -1368,15 +1833,18 @@ struct Driver {
                 add(dst, gcur, 2 * g.n1(l));
                 return dst;
             }
-            const dim3 sg = grid_smooth(g.W[l], g.H[l], g.B);
-            const size_t nb = (size_t)sg.x * sg.y * sg.z;
+            // iteration i reads the tape's pass inputs sm[2i] (X) and sm[2i+1] (Y); iteration
+            // i > 0 writes bufs[i % 2], iteration 1 writes sb, so dst may be sa
+            const size_t nb = tiles32_of(g, l);
+            T* part = sc_ + S_.part_w[l];
             T* bufs[2] = {sa, sb};
-            for (int j = n - 1; j >= 0; --j) {
-                T* o = j == 0 ? dst : bufs[j % 2];
-                smooth_bwd(l, j % 2, j == 0 && acc, weights + 5 * l, tp + tape.sm[l][j], gcur, o, part + j * nb * 5);
+            for (int i = g.S[l] - 1; i >= 0; --i) {
+                T* o = i == 0 ? dst : bufs[i % 2];
+                smooth_iter_bwd(l, i == 0 && acc, weights + 5 * l, tp + tape.sm[l][2 * i], tp + tape.sm[l][2 * i + 1],
+                                gcur, o, part + i * nb * 5);
                 gcur = o;
             }
-            reduce(part, n * nb, 5, gweights + 5 * l);
+            jobs_add(part, (int)(g.S[l] * nb), 5, gweights + 5 * l);
             return gcur;
         };
 
@@ -1396,33 +1864,31 @@ struct Driver {
             T* gsh = pa + n2;
             T* gvh = pa + n2 + n1;
             T* gco = l == L - 2 ? gfu : gin[3 * (l + 1)];
-            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 0, part};
+            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 0, sc_ + S_.part_g[l]};
             ok(launch_k(dupdate_bwd_frame_k<T>, grid(l), kBlock, 0, s, a0, grad, old, vh, coarse, gamma + l, gflow,
                         gz(gout[3 * l + 2]), ga0, ggr, gsh, gvh, gco, fa, g.H[l], g.W[l], g.H[l + 1], g.W[l + 1],
                         (T)g.maxflow[l]));
-            reduce(part, blocks_of(g, l), 1, ggamma + l);
+            jobs_add(sc_ + S_.part_g[l], (int)blocks_of(g, l), 1, ggamma + l);
+            // iterations N-1 .. 0: the Y sub-step 2i+1 reads tape entry 2i, the X sub-step 2i
+            // reads entry 2i-1 (the input state for i = 0, whose gradient goes to the caller's)
             const T *cf = zbuf, *cs = gsh, *cv = gvh;
             T* bufs[2] = {pb, pa};
-            for (int k = last; k >= 0; --k) {
-                const T *f, *sc, *v;
-                if (k == 0) {
-                    f = in[3 * l];
-                    sc = in[3 * l + 1];
-                    v = in[3 * l + 2];
-                    prop_bwd<true, true>(l, 0, f, sc, v, cf, cs, cv, gin[3 * l], gin[3 * l + 1], gin[3 * l + 2]);
+            for (int i = g.N[l] - 1; i >= 0; --i) {
+                const T* yb = tp + tape.prop[l][2 * i];
+                if (i == 0) {
+                    prop_iter_bwd<true, true>(l, in[3 * l], in[3 * l + 1], in[3 * l + 2], yb, yb + n2, yb + n2 + n1, cf,
+                                              cs, cv, gin[3 * l], gin[3 * l + 1], gin[3 * l + 2]);
                     break;
                 }
-                const T* b = tp + tape.prop[l][k - 1];
-                f = b;
-                sc = b + n2;
-                v = b + n2 + n1;
-                T* o = bufs[(last - k) % 2];
-                prop_bwd<true, false>(l, k % 2, f, sc, v, cf, cs, cv, o, o + n2, o + n2 + n1);
+                const T* xb = tp + tape.prop[l][2 * i - 1];
+                T* o = bufs[(g.N[l] - 1 - i) % 2];
+                prop_iter_bwd<true, false>(l, xb, xb + n2, xb + n2 + n1, yb, yb + n2, yb + n2 + n1, cf, cs, cv, o,
+                                           o + n2, o + n2 + n1);
                 cf = o;
                 cs = o + n2;
                 cv = o + n2 + n1;
             }
-            model_bwd(l, l == 0, ga0, ggr, gby, gbx, gimg[l]);
+            model_bwd(l, l == 0, ga0, ggr, gimg[l]);
         }
         {
             const int l = top;
@@ -1434,30 +1900,32 @@ struct Driver {
             const T* old = first ? a0 : in[3 * l + 1];
             smooth_back(l, gout[3 * l], gfu, true);
             T* gh = pa;
-            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 1, part};
+            const FrameAdj<T> fa{gout[3 * l + 1], first ? 1 : 0, 1, sc_ + S_.part_g[l]};
             ok(launch_k(update_bwd_frame_k<T>, grid(l), kBlock, 0, s, a0, grad, old, fh, gamma + l, (const T*)gfu, ga0,
                         ggr, gin[3 * l + 1], gh, fa, g.H[l], g.W[l], (T)g.maxflow[l]));
-            reduce(part, blocks_of(g, l), 1, ggamma + l);
+            jobs_add(sc_ + S_.part_g[l], (int)blocks_of(g, l), 1, ggamma + l);
             if (gout[3 * l + 2]) add(gin[3 * l + 2], gout[3 * l + 2], n2);
             const T* cur = gh;
             T* bufs[2] = {pb, pa};
-            for (int k = last; k >= 0; --k) {
-                if (k == 0) {
-                    prop_bwd<false, true>(l, 0, in[3 * l], nullptr, nullptr, cur, nullptr, nullptr, gin[3 * l],
-                                          nullptr, nullptr);
+            for (int i = g.N[l] - 1; i >= 0; --i) {
+                const T* yb = tp + tape.prop[l][2 * i];
+                if (i == 0) {
+                    prop_iter_bwd<false, true>(l, in[3 * l], nullptr, nullptr, yb, nullptr, nullptr, cur, nullptr,
+                                               nullptr, gin[3 * l], nullptr, nullptr);
                     break;
                 }
-                T* o = bufs[(last - k) % 2];
-                prop_bwd<false, false>(l, k % 2, tp + tape.prop[l][k - 1], nullptr, nullptr, cur, nullptr, nullptr, o,
-                                       nullptr, nullptr);
+                T* o = bufs[(g.N[l] - 1 - i) % 2];
+                prop_iter_bwd<false, false>(l, tp + tape.prop[l][2 * i - 1], nullptr, nullptr, yb, nullptr, nullptr,
+                                            cur, nullptr, nullptr, o, nullptr, nullptr);
                 cur = o;
             }
-            model_bwd(l, l == 0, ga0, ggr, gby, gbx, gimg[l]);
+            model_bwd(l, l == 0, ga0, ggr, gimg[l]);
         }
         // pyramid adjoint, coarse to fine, added into the finer level's image gradient
         for (int l = L - 1; l >= 1; --l)
             ok(launch_k(pyr_bwd_k<T>, grid3(g.W[l - 1], g.H[l - 1], g.B), kBlock, 0, s, (const T*)gimg[l], gimg[l - 1],
                         g.H[l - 1], g.W[l - 1]));
+        reduce(jobs);
     }
 };
 

@@ -471,8 +471,16 @@ def _frame_backward(flt, first: bool, frame, gamma, weights, state_flat, new_fla
     d = _dt(frame)
     g = _geom(flt, frame.shape[0])
     scratch = _workspace("ff_diff_frame_scratch_bytes", d, g, frame)
-    g_frame, g_gamma, g_weights = torch.zeros_like(frame), torch.zeros_like(gamma), torch.zeros_like(weights)
-    g_state = [torch.zeros_like(t) for t in state_flat]
+    # the gradients the adjoint adds into, carved from one zeroed buffer (one fill per frame);
+    # every piece starts at an even element, so two-element pairs stay aligned
+    like = [frame, gamma, weights] + list(state_flat)
+    sizes = [(t.numel() + 1) & ~1 for t in like]
+    flat = torch.zeros(sum(sizes), dtype=frame.dtype, device=frame.device)
+    views, at = [], 0
+    for t, n in zip(like, sizes):
+        views.append(flat[at:at + t.numel()].view(t.shape))
+        at += n
+    g_frame, g_gamma, g_weights, g_state = views[0], views[1], views[2], views[3:]
     g_new = [_c(t) for t in g_new]
     call("ff_diff_frame_backward", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
          _ptrs(state_flat), _ptrs(new_flat), _p(tape), _ptrs(g_new), _p(_c(g_fu)), _p(g_frame), _p(g_gamma),
