@@ -746,7 +746,8 @@ __device__ __forceinline__ void level_warp(const LevelArgs& a, int nwx, int band
     c.any_split = __any_sync(kFull, c.cc0 != c.b0 || c.cc1 != c.b0 + 1);
     const int i0 = c.ys - lead_rows(N, S);
     const int last = c.ye - 1 + N + kDelay + 2 * S;
-    const int iters = (last - i0 + 1 + 1) & ~1;  // even: the loop body holds two rows
+    // rows of the band's pipeline (an even count when the loop body holds two rows)
+    const int iters = FFB_ROW_UNROLL == 2 ? (last - i0 + 2) & ~1 : last - i0 + 1;
     // Warps whose 64 columns lie inside the image and outside the border columns (all but
     // the first and last window of each band) run the pipeline without column handling.
     if (c.any_edge || c.freeze_cols || c.any_split)  // warp-uniform
