@@ -390,10 +390,14 @@ ff_status ff_color_wheel_default(unsigned char* rgba);
  * level: smoothed flow [B][H][W][2], old image [B][H][W], delta flow [B][H][W][2] (3 pointers
  * per level, level 0 first; inputs and outputs must not overlap).  The forward writes the
  * new state and keeps every intermediate the adjoint needs in `tape`
- * (ff_diff_frame_tape_bytes); `fu_out` (optional) receives the top level's unsmoothed flow.
+ * (ff_diff_frame_tape_bytes); `fu_out` (optional) receives the top level's unsmoothed flow,
+ * `y_out` (optional) a second copy of level 0's smoothed flow (an output of its own, so a
+ * caller can route one gradient to the state and another to the frame's output).
  * The backward ADDS the gradients of the frame, gamma (L), weights (L x 5) and the input
- * state into its outputs; absent output gradients may be NULL; `scratch` is
- * ff_diff_frame_scratch_bytes of device memory.  Sizes return 0 for a bad geometry. */
+ * state into its outputs; absent output gradients may be NULL; `grad_y` (optional) is the
+ * gradient of y_out, image b at grad_y + b * grad_y_bstride elements (rows dense), summed
+ * with the smoothed flow's; `scratch` is ff_diff_frame_scratch_bytes of device memory.
+ * Sizes return 0 for a bad geometry. */
 #define FF_DIFF_MAX_LEVELS 8
 typedef struct ff_diff_geom {
     int batch, levels, border;
@@ -405,7 +409,7 @@ size_t ff_diff_frame_tape_bytes(int dtype, const ff_diff_geom* geom);
 size_t ff_diff_frame_scratch_bytes(int dtype, const ff_diff_geom* geom);
 ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                 const void* weights, const void* const* state_in, void* const* state_out,
-                                void* fu_out, void* tape, void* stream);
+                                void* fu_out, void* y_out, void* tape, void* stream);
 /* The same frame forward without a tape, for inference: identical outputs, with the
  * intermediates in a reused `scratch` of ff_diff_frame_infer_bytes (a few fields per level
  * instead of every sub-step's).  No counterpart in the reference (no adjoint there). */
@@ -416,8 +420,24 @@ ff_status ff_diff_frame_infer(int dtype, const ff_diff_geom* geom, int first, co
 ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                  const void* weights, const void* const* state_in, const void* const* state_out,
                                  const void* tape, const void* const* grad_state_out, const void* grad_fu,
-                                 void* grad_frame, void* grad_gamma, void* grad_weights, void* const* grad_state_in,
-                                 void* scratch, void* stream);
+                                 const void* grad_y, long long grad_y_bstride, void* grad_frame, void* grad_gamma,
+                                 void* grad_weights, void* const* grad_state_in, void* scratch, void* stream);
+
+/* Mean endpoint error of flows (B, T, H, W, 2; dense) against truth over the frames
+ * first..T-1: mean of sqrt(dx^2 + dy^2 + eps), written to the device scalar `loss`. truth has
+ * the same pixel layout; element (b, t, y, x, c) lies at truth[b * truth_bstride + t *
+ * truth_tstride + 2 (y W + x) + c] (truth_tstride 0: one truth frame for every t). `scratch`:
+ * ff_diff_epe_scratch_bytes(dtype) bytes. Deterministic. ff_diff_epe_bwd writes the gradient
+ * of every flow element for the upstream gradient *grad_loss (device scalar): d / |d| * g /
+ * count for frames first.., zero before them and where |d| = 0. No counterpart in the
+ * reference (the differentiable filter's training loss). */
+size_t ff_diff_epe_scratch_bytes(int dtype);
+ff_status ff_diff_epe(int dtype, int B, int T, int H, int W, int first, double eps, const void* flows,
+                      const void* truth, long long truth_bstride, long long truth_tstride, void* loss, void* scratch,
+                      void* stream);
+ff_status ff_diff_epe_bwd(int dtype, int B, int T, int H, int W, int first, double eps, const void* flows,
+                          const void* truth, long long truth_bstride, long long truth_tstride, const void* grad_loss,
+                          void* grad_flows, void* stream);
 
 /* ff_stage_smooth without a workspace and without any allocation. It has no counterpart
  * in the reference. The X-pass scratch is a 32 MiB static device array of the library, so

@@ -380,41 +380,40 @@ __device__ __forceinline__ void prop_adj_at(int j, int n, bool line_in, int bord
     for (int c = 0; c < NC; ++c) acc[c] = T(0);
     if (j >= 2 && j + 2 <= n - 1) {
         // away from the line ends no index clamps: the five positions j-2..j+2 in registers,
-        // the same operations in the same order as the general loop below
+        // the same results as the general loop below
         T px[5][NC], gx[3][NC];
 #pragma unroll
         for (int p = 0; p < 5; ++p) chan(j - 2 + p, px[p]);
 #pragma unroll
         for (int q = 0; q < 3; ++q) gchan(j - 1 + q, gx[q]);
+        // branch-free: every lane runs the same instructions, the upwind branch, the border
+        // freeze and the dominant-neighbour choice are per-lane selects (a frozen output
+        // passes its gradient through: coefficient 1 at q == 1, 0 elsewhere)
 #pragma unroll
         for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
             const int i = j - 1 + q;
-            if (!(line_in && i >= border && i < n - border)) {
-                if (q == 1)
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) acc[c] += gx[1][c];
-                continue;
-            }
+            const bool in = line_in && i >= border && i < n - border;
             const T vm_ = px[q][AXIS], vp_ = px[q + 2][AXIS];
             const bool take_p = Ar<T>::sub(fabs(vp_), fabs(vm_)) > T(0);
             const T dv = take_p ? vp_ : vm_;
             const T t = dt * dv;
+            const bool pos = dv >= T(0);
+            const T dtq = in ? dt : T(0);
+            T coef;  // weight of this output's gradient at j
+            if (q == 1) coef = in ? (pos ? T(1) - t : T(1) + t) : T(1);
+            else if (q == 2) coef = in && pos ? t : T(0);
+            else coef = in && !pos ? -t : T(0);
             T gdv = T(0);
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 const T g_o = gx[q][c];
-                const T g0 = px[q + 1][c];
-                if (dv >= T(0)) {
-                    if (q == 1) acc[c] += g_o * (T(1) - t);
-                    if (q == 2) acc[c] += g_o * t;
-                    gdv -= g_o * dt * (g0 - px[q][c]);
-                } else {
-                    if (q == 1) acc[c] += g_o * (T(1) + t);
-                    if (q == 0) acc[c] -= g_o * t;
-                    gdv -= g_o * dt * (px[q + 2][c] - g0);
-                }
+                const T hi = pos ? px[q + 1][c] : px[q + 2][c];
+                const T lo = pos ? px[q][c] : px[q + 1][c];
+                acc[c] += g_o * coef;
+                gdv -= g_o * dtq * (hi - lo);
             }
-            if ((take_p ? q + 2 : q) == 2) acc[AXIS] += gdv;
+            // the dominant velocity is the chosen neighbour's AXIS component (position 2 = j)
+            if (q != 1) acc[AXIS] += (q == 0 ? take_p : !take_p) ? gdv : T(0);
         }
         return;
     }
@@ -606,7 +605,8 @@ __global__ void dupdate_bwd_k(const T* __restrict__ a0, const T* __restrict__ gr
 
 // ------------------------------------------------------------------ weighted smoothing pass
 template <typename T, int AXIS>
-__global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in, T* __restrict__ out, int H, int W) {
+__global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in, T* __restrict__ out, int H, int W,
+                             T* __restrict__ out2 = nullptr) {
     grid_dep_wait();
     grid_dep_launch();
     PIX_SETUP
@@ -617,9 +617,12 @@ __global__ void smooth_fwd_k(const T* __restrict__ w5, const T* __restrict__ in,
     for (int i = 0; i < 5; ++i)
         kk[i] = AXIS == 0 ? (b * H + y) * W + clampi(x + i - 2, 0, W - 1) : (b * H + clampi(y + i - 2, 0, H - 1)) * W + x;
     const size_t k = (b * H + y) * W + x;
-    for (int ch = 0; ch < 2; ++ch)
-        out[2 * k + ch] = chain5(w, in[2 * kk[0] + ch], in[2 * kk[1] + ch], in[2 * kk[2] + ch], in[2 * kk[3] + ch],
-                                 in[2 * kk[4] + ch]);
+    for (int ch = 0; ch < 2; ++ch) {
+        const T v = chain5(w, in[2 * kk[0] + ch], in[2 * kk[1] + ch], in[2 * kk[2] + ch], in[2 * kk[3] + ch],
+                           in[2 * kk[4] + ch]);
+        out[2 * k + ch] = v;
+        if (out2) out2[2 * k + ch] = v;  // a second copy (the frame driver's level-0 output)
+    }
 }
 
 // Blocks of 32 x 8 threads cover 32 x 32 pixels (kSmoothRows rows per thread), so the
@@ -695,9 +698,11 @@ template <typename T>
 constexpr size_t smooth_iter_smem() {
     return sizeof(typename Pair<T>::V) * (size_t)(kSW * kSW + 3 * kST * kSW);
 }
-template <typename T, bool ACC>
+// G2: a second output gradient gout2 is added to gout (image b at gout2 + b * g2_bstride)
+template <typename T, bool ACC, bool G2>
 __global__ void __launch_bounds__(256) smooth_iter_bwd_k(const T* __restrict__ w5, const T* __restrict__ xin,
                                                          const T* __restrict__ xmid, const T* __restrict__ gout,
+                                                         const T* __restrict__ gout2, long long g2_bstride,
                                                          T* __restrict__ gin, T* __restrict__ part, int H, int W) {
     grid_dep_wait();
     using V = typename Pair<T>::V;
@@ -723,7 +728,14 @@ __global__ void __launch_bounds__(256) smooth_iter_bwd_k(const T* __restrict__ w
         for (int u = 0; u < NG; ++u) {
             const int e = tid + 256 * u, r = e / kSW, c = e - r * kSW;
             const int y = y0 - 2 + r, x = x0 - 2 + c;
-            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) a[u] = go[(size_t)y * W + x];
+            if (e < kSW * kSW && y >= 0 && y < H && x >= 0 && x < W) {
+                a[u] = go[(size_t)y * W + x];
+                if constexpr (G2) {
+                    const V b2 = reinterpret_cast<const V*>(gout2 + blockIdx.z * g2_bstride)[(size_t)y * W + x];
+                    a[u].x += b2.x;
+                    a[u].y += b2.y;
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < NT; ++u) {
@@ -1217,6 +1229,21 @@ __global__ void __launch_bounds__(1024) reduce_jobs_k(ReduceJobs<T> J) {
     if ((int)threadIdx.x < nv) J.dst[j][threadIdx.x] += tot[threadIdx.x];
 }
 
+// dst = (ACC ? dst : 0) + a + b over B images of `per` elements; a dense (nullable, zero),
+// image i of b at b + i * bstride
+template <typename T, bool ACC>
+__global__ void sum2_k(T* __restrict__ dst, const T* __restrict__ a, const T* __restrict__ b, long long bstride,
+                       long long per, int B) {
+    grid_dep_wait();
+    grid_dep_launch();
+    const long long n = (long long)B * per;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long img = i / per;
+        const T v = a ? a[i] + b[img * bstride + (i - img * per)] : b[img * bstride + (i - img * per)];
+        dst[i] = ACC ? dst[i] + v : v;
+    }
+}
+
 // dst += src over n elements
 template <typename T>
 __global__ void add_k(T* __restrict__ dst, const T* __restrict__ src, size_t n) {
@@ -1224,6 +1251,74 @@ __global__ void add_k(T* __restrict__ dst, const T* __restrict__ src, size_t n) 
     grid_dep_launch();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] += src[i];
+}
+
+// ------------------------------------------------------------------ endpoint-error loss
+// flows (B, T, P, 2) dense (P = H * W pixels); truth element (b, t, p, c) at
+// truth[b * tb + t * tt + 2 p + c] (tt = 0: one truth frame for every t).  Frames t >= first
+// count.  Forward: per-block partial sums of sqrt(dx^2 + dy^2 + eps), one per block, reduced
+// in fixed order (deterministic).  Backward: the flow gradient d g / (count |d|) for every
+// element (zero before `first`, and where |d| = 0).
+struct EpeGeom {
+    int B, T, first;
+    long long P, tb, tt;
+};
+constexpr int kEpeThreads = 256, kEpeBlocks = 1024;
+template <typename T>
+__global__ void __launch_bounds__(kEpeThreads) epe_fwd_k(const T* __restrict__ flows, const T* __restrict__ truth,
+                                                         EpeGeom g, T eps, T* __restrict__ part) {
+    grid_dep_wait();
+    grid_dep_launch();
+    using V = typename Pair<T>::V;
+    const long long tf = g.T - g.first, n = (long long)g.B * tf * g.P;
+    T acc[1] = {T(0)};
+    for (long long i = blockIdx.x * (long long)kEpeThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kEpeThreads) {
+        const long long p = i % g.P, bt = i / g.P, t = g.first + bt % tf, b = bt / tf;
+        const V f = reinterpret_cast<const V*>(flows)[(b * g.T + t) * g.P + p];
+        const V r = *reinterpret_cast<const V*>(truth + b * g.tb + t * g.tt + 2 * p);
+        const T dx = f.x - r.x, dy = f.y - r.y;
+        acc[0] += sqrt(dx * dx + dy * dy + eps);
+    }
+    block_sum<T, 1>(acc, part + blockIdx.x, false);
+}
+template <typename T>
+__global__ void __launch_bounds__(1024) epe_sum_k(const T* __restrict__ part, int n, T inv_count, T* loss) {
+    grid_dep_wait();
+    grid_dep_launch();
+    T acc[1] = {T(0)};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] += part[i];
+    __shared__ T tot[1];
+    block_sum<T, 1>(acc, tot, false);
+    __syncthreads();
+    if (threadIdx.x == 0) *loss = tot[0] * inv_count;
+}
+template <typename T>
+__global__ void __launch_bounds__(kEpeThreads) epe_bwd_k(const T* __restrict__ flows, const T* __restrict__ truth,
+                                                         EpeGeom g, T eps, const T* __restrict__ gloss, T inv_count,
+                                                         T* __restrict__ gflows) {
+    grid_dep_wait();
+    grid_dep_launch();
+    using V = typename Pair<T>::V;
+    const T s = *gloss * inv_count;
+    const long long n = (long long)g.B * g.T * g.P;
+    for (long long i = blockIdx.x * (long long)kEpeThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kEpeThreads) {
+        const long long p = i % g.P, bt = i / g.P, t = bt % g.T, b = bt / g.T;
+        V o;
+        o.x = T(0);
+        o.y = T(0);
+        if (t >= g.first) {
+            const V f = reinterpret_cast<const V*>(flows)[i];
+            const V r = *reinterpret_cast<const V*>(truth + b * g.tb + t * g.tt + 2 * p);
+            const T dx = f.x - r.x, dy = f.y - r.y;
+            const T m = sqrt(dx * dx + dy * dy + eps);
+            if (m > T(0)) {
+                const T k = s / m;
+                o.x = dx * k;
+                o.y = dy * k;
+            }
+        }
+        reinterpret_cast<V*>(gflows)[i] = o;
+    }
 }
 
 inline dim3 grid3(int w, int h, int B) { return dim3((w + 31) / 32, (h + 7) / 8, B); }
@@ -1472,13 +1567,13 @@ ff_status ff_diff_smooth(int dtype, int B, int H, int W, int axis, const void* w
         const dim3 g = grid3(W, H, B);
         if (dtype)
             return axis == 0 ? launch_k(smooth_fwd_k<double, 0>, g, kBlock, 0, s, (const double*)w5,
-                                        (const double*)in, (double*)out, H, W)
+                                        (const double*)in, (double*)out, H, W, (double*)nullptr)
                              : launch_k(smooth_fwd_k<double, 1>, g, kBlock, 0, s, (const double*)w5,
-                                        (const double*)in, (double*)out, H, W);
+                                        (const double*)in, (double*)out, H, W, (double*)nullptr);
         return axis == 0 ? launch_k(smooth_fwd_k<float, 0>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
-                                    (float*)out, H, W)
+                                    (float*)out, H, W, (float*)nullptr)
                          : launch_k(smooth_fwd_k<float, 1>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
-                                    (float*)out, H, W);
+                                    (float*)out, H, W, (float*)nullptr);
     });
 }
 
@@ -1502,6 +1597,65 @@ ff_status ff_diff_smooth_bwd(int dtype, int B, int H, int W, int axis, const voi
                          : launch_k(smooth_bwd_k<float, 1>, g, kBlock, 0, s, (const float*)w5, (const float*)in,
                                     (const float*)gout, (float*)gin, (float*)gw5, H, W);
     });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+size_t ff_diff_epe_scratch_bytes(int dtype) { return (size_t)ffb::diff::kEpeBlocks * (dtype ? 8 : 4); }
+
+ff_status ff_diff_epe(int dtype, int B, int T, int H, int W, int first, double eps, const void* flows,
+                      const void* truth, long long truth_bstride, long long truth_tstride, void* loss, void* scratch,
+                      void* stream) {
+    using namespace ffb::diff;
+    if (dtype != 0 && dtype != 1) return ffb_fail(FF_ERR_INVALID_ARGUMENT, "dtype must be 0 (float32) or 1 (float64)");
+    if (B < 1 || T < 1 || H < 1 || W < 1 || first < 0 || first >= T || !(eps >= 0))
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe: bad shape, first frame or eps");
+    if (!flows || !truth || !loss || !scratch) return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe: null pointer");
+    if (!::pairs_aligned(dtype, {flows, truth}) || (truth_bstride | truth_tstride) & 1)
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe: flow pairs must be aligned to two elements");
+    const EpeGeom g{B, T, first, (long long)H * W, truth_bstride, truth_tstride};
+    const double inv = 1.0 / ((double)B * (T - first) * H * W);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if (dtype) {
+        e = ffb::launch_k(epe_fwd_k<double>, dim3(kEpeBlocks), dim3(kEpeThreads), 0, s, (const double*)flows,
+                          (const double*)truth, g, eps, (double*)scratch);
+        if (e == cudaSuccess)
+            e = ffb::launch_k(epe_sum_k<double>, dim3(1), dim3(1024), 0, s, (const double*)scratch, kEpeBlocks, inv,
+                              (double*)loss);
+    } else {
+        e = ffb::launch_k(epe_fwd_k<float>, dim3(kEpeBlocks), dim3(kEpeThreads), 0, s, (const float*)flows,
+                          (const float*)truth, g, (float)eps, (float*)scratch);
+        if (e == cudaSuccess)
+            e = ffb::launch_k(epe_sum_k<float>, dim3(1), dim3(1024), 0, s, (const float*)scratch, kEpeBlocks,
+                              (float)inv, (float*)loss);
+    }
+    return e == cudaSuccess ? FF_OK : ffb_fail(FF_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
+}
+
+ff_status ff_diff_epe_bwd(int dtype, int B, int T, int H, int W, int first, double eps, const void* flows,
+                          const void* truth, long long truth_bstride, long long truth_tstride, const void* grad_loss,
+                          void* grad_flows, void* stream) {
+    using namespace ffb::diff;
+    if (dtype != 0 && dtype != 1) return ffb_fail(FF_ERR_INVALID_ARGUMENT, "dtype must be 0 (float32) or 1 (float64)");
+    if (B < 1 || T < 1 || H < 1 || W < 1 || first < 0 || first >= T || !(eps >= 0))
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe_bwd: bad shape, first frame or eps");
+    if (!flows || !truth || !grad_loss || !grad_flows)
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe_bwd: null pointer");
+    if (!::pairs_aligned(dtype, {flows, truth, grad_flows}) || (truth_bstride | truth_tstride) & 1)
+        return ffb_fail(FF_ERR_INVALID_ARGUMENT, "ff_diff_epe_bwd: flow pairs must be aligned to two elements");
+    const EpeGeom g{B, T, first, (long long)H * W, truth_bstride, truth_tstride};
+    const double inv = 1.0 / ((double)B * (T - first) * H * W);
+    cudaStream_t s = (cudaStream_t)stream;
+    const cudaError_t e =
+        dtype ? ffb::launch_k(epe_bwd_k<double>, dim3(kEpeBlocks), dim3(kEpeThreads), 0, s, (const double*)flows,
+                              (const double*)truth, g, eps, (const double*)grad_loss, inv, (double*)grad_flows)
+              : ffb::launch_k(epe_bwd_k<float>, dim3(kEpeBlocks), dim3(kEpeThreads), 0, s, (const float*)flows,
+                              (const float*)truth, g, (float)eps, (const float*)grad_loss, (float)inv,
+                              (float*)grad_flows);
+    return e == cudaSuccess ? FF_OK : ffb_fail(FF_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
 }
 
 }  // extern "C"
@@ -1665,9 +1819,9 @@ struct Driver {
         }
         ok(e);
     }
-    void smooth(int l, int axis, const T* w5, const T* in, T* out) const {
-        ok(axis == 0 ? launch_k(smooth_fwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l])
-                     : launch_k(smooth_fwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l]));
+    void smooth(int l, int axis, const T* w5, const T* in, T* out, T* out2 = nullptr) const {
+        ok(axis == 0 ? launch_k(smooth_fwd_k<T, 0>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l], out2)
+                     : launch_k(smooth_fwd_k<T, 1>, grid(l), kBlock, 0, s, w5, in, out, g.H[l], g.W[l], out2));
     }
     // one propagation iteration's adjoint (X and Y sub-step): X input x*, Y input y*, output
     // gradient g*o, X input gradient g* (stored, or added when ACC)
@@ -1690,23 +1844,24 @@ struct Driver {
     }
     // one smoothing iteration's adjoint (X and Y pass): input gradient stored (or added),
     // weight sums per block
-    void smooth_iter_bwd(int l, bool acc, const T* w5, const T* xin, const T* xmid, const T* go, T* gi,
-                         T* part) const {
+    void smooth_iter_bwd(int l, bool acc, const T* w5, const T* xin, const T* xmid, const T* go, T* gi, T* part,
+                         const T* go2 = nullptr, long long go2_bstride = 0) const {
         const dim3 gr = grid_tile32(g.W[l], g.H[l], g.B);
         const int H = g.H[l], W = g.W[l];
         constexpr size_t smem = smooth_iter_smem<T>();
-        static bool prepared[64][2] = {};  // the dynamic shared-memory limit, set once per device
+        static bool prepared[64][4] = {};  // the dynamic shared-memory limit, set once per device
         int dev = 0;
         ok(cudaGetDevice(&dev));
-        if (!prepared[dev & 63][acc]) {
-            ok(acc ? cudaFuncSetAttribute(smooth_iter_bwd_k<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem)
-                   : cudaFuncSetAttribute(smooth_iter_bwd_k<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-            prepared[dev & 63][acc] = true;
+        const int v = (acc ? 1 : 0) + (go2 ? 2 : 0);
+        auto kern = v == 0 ? smooth_iter_bwd_k<T, false, false>
+                  : v == 1 ? smooth_iter_bwd_k<T, true, false>
+                  : v == 2 ? smooth_iter_bwd_k<T, false, true>
+                           : smooth_iter_bwd_k<T, true, true>;
+        if (!prepared[dev & 63][v]) {
+            ok(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            prepared[dev & 63][v] = true;
         }
-        ok(acc ? launch_k(smooth_iter_bwd_k<T, true>, gr, kBlock, smem, s, w5, xin, xmid, go, gi, part, H, W)
-               : launch_k(smooth_iter_bwd_k<T, false>, gr, kBlock, smem, s, w5, xin, xmid, go, gi, part, H, W));
+        ok(launch_k(kern, gr, kBlock, smem, s, w5, xin, xmid, go, go2, go2_bstride, gi, part, H, W));
     }
     void model(int l, const T* img, T* a0, T* grad) const {
         ok(launch_k(model_fwd_k<T>, grid(l), kBlock, 0, s, img, a0, grad, g.H[l], g.W[l]));
@@ -1730,8 +1885,9 @@ struct Driver {
     }
 
     // ---- forward
+    // y_out (nullable): a second copy of level 0's smoothed flow
     void forward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in, T* const* out,
-                 T* fu_out, T* tp, bool compact = false) const {
+                 T* fu_out, T* tp, bool compact = false, T* y_out = nullptr) const {
         const Tape tape(g, compact);
         const int L = g.L, top = L - 1;
         auto img = [&](int l) -> const T* { return l == 0 ? frame : tp + tape.img[l]; };
@@ -1756,7 +1912,7 @@ struct Driver {
             ok(launch_k(update_fwd_k<T>, grid(l), kBlock, 0, s, (const T*)a0, (const T*)grad, old, f, gamma + l, fu,
                         g.H[l], g.W[l], (T)g.maxflow[l]));
             if (fu_out) copy(fu_out, fu, n2);
-            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l]);
+            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l], l == 0 ? y_out : nullptr);
             copy(out[3 * l + 2], in[3 * l + 2], n2);
         }
         // delta levels, L-2 down to 0
@@ -1778,22 +1934,29 @@ struct Driver {
             T* flow = tp + tape.sm[l][0];
             ok(launch_k(dupdate_fwd_k<T>, grid(l), kBlock, 0, s, (const T*)a0, (const T*)grad, old, v, coarse,
                         gamma + l, flow, out[3 * l + 2], g.H[l], g.W[l], g.H[l + 1], g.W[l + 1], (T)g.maxflow[l]));
-            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l]);
+            smooth_chain(l, weights + 5 * l, tape, tp, out[3 * l], l == 0 ? y_out : nullptr);
         }
     }
-    // 2S passes from tape.sm[l][0]; pass j writes tape.sm[l][j+1], the last writes `last`
-    void smooth_chain(int l, const T* w5, const Tape& tape, T* tp, T* last) const {
+    // 2S passes from tape.sm[l][0]; pass j writes tape.sm[l][j+1], the last writes `last` (and
+    // `last2`, when given)
+    void smooth_chain(int l, const T* w5, const Tape& tape, T* tp, T* last, T* last2 = nullptr) const {
         const int n = 2 * g.S[l];
-        if (n == 0) copy(last, tp + tape.sm[l][0], 2 * g.n1(l));
-        for (int j = 0; j < n; ++j) smooth(l, j % 2, w5, tp + tape.sm[l][j], j + 1 < n ? tp + tape.sm[l][j + 1] : last);
+        if (n == 0) {
+            copy(last, tp + tape.sm[l][0], 2 * g.n1(l));
+            if (last2) copy(last2, tp + tape.sm[l][0], 2 * g.n1(l));
+        }
+        for (int j = 0; j < n; ++j)
+            smooth(l, j % 2, w5, tp + tape.sm[l][j], j + 1 < n ? tp + tape.sm[l][j + 1] : last, j + 1 < n ? nullptr : last2);
     }
 
     // ---- backward: gradients of the outputs -> gradients of the inputs, ADDED into the
     // caller's buffers.  Inside, every intermediate gradient is stored by the kernel that
     // produces it (no clearing), and only the kernels writing the caller's buffers add.
+    // gy (nullable): a second gradient of level 0's smoothed flow (of the forward's y_out),
+    // image i at gy + i * gy_bstride
     void backward(bool first, const T* frame, const T* gamma, const T* weights, const T* const* in,
-                  const T* const* out, const T* tp, const T* const* gout, const T* gfu_out, T* gframe, T* ggamma,
-                  T* gweights, T* const* gin, T* sc_) const {
+                  const T* const* out, const T* tp, const T* const* gout, const T* gfu_out, const T* gy,
+                  long long gy_bstride, T* gframe, T* ggamma, T* gweights, T* const* gin, T* sc_) const {
         (void)frame;
         const Tape tape(g);
         const Scratch S_(g);
@@ -1827,8 +1990,17 @@ struct Driver {
         // Pass j > 0 writes bufs[j % 2]; pass 1 writes sb, so dst may be sa.
         auto smooth_back = [&](int l, const T* g_last, T* dst, bool acc) -> const T* {
             const int n = 2 * g.S[l];
+            const T* g2 = l == 0 ? gy : nullptr;  // level 0: the second gradient joins here
             const T* gcur = gz(g_last);
             if (n == 0) {
+                if (g2) {
+                    const long long per = 2LL * g.H[l] * g.W[l];
+                    const unsigned nb = (unsigned)std::min<long long>((g.B * per + 255) / 256, 4096);
+                    ok(acc ? launch_k(sum2_k<T, true>, dim3(nb), dim3(256), 0, s, dst, g_last, g2, gy_bstride, per, g.B)
+                           : launch_k(sum2_k<T, false>, dim3(nb), dim3(256), 0, s, dst, g_last, g2, gy_bstride, per,
+                                      g.B));
+                    return dst;
+                }
                 if (!acc) return gcur;
                 add(dst, gcur, 2 * g.n1(l));
                 return dst;
@@ -1841,7 +2013,7 @@ struct Driver {
             for (int i = g.S[l] - 1; i >= 0; --i) {
                 T* o = i == 0 ? dst : bufs[i % 2];
                 smooth_iter_bwd(l, i == 0 && acc, weights + 5 * l, tp + tape.sm[l][2 * i], tp + tape.sm[l][2 * i + 1],
-                                gcur, o, part + i * nb * 5);
+                                gcur, o, part + i * nb * 5, i == g.S[l] - 1 ? g2 : nullptr, gy_bstride);
                 gcur = o;
             }
             jobs_add(part, (int)(g.S[l] * nb), 5, gweights + 5 * l);
@@ -1965,7 +2137,7 @@ size_t ff_diff_frame_scratch_bytes(int dtype, const ff_diff_geom* geom) {
 
 ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                 const void* weights, const void* const* state_in, void* const* state_out,
-                                void* fu_out, void* tape, void* stream) {
+                                void* fu_out, void* y_out, void* tape, void* stream) {
     return ffb::diff::run_frame([&] {
         const ffb::diff::Geo g = ffb::diff::geo_of(geom);
         if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
@@ -1974,14 +2146,17 @@ ff_status ff_diff_frame_forward(int dtype, const ff_diff_geom* geom, int first, 
         for (int k = 0; k < 3 * g.L; ++k)
             if (!::pairs_aligned(dtype, {state_in[k], state_out[k]}))
                 throw std::invalid_argument("state fields must be aligned to two elements (8 or 16 bytes)");
+        if (!::pairs_aligned(dtype, {y_out})) throw std::invalid_argument("y_out must be aligned to two elements");
         if (dtype) {
             ffb::diff::Driver<double>(g, (cudaStream_t)stream)
                 .forward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
-                         (const double* const*)state_in, (double* const*)state_out, (double*)fu_out, (double*)tape);
+                         (const double* const*)state_in, (double* const*)state_out, (double*)fu_out, (double*)tape,
+                         false, (double*)y_out);
         } else {
             ffb::diff::Driver<float>(g, (cudaStream_t)stream)
                 .forward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
-                         (const float* const*)state_in, (float* const*)state_out, (float*)fu_out, (float*)tape);
+                         (const float* const*)state_in, (float* const*)state_out, (float*)fu_out, (float*)tape, false,
+                         (float*)y_out);
         }
     });
 }
@@ -2022,8 +2197,8 @@ ff_status ff_diff_frame_infer(int dtype, const ff_diff_geom* geom, int first, co
 ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first, const void* frame, const void* gamma,
                                  const void* weights, const void* const* state_in, const void* const* state_out,
                                  const void* tape, const void* const* grad_state_out, const void* grad_fu,
-                                 void* grad_frame, void* grad_gamma, void* grad_weights, void* const* grad_state_in,
-                                 void* scratch, void* stream) {
+                                 const void* grad_y, long long grad_y_bstride, void* grad_frame, void* grad_gamma,
+                                 void* grad_weights, void* const* grad_state_in, void* scratch, void* stream) {
     return ffb::diff::run_frame([&] {
         const ffb::diff::Geo g = ffb::diff::geo_of(geom);
         if (dtype != 0 && dtype != 1) throw std::invalid_argument("dtype must be 0 (float32) or 1 (float64)");
@@ -2033,17 +2208,21 @@ ff_status ff_diff_frame_backward(int dtype, const ff_diff_geom* geom, int first,
         for (int k = 0; k < 3 * g.L; ++k)
             if (!::pairs_aligned(dtype, {state_in[k], state_out[k], grad_state_out[k], grad_state_in[k]}))
                 throw std::invalid_argument("state fields must be aligned to two elements (8 or 16 bytes)");
+        if (!::pairs_aligned(dtype, {grad_y}) || (grad_y && (grad_y_bstride & 1)))
+            throw std::invalid_argument("grad_y must be aligned to two elements, with an even image stride");
         if (dtype) {
             ffb::diff::Driver<double>(g, (cudaStream_t)stream)
                 .backward(first != 0, (const double*)frame, (const double*)gamma, (const double*)weights,
                           (const double* const*)state_in, (const double* const*)state_out, (const double*)tape,
-                          (const double* const*)grad_state_out, (const double*)grad_fu, (double*)grad_frame,
+                          (const double* const*)grad_state_out, (const double*)grad_fu, (const double*)grad_y,
+                          grad_y_bstride, (double*)grad_frame,
                           (double*)grad_gamma, (double*)grad_weights, (double* const*)grad_state_in, (double*)scratch);
         } else {
             ffb::diff::Driver<float>(g, (cudaStream_t)stream)
                 .backward(first != 0, (const float*)frame, (const float*)gamma, (const float*)weights,
                           (const float* const*)state_in, (const float* const*)state_out, (const float*)tape,
-                          (const float* const*)grad_state_out, (const float*)grad_fu, (float*)grad_frame,
+                          (const float* const*)grad_state_out, (const float*)grad_fu, (const float*)grad_y,
+                          grad_y_bstride, (float*)grad_frame,
                           (float*)grad_gamma, (float*)grad_weights, (float* const*)grad_state_in, (float*)scratch);
         }
     });

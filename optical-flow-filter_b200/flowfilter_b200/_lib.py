@@ -172,10 +172,14 @@ SIGNATURES = {
                                     _i, _i, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]),
     "ff_diff_frame_tape_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_scratch_bytes": (ctypes.c_size_t, [_i, _vp]),
-    "ff_diff_frame_forward": (_st, [_i, _vp, _i] + [_vp] * 8),
+    "ff_diff_frame_forward": (_st, [_i, _vp, _i] + [_vp] * 9),
     "ff_diff_frame_infer_bytes": (ctypes.c_size_t, [_i, _vp]),
     "ff_diff_frame_infer": (_st, [_i, _vp, _i] + [_vp] * 8),
-    "ff_diff_frame_backward": (_st, [_i, _vp, _i] + [_vp] * 14),
+    "ff_diff_epe_scratch_bytes": (ctypes.c_size_t, [_i]),
+    "ff_diff_epe": (_st, [_i] * 6 + [ctypes.c_double, _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, _vp, _vp, _vp]),
+    "ff_diff_epe_bwd": (_st, [_i] * 6 + [ctypes.c_double, _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, _vp, _vp,
+                                         _vp]),
+    "ff_diff_frame_backward": (_st, [_i, _vp, _i] + [_vp] * 9 + [ctypes.c_longlong] + [_vp] * 6),
 }
 
 _lib = None

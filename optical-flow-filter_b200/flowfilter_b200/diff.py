@@ -405,9 +405,76 @@ class DiffPyramidalFlowFilter:
 def endpoint_error(flows, truth, first: int = 0, eps: float = 0.0):
     """Mean endpoint error over frames first.. of flows (B, T, H, W, 2) against truth of the
     same shape (or broadcastable).  eps > 0 is added under the square root, which keeps the
-    gradient finite where a flow equals the truth exactly (used by fit())."""
-    d = flows[:, first:] - truth[:, first:]
-    return (d[..., 0] ** 2 + d[..., 1] ** 2 + eps).sqrt().mean()
+    gradient finite where a flow equals the truth exactly (used by fit()); with eps = 0 the
+    gradient there is zero.  One autograd node: the backward writes the flow gradient in one
+    pass (zero for the frames before ``first``)."""
+    torch = _torch()
+    if isinstance(truth, torch.Tensor) and truth.requires_grad:
+        d = flows[:, first:] - truth[:, first:]
+        return (d[..., 0] ** 2 + d[..., 1] ** 2 + eps).sqrt().mean()
+    global _EPE
+    if _EPE is None:
+        _EPE = _epe_function()
+    return _EPE.apply(flows, truth, int(first), float(eps))
+
+
+_EPE = None
+
+
+def _epe_function():
+    torch = _torch()
+
+    def on_device(flows, first):
+        return (flows.is_cuda and flows.dtype in (torch.float32, torch.float64) and flows.dim() == 5
+                and flows.shape[-1] == 2 and 0 <= first < flows.shape[1])
+
+    class EndpointError(torch.autograd.Function):
+        """CUDA float tensors: ff_diff_epe / ff_diff_epe_bwd (one pass each way); otherwise
+        the same arithmetic from torch operations."""
+
+        @staticmethod
+        def forward(ctx, flows, truth, first, eps):
+            ctx.first, ctx.eps, ctx.shape = first, eps, flows.shape
+            if on_device(flows, first):
+                f = flows.contiguous()
+                tr = torch.as_tensor(truth, dtype=f.dtype, device=f.device).expand(f.shape)
+                if tr.stride()[2:] != f.stride()[2:]:
+                    tr = tr.contiguous()
+                B, T, H, W = f.shape[:4]
+                d = _dt(f)
+                loss = f.new_empty(())
+                scratch = f.new_empty(lib().ff_diff_epe_scratch_bytes(d) // f.element_size())
+                call("ff_diff_epe", d, B, T, H, W, first, eps, _p(f), _p(tr), tr.stride(0), tr.stride(1), _p(loss),
+                     _p(scratch), _stream())
+                ctx.device = True
+                ctx.save_for_backward(f, tr)
+                return loss
+            d = flows[:, first:] - truth[:, first:]
+            n = torch.linalg.vector_norm(d, dim=-1)
+            if eps > 0:
+                n = n.square_().add_(eps).sqrt_()
+            ctx.device = False
+            ctx.save_for_backward(d, n)
+            return n.mean()
+
+        @staticmethod
+        def backward(ctx, g):
+            if ctx.device:
+                f, tr = ctx.saved_tensors
+                B, T, H, W = f.shape[:4]
+                out = torch.empty_like(f)
+                call("ff_diff_epe_bwd", _dt(f), B, T, H, W, ctx.first, ctx.eps, _p(f), _p(tr), tr.stride(0),
+                     tr.stride(1), _p(g.contiguous()), _p(out), _stream())
+                return out, None, None, None
+            d, n = ctx.saved_tensors
+            # d |d|^-1 g / count; where |d| = 0 (eps = 0) so is d, and the gradient is zero
+            scale = torch.div(g / n.numel(), n.clamp_min(1e-30))
+            out = d.new_empty(ctx.shape)
+            out[:, :ctx.first].zero_()
+            torch.mul(d, scale.unsqueeze(-1), out=out[:, ctx.first:])
+            return out, None, None, None
+
+    return EndpointError
 
 
 MAX_LEVELS = 8  # FF_DIFF_MAX_LEVELS
@@ -449,7 +516,8 @@ def _ptrs(ts):
 def _frame_forward(flt, frame, gamma, weights, state_flat, first: bool):
     """One frame through ff_diff_frame_forward (one host call launches the whole frame).
     Returns (new state, flat; the top level's unsmoothed flow for one level, else None; the
-    tape the adjoint reads)."""
+    tape the adjoint reads; for several levels a copy of level 0's smoothed flow, the frame's
+    output, else None)."""
     d = _dt(frame)
     B = frame.shape[0]
     g = _geom(flt, B)
@@ -458,15 +526,16 @@ def _frame_forward(flt, frame, gamma, weights, state_flat, first: bool):
     for h, w in flt.shapes:
         new += [frame.new_empty((B, h, w, 2)), frame.new_empty((B, h, w)), frame.new_empty((B, h, w, 2))]
     fu = frame.new_empty((B,) + tuple(flt.shapes[0]) + (2,)) if flt.L == 1 else None
+    y = frame.new_empty((B,) + tuple(flt.shapes[0]) + (2,)) if flt.L > 1 else None
     call("ff_diff_frame_forward", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
-         _ptrs(state_flat), _ptrs(new), _p(fu), _p(tape), _stream())
-    return new, fu, tape
+         _ptrs(state_flat), _ptrs(new), _p(fu), _p(y), _p(tape), _stream())
+    return new, fu, tape, y
 
 
-def _frame_backward(flt, first: bool, frame, gamma, weights, state_flat, new_flat, tape, g_new, g_fu):
+def _frame_backward(flt, first: bool, frame, gamma, weights, state_flat, new_flat, tape, g_new, g_fu, g_y=None):
     """Adjoint of one frame through ff_diff_frame_backward: gradients of the new state (None
-    = zero) and of the top level's unsmoothed flow -> gradients of the frame, gamma, weights
-    and the input state."""
+    = zero), of the top level's unsmoothed flow and of the frame's output y -> gradients of
+    the frame, gamma, weights and the input state."""
     torch = _torch()
     d = _dt(frame)
     g = _geom(flt, frame.shape[0])
@@ -482,9 +551,14 @@ def _frame_backward(flt, first: bool, frame, gamma, weights, state_flat, new_fla
         at += n
     g_frame, g_gamma, g_weights, g_state = views[0], views[1], views[2], views[3:]
     g_new = [_c(t) for t in g_new]
+    # y's gradient is often one frame of a (B, T, H, W, 2) gradient: read in place when its
+    # images are dense (any image stride)
+    if g_y is not None and (g_y.dim() != 4 or g_y.stride()[1:] != (2 * g_y.shape[2], 2, 1) or g_y.stride(0) % 2):
+        g_y = g_y.contiguous()
     call("ff_diff_frame_backward", d, ctypes.byref(g), 1 if first else 0, _p(frame), _p(gamma), _p(weights),
-         _ptrs(state_flat), _ptrs(new_flat), _p(tape), _ptrs(g_new), _p(_c(g_fu)), _p(g_frame), _p(g_gamma),
-         _p(g_weights), _ptrs(g_state), _p(scratch), _stream())
+         _ptrs(state_flat), _ptrs(new_flat), _p(tape), _ptrs(g_new), _p(_c(g_fu)), _p(g_y),
+         g_y.stride(0) if g_y is not None else 0, _p(g_frame), _p(g_gamma), _p(g_weights), _ptrs(g_state),
+         _p(scratch), _stream())
     return g_frame, g_gamma, g_weights, g_state
 
 
@@ -500,13 +574,18 @@ def _frame_function():
         def forward(ctx, flt, first, frame, gamma, weights, *state_flat):
             state_flat = [t.contiguous() for t in state_flat]
             frame, gamma, weights = frame.contiguous(), gamma.contiguous(), weights.contiguous()
-            new, fu, tape = _frame_forward(flt, frame, gamma, weights, state_flat, first)
+            new, fu, tape, y = _frame_forward(flt, frame, gamma, weights, state_flat, first)
             ctx.flt, ctx.first = flt, first
+            ctx.set_materialize_grads(False)  # outputs nobody differentiates: None, not zeros
             if torch.is_grad_enabled() or any(ctx.needs_input_grad):
                 # the tape and the outputs the adjoint reads go through save_for_backward, so an
                 # enclosing checkpoint can drop them and recompute the frame in the backward pass
                 ctx.save_for_backward(frame, gamma, weights, tape, *state_flat, *new)
-            return (*new, fu if fu is not None else frame.new_zeros(0))
+            empty = frame.new_zeros(0)
+            # outputs: the new state, the top level's unsmoothed flow (one level), the frame's
+            # output (several levels: a copy of level 0's smoothed flow, so that its gradient
+            # and the next frame's state gradient reach the adjoint separately)
+            return (*new, fu if fu is not None else empty, y if y is not None else empty)
 
         @staticmethod
         def backward(ctx, *grads):
@@ -516,8 +595,9 @@ def _frame_function():
             frame, gamma, weights, tape = saved[:4]
             state_flat, new_flat = list(saved[4:4 + 3 * L]), list(saved[4 + 3 * L:])
             g_fu = grads[3 * L] if L == 1 and grads[3 * L] is not None and grads[3 * L].numel() else None
+            g_y = grads[3 * L + 1] if L > 1 and grads[3 * L + 1] is not None and grads[3 * L + 1].numel() else None
             g_frame, g_gamma, g_weights, g_state = _frame_backward(flt, ctx.first, frame, gamma, weights, state_flat,
-                                                                   new_flat, tape, list(grads[:3 * L]), g_fu)
+                                                                   new_flat, tape, list(grads[:3 * L]), g_fu, g_y)
             return (None, None, g_frame, g_gamma, g_weights, *g_state)
 
     return FrameStep
@@ -564,5 +644,5 @@ def frame_step(flt, frame, state, first: bool):
         return (out[3 * L] if L == 1 else newst[0][0]), newst
     out = _FrameStep.apply(flt, first, frame, flt.gamma, flt.weights, *[t for lvl in state for t in lvl])
     new = [tuple(out[3 * l:3 * l + 3]) for l in range(L)]
-    y = out[3 * L] if L == 1 else new[0][0]
+    y = out[3 * L] if L == 1 else out[3 * L + 1]
     return y, new

@@ -33,6 +33,20 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
 
 
+def test_bindings_pass_as_many_arguments_as_the_header_declares():
+    """Every ctypes binding has one argument type per parameter of its declaration (a binding
+    out of step with its declaration would pass arguments in the wrong places)."""
+    text = open(os.path.join(ROOT, "include", "ffb200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    wrong = {}
+    for name, params in re.findall(r"\b(ff_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = params.strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        if name in _lib.SIGNATURES and len(_lib.SIGNATURES[name][1]) != n:
+            wrong[name] = (n, len(_lib.SIGNATURES[name][1]))
+    assert not wrong, wrong
+
+
 def test_allocation_failure_injection_switches_on_and_off():
     L = _lib.lib()
     assert L.ff_debug_fail_allocation_after(3) == _lib.FF_OK

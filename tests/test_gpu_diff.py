@@ -298,3 +298,33 @@ def test_forward_without_tape_equals_forward_with_tape(dm, cuda, levels, dtype):
     taped = f(frames.clone().requires_grad_(True)).detach()
     assert free.dtype == taped.dtype
     np.testing.assert_array_equal(free.cpu().numpy(), taped.cpu().numpy())
+
+
+@pytest.mark.parametrize("first,eps,broadcast,dtype", [(0, 0.0, False, "float32"), (8, 1e-12, True, "float32"),
+                                                       (3, 0.0, True, "float64"), (1, 0.5, False, "float64")])
+def test_endpoint_error_kernels_match_the_formula(dm, cuda, first, eps, broadcast, dtype):
+    """ff_diff_epe / ff_diff_epe_bwd (the loss on CUDA tensors) against the formula through
+    torch autograd, with a broadcast truth frame and exact zeros in the difference."""
+    torch = cuda
+    dt = getattr(torch, dtype)
+    rng = np.random.default_rng(first + 11)
+    B, T, H, W = 3, 10, 17, 29
+    flows = torch.from_numpy(rng.normal(0, 1, (B, T, H, W, 2))).to(dt).cuda()
+    truth = torch.from_numpy(rng.normal(0, 1, (B, 1 if broadcast else T, H, W, 2))).to(dt).cuda()
+    if broadcast:
+        truth = truth.expand(B, T, H, W, 2)
+    flows[0, -1, 0, :3] = truth[0, -1, 0, :3]  # |d| = 0 pixels
+    res = []
+    for fn in (dm.endpoint_error, lambda f, t, a, e: ((f[:, a:] - t[:, a:]) ** 2).sum(-1).add(e).sqrt().mean()):
+        x = flows.clone().requires_grad_(True)
+        loss = fn(x, truth, first, eps)
+        (3.0 * loss).backward()
+        res.append((loss.item(), x.grad.double().cpu().numpy()))
+    tol = 1e-5 if dtype == "float32" else 1e-12
+    assert res[0][0] == pytest.approx(res[1][0], rel=tol)
+    g0, g1 = res[0][1], res[1][1]
+    if eps == 0:  # the formula's gradient is NaN where |d| = 0; the kernel's is zero
+        assert not g0[0, -1, 0, :3].any()
+        g0[0, -1, 0, :3] = g1[0, -1, 0, :3] = 0
+    np.testing.assert_allclose(g0, g1, rtol=tol, atol=tol * np.abs(g1).max())
+    assert not g0[:, :first].any()
