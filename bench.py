@@ -457,6 +457,10 @@ def bench_batched(steps, warmup):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    b0_ms = timed(lambda t: batch.step(packed[t % BATCH_RING]))  # the default band rule
+    t0 = time.perf_counter()
+    bands = batch.autotune(packed[0], repetitions=3)  # per level size, on a scratch batch
+    tune_s = time.perf_counter() - t0
     b_ms = timed(lambda t: batch.step(packed[t % BATCH_RING]))
     loop = []
     for s in streams:
@@ -480,6 +484,9 @@ def bench_batched(steps, warmup):
         "value": n * steps / (b_ms / 1e3), "unit": "stream-frames/s", "steps": steps,
         "ms_per_step": b_ms / steps, "mpix_per_s": px * steps / (b_ms / 1e3) / 1e6,
         "launches_per_step": batch.launches(),
+        "autotune": {"bands": bands, "seconds": tune_s, "default_bands_ms_per_step": b0_ms / steps,
+                     "method": "BatchFlowFilter.autotune: band rows per level size, largest first, each the "
+                               "fastest of 8..128 rows by CUDA-event-timed steps of a scratch batch"},
         "loop_value": n * steps / (l_ms / 1e3), "loop_ms_per_step": l_ms / steps,
         "speedup_vs_loop": l_ms / b_ms,
         "data": "synthetic: stream i is a seeded bump-flow sequence of its size from seed 100 + i",

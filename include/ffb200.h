@@ -278,10 +278,11 @@ ff_status ff_stage_scale_flow(const float* flow, size_t flow_pitch, int height, 
  * No counterpart in the reference: many independent PyramidalFlowFilter streams of
  * different sizes, levels and parameters advanced together.  Stream i's frame is read from
  * a packed uint8 device buffer at the offset ff_batch_frame_layout gives (rows of width
- * bytes, no padding); one step runs ff_batch_launches kernel launches, which depend on
- * the pyramid depth and on how many distinct (iterations, smoothing) settings the large
- * levels have, not on the number of streams; every stream's results equal those of the
- * same stream filtered alone.  Each stream is an ff_filter owned by the batch (ff_batch_stream):
+ * bytes, no padding); one step runs ff_batch_launches kernel launches (4 for up to 3 levels
+ * per stream within the streaming kernel's iterations and smoothing passes: ingest with
+ * pyramid, one streaming launch per phase, one tile launch), a
+ * number that depends on neither the number of streams nor their parameters; every stream's
+ * results equal those of the same stream filtered alone.  Each stream is an ff_filter owned by the batch (ff_batch_stream):
  * set its parameters and read its results with the ff_filter_* calls; do not destroy it. */
 typedef struct ff_batch ff_batch;
 ff_status ff_batch_create(int n, const int* heights, const int* widths, const int* levels, ff_batch** batch);
@@ -292,10 +293,16 @@ ff_status ff_batch_frame_layout(const ff_batch* batch, size_t* offsets, size_t* 
 ff_status ff_batch_launches(const ff_batch* batch, int* launches);
 /* frames: 16-byte aligned device buffer of total_bytes; stream: cudaStream_t (NULL = legacy) */
 ff_status ff_batch_step(ff_batch* batch, const void* frames, void* stream);
-/* Kernel selection (optional; results do not depend on it): levels of at least min_pixels
- * pixels run the streaming level kernel in bands of band rows, the others the tile-fused
- * kernel.  min_pixels < 0 selects the single filter's threshold, band <= 0 the default. */
+/* Kernel selection (optional; results do not depend on it): the levels that read the
+ * previous frame's coarse flow or are top levels (phase A) run the tile-fused kernel below
+ * min_pixels pixels (< 0: 200000), every other level the streaming level kernel covers runs
+ * it, in bands of band rows (<= 0: the default rule).  Phase-B levels beyond the streaming
+ * kernel (more than 4 iterations or smoothing passes) add a second tile launch. */
 ff_status ff_batch_set_tuning(ff_batch* batch, long long min_pixels, int band);
+/* Levels of height x width pixels run the streaming kernel in bands of band rows (band <= 0
+ * removes the override): the per-size choice the batch autotuner makes.  Results do not
+ * depend on it. */
+ff_status ff_batch_set_level_band(ff_batch* batch, int height, int width, int band);
 
 /* ------------------------------------------------------------ differentiable stages
  * No counterpart in the reference: the float-input filter's stages as forward and adjoint

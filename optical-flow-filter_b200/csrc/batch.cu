@@ -30,12 +30,22 @@ struct PyrJob {
     int first_block;
 };
 
+// one stream's frame: copied into its level-0 image, with levels 1 and 2 of its pyramid
+// built from it in the same blocks (tiles of P2X x P2Y level-1 pixels; a one-level stream's
+// blocks copy tiles of 2 P2X x 2 P2Y level-0 pixels)
 struct IngestJob {
     size_t src;  // byte offset of the frame in the packed buffer (rows of W bytes)
     uint8_t* dst;
     size_t dst_pitch;
     int H, W;
-    int rows_per_block;
+    uint8_t* out1;
+    size_t out1_pitch;
+    int h1, w1;
+    uint8_t* out2;
+    size_t out2_pitch;
+    int h2, w2;
+    int levels;  // levels this launch fills: 1, 2 or 3
+    int tiles_x, tiles_y;
     int first_block;
 };
 
@@ -56,25 +66,106 @@ __device__ __forceinline__ int job_of(const J* jobs, int n, int b) {
     return lo;
 }
 
-// copies every stream's frame out of the packed buffer into its filter's input image
-__global__ void __launch_bounds__(256) ingest_k(const uint8_t* __restrict__ frames, const IngestJob* __restrict__ jobs,
-                                                int n) {
+constexpr int P2X = 64, P2Y = 16;  // level-1 tile of the ingest launch (blocks of 32 x 8 threads)
+
+// Every stream's frame out of the packed buffer into its level-0 image, and levels 1 and 2
+// of its pyramid from the frame.  A block stages the level-0 pixels under its level-1 tile
+// and the one-pixel level-1 ring around it (at clamped coordinates) in shared memory with
+// one batch of loads, copies its part of level 0 out of it, computes the level-1 tile plus
+// ring from it (pyramid_px, common.cuh: the values of a pyramid_down_k pass), and the
+// level-2 pixels under the tile from the ring.  The last tile row and column of a stream also
+// copy the level-0 remainder (odd sizes).
+constexpr int S0Y = 2 * P2Y + 5, S0X = 2 * P2X + 5;  // staged level-0 rows and columns
+__global__ void __launch_bounds__(256) ingest_pyr_k(const uint8_t* __restrict__ frames,
+                                                    const IngestJob* __restrict__ jobs, int n) {
+    __shared__ uint8_t s0[S0Y][S0X + 3];
+    __shared__ uint8_t ring[P2Y + 2][P2X + 2];
     grid_dep_wait();
     grid_dep_launch();
-    const IngestJob j = jobs[job_of(jobs, n, blockIdx.x)];
-    const int r0 = (blockIdx.x - j.first_block) * j.rows_per_block;
-    const int r1 = min(r0 + j.rows_per_block, j.H);
-    for (int r = r0; r < r1; ++r) {
-        const uint8_t* src = frames + j.src + (size_t)r * j.W;
-        uint8_t* dst = j.dst + (size_t)r * j.dst_pitch;
-        if ((j.W & 15) == 0 && ((uintptr_t)src & 15) == 0 && ((uintptr_t)dst & 15) == 0) {
-            const int n16 = j.W >> 4;
-            for (int c = threadIdx.x; c < n16; c += blockDim.x)
-                reinterpret_cast<uint4*>(dst)[c] = __ldg(reinterpret_cast<const uint4*>(src) + c);
+    const IngestJob& j = jobs[job_of(jobs, n, blockIdx.x)];
+    const int b = blockIdx.x - j.first_block;
+    const int tx = b % j.tiles_x, ty = b / j.tiles_x;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const uint8_t* src = frames + j.src;
+    if (j.levels < 2) {  // block-uniform: a one-level stream's tile is a plain copy
+        const int x0 = tx * 2 * P2X, y0 = ty * 2 * P2Y;
+        const int xe = tx == j.tiles_x - 1 ? j.W : min(x0 + 2 * P2X, j.W);
+        const int ye = ty == j.tiles_y - 1 ? j.H : min(y0 + 2 * P2Y, j.H);
+        const int wv = xe - x0, rows = ye - y0;
+        if ((j.W & 3) == 0 && (wv & 3) == 0 && (j.dst_pitch & 3) == 0) {  // 4-byte words
+            const int wq = wv >> 2;
+            for (int k = tid; k < rows * wq; k += 256) {
+                const int r = k / wq, c = k - r * wq;
+                reinterpret_cast<uint32_t*>(j.dst + (size_t)(y0 + r) * j.dst_pitch + x0)[c] =
+                    __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)(y0 + r) * j.W + x0) + c);
+            }
         } else {
-            for (int c = threadIdx.x; c < j.W; c += blockDim.x) dst[c] = __ldg(src + c);
+            for (int k = tid; k < rows * wv; k += 256) {
+                const int r = k / wv, c = k - r * wv;
+                j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = __ldg(src + (size_t)(y0 + r) * j.W + x0 + c);
+            }
+        }
+        return;
+    }
+    const int x1 = tx * P2X, y1 = ty * P2Y;
+    const int X0 = 2 * x1 - 3, Y0 = 2 * y1 - 3;  // staged level-0 origin (unclamped)
+    {
+        constexpr int NS = (S0Y * S0X + 255) / 256;
+        uint8_t v[NS];
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + 256 * u, r = e / S0X, c = e - r * S0X;
+            if (e < S0Y * S0X)
+                v[u] = __ldg(src + (size_t)min(max(Y0 + r, 0), j.H - 1) * j.W + min(max(X0 + c, 0), j.W - 1));
+        }
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + 256 * u, r = e / S0X, c = e - r * S0X;
+            if (e < S0Y * S0X) s0[r][c] = v[u];
         }
     }
+    __syncthreads();
+    {
+        const int x0 = 2 * x1, y0 = 2 * y1;
+        const int xe = tx == j.tiles_x - 1 ? j.W : min(x0 + 2 * P2X, j.W);
+        const int ye = ty == j.tiles_y - 1 ? j.H : min(y0 + 2 * P2Y, j.H);
+        const int wv = xe - x0;
+        for (int k = tid; k < (ye - y0) * wv; k += 256) {
+            const int r = k / wv, c = k - r * wv;
+            j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = s0[y0 + r - Y0][x0 + c - X0];
+        }
+    }
+    for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += 256) {
+        const int i = k % (P2X + 2), r = k / (P2X + 2);
+        const int ux = x1 - 1 + i, uy = y1 - 1 + r;  // unclamped level-1 position
+        const int cx = min(max(ux, 0), j.w1 - 1), cy = min(max(uy, 0), j.h1 - 1);
+        // pyramid_val at (cx, cy): rows 2cy-1..2cy+1, columns 2cx-1..2cx+1 of level 0, clamped
+        float xs[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const uint8_t* row = s0[2 * cy - 1 + q - Y0] + (2 * cx - 1 - X0);
+            const float sv = down3(u8_to_unit(row[0]), u8_to_unit(row[1]), u8_to_unit(row[2]));
+            xs[q] = u8_to_unit(quantize_u8(sv));
+        }
+        const uint8_t val = quantize_u8(down3(xs[0], xs[1], xs[2]));
+        ring[r][i] = val;
+        if (ux == cx && uy == cy && ux >= x1 && ux < x1 + P2X && uy >= y1 && uy < y1 + P2Y)
+            j.out1[(size_t)uy * j.out1_pitch + ux] = val;
+    }
+    if (j.levels < 3) return;  // block-uniform
+    __syncthreads();
+    const int x2 = x1 / 2 + threadIdx.x, y2 = y1 / 2 + threadIdx.y;
+    if (x2 >= j.w2 || y2 >= j.h2) return;
+    // pyramid_val over level 1, whose clamped reads the ring holds
+    float xs[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int r = 2 * y2 - 1 + q - (y1 - 1);
+        const int c = 2 * x2 - 1 - (x1 - 1);
+        const float sv = down3(u8_to_unit(ring[r][c]), u8_to_unit(ring[r][c + 1]), u8_to_unit(ring[r][c + 2]));
+        xs[q] = u8_to_unit(quantize_u8(sv));
+    }
+    j.out2[(size_t)y2 * j.out2_pitch + x2] = quantize_u8(down3(xs[0], xs[1], xs[2]));
 }
 
 // one pyramid depth over every stream that has it: pyramid_down_k per job
@@ -156,10 +247,8 @@ struct Batch::Table {
     TileJob* d_tile = nullptr;
     StreamJob* d_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
+    int launches = 0;  // kernel launches of the graph
 };
-
-// the streaming-kernel launches of a step: (phase, delta, N, S) -> its jobs
-using StreamGroups = std::map<std::tuple<int, int, int, int>, std::vector<StreamJob>>;
 
 Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
     if (n <= 0) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: stream count must be positive");
@@ -181,19 +270,39 @@ void Batch::init(int n, const int* heights, const int* widths, const int* levels
     int blocks = 0;
     for (int i = 0; i < n; ++i) {
         f_.emplace_back(new Filter(Kind::Pyramidal, heights[i], widths[i], levels[i], 1, true));
+        Filter& f = *f_.back();
         max_levels_ = std::max(max_levels_, levels[i]);
         off_.push_back(total_);
         total_ += ((size_t)heights[i] * widths[i] + 255) / 256 * 256;
-        const Level& v = f_.back()->level(0);
+        const Level& v = f.level(0);
         IngestJob j{};
         j.src = off_.back();
         j.dst = (uint8_t*)v.img;
         j.dst_pitch = v.img_pitch;
         j.H = v.H;
         j.W = v.W;
-        j.rows_per_block = std::max(1, 16384 / v.W);
+        j.levels = std::min(f.levels(), 3);
+        if (j.levels >= 2) {
+            const Level& v1 = f.level(1);
+            j.out1 = (uint8_t*)v1.img;
+            j.out1_pitch = v1.img_pitch;
+            j.h1 = v1.H;
+            j.w1 = v1.W;
+            j.tiles_x = (v1.W + P2X - 1) / P2X;
+            j.tiles_y = (v1.H + P2Y - 1) / P2Y;
+        } else {
+            j.tiles_x = (v.W + 2 * P2X - 1) / (2 * P2X);
+            j.tiles_y = (v.H + 2 * P2Y - 1) / (2 * P2Y);
+        }
+        if (j.levels >= 3) {
+            const Level& v2 = f.level(2);
+            j.out2 = (uint8_t*)v2.img;
+            j.out2_pitch = v2.img_pitch;
+            j.h2 = v2.H;
+            j.w2 = v2.W;
+        }
         j.first_block = blocks;
-        blocks += (v.H + j.rows_per_block - 1) / j.rows_per_block;
+        blocks += j.tiles_x * j.tiles_y;
         ing.push_back(j);
     }
     d_ingest_ = to_device(ing);
@@ -201,7 +310,6 @@ void Batch::init(int n, const int* heights, const int* widths, const int* levels
     for (auto& t : tab_) t.reset(new Table);
     check_cuda(cudaFuncSetAttribute(tile_batch_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmemCap),
                "cudaFuncSetAttribute");
-    // full shared carve-out, so the L-2 launch's blocks can share SMs with the top launch's
     check_cuda(cudaFuncSetAttribute(tile_batch_k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     (int)cudaSharedmemCarveoutMaxShared),
                "cudaFuncSetAttribute");
@@ -227,8 +335,6 @@ Batch::~Batch() {
         if (t) release_table(*t);
     if (d_ingest_) cudaFree(d_ingest_);
     if (cap_) cudaStreamDestroy(cap_);
-    for (cudaStream_t q : side_) cudaStreamDestroy(q);
-    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
 }
 
 Filter& Batch::stream(int i) {
@@ -242,10 +348,14 @@ size_t Batch::frame_offset(int i) const {
     return off_[i];
 }
 
+// Phase-B levels (L-2) always stream when the kernel covers them, so only phase A has a tile
+// launch unless a phase-B level has more iterations or smoothing passes than the kernel's 4
 bool Batch::streamed(const Filter& f, int l) const {
     const Level& v = f.level(l);
-    const long min_px = min_px_ >= 0 ? min_px_ : Filter::kFusedMinPixels;
-    return v.item == 1 && (long)v.H * v.W >= min_px && f.streaming_ok(l);
+    const int L = f.levels();
+    const bool late = L >= 2 && l == L - 2;
+    const long min_px = min_px_ >= 0 ? min_px_ : kDefaultTileBelow;
+    return v.item == 1 && (late || (long)v.H * v.W >= min_px) && f.streaming_ok(l);
 }
 
 void Batch::set_tuning(long min_pixels, int band) {
@@ -254,19 +364,23 @@ void Batch::set_tuning(long min_pixels, int band) {
     ++tune_gen_;
 }
 
+void Batch::set_level_band(int height, int width, int band) {
+    if (band > 0) level_band_[{height, width}] = band;
+    else level_band_.erase({height, width});
+    ++tune_gen_;
+}
+
 int Batch::launches_per_step() const {
-    bool tile_a = false, tile_b = false;
-    std::map<std::tuple<int, int, int, int>, int> groups;
+    bool stream_a = false, stream_b = false, tile_a = false, tile_b = false;
     for (auto& f : f_) {
         const int L = f->levels();
         for (int l = 0; l < L; ++l) {
-            const Level& v = f->level(l);
-            const int late = L >= 2 && l == L - 2;
-            if (streamed(*f, l)) groups[{late, v.delta, v.iters, v.smooth}] = 1;
-            else (late ? tile_b : tile_a) = true;
+            const bool late = L >= 2 && l == L - 2;
+            (streamed(*f, l) ? (late ? stream_b : stream_a) : (late ? tile_b : tile_a)) = true;
         }
     }
-    return 1 + (max_levels_ - 1) + (int)tile_a + (int)tile_b + (int)groups.size();
+    // the ingest and pyramid launch, one per pyramid depth beyond 2, one per phase and kernel
+    return 1 + std::max(max_levels_ - 3, 0) + (int)stream_a + (int)stream_b + (int)tile_a + (int)tile_b;
 }
 
 bool Batch::matches(const Table& t) const {
@@ -276,11 +390,19 @@ bool Batch::matches(const Table& t) const {
     return true;
 }
 
+// band rows of a streamed level: its size's override, the batch's band, or the default rule
+int Batch::band_of(const Level& v, int rule_band) const {
+    const auto it = level_band_.find({v.H, v.W});
+    const int b = it != level_band_.end() ? it->second : (band_ > 0 ? band_ : rule_band);
+    return std::min(std::max(b, 8), v.H);
+}
+
 void Batch::build(Table& t) {
     release_table(t);
+    // pyramid depths beyond 2 (levels 1 and 2 come with the ingest launch): one launch each
     std::vector<PyrJob> pyr;
     std::vector<int> pyr_first(max_levels_, 0), pyr_count(max_levels_, 0), pyr_blocks(max_levels_, 0);
-    for (int d = 1; d < max_levels_; ++d) {
+    for (int d = 3; d < max_levels_; ++d) {
         pyr_first[d] = (int)pyr.size();
         int blocks = 0;
         for (auto& f : f_) {
@@ -304,22 +426,14 @@ void Batch::build(Table& t) {
         pyr_count[d] = (int)pyr.size() - pyr_first[d];
         pyr_blocks[d] = blocks;
     }
-    // phase A: top levels and levels 0..L-3; phase B: levels L-2.  Large levels go to the
-    // streaming launches of their phase, the others to the phase's tile launch.
-    std::vector<TileJob> ja, jb;
-    int blocks_a = 0, blocks_b = 0;
-    size_t smem_a = 0, smem_b = 0;
-    StreamGroups groups;
-    std::map<std::tuple<int, int, int, int>, int> group_blocks;
-    // Band rows: every band recomputes (2S + N)-row lead and tail windows, so long bands
-    // waste less, while the streaming branches need enough warps to balance over the SMs.
-    // One band for the step: the longest of 256..32 rows that gives phase A's streaming
-    // levels (phase B's when A has none) kWaves waves of resident warps (fitted to the
-    // 64-stream and single-size 640x480 .. 1920x1080 mixes on B200).
+    // Default band: one for the step, the longest of 256..32 rows that gives phase A's
+    // streamed levels kWaves waves of resident warps (every band recomputes (2S + N)-row
+    // lead and tail windows, so long bands waste less, while the phase needs enough warps to
+    // balance over the SMs).  Sizes with an override (set_level_band) keep theirs.
     constexpr int kBands[] = {256, 128, 64, 32};
     constexpr double kWaves = 3.5;
-    int band = band_;
-    if (band <= 0) {
+    int rule = 32;
+    {
         const double resident = (double)fused_resident_warps();
         auto warps_at = [&](int phase, int b) {
             long warps = 0;
@@ -329,83 +443,77 @@ void Batch::build(Table& t) {
                     if ((L >= 2 && l == L - 2) != (phase == 1) || !streamed(*f, l)) continue;
                     const Level& v = f->level(l);
                     int nwx = 0, nby = 0;
-                    fused_warp_grid(v.iters, v.smooth, v.W, v.H, b, &nwx, &nby);
+                    fused_warp_grid(v.iters, v.smooth, v.W, v.H, std::min(std::max(b, 8), v.H), &nwx, &nby);
                     warps += (long)nwx * nby;
                 }
             }
             return warps;
         };
         const int phase = warps_at(0, 8) > 0 ? 0 : 1;
-        band = 32;
         for (int b : kBands)
             if (warps_at(phase, b) >= kWaves * resident) {
-                band = b;
+                rule = b;
                 break;
             }
     }
-    // which launch of phase A holds each stream's top level (a group key, or the tile
-    // launch), and the streams of each phase-B launch: a phase-B launch waits only for the
-    // phase-A launches holding its streams' top levels
-    std::vector<std::tuple<int, int, int, int>> top_key(f_.size());
-    std::vector<char> top_tiled(f_.size(), 0);
-    std::map<std::tuple<int, int, int, int>, std::vector<int>> group_streams;
-    std::vector<int> jb_streams;
-    for (size_t si = 0; si < f_.size(); ++si) {
-        Filter* f = f_[si].get();
+    // phase A: top levels and levels 0..L-3 (they read the previous frame's coarse flow);
+    // phase B: levels L-2 (they read this frame's top-level flow).  Streamed levels go to the
+    // phase's streaming launch, the others to its tile launch.
+    std::vector<StreamJob> sj[2];
+    std::vector<TileJob> tj[2];
+    int sblocks[2] = {0, 0}, ssmem[2] = {0, 0}, tblocks[2] = {0, 0};
+    size_t tsmem[2] = {0, 0};
+    for (auto& fp : f_) {
+        Filter* f = fp.get();
         const int L = f->levels();
         for (int l = 0; l < L; ++l) {
             const Level& v = f->level(l);
-            const std::tuple<int, int, int, int> key{L >= 2 && l == L - 2, v.delta, v.iters, v.smooth};
-            if (l == L - 1) {
-                top_key[si] = key;
-                top_tiled[si] = !streamed(*f, l);
-            }
+            const int ph = L >= 2 && l == L - 2 ? 1 : 0;
             if (streamed(*f, l)) {
-                group_streams[key].push_back((int)si);
                 StreamJob j{};
                 j.a = f->level_args(l);
-                j.band = std::min(std::max(band, 8), v.H);
-                int& blocks = group_blocks[key];
-                j.first_block = blocks;
-                blocks += fused_warp_grid(v.iters, v.smooth, v.W, v.H, j.band, &j.nwx, &j.nby);
-                groups[key].push_back(j);
+                j.band = band_of(v, rule);
+                j.kind = stream_kind(v.delta, v.iters, v.smooth);
+                j.first_block = sblocks[ph];
+                sblocks[ph] += fused_warp_grid(v.iters, v.smooth, v.W, v.H, j.band, &j.nwx, &j.nby);
+                ssmem[ph] = std::max(ssmem[ph], stream_block_smem(v.delta, v.smooth));
+                sj[ph].push_back(j);
                 continue;
             }
             TileJob j{};
             j.a = f->level_args(l);
+            j.a.pdl_late_wait = 0;
+            j.a.pdl_early_trigger = 0;
             j.delta = v.delta ? 1 : 0;
             size_t smem = 0;
             j.g = batch_geom(v.delta, v.iters, v.smooth, v.W, v.H, &smem);
-            const int tiles = j.g.tiles_x * ((v.H + j.g.TH - 1) / j.g.TH);
-            const bool late = L >= 2 && l == L - 2;
-            // the tile launch of phase B follows that of phase A on one stream: its jobs wait
-            // for it only before their update, and A lets B's blocks start at once
-            j.a.pdl_late_wait = late ? 1 : 0;
-            j.a.pdl_early_trigger = late ? 0 : 1;
-            if (late) {
-                jb_streams.push_back((int)si);
-                j.first_block = blocks_b;
-                blocks_b += tiles;
-                smem_b = std::max(smem_b, smem);
-                jb.push_back(j);
-            } else {
-                j.first_block = blocks_a;
-                blocks_a += tiles;
-                smem_a = std::max(smem_a, smem);
-                ja.push_back(j);
-            }
+            j.first_block = tblocks[ph];
+            tblocks[ph] += j.g.tiles_x * ((v.H + j.g.TH - 1) / j.g.TH);
+            tsmem[ph] = std::max(tsmem[ph], smem);
+            tj[ph].push_back(j);
         }
     }
-    std::vector<TileJob> all(ja);
-    all.insert(all.end(), jb.begin(), jb.end());
-    std::vector<StreamJob> sall;
-    std::vector<size_t> sfirst;
-    for (auto& kv : groups) {
-        sfirst.push_back(sall.size());
-        sall.insert(sall.end(), kv.second.begin(), kv.second.end());
+    // longest warps first: blocks start in index order, so the phase's tail is short warps
+    // (a warp's time ~ its pipeline rows x the stages per row)
+    for (auto& v : sj) {
+        auto cost = [&](const StreamJob& j) {
+            const int N = ((j.kind >> 2) & 3) + 1, S = (j.kind & 3) + 1;
+            return (long)(j.band + 2 * N + 4 * S) * (2 * N + 2 * S + 4);
+        };
+        std::stable_sort(v.begin(), v.end(), [&](const StreamJob& x, const StreamJob& y) { return cost(x) > cost(y); });
+        int blocks = 0;
+        for (auto& j : v) {
+            j.first_block = blocks;
+            int nwx = 0, nby = 0;
+            blocks += fused_warp_grid(((j.kind >> 2) & 3) + 1, (j.kind & 3) + 1, j.a.W, j.a.H, j.band, &nwx, &nby);
+        }
     }
+    std::vector<StreamJob> sall(sj[0]);
+    sall.insert(sall.end(), sj[1].begin(), sj[1].end());
+    std::vector<TileJob> tall(tj[0]);
+    tall.insert(tall.end(), tj[1].begin(), tj[1].end());
     t.d_pyr = to_device(pyr);
-    t.d_tile = to_device(all);
+    t.d_tile = to_device(tall);
     t.d_stream = to_device(sall);
     t.parity.clear();
     t.gen.clear();
@@ -414,92 +522,50 @@ void Batch::build(Table& t) {
         t.gen.push_back(f->config_generation());
     }
     t.tune_gen = tune_gen_;
-    const int ngroups = (int)groups.size();
-    while ((int)side_.size() < ngroups) {
-        cudaStream_t q = nullptr;
-        check_cuda(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "cudaStreamCreate");
-        side_.push_back(q);
-    }
-    while ((int)ev_.size() < 2 + ngroups) {
-        cudaEvent_t ev = nullptr;
-        check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
-        ev_.push_back(ev);
-    }
-    // phase-A launches each phase-B launch waits for (-1: the tile launch)
-    std::map<std::tuple<int, int, int, int>, int> gindex;
-    for (auto& kv : groups) {
-        const int i = (int)gindex.size();
-        gindex[kv.first] = i;
-    }
-    auto deps_of = [&](const std::vector<int>& streams) {
-        std::vector<int> d;
-        for (int si : streams) {
-            const int k = top_tiled[si] ? -1 : gindex.at(top_key[si]);
-            if (std::find(d.begin(), d.end(), k) == d.end()) d.push_back(k);
-        }
-        return d;
-    };
-    // capture: pyramid depths; phase A: the tile launch on the capture stream and each
-    // streaming group on a branch forked after the pyramid; phase B: the tile launch on the
-    // capture stream after phase A's tile launch, and each streaming group on a branch; a
-    // phase-B launch waits for the phase-A launches holding its streams' top levels; join
+    // capture: the deeper pyramid depths, then per phase its streaming launch and its tile
+    // launch, all on one stream (each launch waits for the previous one)
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t e = cudaSuccess;
     auto ok = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
     };
-    for (int d = 1; d < max_levels_; ++d)
-        if (pyr_count[d] > 0)
+    int launches = 0;
+    for (int d = 3; d < max_levels_; ++d)
+        if (pyr_count[d] > 0) {
             ok(launch_k(pyramid_batch_k, dim3(pyr_blocks[d]), dim3(256), 0, cap_,
                         (const PyrJob*)(t.d_pyr + pyr_first[d]), pyr_count[d]));
-    ok(cudaEventRecord(ev_[0], cap_));
-    auto branch = [&](int i, const std::tuple<int, int, int, int>& key, const std::vector<StreamJob>& jobs) {
-        ok(launch_fused_batch(std::get<1>(key) != 0, std::get<2>(key), std::get<3>(key), t.d_stream + sfirst[i],
-                              (int)jobs.size(), group_blocks.at(key), side_[i]));
-        ok(cudaEventRecord(ev_[2 + i], side_[i]));
-    };
-    for (auto& kv : groups) {
-        const int i = gindex[kv.first];
-        if (std::get<0>(kv.first) != 0) continue;
-        ok(cudaStreamWaitEvent(side_[i], ev_[0], 0));
-        branch(i, kv.first, kv.second);
+            ++launches;
+        }
+    for (int ph = 0; ph < 2; ++ph) {
+        if (!sj[ph].empty()) {
+            ok(launch_stream_mega(t.d_stream + (ph ? sj[0].size() : 0), (int)sj[ph].size(), sblocks[ph], ssmem[ph],
+                                  cap_));
+            ++launches;
+        }
+        if (!tj[ph].empty()) {
+            ok(launch_k(tile_batch_k, dim3(tblocks[ph]), dim3(kTileThreads), tsmem[ph], cap_,
+                        (const TileJob*)(t.d_tile + (ph ? tj[0].size() : 0)), (int)tj[ph].size()));
+            ++launches;
+        }
     }
-    if (!ja.empty())
-        ok(launch_k(tile_batch_k, dim3(blocks_a), dim3(kTileThreads), smem_a, cap_, (const TileJob*)t.d_tile,
-                    (int)ja.size()));
-    ok(cudaEventRecord(ev_[1], cap_));  // phase A's tile launch (or the pyramid) done
-    for (auto& kv : groups) {
-        const int i = gindex[kv.first];
-        if (std::get<0>(kv.first) != 1) continue;
-        ok(cudaStreamWaitEvent(side_[i], ev_[1], 0));
-        for (int k : deps_of(group_streams.at(kv.first)))
-            if (k >= 0) ok(cudaStreamWaitEvent(side_[i], ev_[2 + k], 0));
-        branch(i, kv.first, kv.second);
-    }
-    if (!jb.empty()) {
-        for (int k : deps_of(jb_streams))
-            if (k >= 0) ok(cudaStreamWaitEvent(cap_, ev_[2 + k], 0));
-        ok(launch_k(tile_batch_k, dim3(blocks_b), dim3(kTileThreads), smem_b, cap_,
-                    (const TileJob*)(t.d_tile + ja.size()), (int)jb.size()));
-    }
-    for (int i = 0; i < ngroups; ++i) ok(cudaStreamWaitEvent(cap_, ev_[2 + i], 0));
     cudaError_t ec = cudaStreamEndCapture(cap_, &g);
     check_cuda(e, "batch capture");
     check_cuda(ec, "cudaStreamEndCapture");
     e = cudaGraphInstantiateWithFlags(&t.graph, g, 0);
     cudaGraphDestroy(g);
     check_cuda(e, "cudaGraphInstantiate");
+    t.launches = launches;
     log_message(FF_LOG_INFO, "batch: step graph built for " + std::to_string(f_.size()) + " streams, " +
-                                 std::to_string(launches_per_step()) + " launches, streaming band " +
-                                 std::to_string(band) + " rows");
+                                 std::to_string(1 + launches) + " launches, default streaming band " +
+                                 std::to_string(rule) + " rows");
 }
 
 void Batch::step(const void* frames, cudaStream_t s) {
     if (!frames) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: null frame buffer");
     if ((uintptr_t)frames % 16) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: the frame buffer must be 16-byte aligned");
     for (auto& f : f_) f->batch_begin(s);
-    check_cuda(launch_k(ingest_k, dim3(ingest_blocks_), dim3(256), 0, s, (const uint8_t*)frames,
+    check_cuda(launch_k(ingest_pyr_k, dim3(ingest_blocks_), dim3(32, 8), 0, s, (const uint8_t*)frames,
                         (const IngestJob*)d_ingest_, size()),
                "batch ingest");
     bool first = false;

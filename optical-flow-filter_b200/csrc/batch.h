@@ -2,26 +2,29 @@
 //
 // A Batch owns one pyramidal Filter per stream; streams differ in size, levels and
 // parameters.  One step advances every stream by one frame with a number of kernel launches
-// that does not grow with the number of streams:
+// that does not grow with the number of streams nor with their parameters:
 //
-//   ingest      one kernel copies every stream's frame out of one packed device buffer
-//   pyramid     one launch per pyramid depth, over all streams that have that level
-//   levels A    every top level and every delta level that reads the previous frame's
-//               coarse flow (levels 0..L-3)
-//   levels B    the levels L-2, which read this frame's unsmoothed top-level flow
+//   ingest      one kernel copies every stream's frame out of one packed device buffer into
+//               its level-0 image and builds pyramid levels 1 and 2 from it
+//   (deeper pyramid levels, when a stream has more than 3: one launch per depth)
+//   levels A    one streaming-kernel launch over every top level and every delta level that
+//               reads the previous frame's coarse flow (levels 0..L-3)
+//   levels B    one streaming-kernel launch over the levels L-2, which read this frame's
+//               unsmoothed top-level flow
 //
-// In each phase the small levels go to one tile-fused launch, and the large ones (as
-// large as the levels a single filter streams) to one streaming-kernel launch per
-// (delta, propagation iterations, smoothing iterations) group; the launches of a phase
-// are branches of the step graph that run side by side.  Each batched launch walks a
-// device table of jobs (one per stream-level), each job a contiguous range of CTAs.  The
-// pyramid and level launches of a step are replayed from a CUDA graph.  Every stream's
-// results are those of the same stream filtered alone.
+// A phase launch walks a device table of jobs (one per stream-level), each job a contiguous
+// range of blocks running the instantiation of the streaming kernel for its (delta,
+// iterations, smoothing) (level_mega.cu).  Levels the streaming kernel does not cover (more
+// than 4 iterations or smoothing passes) go to one tile-kernel launch per phase.  The phase
+// launches of a step are replayed from a CUDA graph.  Every stream's results are those of the
+// same stream filtered alone, whatever the tuning.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "filter.h"
@@ -48,10 +51,13 @@ public:
     int launches_per_step() const;
     // advance every stream by one frame read from `frames` (frame_bytes() bytes on the device)
     void step(const void* frames, cudaStream_t s);
-    // levels of at least min_pixels pixels (< 0: the single filter's threshold) run the
-    // streaming kernel in bands of `band` rows (<= 0: chosen per phase); the others the
-    // tile kernel
+    // phase-A levels of fewer than min_pixels pixels (< 0: kDefaultTileBelow) run the tile
+    // kernel, every other level the streaming kernel covers runs it, in bands of `band` rows
+    // (<= 0: chosen per step)
     void set_tuning(long min_pixels, int band);
+    static constexpr long kDefaultTileBelow = 200000;
+    // levels of height x width pixels run in bands of `band` rows (<= 0: no override)
+    void set_level_band(int height, int width, int band);
 
 private:
     struct Table;
@@ -60,6 +66,7 @@ private:
     bool matches(const Table& t) const;
     void release_table(Table& t);
     bool streamed(const Filter& f, int l) const;
+    int band_of(const Level& v, int rule_band) const;
 
     std::vector<std::unique_ptr<Filter>> f_;
     std::vector<size_t> off_;
@@ -71,9 +78,8 @@ private:
     int max_levels_ = 0;
     long min_px_ = -1;
     int band_ = 0;
+    std::map<std::pair<int, int>, int> level_band_;  // (height, width) -> band rows
     unsigned long long tune_gen_ = 0;
-    std::vector<cudaStream_t> side_;  // capture branches of the streaming launches
-    std::vector<cudaEvent_t> ev_;     // fork and join events of those branches
 };
 
 }  // namespace ffb

@@ -731,6 +731,14 @@ ff_status ff_batch_set_tuning(ff_batch* b, long long min_pixels, int band) {
     });
 }
 
+ff_status ff_batch_set_level_band(ff_batch* b, int height, int width, int band) {
+    return guard([&] {
+        need(b, "batch");
+        if (height <= 0 || width <= 0) throw ffb::Error(FF_ERR_INVALID_ARGUMENT, "batch: level size must be positive");
+        b->impl->set_level_band(height, width, band);
+    });
+}
+
 ff_status ff_batch_step(ff_batch* b, const void* frames, void* stream) {
     return guard([&] {
         need(b, "batch");

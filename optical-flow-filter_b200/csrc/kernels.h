@@ -75,14 +75,18 @@ struct StreamJob {
     LevelArgs a;
     int nwx, nby, band;
     int first_block;
+    int kind;  // stream_kind(delta, N, S): the instantiation the phase kernel runs
 };
 // the warp grid of a level of W x H pixels cut into bands of `band` rows; returns the
 // blocks it takes
 int fused_warp_grid(int N, int S, int W, int H, int band, int* nwx, int* nby);
 // warps of the streaming kernel resident on the current device at once
 int fused_resident_warps();
-// one launch over jobs (blocks in total) that share (delta, N, S)
-cudaError_t launch_fused_batch(bool delta, int N, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
+// one launch over jobs of any (delta, N, S) (level_mega.cu): StreamJob::kind selects each
+// job's instantiation; smem = the largest stream_block_smem of the jobs
+int stream_kind(bool delta, int N, int S);
+int stream_block_smem(bool delta, int S);
+cudaError_t launch_stream_mega(const StreamJob* jobs, int n, int blocks, int smem, cudaStream_t s);
 
 // ---- tile-fused per-level kernels (tile_level.cu); cfg 0 = automatic tile shape
 int tile_config_count();

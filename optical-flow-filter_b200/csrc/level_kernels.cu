@@ -7,10 +7,6 @@ cudaError_t launch_level_n1(bool delta, int item, int S, const LevelArgs& a, cud
 cudaError_t launch_level_n2(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
 cudaError_t launch_level_n3(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
 cudaError_t launch_level_n4(bool delta, int item, int S, const LevelArgs& a, cudaStream_t s);
-cudaError_t launch_level_batch_n1(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
-cudaError_t launch_level_batch_n2(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
-cudaError_t launch_level_batch_n3(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
-cudaError_t launch_level_batch_n4(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s);
 
 // instantiated: propagation iterations 1..4, smoothing iterations 1..4; delta levels on
 // uint8 images, top levels on uint8 or float images.  Other combinations run the
@@ -45,16 +41,6 @@ int fused_resident_warps() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return (sms > 0 ? sms : 148) * lvl::kBlocksPerSM * lvl::kWarpsPerBlock;
-}
-
-cudaError_t launch_fused_batch(bool delta, int N, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
-    switch (N) {
-        case 1: return launch_level_batch_n1(delta, S, jobs, n, blocks, s);
-        case 2: return launch_level_batch_n2(delta, S, jobs, n, blocks, s);
-        case 3: return launch_level_batch_n3(delta, S, jobs, n, blocks, s);
-        case 4: return launch_level_batch_n4(delta, S, jobs, n, blocks, s);
-    }
-    return cudaErrorNotSupported;
 }
 
 }  // namespace ffb

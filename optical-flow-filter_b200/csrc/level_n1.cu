@@ -31,15 +31,4 @@ cudaError_t launch_level_n1(bool delta, int item, int S, const LevelArgs& a, cud
     return cudaErrorNotSupported;
 }
 
-cudaError_t launch_level_batch_n1(bool delta, int S, const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
-    using lvl::launch_batch;
-    switch (S) {
-        case 1: return delta ? launch_batch<true, 1, 1>(jobs, n, blocks, s) : launch_batch<false, 1, 1>(jobs, n, blocks, s);
-        case 2: return delta ? launch_batch<true, 1, 2>(jobs, n, blocks, s) : launch_batch<false, 1, 2>(jobs, n, blocks, s);
-        case 3: return delta ? launch_batch<true, 1, 3>(jobs, n, blocks, s) : launch_batch<false, 1, 3>(jobs, n, blocks, s);
-        case 4: return delta ? launch_batch<true, 1, 4>(jobs, n, blocks, s) : launch_batch<false, 1, 4>(jobs, n, blocks, s);
-    }
-    return cudaErrorNotSupported;
-}
-
 }  // namespace ffb

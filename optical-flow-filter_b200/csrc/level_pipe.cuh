@@ -763,43 +763,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM) level_k(Lev
     level_warp<DELTA, N, S, P>(a, nwx, band, blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5));
 }
 
-// many levels of one (DELTA, N, S) in one launch: each job a contiguous range of blocks
-// (jobs sorted by first_block, the first at 0; a block never spans two jobs)
-template <bool DELTA, int N, int S>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSM)
-    level_batch_k(const StreamJob* __restrict__ jobs, int n) {
-    grid_dep_wait();
-    grid_dep_launch();
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].first_block <= (int)blockIdx.x) lo = mid;
-        else hi = mid - 1;
-    }
-    const StreamJob& j = jobs[lo];
-    level_warp<DELTA, N, S, uint8_t>(j.a, j.nwx, j.band,
-                                     ((int)blockIdx.x - j.first_block) * kWarpsPerBlock + (threadIdx.x >> 5));
-}
-
-template <bool DELTA, int N, int S>
-cudaError_t launch_batch(const StreamJob* jobs, int n, int blocks, cudaStream_t s) {
-    const int smem = kWarpsPerBlock * WarpMem<DELTA, S>::BYTES;
-    static std::atomic<unsigned long long> prepared{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(prepared.load() & bit)) {
-        cudaError_t e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>,
-                                             cudaFuncAttributePreferredSharedMemoryCarveout,
-                                             (int)cudaSharedmemCarveoutMaxShared);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(level_batch_k<DELTA, N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        prepared.fetch_or(bit);
-    }
-    return launch_k(level_batch_k<DELTA, N, S>, dim3(blocks), dim3(kWarpsPerBlock * 32), smem, s, jobs, n);
-}
-
 template <bool DELTA, int N, int S, typename P>
 cudaError_t launch(const LevelArgs& a, cudaStream_t s) {
     constexpr int HX = halo_x(N, S);

@@ -148,6 +148,7 @@ SIGNATURES = {
     "ff_batch_step": (_st, [_vp, _vp, _vp]),
     "ff_debug_fail_allocation_after": (_st, [ctypes.c_longlong]),
     "ff_batch_set_tuning": (_st, [_vp, ctypes.c_longlong, _i]),
+    "ff_batch_set_level_band": (_st, [_vp, _i, _i, _i]),
     "ff_diff_pyramid": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),
     "ff_diff_pyramid_bwd": (_st, [_i, _i, _i, _i, _vp, _vp, _vp]),
     "ff_diff_model": (_st, [_i, _i, _i, _i, _vp, _vp, _vp, _vp]),

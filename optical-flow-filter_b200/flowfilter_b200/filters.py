@@ -612,9 +612,97 @@ class BatchFlowFilter:
         return n.value
 
     def setTuning(self, minPixels: int = -1, band: int = 0) -> None:
-        """Levels of at least ``minPixels`` pixels run the streaming level kernel in bands of
-        ``band`` rows, the others the tile kernel (-1 / 0: defaults).  Results are unchanged."""
+        """Top levels and levels reading the previous frame's coarse flow (phase A) below
+        ``minPixels`` pixels run the tile kernel (-1: 200000), every other level the streaming
+        kernel covers runs it in bands of ``band`` rows (0: the default rule).  Results are
+        unchanged."""
         call("ff_batch_set_tuning", self._h, int(minPixels), int(band))
+
+    def setLevelBand(self, height: int, width: int, band: int) -> None:
+        """Levels of ``height`` x ``width`` pixels run in bands of ``band`` rows (0: no
+        override).  Results are unchanged."""
+        call("ff_batch_set_level_band", self._h, int(height), int(width), int(band))
+
+    def levelSizes(self) -> list:
+        """Distinct (height, width) of the streams' pyramid levels, largest first."""
+        sizes = set()
+        for hh, ww, L in self.shapes:
+            for l in range(L):
+                sizes.add((hh >> l, ww >> l))
+        return sorted(sizes, key=lambda s: (-s[0] * s[1], s))
+
+    def _signature(self) -> str:
+        import hashlib
+        import json
+
+        streams = [[list(sh), st.gamma, st.smoothIterations, st.maxflow, st.propagationBorder]
+                   for sh, st in zip(self.shapes, self._streams)]
+        return hashlib.sha256(json.dumps(streams).encode()).hexdigest()
+
+    def autotune(self, frames, repetitions: int = 3, cache: str | None = None,
+                 bands=(8, 12, 16, 24, 32, 48, 64, 96, 128)) -> dict:
+        """Picks the streaming kernel's band rows per level size by timing: a scratch batch
+        with this batch's streams and parameters steps on ``frames`` (a packed step buffer,
+        see pack()); level sizes are tuned one at a time, largest first, each keeping the band
+        whose step is fastest (median of ``repetitions`` CUDA-event-timed steps) with the
+        sizes before it fixed.  The choice is applied here (setLevelBand) and returned as
+        {"HxW": band}.  With ``cache`` (a JSON file), a choice stored for the same streams and
+        parameters is applied without timing, and a new one is stored.  This batch's streams
+        are not stepped, and results do not depend on the choice."""
+        import json
+        import os
+
+        torch = _torch()
+        key = self._signature()
+        store = {}
+        if cache and os.path.exists(cache):
+            with open(cache) as fh:
+                store = json.load(fh)
+            if key in store:
+                choice = store[key]
+                for name, b in choice.items():
+                    hh, ww = (int(v) for v in name.split("x"))
+                    self.setLevelBand(hh, ww, b)
+                return choice
+        scratch = BatchFlowFilter(self.shapes)
+        for st, mine in zip(scratch._streams, self._streams):
+            st.gamma = mine.gamma
+            st.smoothIterations = mine.smoothIterations
+            st.maxflow = mine.maxflow
+            st.propagationBorder = mine.propagationBorder
+        scratch.step(frames)  # the first frame runs each stream on its own
+
+        def step_ms():
+            scratch.step(frames)  # rebuilds the step graph after a band change
+            ms = []
+            for _ in range(max(1, int(repetitions))):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                scratch.step(frames)
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return sorted(ms)[len(ms) // 2]
+
+        choice = {}
+        for hh, ww in self.levelSizes():
+            best = None
+            for b in sorted({min(int(v), hh) for v in bands if v > 0}):
+                scratch.setLevelBand(hh, ww, b)
+                t = step_ms()
+                if best is None or t < best[0]:
+                    best = (t, b)
+            scratch.setLevelBand(hh, ww, best[1])
+            choice[f"{hh}x{ww}"] = best[1]
+        del scratch
+        for name, b in choice.items():
+            hh, ww = (int(v) for v in name.split("x"))
+            self.setLevelBand(hh, ww, b)
+        if cache:
+            store[key] = choice
+            with open(cache, "w") as fh:
+                json.dump(store, fh, indent=1, sort_keys=True)
+        return choice
 
     def pack(self, frames, out=None):
         """Pack one (H, W) uint8 CUDA tensor per stream into a step buffer (device copies)."""

@@ -37,10 +37,12 @@ def ffb(cuda):
     return flowfilter_b200
 
 
-def run_against_alone(ffb, cuda, streams, t_frames=8, tuning=None, retune=None, launches=None):
+def run_against_alone(ffb, cuda, streams, t_frames=8, tuning=None, retune=None, launches=None, level_bands=(),
+                      prepare=None):
     """Steps a batch of `streams` and the same streams as single filters over seeded frames
     and asserts identical flow and image every frame.  tuning / retune: setTuning arguments
-    before the first frame / from frame 3 on."""
+    before the first frame / from frame 3 on; level_bands: setLevelBand arguments from frame
+    2 on; prepare(batch, step_buffer): called before the first frame."""
     seqs = [case_frames(dict(seq="bumps", frames=t_frames, kw=dict(height=s[0], width=s[1], sigma=1.0, seed=11 + i,
                                                                     n_bumps=2, bump_sigma=max(s[0], s[1]) / 3,
                                                                     amp=2.0)))
@@ -56,7 +58,13 @@ def run_against_alone(ffb, cuda, streams, t_frames=8, tuning=None, retune=None, 
         launches(batch.launches())
     dev = [cuda.from_numpy(q).cuda() for q in seqs]
     buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
+    if prepare is not None:
+        batch.pack([d[0] for d in dev], out=buf)
+        prepare(batch, buf)
     for t in range(t_frames):
+        if t == 2:
+            for lb in level_bands:
+                batch.setLevelBand(*lb)
         if t == 3 and retune is not None:
             batch.setTuning(*retune)
         if t == 5:  # a parameter change rebuilds the batch's job tables
@@ -77,7 +85,11 @@ def run_against_alone(ffb, cuda, streams, t_frames=8, tuning=None, retune=None, 
 
 def test_batch_matches_streams_alone(ffb, cuda):
     def launches(n):
-        assert n == 1 + (4 - 1) + 2  # ingest, 3 pyramid depths, the two tile launches
+        # ingest with pyramid levels 1-2, pyramid depth 3, phase A's tile launch (its levels
+        # are all below 200000 pixels), phase B's streaming launch and its tile launch (level 0
+        # of the 2-level 120x160 stream has 6 propagation iterations, beyond the streaming
+        # kernel's 4)
+        assert n == 1 + 1 + 1 + 2
 
     run_against_alone(ffb, cuda, STREAMS, launches=launches)
 
@@ -88,7 +100,35 @@ def test_batch_streaming_launches_match_streams_alone(ffb, cuda):
     (band seams)."""
     seen = []
     run_against_alone(ffb, cuda, STREAMS, tuning=(0, 0), retune=(0, 8), launches=seen.append)
-    assert seen[0] > 1 + (4 - 1) + 2
+    assert seen[0] == 1 + 1 + 2 + 2  # both phases stream, and tile what has 6 or 8 iterations
+
+
+def test_batch_level_bands_match_streams_alone(ffb, cuda):
+    """Per-size band overrides (the autotuner's knob) from frame 2 on: 8-row bands at the
+    96x128 and 130x130 level-0 sizes, 12 rows at 60x80, the default elsewhere."""
+    run_against_alone(ffb, cuda, STREAMS, level_bands=[(96, 128, 8), (130, 130, 8), (60, 80, 12), (61, 77, 0)])
+
+
+def test_batch_autotune_keeps_results_and_caches(ffb, cuda, tmp_path):
+    """autotune() times a scratch batch (this batch is not stepped), applies one band per
+    level size, stores the choice in the JSON cache and reapplies it from there; the batch
+    still gives every stream's results alone."""
+    cache = str(tmp_path / "bands.json")
+    chosen = []
+
+    def prepare(batch, buf):
+        choice = batch.autotune(buf, repetitions=1, cache=cache, bands=(8, 16, 32))
+        assert set(choice) == {f"{h}x{w}" for h, w in batch.levelSizes()}
+        assert all(1 <= b <= int(k.split("x")[0]) for k, b in choice.items())
+        again = batch.autotune(buf, repetitions=1, cache=cache)
+        assert again == choice
+        chosen.append(choice)
+
+    run_against_alone(ffb, cuda, STREAMS[:4], t_frames=5, prepare=prepare)
+    import json
+
+    with open(cache) as fh:
+        assert list(json.load(fh).values()) == chosen
 
 
 def test_batch_mixed_kernels_match_streams_alone(ffb, cuda):
@@ -99,8 +139,8 @@ def test_batch_mixed_kernels_match_streams_alone(ffb, cuda):
 
 
 def test_batch_default_selection_streams_large_levels(ffb, cuda):
-    """Levels as large as the ones a single filter streams take the streaming launches by
-    default, beside small streams in the tile launches."""
+    """By default phase-A levels of 200000 pixels or more and every phase-B level stream, the
+    small phase-A levels tile: four launches."""
     streams = [
         (480, 640, 2, [10.0, 50.0], [2, 4], 4.0, 3),
         (544, 960, 1, [20.0], [3], 4.0, 3),
@@ -110,7 +150,7 @@ def test_batch_default_selection_streams_large_levels(ffb, cuda):
     ]
     seen = []
     run_against_alone(ffb, cuda, streams, t_frames=6, launches=seen.append)
-    assert seen[0] > 1 + (3 - 1) + 2
+    assert seen[0] == 4  # ingest with pyramid, a streaming launch per phase, phase A's tiles
 
 
 def test_batch_frame_layout_and_errors(ffb, cuda):
@@ -133,7 +173,8 @@ def test_sixty_four_stream_mix_matches_streams_alone(ffb, cuda):
     """The benchmark's 64-stream mix (16 each at 320x240, 640x480, 1280x720, 1920x1080; levels,
     gamma and smoothing seeded per stream; stream i's frames from seed 100 + i) at the default
     kernel selection: every stream bit for bit equal to the same stream filtered alone, over
-    four frames.  Its large levels run the batched streaming kernel at the batch's own bands."""
+    four frames, in four launches: the large levels in the streaming launches at the batch's
+    own bands, the small phase-A levels in the tile launch."""
     import bench
 
     streams = bench.batched_streams()
@@ -146,7 +187,7 @@ def test_sixty_four_stream_mix_matches_streams_alone(ffb, cuda):
         bench.configure_stream(f, s)
         bench.configure_stream(batch.stream(i), s)
         alone.append(f)
-    assert batch.launches() > 1 + 2 + 2  # streaming launches are in the step
+    assert batch.launches() == 4  # ingest with pyramid, a streaming launch per phase, phase A's tiles
     dev = [cuda.from_numpy(q).cuda() for q in seqs]
     buf = cuda.empty(batch.frameBytes(), dtype=cuda.uint8, device="cuda")
     for t in range(4):
