@@ -459,7 +459,7 @@ def bench_batched(steps, warmup):
 
     b0_ms = timed(lambda t: batch.step(packed[t % BATCH_RING]))  # the default band rule
     t0 = time.perf_counter()
-    bands = batch.autotune(packed[0], repetitions=3)  # per level size, on a scratch batch
+    bands = batch.autotune(packed[0], repetitions=5)  # per level size, on a scratch batch
     tune_s = time.perf_counter() - t0
     b_ms = timed(lambda t: batch.step(packed[t % BATCH_RING]))
     loop = []
@@ -486,7 +486,8 @@ def bench_batched(steps, warmup):
         "launches_per_step": batch.launches(),
         "autotune": {"bands": bands, "seconds": tune_s, "default_bands_ms_per_step": b0_ms / steps,
                      "method": "BatchFlowFilter.autotune: band rows per level size, largest first, each the "
-                               "fastest of 8..128 rows by CUDA-event-timed steps of a scratch batch"},
+                               "fastest of the default rule (0) and 8..128 rows by CUDA-event-timed "
+                               "steps of a scratch batch"},
         "loop_value": n * steps / (l_ms / 1e3), "loop_ms_per_step": l_ms / steps,
         "speedup_vs_loop": l_ms / b_ms,
         "data": "synthetic: stream i is a seeded bump-flow sequence of its size from seed 100 + i",

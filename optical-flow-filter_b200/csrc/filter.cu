@@ -864,12 +864,20 @@ void Filter::autotune(int reps, void* flush, size_t flush_bytes) {
             while (l < L_ && ++idx[l] == cand[l].size()) idx[l++] = 0;
             if (l == L_) break;
         }
-        // the four best again, over three times the frames
+        // the six best again, in five interleaved rounds (clock or thermal drift during the
+        // rounds then touches every finalist alike); a finalist's score is the median of its
+        // rounds' medians
         std::sort(scored.begin(), scored.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        const size_t K = std::min<size_t>(scored.size(), 6);
+        constexpr int kRounds = 5;
+        std::vector<std::vector<float>> rounds(K);
+        for (int r = 0; r < kRounds; ++r)
+            for (size_t k = 0; k < K; ++k) rounds[k].push_back(score(scored[k].second, frames));
         std::vector<size_t> best_idx = scored[0].second;
         float best_ms = -1.f;
-        for (size_t k = 0; k < scored.size() && k < 4; ++k) {
-            const float ms = score(scored[k].second, 3 * frames);
+        for (size_t k = 0; k < K; ++k) {
+            std::nth_element(rounds[k].begin(), rounds[k].begin() + kRounds / 2, rounds[k].end());
+            const float ms = rounds[k][kRounds / 2];
             if (best_ms < 0.f || ms < best_ms) {
                 best_ms = ms;
                 best_idx = scored[k].second;

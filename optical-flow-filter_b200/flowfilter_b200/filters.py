@@ -645,8 +645,8 @@ class BatchFlowFilter:
         with this batch's streams and parameters steps on ``frames`` (a packed step buffer,
         see pack()); level sizes are tuned one at a time, largest first, each keeping the band
         whose step is fastest (median of ``repetitions`` CUDA-event-timed steps) with the
-        sizes before it fixed.  The choice is applied here (setLevelBand) and returned as
-        {"HxW": band}.  With ``cache`` (a JSON file), a choice stored for the same streams and
+        sizes before it fixed (0: the batch's default rule stays).  The choice is applied
+        here (setLevelBand) and returned as {"HxW": band}.  With ``cache`` (a JSON file), a choice stored for the same streams and
         parameters is applied without timing, and a new one is stored.  This batch's streams
         are not stepped, and results do not depend on the choice."""
         import json
@@ -687,7 +687,8 @@ class BatchFlowFilter:
         choice = {}
         for hh, ww in self.levelSizes():
             best = None
-            for b in sorted({min(int(v), hh) for v in bands if v > 0}):
+            # 0: the batch's own band rule (no override), kept unless a band beats it
+            for b in [0] + sorted({min(int(v), hh) for v in bands if v > 0}):
                 scratch.setLevelBand(hh, ww, b)
                 t = step_ms()
                 if best is None or t < best[0]:

@@ -119,7 +119,7 @@ def test_batch_autotune_keeps_results_and_caches(ffb, cuda, tmp_path):
     def prepare(batch, buf):
         choice = batch.autotune(buf, repetitions=1, cache=cache, bands=(8, 16, 32))
         assert set(choice) == {f"{h}x{w}" for h, w in batch.levelSizes()}
-        assert all(1 <= b <= int(k.split("x")[0]) for k, b in choice.items())
+        assert all(0 <= b <= int(k.split("x")[0]) for k, b in choice.items())
         again = batch.autotune(buf, repetitions=1, cache=cache)
         assert again == choice
         chosen.append(choice)
