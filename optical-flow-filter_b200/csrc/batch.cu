@@ -75,10 +75,12 @@ constexpr int P2X = 64, P2Y = 16;  // level-1 tile of the ingest launch (blocks 
 // ring from it (pyramid_px, common.cuh: the values of a pyramid_down_k pass), and the
 // level-2 pixels under the tile from the ring.  The last tile row and column of a stream also
 // copy the level-0 remainder (odd sizes).
-constexpr int S0Y = 2 * P2Y + 5, S0X = 2 * P2X + 5;  // staged level-0 rows and columns
+// staged level-0 rows and columns: the tile's 2 P2Y x 2 P2X pixels, 3 before and 2 after in
+// each direction, the columns from a 4-byte boundary (4 before)
+constexpr int S0Y = 2 * P2Y + 5, S0X = 2 * P2X + 8;
 __global__ void __launch_bounds__(256) ingest_pyr_k(const uint8_t* __restrict__ frames,
                                                     const IngestJob* __restrict__ jobs, int n) {
-    __shared__ uint8_t s0[S0Y][S0X + 3];
+    __shared__ __align__(16) uint8_t s0[S0Y][S0X];
     __shared__ uint8_t ring[P2Y + 2][P2X + 2];
     grid_dep_wait();
     grid_dep_launch();
@@ -87,36 +89,61 @@ __global__ void __launch_bounds__(256) ingest_pyr_k(const uint8_t* __restrict__ 
     const int tx = b % j.tiles_x, ty = b / j.tiles_x;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const uint8_t* src = frames + j.src;
+    const int W = j.W, H = j.H;
+    const bool words = (W & 3) == 0 && (j.dst_pitch & 3) == 0;  // rows are 4-byte aligned
     if (j.levels < 2) {  // block-uniform: a one-level stream's tile is a plain copy
         const int x0 = tx * 2 * P2X, y0 = ty * 2 * P2Y;
-        const int xe = tx == j.tiles_x - 1 ? j.W : min(x0 + 2 * P2X, j.W);
-        const int ye = ty == j.tiles_y - 1 ? j.H : min(y0 + 2 * P2Y, j.H);
+        const int xe = tx == j.tiles_x - 1 ? W : min(x0 + 2 * P2X, W);
+        const int ye = ty == j.tiles_y - 1 ? H : min(y0 + 2 * P2Y, H);
         const int wv = xe - x0, rows = ye - y0;
-        if ((j.W & 3) == 0 && (wv & 3) == 0 && (j.dst_pitch & 3) == 0) {  // 4-byte words
+        if (words) {
             const int wq = wv >> 2;
             for (int k = tid; k < rows * wq; k += 256) {
                 const int r = k / wq, c = k - r * wq;
                 reinterpret_cast<uint32_t*>(j.dst + (size_t)(y0 + r) * j.dst_pitch + x0)[c] =
-                    __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)(y0 + r) * j.W + x0) + c);
+                    __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)(y0 + r) * W + x0) + c);
             }
         } else {
             for (int k = tid; k < rows * wv; k += 256) {
                 const int r = k / wv, c = k - r * wv;
-                j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = __ldg(src + (size_t)(y0 + r) * j.W + x0 + c);
+                j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = __ldg(src + (size_t)(y0 + r) * W + x0 + c);
             }
         }
         return;
     }
     const int x1 = tx * P2X, y1 = ty * P2Y;
-    const int X0 = 2 * x1 - 3, Y0 = 2 * y1 - 3;  // staged level-0 origin (unclamped)
-    {
+    const int X0 = 2 * x1 - 4, Y0 = 2 * y1 - 3;  // staged level-0 origin (unclamped)
+    if (words) {
+        constexpr int WQ = S0X / 4, NS = (S0Y * WQ + 255) / 256;
+        uint32_t v[NS];
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + 256 * u, r = e / WQ, c = e - r * WQ;
+            if (e < S0Y * WQ) {
+                const uint8_t* row = src + (size_t)min(max(Y0 + r, 0), H - 1) * W;
+                const int x = X0 + 4 * c;
+                if (x >= 0 && x + 3 < W) {
+                    v[u] = __ldg(reinterpret_cast<const uint32_t*>(row + x));
+                } else {  // a word beyond an edge: its clamped bytes
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) w |= (uint32_t)__ldg(row + min(max(x + q, 0), W - 1)) << (8 * q);
+                    v[u] = w;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + 256 * u, r = e / WQ, c = e - r * WQ;
+            if (e < S0Y * WQ) reinterpret_cast<uint32_t*>(s0[r])[c] = v[u];
+        }
+    } else {
         constexpr int NS = (S0Y * S0X + 255) / 256;
         uint8_t v[NS];
 #pragma unroll
         for (int u = 0; u < NS; ++u) {
             const int e = tid + 256 * u, r = e / S0X, c = e - r * S0X;
-            if (e < S0Y * S0X)
-                v[u] = __ldg(src + (size_t)min(max(Y0 + r, 0), j.H - 1) * j.W + min(max(X0 + c, 0), j.W - 1));
+            if (e < S0Y * S0X) v[u] = __ldg(src + (size_t)min(max(Y0 + r, 0), H - 1) * W + min(max(X0 + c, 0), W - 1));
         }
 #pragma unroll
         for (int u = 0; u < NS; ++u) {
@@ -127,12 +154,21 @@ __global__ void __launch_bounds__(256) ingest_pyr_k(const uint8_t* __restrict__ 
     __syncthreads();
     {
         const int x0 = 2 * x1, y0 = 2 * y1;
-        const int xe = tx == j.tiles_x - 1 ? j.W : min(x0 + 2 * P2X, j.W);
-        const int ye = ty == j.tiles_y - 1 ? j.H : min(y0 + 2 * P2Y, j.H);
-        const int wv = xe - x0;
-        for (int k = tid; k < (ye - y0) * wv; k += 256) {
-            const int r = k / wv, c = k - r * wv;
-            j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = s0[y0 + r - Y0][x0 + c - X0];
+        const int xe = tx == j.tiles_x - 1 ? W : min(x0 + 2 * P2X, W);
+        const int ye = ty == j.tiles_y - 1 ? H : min(y0 + 2 * P2Y, H);
+        const int wv = xe - x0, rows = ye - y0;
+        if (words) {  // x0 - X0 = 4: word-aligned in s0 as in the image row
+            const int wq = wv >> 2;
+            for (int k = tid; k < rows * wq; k += 256) {
+                const int r = k / wq, c = k - r * wq;
+                reinterpret_cast<uint32_t*>(j.dst + (size_t)(y0 + r) * j.dst_pitch + x0)[c] =
+                    reinterpret_cast<const uint32_t*>(s0[y0 + r - Y0] + 4)[c];
+            }
+        } else {
+            for (int k = tid; k < rows * wv; k += 256) {
+                const int r = k / wv, c = k - r * wv;
+                j.dst[(size_t)(y0 + r) * j.dst_pitch + x0 + c] = s0[y0 + r - Y0][x0 + c - X0];
+            }
         }
     }
     for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += 256) {
@@ -260,12 +296,18 @@ Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
         // filters go with f_)
         if (d_ingest_) cudaFree(d_ingest_);
         if (cap_) cudaStreamDestroy(cap_);
+        if (side_) cudaStreamDestroy(side_);
+        if (fork_) cudaEventDestroy(fork_);
+        if (join_) cudaEventDestroy(join_);
         throw;
     }
 }
 
 void Batch::init(int n, const int* heights, const int* widths, const int* levels) {
     check_cuda(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+    check_cuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
     std::vector<IngestJob> ing;
     int blocks = 0;
     for (int i = 0; i < n; ++i) {
@@ -335,6 +377,9 @@ Batch::~Batch() {
         if (t) release_table(*t);
     if (d_ingest_) cudaFree(d_ingest_);
     if (cap_) cudaStreamDestroy(cap_);
+    if (side_) cudaStreamDestroy(side_);
+    if (fork_) cudaEventDestroy(fork_);
+    if (join_) cudaEventDestroy(join_);
 }
 
 Filter& Batch::stream(int i) {
@@ -522,8 +567,9 @@ void Batch::build(Table& t) {
         t.gen.push_back(f->config_generation());
     }
     t.tune_gen = tune_gen_;
-    // capture: the deeper pyramid depths, then per phase its streaming launch and its tile
-    // launch, all on one stream (each launch waits for the previous one)
+    // capture: the deeper pyramid depths; phase A's streaming launch, with its tile launch on
+    // a branch beside it (the small levels fill the streaming launch's tail); phase B's
+    // launches after both
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t e = cudaSuccess;
@@ -538,15 +584,24 @@ void Batch::build(Table& t) {
             ++launches;
         }
     for (int ph = 0; ph < 2; ++ph) {
+        const bool branch = ph == 0 && !tj[0].empty() && !sj[0].empty();
+        if (branch) {
+            ok(cudaEventRecord(fork_, cap_));
+            ok(cudaStreamWaitEvent(side_, fork_, 0));
+        }
         if (!sj[ph].empty()) {
             ok(launch_stream_mega(t.d_stream + (ph ? sj[0].size() : 0), (int)sj[ph].size(), sblocks[ph], ssmem[ph],
                                   cap_));
             ++launches;
         }
         if (!tj[ph].empty()) {
-            ok(launch_k(tile_batch_k, dim3(tblocks[ph]), dim3(kTileThreads), tsmem[ph], cap_,
+            ok(launch_k(tile_batch_k, dim3(tblocks[ph]), dim3(kTileThreads), tsmem[ph], branch ? side_ : cap_,
                         (const TileJob*)(t.d_tile + (ph ? tj[0].size() : 0)), (int)tj[ph].size()));
             ++launches;
+        }
+        if (branch) {
+            ok(cudaEventRecord(join_, side_));
+            ok(cudaStreamWaitEvent(cap_, join_, 0));
         }
     }
     cudaError_t ec = cudaStreamEndCapture(cap_, &g);

@@ -75,6 +75,8 @@ private:
     int ingest_blocks_ = 0;
     std::unique_ptr<Table> tab_[2];
     cudaStream_t cap_ = nullptr;
+    cudaStream_t side_ = nullptr;  // capture branch of phase A's tile launch
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     int max_levels_ = 0;
     long min_px_ = -1;
     int band_ = 0;
