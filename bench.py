@@ -183,7 +183,7 @@ class ClockSampler:
                     for b, name in self.REASONS.items():
                         if bits & b:
                             self.reasons.add(name)
-                    time.sleep(0.002)
+                    time.sleep(0.02)
 
             self._thread = threading.Thread(target=poll, daemon=True)
             self._thread.start()
@@ -285,12 +285,30 @@ def make_filter(w):
 TUNING_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "flowfilter_b200", "tuning.json")
 
 
+_LIB_DIGEST = None
+
+
+def lib_digest():
+    """sha256 prefix of the loaded libffb200.so: a tuning choice belongs to one build."""
+    global _LIB_DIGEST
+    if _LIB_DIGEST is None:
+        import hashlib
+
+        from flowfilter_b200 import _lib
+
+        with open(_lib.LIB_PATH, "rb") as fh:
+            _LIB_DIGEST = hashlib.sha256(fh.read()).hexdigest()[:16]
+    return _LIB_DIGEST
+
+
 def tuned(f, w, key=None, flush=None):
-    """Apply the cached autotuning result for this workload and GPU, or autotune now (after
-    the filter computed a frame) and cache it, so repeated runs make the same choice."""
+    """Apply the cached autotuning result for this workload, GPU and library build, or
+    autotune now (after the filter computed a frame) and cache it, so repeated runs of one
+    build make the same choice."""
     import torch
 
-    key = key or f"{torch.cuda.get_device_name()}|{w['H']}x{w['W']}|L{w['levels']}|m{w['maxflow']}|s{w['smooth']}"
+    key = key or (f"{torch.cuda.get_device_name()}|{lib_digest()}|{w['H']}x{w['W']}|L{w['levels']}"
+                  f"|m{w['maxflow']}|s{w['smooth']}")
     cache = {}
     if os.path.exists(TUNING_CACHE):
         try:
@@ -306,6 +324,21 @@ def tuned(f, w, key=None, flush=None):
     os.makedirs(os.path.dirname(TUNING_CACHE), exist_ok=True)
     with open(TUNING_CACHE, "w") as fh:
         json.dump(cache, fh, indent=1)
+
+
+def pretune(w, dev_frames, flush, frames=9):
+    """Autotune a filter of workload w on `frames` computed frames and cache the choice
+    (tuned()), before any clock sampling: the timed runs then apply the cached choice."""
+    import torch
+
+    f = make_filter(w)
+    ring = dev_frames.shape[0]
+    for t in range(frames):
+        f.loadImage(dev_frames[t % ring])
+        f.computeAsync()
+    torch.cuda.synchronize()
+    tuned(f, w, flush=flush)
+    del f
 
 
 def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, tune=True, label="timed"):
@@ -714,6 +747,9 @@ def bench_b200(args):
     w = WORKLOADS[PRIMARY]
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
+    # kernel choice first, outside the clock sampling (its NVML polling must not disturb the
+    # autotuner's per-frame timings)
+    pretune(w, torch.from_numpy(make_frames(w)).cuda(), flush)
     # ---- timed region: device time of K frames, L2 flushed between frames
     barrier(world)
     with ClockSampler(gpu_uuid(local)) as clk:

@@ -388,7 +388,13 @@ __device__ __forceinline__ void prop_adj_at(int j, int n, bool line_in, int bord
         for (int q = 0; q < 3; ++q) gchan(j - 1 + q, gx[q]);
         // branch-free: every lane runs the same instructions, the upwind branch, the border
         // freeze and the dominant-neighbour choice are per-lane selects (a frozen output
-        // passes its gradient through: coefficient 1 at q == 1, 0 elsewhere)
+        // passes its gradient through: coefficient 1 at q == 1, 0 elsewhere).  The upwind
+        // differences of neighbouring positions are shared by the three outputs.
+        T dif[4][NC];  // dif[p] = position p+1 minus position p
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) dif[p][c] = px[p + 1][c] - px[p][c];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {  // output i = j - 1 + q reads positions q, q+1, q+2
             const int i = j - 1 + q;
@@ -407,10 +413,8 @@ __device__ __forceinline__ void prop_adj_at(int j, int n, bool line_in, int bord
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 const T g_o = gx[q][c];
-                const T hi = pos ? px[q + 1][c] : px[q + 2][c];
-                const T lo = pos ? px[q][c] : px[q + 1][c];
                 acc[c] += g_o * coef;
-                gdv -= g_o * dtq * (hi - lo);
+                gdv -= g_o * dtq * (pos ? dif[q][c] : dif[q + 1][c]);  // upwind difference
             }
             // the dominant velocity is the chosen neighbour's AXIS component (position 2 = j)
             if (q != 1) acc[AXIS] += (q == 0 ? take_p : !take_p) ? gdv : T(0);
@@ -884,7 +888,12 @@ struct PropTile {
 template <typename T, bool PAYLOAD, typename F>
 __device__ __forceinline__ void stage_px(F& dst, int r, int c, const T* f, const T* s, const T* v, size_t k) {
     constexpr int P = 2 * sizeof(T);
-    cp_async<P>(&dst.f[r][c], f + 2 * k);
+    if (f) {
+        cp_async<P>(&dst.f[r][c], f + 2 * k);
+    } else {  // an absent gradient: zeros
+        dst.f[r][c].x = T(0);
+        dst.f[r][c].y = T(0);
+    }
     if constexpr (PAYLOAD) {
         cp_async<sizeof(T)>(&dst.s[r][c], s + k);
         cp_async<P>(&dst.v[r][c], v + 2 * k);
@@ -1965,9 +1974,15 @@ struct Driver {
         T* gimg[FF_DIFF_MAX_LEVELS];
         gimg[0] = gframe;
         for (int l = 1; l < L; ++l) gimg[l] = sc_ + S_.gimg[l];
+        // zeros standing in for an absent output gradient, cleared at the first such use
         T* const zbuf = sc_ + S_.zero;
-        zero(zbuf, 2 * g.n1(0));
-        auto gz = [&](const T* p) { return p ? p : (const T*)zbuf; };
+        bool zeroed = false;
+        auto gz = [&](const T* p) {
+            if (p) return p;
+            if (!zeroed) zero(zbuf, 2 * g.n1(0));
+            zeroed = true;
+            return (const T*)zbuf;
+        };
         // gradient of the top level's unsmoothed flow: the caller's, the coarse reads of level
         // L-2 (scattered by its update adjoint) and the top's smoothing adjoint, in that order
         T* gfu = sc_ + S_.gfu;
@@ -2043,7 +2058,7 @@ struct Driver {
             jobs_add(sc_ + S_.part_g[l], (int)blocks_of(g, l), 1, ggamma + l);
             // iterations N-1 .. 0: the Y sub-step 2i+1 reads tape entry 2i, the X sub-step 2i
             // reads entry 2i-1 (the input state for i = 0, whose gradient goes to the caller's)
-            const T *cf = zbuf, *cs = gsh, *cv = gvh;
+            const T *cf = nullptr, *cs = gsh, *cv = gvh;  // f is not read after propagation: no gradient
             T* bufs[2] = {pb, pa};
             for (int i = g.N[l] - 1; i >= 0; --i) {
                 const T* yb = tp + tape.prop[l][2 * i];
