@@ -29,25 +29,84 @@ __global__ void pyramid_down_k(CView<P> in, View<P> out) {
     pyramid_px(in, out, x, y);
 }
 
-// Two pyramid steps in one launch: a block computes a 64 x 16 tile of level 1 (plus the
-// one-pixel ring that level 2 reads, at clamped coordinates) into shared memory, stores the
-// tile, and computes the 32 x 8 level-2 pixels under it from shared memory: the same values
-// as two pyramid_down_k launches.  Level 1 is H1 x W1 = (H/2) x (W/2), level 2 (H1/2) x (W1/2).
+// Two pyramid steps in one launch: a block stages the level-0 pixels under its 64 x 16
+// level-1 tile, plus those the one-pixel level-1 ring around it reads (at clamped
+// coordinates), in shared memory with one batch of loads; computes the tile and the ring
+// into shared memory, stores the tile, and computes the 32 x 8 level-2 pixels under it from
+// the ring: the same values as two pyramid_down_k launches.  Level 1 is H1 x W1 =
+// (H/2) x (W/2), level 2 (H1/2) x (W1/2).
 constexpr int P2X = 2 * BX, P2Y = 2 * BY;  // level-1 tile
+constexpr int S0Y = 2 * P2Y + 5;           // staged level-0 rows: 3 before the tile's, 2 after
+constexpr int S0X = 2 * P2X + 8;           // staged level-0 columns: from 4 before the tile's
 template <typename P>
-__global__ void pyramid_down2_k(CView<P> in, View<P> out1, View<P> out2) {
+__global__ void __launch_bounds__(BX * BY) pyramid_down2_k(CView<P> in, View<P> out1, View<P> out2) {
+    __shared__ __align__(16) P s0[S0Y][S0X];
     __shared__ P ring[P2Y + 2][P2X + 2];
     grid_dep_wait();
     grid_dep_launch();
     const int x1 = blockIdx.x * P2X, y1 = blockIdx.y * P2Y;  // level-1 tile origin
-    const int H1 = out1.h, W1 = out1.w;
-    const CView<P> lv1{out1.ptr, out1.pitch, H1, W1};
+    const int H1 = out1.h, W1 = out1.w, H = in.h, W = in.w;
+    const int X0 = 2 * x1 - 4, Y0 = 2 * y1 - 3;  // staged level-0 origin (unclamped)
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += blockDim.x * blockDim.y) {
+    constexpr int T = BX * BY;
+    // 4-byte words of uint8 rows whose pitch keeps them aligned, else single pixels
+    const bool words = sizeof(P) == 1 && (in.pitch & 3) == 0 && ((uintptr_t)in.ptr & 3) == 0;
+    if (words) {
+        constexpr int WQ = S0X / 4, NS = (S0Y * WQ + T - 1) / T;
+        uint32_t v[NS];
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + T * u, r = e / WQ, c = e - r * WQ;
+            if (e < S0Y * WQ) {
+                const uint8_t* row = reinterpret_cast<const uint8_t*>(in.row(min(max(Y0 + r, 0), H - 1)));
+                const int x = X0 + 4 * c;
+                if (x >= 0 && x + 3 < W) {
+                    v[u] = __ldg(reinterpret_cast<const uint32_t*>(row + x));
+                } else {  // a word beyond an edge: its clamped pixels
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) w |= (uint32_t)__ldg(row + min(max(x + q, 0), W - 1)) << (8 * q);
+                    v[u] = w;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + T * u, r = e / WQ, c = e - r * WQ;
+            if (e < S0Y * WQ) reinterpret_cast<uint32_t*>(&s0[r][0])[c] = v[u];
+        }
+    } else {
+        constexpr int NS = (S0Y * S0X + T - 1) / T;
+        P v[NS];
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + T * u, r = e / S0X, c = e - r * S0X;
+            if (e < S0Y * S0X) v[u] = in.clamped(X0 + c, Y0 + r);
+        }
+#pragma unroll
+        for (int u = 0; u < NS; ++u) {
+            const int e = tid + T * u, r = e / S0X, c = e - r * S0X;
+            if (e < S0Y * S0X) s0[r][c] = v[u];
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < (P2X + 2) * (P2Y + 2); k += T) {
         const int i = k % (P2X + 2), j = k / (P2X + 2);
         const int ux = x1 - 1 + i, uy = y1 - 1 + j;  // unclamped level-1 position
         const int cx = min(max(ux, 0), W1 - 1), cy = min(max(uy, 0), H1 - 1);
-        const P v = pyramid_val(in, cx, cy);
+        // pyramid_val at (cx, cy): level-0 rows 2cy-1..2cy+1, columns 2cx-1..2cx+1, clamped
+        float xs[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const P* row = &s0[2 * cy - 1 + q - Y0][2 * cx - 1 - X0];
+            const float sv = down3(Pix<P>::get(row[0]), Pix<P>::get(row[1]), Pix<P>::get(row[2]));
+            if constexpr (sizeof(P) == 1) xs[q] = u8_to_unit(quantize_u8(sv));
+            else xs[q] = sv;
+        }
+        const float sv = down3(xs[0], xs[1], xs[2]);
+        P v;
+        if constexpr (sizeof(P) == 1) v = quantize_u8(sv);
+        else v = sv;
         ring[j][i] = v;
         if (ux == cx && uy == cy && ux >= x1 && ux < x1 + P2X && uy >= y1 && uy < y1 + P2Y) out1.at(ux, uy) = v;
     }
