@@ -78,13 +78,15 @@ constexpr int P2X = 64, P2Y = 16;  // level-1 tile of the ingest launch (blocks 
 // staged level-0 rows and columns: the tile's 2 P2Y x 2 P2X pixels, 3 before and 2 after in
 // each direction, the columns from a 4-byte boundary (4 before)
 constexpr int S0Y = 2 * P2Y + 5, S0X = 2 * P2X + 8;
-__global__ void __launch_bounds__(256) ingest_pyr_k(const uint8_t* __restrict__ frames,
-                                                    const IngestJob* __restrict__ jobs, int n) {
+// block_job[b]: the job of block b (a table, so a block finds its job in one load)
+__global__ void __launch_bounds__(256, 6) ingest_pyr_k(const uint8_t* __restrict__ frames,
+                                                       const IngestJob* __restrict__ jobs,
+                                                       const unsigned short* __restrict__ block_job) {
     __shared__ __align__(16) uint8_t s0[S0Y][S0X];
     __shared__ uint8_t ring[P2Y + 2][P2X + 2];
     grid_dep_wait();
     grid_dep_launch();
-    const IngestJob& j = jobs[job_of(jobs, n, blockIdx.x)];
+    const IngestJob& j = jobs[block_job[blockIdx.x]];
     const int b = blockIdx.x - j.first_block;
     const int tx = b % j.tiles_x, ty = b / j.tiles_x;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -295,6 +297,7 @@ Batch::Batch(int n, const int* heights, const int* widths, const int* levels) {
         // a failed constructor runs no destructor: release what init made (the streams'
         // filters go with f_)
         if (d_ingest_) cudaFree(d_ingest_);
+        if (d_ingest_block_) cudaFree(d_ingest_block_);
         if (cap_) cudaStreamDestroy(cap_);
         if (side_) cudaStreamDestroy(side_);
         if (fork_) cudaEventDestroy(fork_);
@@ -349,6 +352,12 @@ void Batch::init(int n, const int* heights, const int* widths, const int* levels
     }
     d_ingest_ = to_device(ing);
     ingest_blocks_ = blocks;
+    if (n > 65535) throw Error(FF_ERR_UNSUPPORTED, "batch: at most 65535 streams");
+    std::vector<unsigned short> block_job(blocks);
+    for (int i = 0; i < n; ++i)
+        for (int b = ing[i].first_block; b < ing[i].first_block + ing[i].tiles_x * ing[i].tiles_y; ++b)
+            block_job[b] = (unsigned short)i;
+    d_ingest_block_ = to_device(block_job);
     for (auto& t : tab_) t.reset(new Table);
     check_cuda(cudaFuncSetAttribute(tile_batch_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmemCap),
                "cudaFuncSetAttribute");
@@ -376,6 +385,7 @@ Batch::~Batch() {
     for (auto& t : tab_)
         if (t) release_table(*t);
     if (d_ingest_) cudaFree(d_ingest_);
+    if (d_ingest_block_) cudaFree(d_ingest_block_);
     if (cap_) cudaStreamDestroy(cap_);
     if (side_) cudaStreamDestroy(side_);
     if (fork_) cudaEventDestroy(fork_);
@@ -621,7 +631,7 @@ void Batch::step(const void* frames, cudaStream_t s) {
     if ((uintptr_t)frames % 16) throw Error(FF_ERR_INVALID_ARGUMENT, "batch: the frame buffer must be 16-byte aligned");
     for (auto& f : f_) f->batch_begin(s);
     check_cuda(launch_k(ingest_pyr_k, dim3(ingest_blocks_), dim3(32, 8), 0, s, (const uint8_t*)frames,
-                        (const IngestJob*)d_ingest_, size()),
+                        (const IngestJob*)d_ingest_, (const unsigned short*)d_ingest_block_),
                "batch ingest");
     bool first = false;
     for (auto& f : f_) first |= f->any_first();

@@ -72,6 +72,7 @@ private:
     std::vector<size_t> off_;
     size_t total_ = 0;
     IngestJob* d_ingest_ = nullptr;
+    unsigned short* d_ingest_block_ = nullptr;  // job of each ingest block
     int ingest_blocks_ = 0;
     std::unique_ptr<Table> tab_[2];
     cudaStream_t cap_ = nullptr;
