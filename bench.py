@@ -443,16 +443,19 @@ def batched_streams(seed=100):
     return out
 
 
-def batched_sequences(streams, frames):
+def batched_sequences(streams, frames, ids=None):
     """Stream i's frames: the bump-flow sequence of its size from seed 100 + i (uint8
-    [frames, H, W] each), generated on a thread pool (numpy releases the GIL)."""
+    [frames, H, W] each; ids: the streams' indices in the full mix), generated on a thread
+    pool (numpy releases the GIL)."""
     from concurrent.futures import ThreadPoolExecutor
 
     from flowfilter_b200 import synthetic
 
-    def one(i):
-        s = streams[i]
-        return synthetic.seq_bumps(frames=frames, height=s["H"], width=s["W"], seed=100 + i)
+    ids = list(range(len(streams))) if ids is None else list(ids)
+
+    def one(k):
+        s = streams[k]
+        return synthetic.seq_bumps(frames=frames, height=s["H"], width=s["W"], seed=100 + ids[k])
 
     with ThreadPoolExecutor(min(8, os.cpu_count() or 1)) as ex:
         return list(ex.map(one, range(len(streams))))
@@ -464,15 +467,23 @@ def configure_stream(f, s):
     f.maxflow = s["maxflow"]
 
 
-def bench_batched(steps, warmup):
+def bench_batched(steps, warmup, world=1, rank=0):
     """The 64-stream mixed-size step: one BatchFlowFilter step against a loop that runs the
     64 streams one after another as single-stream filters (graph replay each), both over
-    frames already in HBM.  The 64 streams' state (~1 GB) exceeds L2, so no flush."""
+    frames already in HBM.  The 64 streams' state (~1 GB) exceeds L2, so no flush.  With
+    several ranks the 64 streams are split over them (BatchFlowFilter.shard, by compulsory
+    bytes): each rank steps its own batch, and the rates are all streams over the slowest
+    rank's time."""
     import torch
     from flowfilter_b200 import BatchFlowFilter, PyramidalFlowFilter, synthetic
 
     streams = batched_streams()
-    seqs = [torch.from_numpy(q).cuda() for q in batched_sequences(streams, BATCH_RING)]
+    total = len(streams)
+    ids = list(range(total))
+    if world > 1:
+        ids = BatchFlowFilter.shard([(s["H"], s["W"], s["levels"]) for s in streams], world)[rank]
+        streams = [streams[i] for i in ids]
+    seqs = [torch.from_numpy(q).cuda() for q in batched_sequences(streams, BATCH_RING, ids)]
     batch = BatchFlowFilter([(s["H"], s["W"], s["levels"]) for s in streams])
     for i, s in enumerate(streams):
         configure_stream(batch.stream(i), s)
@@ -509,11 +520,14 @@ def bench_batched(steps, warmup):
                 f.setGraphs(True)
 
     l_ms = timed(loop_step)
-    px = sum(s["H"] * s["W"] for s in streams)
-    n = len(streams)
+    b0_ms, b_ms, l_ms = (max_over_ranks(world, v) for v in (b0_ms, b_ms, l_ms))
+    px = sum(s["H"] * s["W"] for s in batched_streams())
+    n = total
     return {
         "workload": f"{n} streams: {BATCH_PER_SIZE} each at " + ", ".join(f"{w}x{h}" for h, w in BATCH_SIZES)
-                    + "; levels 1-3, gamma log-uniform [2,100], smoothing 1-4, maxflow 4 (seed 100)",
+                    + "; levels 1-3, gamma log-uniform [2,100], smoothing 1-4, maxflow 4 (seed 100)"
+                    + (f"; split over {world} ranks by compulsory bytes ({len(streams)} streams here)"
+                       if world > 1 else ""),
         "value": n * steps / (b_ms / 1e3), "unit": "stream-frames/s", "steps": steps,
         "ms_per_step": b_ms / steps, "mpix_per_s": px * steps / (b_ms / 1e3) / 1e6,
         "launches_per_step": batch.launches(),
@@ -785,7 +799,7 @@ def bench_b200(args):
 
     # ---- the 64-stream batched step (each rank its own batch: replicas)
     barrier(world)
-    batched = bench_batched(min(args.steps, 200), max(args.warmup, 3))
+    batched = bench_batched(min(args.steps, 200), max(args.warmup, 3), world, rank)
     barrier(world)
 
     differentiable = bench_differentiable(args.steps)

@@ -529,6 +529,8 @@ void Batch::build(Table& t) {
                 j.a = f->level_args(l);
                 j.band = band_of(v, rule);
                 j.kind = stream_kind(v.delta, v.iters, v.smooth);
+                if (v.iters < 1 || v.iters > 4 || v.smooth < 1 || v.smooth > 4)  // the phase kernel's instantiations
+                    throw Error(FF_ERR_LOGIC, "batch: a streamed level outside the streaming kernel's range");
                 j.first_block = sblocks[ph];
                 sblocks[ph] += fused_warp_grid(v.iters, v.smooth, v.W, v.H, j.band, &j.nwx, &j.nby);
                 ssmem[ph] = std::max(ssmem[ph], stream_block_smem(v.delta, v.smooth));

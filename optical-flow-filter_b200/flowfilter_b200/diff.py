@@ -278,7 +278,8 @@ class DiffPyramidalFlowFilter:
     def parameters(self):
         return [self.gamma, self.weights]
 
-    def fit(self, frames, truth, steps: int = 200, lr: float = 0.05, first: int = 8, fit_weights: bool = True):
+    def fit(self, frames, truth, steps: int = 200, lr: float = 0.05, first: int = 8, fit_weights: bool = True,
+            group=None):
         """Fits the per-level gamma and, with fit_weights, the per-level 5-tap smoothing
         weights by Adam on the mean endpoint error of the flows against ``truth``
         (B, T, H, W, 2) over frames first.. .  gamma is fitted through its logarithm (it stays
@@ -286,7 +287,12 @@ class DiffPyramidalFlowFilter:
         and sum to 1, as the reference's 0.2 box does, which is the softmax of equal logits).
         Checkpointing follows ``checkpoint_every``.  Returns the loss of every step, the final
         loss and the device milliseconds of the steps; the fitted values are left in gamma /
-        weights."""
+        weights.
+
+        Data parallel: when torch.distributed is initialised with more than one rank (or
+        ``group`` is given), each rank passes its own share of the sequences (equal batch
+        sizes) and every step averages the parameter gradients and the loss over the ranks
+        (one all-reduce each), so all ranks take the same Adam steps."""
         torch = _torch()
         log_g = torch.log(self.gamma.detach().clone()).requires_grad_(True)
         w0 = self.weights.detach().clone()
@@ -301,14 +307,20 @@ class DiffPyramidalFlowFilter:
             loss = endpoint_error(self(frames), truth, first=first, eps=1e-12)
             opt.zero_grad()
             loss.backward()
+            params = [log_g, logits] if fit_weights else [log_g]
+            average_over_ranks([p.grad for p in params], group)
+            lv = loss.detach().reshape(1).clone()
+            average_over_ranks([lv], group)
             opt.step()
-            losses.append(loss.detach())
+            losses.append(lv[0])
         e1.record()
         torch.cuda.synchronize()
         self.gamma = log_g.detach().exp().requires_grad_(True)
         self.weights = (torch.softmax(logits.detach(), 1) if fit_weights else w0).clone().requires_grad_(True)
         with torch.no_grad():
-            final = float(endpoint_error(self(frames), truth, first=first))
+            fl = endpoint_error(self(frames), truth, first=first).reshape(1).clone()
+            average_over_ranks([fl], group)
+            final = float(fl[0])
         return {"losses": [float(x) for x in losses], "final": final, "ms": e0.elapsed_time(e1)}
 
     def _smooth(self, x, l):
@@ -400,6 +412,27 @@ class DiffPyramidalFlowFilter:
             state = unflat(list(res[1:]))
             t0 = t1
         return torch.cat(outs, 1)
+
+
+def average_over_ranks(tensors, group=None) -> int:
+    """Replaces every tensor with its mean over the ranks of ``group`` (the default process
+    group when torch.distributed is initialised; nothing happens with one rank): one
+    all-reduce of their flattened concatenation.  Returns the number of ranks."""
+    torch = _torch()
+    dist = torch.distributed
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        return 1
+    world = dist.get_world_size(group)
+    if world == 1 or not tensors:
+        return world
+    flat = torch.cat([t.reshape(-1) for t in tensors])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    flat /= world
+    at = 0
+    for t in tensors:
+        t.copy_(flat[at:at + t.numel()].view_as(t))
+        at += t.numel()
+    return world
 
 
 def endpoint_error(flows, truth, first: int = 0, eps: float = 0.0):

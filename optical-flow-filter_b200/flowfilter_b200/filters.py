@@ -618,6 +618,31 @@ class BatchFlowFilter:
         unchanged."""
         call("ff_batch_set_tuning", self._h, int(minPixels), int(band))
 
+    @staticmethod
+    def streamBytes(height: int, width: int, levels: int) -> int:
+        """Compulsory HBM bytes of one frame of a stream: the uint8 frame, 40 B of state read
+        and written plus 2 B of coarse flow per pixel of every delta level, 24 B per pixel of
+        the top level."""
+        total, h, w = height * width, height, width
+        for l in range(levels):
+            total += h * w * (24 if l == levels - 1 else 42)
+            h, w = h // 2, w // 2
+        return total
+
+    @staticmethod
+    def shard(shapes, ranks: int) -> list:
+        """Streams split over ``ranks`` GPUs (one batch each): the stream indices of every
+        rank, assigned greedily, largest compulsory bytes first, each to the rank with the
+        least so far."""
+        order = sorted(range(len(shapes)), key=lambda i: (-BatchFlowFilter.streamBytes(*shapes[i]), i))
+        load = [0] * ranks
+        out = [[] for _ in range(ranks)]
+        for i in order:
+            r = min(range(ranks), key=lambda k: (load[k], k))
+            out[r].append(i)
+            load[r] += BatchFlowFilter.streamBytes(*shapes[i])
+        return [sorted(v) for v in out]
+
     def setLevelBand(self, height: int, width: int, band: int) -> None:
         """Levels of ``height`` x ``width`` pixels run in bands of ``band`` rows (0: no
         override).  Results are unchanged."""
