@@ -107,13 +107,16 @@ def level0_kernel_bytes(w):
 
 
 def kernels_per_frame(w, tuning: str) -> int:
-    """Kernel launches of one frame: L-1 pyramid steps, then per level one fused kernel
-    (streaming or tile) or the per-stage kernels (model, 2N propagation passes, update,
-    2S smoothing passes)."""
+    """Kernel launches of one frame: the pyramid (levels 1 and 2 in one launch, each deeper
+    level one more), then per level one fused kernel (streaming or tile) or the per-stage
+    kernels (model, 2N propagation passes, update, 2S smoothing passes)."""
     L = w["levels"]
     parts = [p.strip() for p in tuning.split(";")]
     # a two-level pyramid whose top level runs the tile kernel makes level 1 inside it
-    n = 0 if (L == 2 and len(parts) > 1 and "tile" in parts[1]) else L - 1
+    if L == 2 and len(parts) > 1 and "tile" in parts[1]:
+        n = 0
+    else:
+        n = L - 1 if L <= 2 else 1 + (L - 3)
     for l in range(L):
         m = w["maxflow"] / (2 ** min(l, L - 1))
         N = int(np.ceil(np.float32(m)))
