@@ -304,44 +304,85 @@ def lib_digest():
     return _LIB_DIGEST
 
 
-def tuned(f, w, key=None, flush=None):
-    """Apply the cached autotuning result for this workload, GPU and library build, or
-    autotune now (after the filter computed a frame) and cache it, so repeated runs of one
-    build make the same choice."""
+def tuning_key(w):
     import torch
 
-    key = key or (f"{torch.cuda.get_device_name()}|{lib_digest()}|{w['H']}x{w['W']}|L{w['levels']}"
-                  f"|m{w['maxflow']}|s{w['smooth']}")
-    cache = {}
+    return (f"{torch.cuda.get_device_name()}|{lib_digest()}|{w['H']}x{w['W']}|L{w['levels']}"
+            f"|m{w['maxflow']}|s{w['smooth']}")
+
+
+def load_tuning_cache():
     if os.path.exists(TUNING_CACHE):
         try:
             with open(TUNING_CACHE) as fh:
-                cache = json.load(fh)
+                return json.load(fh)
         except (OSError, ValueError):
-            cache = {}
-    if key in cache:
-        f.setTuningState(cache[key])
-        return
-    f.autotune(5, flush)
-    cache[key] = f.tuningState()
+            pass
+    return {}
+
+
+def store_tuning(key, state):
+    cache = load_tuning_cache()
+    cache[key] = state
     os.makedirs(os.path.dirname(TUNING_CACHE), exist_ok=True)
     with open(TUNING_CACHE, "w") as fh:
         json.dump(cache, fh, indent=1)
 
 
-def pretune(w, dev_frames, flush, frames=9):
-    """Autotune a filter of workload w on `frames` computed frames and cache the choice
-    (tuned()), before any clock sampling: the timed runs then apply the cached choice."""
+def tuned(f, w, key=None, flush=None):
+    """Apply the cached autotuning result for this workload, GPU and library build, or
+    autotune now (after the filter computed a frame) and cache it, so repeated runs of one
+    build make the same choice."""
+    key = key or tuning_key(w)
+    cache = load_tuning_cache()
+    if key in cache:
+        f.setTuningState(cache[key])
+        return
+    f.autotune(5, flush)
+    store_tuning(key, f.tuningState())
+
+
+def pretune(w, dev_frames, flush, frames=9, rounds=3, timed_frames=60):
+    """The kernel choice of workload w, made before any clock sampling and cached (the timed
+    runs apply it through tuned()): `rounds` autotunes, each on a filter that computed
+    `frames` frames, and of the choices they make the one whose frames run fastest in the
+    bench's own timed loop (median of `timed_frames` frames, L2 flushed before each)."""
     import torch
 
-    f = make_filter(w)
+    key = tuning_key(w)
+    if key in load_tuning_cache():
+        return
     ring = dev_frames.shape[0]
-    for t in range(frames):
-        f.loadImage(dev_frames[t % ring])
-        f.computeAsync()
-    torch.cuda.synchronize()
-    tuned(f, w, flush=flush)
-    del f
+    best = None
+    seen = []
+    for _ in range(rounds):
+        f = make_filter(w)
+        for t in range(frames):
+            f.loadImage(dev_frames[t % ring])
+            f.computeAsync()
+        torch.cuda.synchronize()
+        f.autotune(5, flush)
+        state = f.tuningState()
+        if state in seen:
+            continue
+        seen.append(state)
+        f.setGraphs(True)
+        for t in range(5):
+            f.loadImage(dev_frames[t % ring])
+            f.computeAsync()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(timed_frames)]
+        for k in range(timed_frames):
+            flush.zero_()
+            ev[k][0].record()
+            f.loadImage(dev_frames[k % ring])
+            f.computeAsync()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        ms = sorted(a.elapsed_time(b) for a, b in ev)[timed_frames // 2]
+        if best is None or ms < best[0]:
+            best = (ms, state)
+        del f
+    store_tuning(key, best[1])
 
 
 def device_run(w, dev_frames, steps, warmup, flush, graphs=True, profile=False, tune=True, label="timed"):
