@@ -137,8 +137,13 @@ Filter::Filter(Kind kind, int H, int W, int levels, int item, bool own_input)
         own_stream_ = true;
         check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
         check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
-        check_cuda(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
-        check_cuda(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
+        // the frame graph's chain pyramid -> top -> level L-2 (captured on cap_) at the highest
+        // stream priority, level 0 (on side_) at the lowest: when both have blocks waiting,
+        // the latency-bound chain's are dispatched first (graphs keep node priorities)
+        int lo_p = 0, hi_p = 0;
+        check_cuda(cudaDeviceGetStreamPriorityRange(&lo_p, &hi_p), "cudaDeviceGetStreamPriorityRange");
+        check_cuda(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, lo_p), "cudaStreamCreate");
+        check_cuda(cudaStreamCreateWithPriority(&cap_, cudaStreamNonBlocking, hi_p), "cudaStreamCreate");
         for (cudaEvent_t* e : {&ev_fork_, &ev_pyr_, &ev_join_, &done_})
             check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
         check_cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
@@ -1058,7 +1063,7 @@ void Filter::compute_async(cudaStream_t s) {
             }
             cudaGraph_t g = nullptr;
             check_cuda(cudaStreamEndCapture(cap_, &g), "cudaStreamEndCapture");
-            cudaError_t e = cudaGraphInstantiateWithFlags(&ge, g, 0);
+            cudaError_t e = cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             check_cuda(e, "cudaGraphInstantiate");
         }
