@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Throughput benchmark of the flow-filter hot path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}] [--config {0,1,2,3,4}]
     python bench.py --profile WORKLOAD --steps K --warmup W     (profiler target only)
     python bench.py --profile-next --steps K --warmup W         (profiler target: FlowToColor, rotation)
     python bench.py --profile-batched --steps K --warmup W      (profiler target: the 64-stream batched step)
@@ -24,6 +24,11 @@ flushed (a 256 MiB write) between steps outside those events, so every frame rea
 state from HBM.  value = frames of all ranks / max over ranks of the summed step time.
 --gpus N runs N independent replicas (one process per GPU, torch.distributed for the
 barrier and the max over ranks); the path does not shard.
+
+--config N prints one configuration's line alone: 0 the single-level FlowFilter at 320x240
+(gamma 10, smoothing 1, maxflow 4, a constant translation of (0.7, -0.4) px/frame), 1 the
+reference's published 640x480 configuration, 2 the default run above, 3 the batched step,
+4 the differentiable filter (forward+backward frames/s).
 
 --impl reference times the reference's CPU path restated in C++ (oracle/, the same
 arithmetic as the reference kernels) on all host cores: the reference has no CPU
@@ -49,6 +54,9 @@ for _p in (ROOT, PKG):
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
+    # single-level FlowFilter on a constant translation (the reference's CPU-runnable case)
+    "constant_320x240_L1": dict(seq="constant", H=240, W=320, levels=1, gamma=[10.0], smooth=[1], maxflow=4.0,
+                                ring=100, filter="FlowFilter"),
     # the reference's published notebook configuration (notebooks/GPU_example.ipynb)
     "rotzoom_640x480_L2": dict(seq="rotzoom", H=480, W=640, levels=2, gamma=[10.0, 50.0], smooth=[2, 4],
                                maxflow=4.0, ring=96),
@@ -61,6 +69,13 @@ PRIMARY = "bumps_2048x1088_L3"
 # the reference's published configuration, reported beside it
 EXTRA = "rotzoom_640x480_L2"
 METRIC = "frames/s (PyramidalFlowFilter forward, flow err <= 1e-4 px vs reference)"
+# --config N: 0-2 one filter workload each, 3 the 64-stream batched step, 4 the differentiable filter
+CONFIGS = {0: "constant_320x240_L1", 1: "rotzoom_640x480_L2", 2: "bumps_2048x1088_L3", 3: "batched", 4: "differentiable"}
+
+
+def metric_of(name):
+    w = WORKLOADS[name]
+    return METRIC.replace("PyramidalFlowFilter", w.get("filter", "PyramidalFlowFilter"))
 # reference notebook: 1.172 ms/frame on its textured sequence for the 640x480 2-level
 # configuration (notebooks/GPU_example.ipynb:292); 0.996 ms/frame on all-zero frames (:400).
 # Nothing is published for 2048x1088.
@@ -68,6 +83,7 @@ PUBLISHED_FPS = {"rotzoom_640x480_L2": 1000.0 / 1.172}
 FLUSH_BYTES = 256 << 20
 L2_NOTE = "flushed between steps (256 MiB write outside the step events)"
 SEQUENCE = {
+    "constant": "seeded blurred noise (sigma 2, seed 0) translated by (0.7, -0.4) px/frame",
     "rotzoom": "seeded blurred noise (sigma 1.5, seed 1), rotation 0.5 deg + zoom 1.004 per frame",
     "bumps": "seeded blurred noise (sigma 1, seed 2) + N(0, 3 DN) sensor noise, flow = 8 Gaussian bumps "
              "(sigma 150 px, amplitude U[-3, 3] px/frame)",
@@ -77,8 +93,11 @@ SEQUENCE = {
 def bench_config(name):
     """The workload as both arms print it (identical keys and values in both)."""
     w = WORKLOADS[name]
-    return {"workload": name, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"], "gamma": w["gamma"],
-            "smoothIterations": w["smooth"], "maxflow": w["maxflow"], "l2": L2_NOTE}
+    out = {"workload": name, "frames": f"{w['W']}x{w['H']} uint8", "levels": w["levels"], "gamma": w["gamma"],
+           "smoothIterations": w["smooth"], "maxflow": w["maxflow"], "l2": L2_NOTE}
+    if "filter" in w:
+        out["filter"] = w["filter"]
+    return out
 
 
 def level_shapes(w):
@@ -129,6 +148,8 @@ def kernels_per_frame(w, tuning: str) -> int:
 def make_frames(w):
     from flowfilter_b200 import synthetic
 
+    if w["seq"] == "constant":
+        return synthetic.seq_constant(frames=w["ring"], height=w["H"], width=w["W"])
     if w["seq"] == "rotzoom":
         return synthetic.seq_rotzoom(frames=w["ring"], height=w["H"], width=w["W"])
     return synthetic.seq_bumps(frames=w["ring"], height=w["H"], width=w["W"])
@@ -278,6 +299,12 @@ def gpu_uuid(local):
 def make_filter(w):
     import flowfilter_b200 as ffb
 
+    if w.get("filter") == "FlowFilter":
+        f = ffb.FlowFilter(w["H"], w["W"])
+        f.gamma = w["gamma"][0]
+        f.smoothIterations = w["smooth"][0]
+        f.maxflow = w["maxflow"]
+        return f
     f = ffb.PyramidalFlowFilter(w["H"], w["W"], w["levels"])
     f.gamma = w["gamma"]
     f.smoothIterations = w["smooth"]
@@ -445,16 +472,25 @@ def e2e_run(w, frames, steps, warmup):
     return (t1 - t0) * 1000.0
 
 
+def oracle_filter(O, w):
+    """The oracle's filter of a workload (the same kind and parameters as make_filter)."""
+    if w.get("filter") == "FlowFilter":
+        return O.Filter.flowfilter(w["H"], w["W"], smooth_iterations=w["smooth"][0], maxflow=w["maxflow"],
+                                   gamma=w["gamma"][0])
+    f = O.Filter.pyramidal(w["H"], w["W"], w["levels"])
+    f.set_gammas(w["gamma"])
+    f.set_smooths(w["smooth"])
+    f.set_max_flow(w["maxflow"])
+    return f
+
+
 def cpu_port_fps(w, frames, seconds=10.0, max_frames=2000, threads=None):
     """The oracle (C++ restatement of the reference path) on the host cores."""
     import oracle as O
 
     threads = threads or os.cpu_count() or 1
     O.set_threads(threads)
-    f = O.Filter.pyramidal(w["H"], w["W"], w["levels"])
-    f.set_gammas(w["gamma"])
-    f.set_smooths(w["smooth"])
-    f.set_max_flow(w["maxflow"])
+    f = oracle_filter(O, w)
     ring = frames.shape[0]
     f.load(frames[0])
     f.compute()
@@ -800,9 +836,16 @@ def d2h_ceiling(nbytes, reps=20):
 def bench_b200(args):
     import torch
 
+    if args.config == 3:
+        return bench_batched_line(args)
+    if args.config == 4:
+        return bench_differentiable_line(args)
     world, rank, local = dist_setup()
     hbm_peak, peak_kind = peaks()
-    w = WORKLOADS[PRIMARY]
+    # --config 0 and 1 time that workload alone; the default run (config 2) adds the other legs
+    name = CONFIGS[args.config] if args.config is not None else PRIMARY
+    full = name == PRIMARY
+    w = WORKLOADS[name]
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     # kernel choice first, outside the clock sampling (its NVML polling must not disturb the
@@ -811,7 +854,7 @@ def bench_b200(args):
     # ---- timed region: device time of K frames, L2 flushed between frames
     barrier(world)
     with ClockSampler(gpu_uuid(local)) as clk:
-        prim, filt, frames = workload_leg(world, PRIMARY, args.steps, args.warmup, flush, hbm_peak)
+        prim, filt, frames = workload_leg(world, name, args.steps, args.warmup, flush, hbm_peak)
     step_ms = prim["ms_per_step"] * args.steps
     value = prim["value"]
 
@@ -824,10 +867,11 @@ def bench_b200(args):
         et.append(filt.elapsedTime())
     elapsed_ms = float(np.mean(et))
 
-    # ---- FlowToColor of the level-0 flow (the step after the filter in the reference's
-    # demos): device time per launch, back to back, the flow L2-resident as after a frame
-    ftc_us = bench_flow_to_color(filt, min(args.steps, 1000))
-    rot = bench_rotational_predictor(min(args.steps, 1000))
+    if full:
+        # ---- FlowToColor of the level-0 flow (the step after the filter in the reference's
+        # demos): device time per launch, back to back, the flow L2-resident as after a frame
+        ftc_us = bench_flow_to_color(filt, min(args.steps, 1000))
+        rot = bench_rotational_predictor(min(args.steps, 1000))
 
     # ---- end to end through the public API with host buffers
     e2e_steps = min(max(args.steps, 200), 2000)
@@ -835,18 +879,19 @@ def bench_b200(args):
     e2e_fps = aggregate_rate(world, e2e_steps, e2e_ms)
     ceiling = d2h_ceiling(w["H"] * w["W"] * 8)
 
-    # ---- the reference's published configuration beside it
-    extra, efilt, _ = workload_leg(world, EXTRA, min(args.steps * 4, 4000), args.warmup, flush, hbm_peak)
-    extra["vs_published"] = extra["value"] / world / PUBLISHED_FPS[EXTRA]
-    extra["published_fps"] = PUBLISHED_FPS[EXTRA]
-    extra["sequence"] = SEQUENCE[WORKLOADS[EXTRA]["seq"]]
+    if full:
+        # ---- the reference's published configuration beside it
+        extra, efilt, _ = workload_leg(world, EXTRA, min(args.steps * 4, 4000), args.warmup, flush, hbm_peak)
+        extra["vs_published"] = extra["value"] / world / PUBLISHED_FPS[EXTRA]
+        extra["published_fps"] = PUBLISHED_FPS[EXTRA]
+        extra["sequence"] = SEQUENCE[WORKLOADS[EXTRA]["seq"]]
 
-    # ---- the 64-stream batched step (each rank its own batch: replicas)
-    barrier(world)
-    batched = bench_batched(min(args.steps, 200), max(args.warmup, 3), world, rank)
-    barrier(world)
+        # ---- the 64-stream batched step (each rank its own batch: replicas)
+        barrier(world)
+        batched = bench_batched(min(args.steps, 200), max(args.warmup, 3), world, rank)
+        barrier(world)
 
-    differentiable = bench_differentiable(args.steps)
+        differentiable = bench_differentiable(args.steps)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -858,42 +903,103 @@ def bench_b200(args):
     if rank == 0:
         roof = dict(prim["roofline"])
         roof["peak_kind"] = peak_kind
-        roof["issue"] = issue_roofline(ncu_traffic(PRIMARY, "warp_instructions_per_launch"), roof["launch_ms"],
-                                       clk.summary())
+        instr = ncu_traffic(name, "warp_instructions_per_launch")
+        if instr is not None:
+            roof["issue"] = issue_roofline(instr, roof["launch_ms"], clk.summary())
+        published = PUBLISHED_FPS.get(name)
         line = {
-            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_of(name), "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "weak", "vs_baseline": value / world / published if published else None,
             "dtype": "f32", "data": "synthetic",
-            "config": bench_config(PRIMARY),
+            "config": bench_config(name),
             "notes": {"sequence": SEQUENCE[w["seq"]], "step": "loadImage (device frame) + compute(), CUDA-graph replay",
                       "kernels": filt.tuning(), "parallelism": f"replicas x{world}",
-                      "vs_baseline": "null: the reference publishes no figure for this configuration"},
+                      "vs_baseline": (f"per GPU against the reference notebook's {published:.0f} frames/s "
+                                      "(notebooks/GPU_example.ipynb:292)") if published else
+                                     "null: the reference publishes no figure for this configuration"},
             "mpix_per_s": prim["mpix_per_s"],
             "frame_bytes": prim["frame_bytes"], "frame_gbs": prim["frame_gbs"],
             "frame_roofline_frac": prim["frame_roofline_frac"],
             "roofline": roof,
-            "flow_to_color": {"launch_us": ftc_us, "pixels": w["H"] * w["W"],
-                              "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
-                              "note": f"ff_flow_to_color on the {w['W']}x{w['H']} level-0 flow, default wheel; "
-                                      "12 B/px (float2 in, RGBA out)"},
-            "rotational_predictor": rot,
             "elapsed_time_ms": {"value": elapsed_ms, "frames": len(et),
-                                "path": "PyramidalFlowFilter.loadImage(host numpy) + compute(); mean elapsedTime(), "
-                                        "as the reference notebook measures"},
+                                "path": f"{w.get('filter', 'PyramidalFlowFilter')}.loadImage(host numpy) + compute(); "
+                                        "mean elapsedTime(), as the reference notebook measures"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": w["H"] * w["W"],
                     "d2h_bytes_per_step": w["H"] * w["W"] * 8, "steps": e2e_steps,
                     "d2h_ceiling": ceiling,
-                    "path": "flowfilter_b200.PyramidalFlowFilter.processAsync(pinned host frame -> pinned host flow), "
-                            "synchronize() at the end; wall clock"},
+                    "path": f"flowfilter_b200.{w.get('filter', 'PyramidalFlowFilter')}.processAsync(pinned host frame "
+                            "-> pinned host flow), synchronize() at the end; wall clock"},
             "gpu_launches": args.steps * prim["launches_per_frame"],
             "clocks": clk.summary(),
-            "extra": extra,
-            "batched": batched,
-            "differentiable": differentiable,
         }
+        if full:
+            line["flow_to_color"] = {"launch_us": ftc_us, "pixels": w["H"] * w["W"],
+                                     "achieved_GBps": w["H"] * w["W"] * 12 / (ftc_us * 1e-6) / 1e9,
+                                     "note": f"ff_flow_to_color on the {w['W']}x{w['H']} level-0 flow, default "
+                                             "wheel; 12 B/px (float2 in, RGBA out)"}
+            line["rotational_predictor"] = rot
+            line["extra"] = extra
+            line["batched"] = batched
+            line["differentiable"] = differentiable
         print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def bench_batched_line(args):
+    """--config 3: the 64-stream batched step as the line's metric (device-resident packed
+    frames; the loop of single filters over the same streams beside it)."""
+    world, rank, local = dist_setup()
+    barrier(world)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        b = bench_batched(args.steps, args.warmup, world, rank)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "stream-frames/s (BatchFlowFilter step over 64 mixed-size streams, each stream bit-exact with "
+                      "its single filter)",
+            "value": b["value"], "unit": "stream-frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": b["ms_per_step"], "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+            "data": b["data"],
+            "config": {"workload": "batched_64streams", "streams": b["workload"],
+                       "l2": "no flush: the 64 streams' state (about 1 GB) exceeds L2"},
+            "gpu_launches": args.steps * b["launches_per_step"],
+            "e2e": None,
+            "notes": {"e2e": "null: the batched step takes device-resident packed frames (BatchFlowFilter.pack); "
+                             "no host-buffer entry point"},
+            "clocks": clk.summary(), "batched": b,
+        }), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def bench_differentiable_line(args):
+    """--config 4: forward+backward of the differentiable filter as the line's metric."""
+    world, rank, local = dist_setup()
+    with ClockSampler(gpu_uuid(local)) as clk:
+        d = bench_differentiable(args.steps)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "frames/s (differentiable PyramidalFlowFilter forward+backward, 16 x 32 frames of 256x256)",
+            "value": d["fwd_bwd_frames_per_s"], "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": d["fwd_bwd_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": d["data"],
+            "config": {"workload": "differentiable_16x32x256x256", "levels": 2, "gamma": [10.0, 50.0],
+                       "smoothIterations": [2, 4], "maxflow": 4.0},
+            "e2e": None,
+            "gpu_launches": None,
+            "notes": {"e2e": "null: frames and known flows are device-resident tensors; the fit's per-step time "
+                             "(Adam, loss read back) is under differentiable.fit",
+                      "gpu_launches": "not counted in this process; the launch list of one forward+backward is "
+                                      "profiles/launches_differentiable_16x32x256x256.md"},
+            "clocks": clk.summary(), "differentiable": d,
+        }), flush=True)
     if world > 1:
         import torch.distributed as dist
 
@@ -905,16 +1011,19 @@ def bench_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.config in (3, 4):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                          + ("batched step" if args.config == 3 else "gradient path")
+                          + "; its per-stream filter is timed by --config 0-2"}), flush=True)
+        return
     import oracle as O
 
-    w = WORKLOADS[PRIMARY]
+    name = CONFIGS[args.config] if args.config is not None else PRIMARY
+    w = WORKLOADS[name]
     frames = make_frames(w)
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    f = O.Filter.pyramidal(w["H"], w["W"], w["levels"])
-    f.set_gammas(w["gamma"])
-    f.set_smooths(w["smooth"])
-    f.set_max_flow(w["maxflow"])
+    f = oracle_filter(O, w)
     ring = frames.shape[0]
     for t in range(args.warmup):
         f.load(frames[t % ring])
@@ -926,10 +1035,10 @@ def bench_reference(args):
     dt = time.perf_counter() - t0
     fps = args.steps / dt
     line = {
-        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_of(name), "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1000.0 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": bench_config(PRIMARY),
+        "config": bench_config(name),
         "notes": {"sequence": SEQUENCE[w["seq"]],
                   "step": "one frame of the reference's CUDA path restated in C++ (oracle/), on the host cores"},
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
@@ -1067,6 +1176,10 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", type=int, choices=sorted(CONFIGS), default=None,
+                    help="one configuration alone: 0 320x240 FlowFilter, 1 640x480 2 levels, 2 2048x1088 3 levels "
+                         "(the default run, with every other leg), 3 the 64-stream batched step, 4 the "
+                         "differentiable filter")
     ap.add_argument("--profile-next", action="store_true",
                     help="profiler target: the flow-to-colour and rotational-predictor kernels (no JSON line)")
     ap.add_argument("--profile-batched", action="store_true",
